@@ -1,0 +1,315 @@
+"""Benchmark: LDL^T factor + solve of the 100^3 complex-symmetric Helmholtz
+operator (PML, 10 points per wavelength, smoothed random velocity, 4 complex
+N(0,1) right-hand sides), FP32 fronts + FP64 iterative refinement to relative
+residual <= 1e-10, against the plain FP64 factor + solve on the same GPU.
+
+One step = assemble the fronts from A's values, multifrontal LDL^T, and the
+refined solve, all on the device through the C ABI (libcliqgpu.so).  The
+factor arena (10 GB for CFP32, 20 GB for CFP64) is far larger than the 126 MB
+L2, so consecutive steps cannot hit in L2 without a flush.
+
+Usage: python bench.py [--gpus N --steps K --warmup W --impl ours|reference]
+Multi-GPU (torchrun): every rank solves its own independent copy (replicas;
+the single-GPU path has no exchange step), timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LDL^T factor+solve s, FP32+IR vs FP64 on 1 B200, 100^3 Helmholtz, resid<=1e-10"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=100)
+    p.add_argument("--nrhs", type=int, default=4)
+    p.add_argument("--cutoff", type=int, default=128)
+    p.add_argument("--tol", type=float, default=1e-10)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline sample")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(n, nrhs, seed):
+    from clique_b200 import operators as ops
+    A, omega, c = ops.helmholtz_workload_3d(n, seed=seed)
+    B = ops.random_rhs(A.n, nrhs, seed=seed + 1, complex_=True)
+    return A, B, omega
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the oracle (C restatement of Clique's path,
+# OpenBLAS-backed dense kernels), on a bounded sample of the workload
+# ---------------------------------------------------------------------------
+def cpu_flops(n, cutoff):
+    """Clique's FactorizationWork model for the n^3 grid (complex: x4)."""
+    import clique_b200 as cliq
+    from clique_b200 import operators as ops
+    A = ops.laplacian_3d(n, n, n)
+    _, _, info = cliq.NaturalNestedDissection(n, n, n, A, cutoff)
+    tot = 0.0
+    for nd in info.localNodes:
+        m, k = nd.size + len(nd.lowerStruct), nd.size
+        tot += k ** 3 / 3 + (m - k) * k * k + (m - k) ** 2 * k
+    return 4 * tot
+
+
+def cpu_run(n, nrhs, cutoff, seed, threads):
+    from oracle import oracle as O
+    O.enable_blas(threads)
+    A, B, _ = workload(n, nrhs, seed)
+    S = O.Symbolic(n, n, n, A.rowptr, A.colind, cutoff=cutoff)
+    t0 = time.perf_counter()
+    F = O.Fronts(S, A.values, is_complex=True)
+    F.ldl(96)
+    X = F.solve(B.copy(order="F"))
+    t1 = time.perf_counter()
+    res = np.linalg.norm(A.to_scipy() @ X - B) / np.linalg.norm(B)
+    del F
+    return t1 - t0, res
+
+
+def cpu_baseline(args, target_n):
+    threads = os.cpu_count() or 1
+    n0 = 30
+    t0, _ = cpu_run(n0, args.nrhs, args.cutoff, args.seed, threads)
+    rate = cpu_flops(n0, args.cutoff) / t0
+    # largest sample grid whose estimated time fits the budget (flops grow like n^6)
+    f_target = cpu_flops(target_n, args.cutoff)
+    n = int(target_n * min(1.0, (args.cpu_budget * rate / f_target)) ** (1.0 / 6.0))
+    n = max(n0, min(target_n, n))
+    t, res = cpu_run(n, args.nrhs, args.cutoff, args.seed, threads)
+    scale = f_target / cpu_flops(n, args.cutoff)
+    return {"value": t * scale, "unit": "s", "cores": threads, "kind": "port",
+            "sample": f"oracle (C restatement, OpenBLAS {threads} threads, nb=96) FP64-complex factor+solve of the "
+                      f"{n}^3 Helmholtz workload in {t:.2f} s (residual {res:.1e}), scaled to {target_n}^3 by "
+                      f"Clique's FactorizationWork flop model (x{scale:.1f})",
+            "sample_n": n, "sample_s": t}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vals = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args, args.n)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{args.n}^3 complex Helmholtz PML, {args.nrhs} RHS, natural ND cutoff {args.cutoff}",
+                       "parallelism": "cpu"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import clique_b200 as cliq
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    A, B, omega = workload(args.n, args.nrhs, args.seed)
+    n = args.n
+    stream = torch.cuda.current_stream()
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, args.cutoff)
+    vals_d = torch.from_numpy(A.values).cuda()
+    B_d = torch.from_numpy(B).cuda().t().contiguous().t()
+
+    L32 = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single", stream=stream.cuda_stream)
+
+    def step32():
+        L32.Initialize(vals_d)
+        cliq.LDL(info, L32)
+        X, it, rr = cliq.RefinedSolve(L32, B_d, args.tol, 30)
+        return it, rr
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        it, rr = step32()
+    torch.cuda.synchronize()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        ev0.record()
+        its, rrs = [], []
+        for _ in range(args.steps):
+            it, rr = step32()
+            its.append(it); rrs.append(rr)
+        ev1.record()
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    factor_flops = L32.FactorizationWork()
+    launches = L32.last_launches()
+
+    # end-to-end through the C ABI with host buffers
+    L32h = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
+    def step_host():
+        L32h.Initialize(A.values)
+        cliq.LDL(info, L32h)
+        return cliq.RefinedSolve(L32h, B, args.tol, 30)
+    step_host()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        Xh, ith, rrh = step_host()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    del L32h
+
+    fp64 = None
+    if not args.no_fp64:
+        L64 = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double", stream=stream.cuda_stream)
+        X64 = torch.zeros_like(B_d)
+
+        def step64():
+            L64.Initialize(vals_d)
+            cliq.LDL(info, L64)
+            X64.copy_(B_d)
+            cliq.Solve(info, L64, X64)
+        for _ in range(max(1, args.warmup)):
+            step64()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            step64()
+        ev1.record()
+        torch.cuda.synchronize()
+        fp64_ms = ev0.elapsed_time(ev1) / args.steps
+        Xc = X64.cpu().numpy()
+        res64 = float(np.linalg.norm(A.to_scipy() @ Xc - B) / np.linalg.norm(B))
+        fp64 = {"fp64_plain_s": fp64_ms / 1e3, "fp64_residual": res64,
+                "speedup_vs_fp64": fp64_ms / ms}
+        del L64
+
+    line = {"metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64+c128-IR", "data": "synthetic",
+            "config": {"workload": f"{n}^3 complex-symmetric Helmholtz PML (omega={omega:.2f}, 10 ppw), "
+                                   f"{args.nrhs} RHS, natural ND cutoff {args.cutoff}",
+                       "precision": "CFP32 fronts, FP64 pivots, FP64 refinement", "tol": args.tol,
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (factor arena >> 126 MB)"},
+            "refine_iters": its, "relres": max(rrs), "factor_gflop": factor_flops / 1e9,
+            "factor_tflops_effective": factor_flops / (ms / 1e3) / 1e12,
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(A.values.nbytes + B.nbytes),
+                    "d2h_bytes_per_step": int(B.nbytes)},
+            "clocks": clk.summary()}
+    if fp64:
+        line.update(fp64)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args, n)
+        except Exception as e:  # the baseline must not hide the GPU number
+            line["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

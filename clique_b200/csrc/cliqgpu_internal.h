@@ -1,0 +1,168 @@
+// Internal declarations of the cliqgpu library (not part of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/cliqgpu.h"
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#else
+struct CUstream_st;
+typedef struct CUstream_st* cudaStream_t;
+#endif
+
+namespace cliqgpu {
+
+// ---------------------------------------------------------------------------
+// host symbolic analysis (single process)
+// ---------------------------------------------------------------------------
+struct Symbolic {
+    int num_nodes = 0;
+    int64_t n = 0;
+    std::vector<int> size, off, my_off, parent, sep_parent, children, on_left;
+    std::vector<std::vector<int>> lower, orig_lower, orig_rel, left_rel, right_rel, inds;
+    std::vector<int> map, inv_map;
+    // flattened CSR views for cliq_symm_info
+    std::vector<int64_t> lower_ptr, orig_ptr;
+    std::vector<int> lower_flat, orig_flat;
+    void finalize_views();
+};
+
+int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                              int cutoff, Symbolic& S);
+
+void set_last_error(const std::string& msg);
+
+// ---------------------------------------------------------------------------
+// device-side descriptors
+// ---------------------------------------------------------------------------
+constexpr int kTile = 64;        // rows per solve block, GEMM tile edge
+constexpr int kEACols = 16;      // columns per extend-add work item
+
+// One front as the kernels see it.  Offsets are in elements (a complex
+// element is two scalars).
+struct FrontDev {
+    int64_t L;          // frontL (m x n, ld m) in the factor arena
+    int64_t U;          // update ABR (u x u, ld u) in pool[pool]
+    int64_t CU[2];      // children's updates in the other pool (-1: none)
+    int64_t cmap;       // child maps: [m] left then [m] right (int32, -1 = absent), -1 for leaves
+    int64_t lower;      // offset of lowerStruct in the flattened array
+    int64_t W;          // solve workspace offset (multiply by nrhs) in wpool[pool]
+    int64_t CW[2];      // children's solve workspace offsets (in the other wpool)
+    int32_t m, n, off, u;
+    int32_t cu[2];      // children's update sizes
+    int32_t pool;       // parity of the depth
+    int32_t flag_base;  // first chain-solve flag of this front
+};
+
+// One GEMM update problem: C -= A diag(d) op(B)^T restricted to i >= j.
+struct GemmProb {
+    int64_t A, B, C, d;   // A, B in the arena; C in the arena (cpool < 0) or a pool; d in the D array
+    int32_t lda, ldc, M, N, K, cpool;
+};
+
+struct Launch {
+    enum Kind { EXTEND_ADD, DIAG, PANEL, GEMM } kind;
+    int64_t items;        // offset into the int2 item array (EXTEND_ADD / DIAG / PANEL) or prob array (GEMM)
+    int32_t nitems;
+    int64_t prefix;       // GEMM: offset into the tile prefix array
+    int64_t nblocks;      // grid size
+    int32_t k;            // DIAG / PANEL: column offset of the step
+    int32_t depth;
+};
+
+struct SolveLevel {
+    int64_t fronts;       // offset into level_fronts (int32 front ids)
+    int32_t nfronts;
+    int64_t fwd_items;    // offset into chain item array (int2: front, block)
+    int32_t nfwd;
+    int64_t bwd_items;
+    int32_t nbwd;
+    int32_t depth;
+};
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+struct Plan {
+    // options
+    int field = CLIQ_REAL, precision = CLIQ_FP64, conjugate = 0, nb = 64, keep_matrix = 0;
+    bool cplx() const { return field == CLIQ_COMPLEX; }
+    int scalar_bytes() const { return precision == CLIQ_FP64 ? 8 : 4; }
+    int elem_bytes() const { return scalar_bytes() * (cplx() ? 2 : 1); }
+
+    int64_t n = 0, nnz = 0;
+    int num_fronts = 0, max_depth = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // host copies of structure
+    std::vector<FrontDev> hfronts;
+    std::vector<int> depth;
+    std::vector<std::vector<int>> level_list;   // fronts per depth
+    std::vector<Launch> launches;
+    std::vector<SolveLevel> solve_levels;       // indexed by depth
+    double factor_flops = 0, solve_flops = 0, factor_entries = 0;
+    int64_t arena_elems = 0, pool_elems[2] = {0, 0}, wpool_elems[2] = {0, 0}, tinv_slots = 0;
+    int64_t flags_total = 0;
+
+    // device buffers
+    void* L = nullptr;            // factor arena (storage precision)
+    double* D = nullptr;          // pivots, FP64 (complex: interleaved), length n
+    void* pool[2] = {nullptr, nullptr};
+    void* tinv = nullptr;         // per-front inverse diagonal blocks, FP64 storage
+    FrontDev* fronts = nullptr;
+    int32_t* cmaps = nullptr;
+    int32_t* lower = nullptr;     // flattened lowerStruct (ND indices)
+    int32_t* items = nullptr;     // int2 items for extend-add / diag / panel / chain solves
+    GemmProb* probs = nullptr;
+    int64_t* prefix = nullptr;
+    int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
+    int32_t* perm = nullptr;      // inverse map: ND -> natural
+    int32_t* level_fronts = nullptr;
+    int32_t* flags = nullptr;
+    int32_t* tickets = nullptr;
+    int32_t* status = nullptr;    // [0] first zero pivot + 1 (min), [1] timeout flag
+    int64_t* rowptr = nullptr;    // FP64 matrix (keep_matrix)
+    int32_t* colind = nullptr;
+    double* aval = nullptr;
+    // solve workspaces (grown on demand)
+    void* wpool[2] = {nullptr, nullptr};
+    void* xnodal = nullptr;       // n x nrhs in storage precision
+    double* xwork = nullptr;      // FP64 workspaces for refinement (3 * n * nrhs)
+    double* norms = nullptr;      // 2 * nrhs
+    int32_t ws_nrhs = 0;
+    int64_t device_bytes = 0;
+
+    int32_t epoch = 0;
+    bool assembled = false, factored = false;
+    int64_t last_launches = 0;
+
+    // host-side staging for host-resident inputs/outputs
+    std::vector<int32_t> hitems;
+};
+
+// launchers (factor_kernels.cu)
+template <class T, bool C>
+int run_factor(Plan& P);
+// launchers (solve_kernels.cu)
+template <class T, bool C>
+int run_solve_nodal(Plan& P, void* xn, int nrhs);   // xn: n x nrhs in storage precision, ND order
+// misc (misc_kernels.cu)
+int launch_assemble(Plan& P, const double* dvals);
+int launch_pull(Plan& P, const int32_t* perm, const double* X, int64_t ldx, int nrhs, void* xn, double scale);
+int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t ldx, int nrhs, double scale, int accumulate);
+int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double beta_r, double beta_i,
+                double* Y, int64_t ld, int nrhs);
+int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
+
+int check_cuda(const char* where);
+int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
+               const int32_t* colind);
+void free_plan(Plan& P);
+int read_status(Plan& P, int64_t* zero_pivot);
+
+}  // namespace cliqgpu

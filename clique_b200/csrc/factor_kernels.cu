@@ -1,0 +1,338 @@
+// Numeric multifrontal factorization on the device.
+//
+// The reference factors one front at a time in post-order (LocalLDL,
+// include/clique/numeric/ldl/local.hpp:25-122): zero the update, extend-add
+// the two children's updates through leftRelInds/rightRelInds, then
+// FrontLDL (ldl/local_front.hpp:30-71) -- a right-looking loop over nb-wide
+// column blocks doing LDL of the diagonal block, a TRSM of the panel, the
+// in-front GEMM update of the remaining panel columns and a rank-nb Trrk
+// update of ABR.
+//
+// Here every tree level (all fronts at one depth) is processed at once:
+//   1. extend_add_kernel  -- gather form of the extend-add: each entry of the
+//      parent's lower triangle is written exactly once (frontL += children,
+//      ABR := children), using per-front inverse maps of the relative indices.
+//   2. for k in steps of nb over the level's widest front:
+//        diag_ldl_kernel  -- LDL of the kb x kb diagonal block in shared memory
+//                            in FP64, writes L11, D (FP64) and U = L11^{-T}.
+//        panel_kernel     -- S21 = A21 U, L21 = S21 D^{-1} (row blocks of 64).
+//        gemm (trailing)  -- A22 -= L21 D L21^T over the remaining panel columns.
+//   3. gemm (Schur)       -- ABR -= L_B D L_B^T once with K = n, instead of the
+//      reference's n/nb rank-nb Trrk passes (same sum, one pass over ABR).
+// D is kept in FP64 for every storage precision.
+#include <climits>
+#include <cstdio>
+
+#include "cliqgpu_internal.h"
+#include "device_common.cuh"
+
+namespace cliqgpu {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------
+// 1. extend-add (gather form)
+// ---------------------------------------------------------------------------
+template <class T, bool C>
+__global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
+                                                              T* __restrict__ L, T* __restrict__ pool0, T* __restrict__ pool1,
+                                                              const int32_t* __restrict__ cmaps) {
+    using X = V<T, C>;
+    const int4 it = items[blockIdx.x];
+    const FrontDev f = F[it.x];
+    const int j0 = it.y;
+    T* up = f.pool == 0 ? pool0 : pool1;
+    const T* cp = f.pool == 0 ? pool1 : pool0;
+    const int32_t* lm = f.cmap >= 0 ? cmaps + f.cmap : nullptr;
+    const int32_t* rm = lm ? lm + f.m : nullptr;
+    for (int jj = 0; jj < kEACols; ++jj) {
+        const int j = j0 + jj;
+        if (j >= f.m) break;
+        const int lj = lm ? lm[j] : -1, rj = rm ? rm[j] : -1;
+        if (j < f.n && lj < 0 && rj < 0) continue;
+        for (int i = j + threadIdx.x; i < f.m; i += blockDim.x) {
+            X v = X{};
+            if (lj >= 0) {
+                const int li = lm[i];
+                if (li >= 0) v += ldv<T, C>(cp, f.CU[0] + li + (int64_t)lj * f.cu[0]);
+            }
+            if (rj >= 0) {
+                const int ri = rm[i];
+                if (ri >= 0) v += ldv<T, C>(cp, f.CU[1] + ri + (int64_t)rj * f.cu[1]);
+            }
+            if (j < f.n) {
+                const int64_t e = f.L + i + (int64_t)j * f.m;
+                stv<T, C>(L, e, ldv<T, C>(L, e) + v);
+            } else {
+                stv<T, C>(up, f.U + (i - f.n) + (int64_t)(j - f.n) * f.u, v);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2a. LDL of the diagonal block (one CTA per front), FP64 in shared memory
+// ---------------------------------------------------------------------------
+template <class T, bool C, bool CJ>
+__global__ void __launch_bounds__(kThreads) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
+                                                            T* __restrict__ L, double* __restrict__ D, T* __restrict__ tinv,
+                                                            int32_t* __restrict__ status) {
+    using W = DV<C>;
+    using X = V<T, C>;
+    constexpr int nb = kTile, ld = kTile + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    W* sA = reinterpret_cast<W*>(smem_raw);
+    W* sX = sA + nb * ld;
+    const int4 it = items[blockIdx.x];
+    const FrontDev f = F[it.x];
+    const int slot = it.y;
+    const int kb = min(nb, f.n - k);
+    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
+        const int i = idx % kb, j = idx / kb;
+        W v{};
+        if (i >= j) v = conv<W>(ldv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m));
+        sA[i * ld + j] = v;
+        sX[i * ld + j] = W{};
+    }
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        const W d = sA[j * ld + j];
+        if (threadIdx.x == 0 && is_zero(d)) atomicMin(&status[0], f.off + k + j + 1);
+        const int r = kb - j - 1;
+        for (int idx = threadIdx.x; idx < r * r; idx += blockDim.x) {
+            const int ii = idx % r, cc = idx / r;
+            if (ii >= cc) {
+                const int i = j + 1 + ii, c = j + 1 + cc;
+                sA[i * ld + c] -= sA[i * ld + j] * (opc<CJ>(sA[c * ld + j]) / d);
+            }
+        }
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) sA[i * ld + j] = sA[i * ld + j] / d;
+    }
+    __syncthreads();
+    // Linv = L11^{-1} (unit lower), one column per thread
+    for (int c = threadIdx.x; c < kb; c += blockDim.x) {
+        sX[c * ld + c] = vone<W>();
+        for (int i = c + 1; i < kb; ++i) {
+            W acc = sA[i * ld + c];
+            for (int t = c + 1; t < i; ++t) mac(acc, sA[i * ld + t], sX[t * ld + c]);
+            sX[i * ld + c] = W{} - acc;
+        }
+    }
+    __syncthreads();
+    // U = op(Linv)^T, row-major kb x kb (upper unit) into the slot; L11 and D back to global
+    X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const int t = idx / nb, c = idx % nb;
+        X v{};
+        if (t < kb && c < kb && t <= c) v = conv<X>(opc<CJ>(sX[c * ld + t]));
+        U[idx] = v;
+    }
+    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
+        const int i = idx % kb, j = idx / kb;
+        if (i > j) stv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m, conv<X>(sA[i * ld + j]));
+        else if (i == j) {
+            stv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m, vone<X>());
+            reinterpret_cast<W*>(D)[f.off + k + j] = sA[j * ld + j];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2b. panel: S21 = A21 U, L21 = S21 D^{-1} for one 64-row block
+// ---------------------------------------------------------------------------
+template <class T, bool C>
+__global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
+                                                         T* __restrict__ L, const double* __restrict__ D, const T* __restrict__ tinv) {
+    using X = V<T, C>;
+    using W = DV<C>;
+    constexpr int nb = kTile, ldA = kTile + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    X* sU = reinterpret_cast<X*>(smem_raw);      // nb x nb row-major
+    X* sA = sU + nb * nb;                          // 64 x ldA
+    X* sR = sA + kTile * ldA;                      // reciprocal pivots
+    const int4 it = items[blockIdx.x];
+    const FrontDev f = F[it.x];
+    const int slot = it.y, rb = it.z;
+    const int kb = min(nb, f.n - k);
+    const int r0 = k + kb + kTile * rb;
+    const int rows = min(kTile, f.m - r0);
+    const X* U = reinterpret_cast<const X*>(tinv) + (int64_t)slot * nb * nb;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) sU[idx] = U[idx];
+    for (int idx = threadIdx.x; idx < kTile * nb; idx += blockDim.x) {
+        const int r = idx % kTile, t = idx / kTile;
+        X v{};
+        if (r < rows && t < kb) v = ldv<T, C>(L, f.L + (r0 + r) + (int64_t)(k + t) * f.m);
+        sA[r * ldA + t] = v;
+    }
+    if (threadIdx.x < kb) {
+        const W d = reinterpret_cast<const W*>(D)[f.off + k + threadIdx.x];
+        sR[threadIdx.x] = conv<X>(W{} + vone<W>() / d);
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    X acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = X{};
+    for (int t = 0; t < kb; ++t) {
+        X av[4], uv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = sA[(ty + 16 * a) * ldA + t];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) uv[b] = sU[t * nb + tx + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) mac(acc[a][b], av[a], uv[b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int c = tx + 16 * b;
+        if (c >= kb) continue;
+        const X rd = sR[c];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int r = ty + 16 * a;
+            if (r < rows) stv<T, C>(L, f.L + (r0 + r) + (int64_t)(k + c) * f.m, acc[a][b] * rd);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. tiled update C -= A diag(d) op(B)^T on the lower trapezoid (i >= j)
+// ---------------------------------------------------------------------------
+template <class T, bool C, bool CJ>
+__global__ void __launch_bounds__(kThreads) gemm_update_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
+                                                               int nprobs, T* __restrict__ L, T* __restrict__ pool0,
+                                                               T* __restrict__ pool1, const double* __restrict__ D) {
+    using X = V<T, C>;
+    using W = DV<C>;
+    constexpr int BM = 64, BK = C ? 8 : 16, PAD = 1;
+    __shared__ X sA[BK][BM + PAD];
+    __shared__ X sB[BK][BM + PAD];
+    const int64_t bid = blockIdx.x;
+    int lo = 0, hi = nprobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const GemmProb pr = probs[lo];
+    int64_t t = bid - prefix[lo];
+    const int Mt = (pr.M + BM - 1) / BM;
+    int tj = 0;
+    while (t >= Mt - tj) { t -= Mt - tj; ++tj; }
+    const int ti = tj + (int)t;
+    const int i0 = ti * BM, j0 = tj * BM;
+    T* Cbase = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    X acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = X{};
+    for (int k0 = 0; k0 < pr.K; k0 += BK) {
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / kThreads; ++q) {
+            const int idx = threadIdx.x + kThreads * q;
+            const int r = idx % BM, kk = idx / BM;
+            const int kg = k0 + kk;
+            X av{}, bv{};
+            if (kg < pr.K) {
+                if (i0 + r < pr.M) av = ldv<T, C>(L, pr.A + (i0 + r) + (int64_t)kg * pr.lda);
+                if (j0 + r < pr.N) {
+                    const X dv = conv<X>(reinterpret_cast<const W*>(D)[pr.d + kg]);
+                    bv = dv * opc<CJ>(ldv<T, C>(L, pr.B + (j0 + r) + (int64_t)kg * pr.lda));
+                }
+            }
+            sA[kk][r] = av;
+            sB[kk][r] = bv;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            X av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = sA[kk][ty + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bv[b] = sB[kk][tx + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) mac(acc[a][b], av[a], bv[b]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int j = j0 + tx + 16 * b;
+        if (j >= pr.N) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = i0 + ty + 16 * a;
+            if (i < pr.M && i >= j) {
+                const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
+                stv<T, C>(Cbase, e, ldv<T, C>(Cbase, e) - acc[a][b]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+template <class T, bool C, bool CJ>
+static int run_factor_impl(Plan& P) {
+    using X = V<T, C>;
+    using W = DV<C>;
+    const size_t smem_diag = 2 * sizeof(W) * kTile * (kTile + 1);
+    const size_t smem_panel = sizeof(X) * (kTile * kTile + kTile * (kTile + 1) + kTile);
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(diag_ldl_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag);
+        cudaFuncSetAttribute(panel_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel);
+        attr_done = true;
+    }
+    T* L = reinterpret_cast<T*>(P.L);
+    T* p0 = reinterpret_cast<T*>(P.pool[0]);
+    T* p1 = reinterpret_cast<T*>(P.pool[1]);
+    const int4* items = reinterpret_cast<const int4*>(P.items);
+    int64_t launches = 0;
+    for (const Launch& ln : P.launches) {
+        if (ln.nblocks <= 0) continue;
+        switch (ln.kind) {
+            case Launch::EXTEND_ADD:
+                extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
+                break;
+            case Launch::DIAG:
+                diag_ldl_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, smem_diag, P.stream>>>(
+                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), P.status);
+                break;
+            case Launch::PANEL:
+                panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
+                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv));
+                break;
+            case Launch::GEMM:
+                gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(
+                    P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
+                break;
+        }
+        ++launches;
+    }
+    P.last_launches = launches;
+    return check_cuda("factor launch");
+}
+
+template <class T, bool C>
+int run_factor(Plan& P) {
+    if (P.conjugate && C) return run_factor_impl<T, C, true>(P);
+    return run_factor_impl<T, C, false>(P);
+}
+
+template int run_factor<float, false>(Plan&);
+template int run_factor<float, true>(Plan&);
+template int run_factor<double, false>(Plan&);
+template int run_factor<double, true>(Plan&);
+
+}  // namespace cliqgpu

@@ -1,0 +1,153 @@
+// Bandwidth-bound helpers: front assembly, nodal pull/push with precision
+// conversion, FP64 CSR multiply and column norms for refinement.
+#include "cliqgpu_internal.h"
+#include "device_common.cuh"
+
+namespace cliqgpu {
+
+static inline unsigned grid_for(int64_t work, int threads) {
+    int64_t b = (work + threads - 1) / threads;
+    const int64_t cap = 148 * 16;
+    if (b > cap) b = cap;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+// DistSymmFrontTree::Initialize value scatter (dist_symm_front_tree/impl.hpp:275-294):
+// frontL[dest[e]] = conj?(A[e]); entries above the front's diagonal have dest = -1.
+template <class T, bool C, bool CJ>
+__global__ void assemble_kernel(const int64_t* __restrict__ dest, const double* __restrict__ vals, int64_t nnz, T* __restrict__ L) {
+    using Xv = V<T, C>;
+    using W = DV<C>;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = dest[e];
+        if (d < 0) continue;
+        W v = reinterpret_cast<const W*>(vals)[e];
+        v = opc<CJ>(v);
+        stv<T, C>(L, d, conv<Xv>(v));
+    }
+}
+
+template <class T, bool C>
+static int assemble_t(Plan& P, const double* dvals) {
+    cudaMemsetAsync(P.L, 0, (size_t)P.arena_elems * P.elem_bytes(), P.stream);
+    if (P.conjugate && C)
+        assemble_kernel<T, C, true><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, dvals, P.nnz, reinterpret_cast<T*>(P.L));
+    else
+        assemble_kernel<T, C, false><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, dvals, P.nnz, reinterpret_cast<T*>(P.L));
+    return check_cuda("assemble");
+}
+
+int launch_assemble(Plan& P, const double* dvals) {
+    if (P.precision == CLIQ_FP64) return P.cplx() ? assemble_t<double, true>(P, dvals) : assemble_t<double, false>(P, dvals);
+    return P.cplx() ? assemble_t<float, true>(P, dvals) : assemble_t<float, false>(P, dvals);
+}
+
+// Pull (dist_nodal_multi_vec/impl.hpp:67-219 at P=1): xn[p, j] = scale * X[inv[p], j]
+template <class T, bool C>
+__global__ void pull_kernel(const double* __restrict__ X, int64_t ldx, int64_t n, int nrhs, const int32_t* __restrict__ perm,
+                            T* __restrict__ xn, double scale) {
+    using Xv = V<T, C>;
+    using W = DV<C>;
+    const int64_t total = n * nrhs;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = idx % n, j = idx / n;
+        W v = reinterpret_cast<const W*>(X)[(perm ? perm[p] : p) + j * ldx];
+        if constexpr (C) { v.r *= scale; v.i *= scale; } else { v *= scale; }
+        stv<T, C>(xn, p + j * n, conv<Xv>(v));
+    }
+}
+
+// Push: X[inv[p], j] (=|+=) scale * xn[p, j]
+template <class T, bool C>
+__global__ void push_kernel(const T* __restrict__ xn, double* __restrict__ X, int64_t ldx, int64_t n, int nrhs,
+                            const int32_t* __restrict__ perm, double scale, int accumulate) {
+    using W = DV<C>;
+    const int64_t total = n * nrhs;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = idx % n, j = idx / n;
+        W v = conv<W>(ldv<T, C>(xn, p + j * n));
+        if constexpr (C) { v.r *= scale; v.i *= scale; } else { v *= scale; }
+        W* dst = reinterpret_cast<W*>(X) + (perm ? perm[p] : p) + j * ldx;
+        if (accumulate) *dst += v; else *dst = v;
+    }
+}
+
+int launch_pull(Plan& P, const int32_t* perm, const double* X, int64_t ldx, int nrhs, void* xn, double scale) {
+    const unsigned g = grid_for(P.n * nrhs, 256);
+    if (P.precision == CLIQ_FP64) {
+        if (P.cplx()) pull_kernel<double, true><<<g, 256, 0, P.stream>>>(X, ldx, P.n, nrhs, perm, (double*)xn, scale);
+        else pull_kernel<double, false><<<g, 256, 0, P.stream>>>(X, ldx, P.n, nrhs, perm, (double*)xn, scale);
+    } else {
+        if (P.cplx()) pull_kernel<float, true><<<g, 256, 0, P.stream>>>(X, ldx, P.n, nrhs, perm, (float*)xn, scale);
+        else pull_kernel<float, false><<<g, 256, 0, P.stream>>>(X, ldx, P.n, nrhs, perm, (float*)xn, scale);
+    }
+    return check_cuda("pull");
+}
+
+int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t ldx, int nrhs, double scale, int accumulate) {
+    const unsigned g = grid_for(P.n * nrhs, 256);
+    if (P.precision == CLIQ_FP64) {
+        if (P.cplx()) push_kernel<double, true><<<g, 256, 0, P.stream>>>((const double*)xn, X, ldx, P.n, nrhs, perm, scale, accumulate);
+        else push_kernel<double, false><<<g, 256, 0, P.stream>>>((const double*)xn, X, ldx, P.n, nrhs, perm, scale, accumulate);
+    } else {
+        if (P.cplx()) push_kernel<float, true><<<g, 256, 0, P.stream>>>((const float*)xn, X, ldx, P.n, nrhs, perm, scale, accumulate);
+        else push_kernel<float, false><<<g, 256, 0, P.stream>>>((const float*)xn, X, ldx, P.n, nrhs, perm, scale, accumulate);
+    }
+    return check_cuda("push");
+}
+
+// Multiply (multiply.hpp:150-165 at P=1): Y := beta Y + alpha A X, one thread per row
+template <bool C>
+__global__ void spmv_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const double* __restrict__ vals,
+                            int64_t n, DV<C> alpha, const double* __restrict__ X, DV<C> beta, double* __restrict__ Y, int64_t ld,
+                            int nrhs) {
+    using W = DV<C>;
+    const W* A = reinterpret_cast<const W*>(vals);
+    const W* x = reinterpret_cast<const W*>(X);
+    W* y = reinterpret_cast<W*>(Y);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e0 = rowptr[i], e1 = rowptr[i + 1];
+        for (int j = 0; j < nrhs; ++j) {
+            W s{};
+            for (int64_t e = e0; e < e1; ++e) mac(s, A[e], x[colind[e] + j * ld]);
+            const int64_t o = i + j * ld;
+            y[o] = beta * y[o] + alpha * s;
+        }
+    }
+}
+
+int launch_spmv(Plan& P, double ar, double ai, const double* X, double br, double bi, double* Y, int64_t ld, int nrhs) {
+    const unsigned g = grid_for(P.n, 256);
+    if (P.cplx())
+        spmv_kernel<true><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.aval, P.n, cx<double>{ar, ai}, X, cx<double>{br, bi}, Y, ld, nrhs);
+    else
+        spmv_kernel<false><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.aval, P.n, ar, X, br, Y, ld, nrhs);
+    return check_cuda("multiply");
+}
+
+// out[j] = sum_i |X[i, j]|^2 (FP64), one block per column
+template <bool C>
+__global__ void col_norms_kernel(const double* __restrict__ X, int64_t ld, int64_t n, double* __restrict__ out) {
+    const int j = blockIdx.x;
+    const int w = C ? 2 : 1;
+    const double* x = X + (int64_t)w * j * ld;
+    double s = 0;
+    for (int64_t i = threadIdx.x; i < n * w; i += blockDim.x) s = fma(x[i], x[i], s);
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) out[j] = s;
+    }
+}
+
+int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out) {
+    if (P.cplx()) col_norms_kernel<true><<<nrhs, 1024, 0, P.stream>>>(X, ld, P.n, out);
+    else col_norms_kernel<false><<<nrhs, 1024, 0, P.stream>>>(X, ld, P.n, out);
+    return check_cuda("norms");
+}
+
+}  // namespace cliqgpu

@@ -1,0 +1,702 @@
+// Plan construction (front layout, level schedule, work lists, assembly map)
+// and the numeric entry points of the C ABI.
+//
+// Memory layout in HBM (one allocation per buffer, sized once per plan):
+//   factor arena  all frontL blocks, column-major m x n, ld m, 128-byte aligned,
+//                 in the storage precision (FP64 plain, FP32 mixed).
+//   D             pivots in FP64 (complex interleaved), ND order, length n.
+//   update pools  two stacks indexed by depth parity: the updates of depth d
+//                 live in pool[d % 2] and are consumed by depth d-1, which
+//                 writes pool[(d-1) % 2]; the reference frees each child
+//                 update right after its extend-add (ldl/local.hpp:80,102).
+//   tinv          one nb x nb inverse diagonal block per front of a step.
+//   work lists    int4 items, GEMM problems and tile prefix sums for every
+//                 launch of the schedule, built here once.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "cliqgpu_internal.h"
+
+struct cliqgpu_plan_s {
+    cliqgpu::Plan p;
+};
+
+namespace cliqgpu {
+
+static std::mutex g_err_mu;
+static std::string g_last_error;
+
+void set_last_error(const std::string& msg) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_last_error = msg;
+}
+
+int check_cuda(const char* where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_last_error(std::string(where) + ": " + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? CLIQ_ERR_OOM : CLIQ_ERR_CUDA;
+    }
+    return CLIQ_OK;
+}
+
+static int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+template <class T>
+static int dev_upload(Plan& P, T** dst, const std::vector<T>& src) {
+    const size_t bytes = sizeof(T) * std::max<size_t>(src.size(), 1);
+    if (cudaMalloc((void**)dst, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error("cudaMalloc failed for " + std::to_string(bytes) + " bytes");
+        return CLIQ_ERR_OOM;
+    }
+    P.device_bytes += bytes;
+    if (!src.empty() && cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return check_cuda("upload");
+    return CLIQ_OK;
+}
+
+static int dev_alloc(Plan& P, void** dst, size_t bytes) {
+    bytes = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(dst, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error("cudaMalloc failed for " + std::to_string(bytes) + " bytes");
+        *dst = nullptr;
+        return CLIQ_ERR_OOM;
+    }
+    P.device_bytes += bytes;
+    return CLIQ_OK;
+}
+
+void free_plan(Plan& P) {
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.prefix, P.dest,
+                    P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
+                    P.wpool[1], P.xnodal, P.xwork, P.norms};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (P.own_stream && P.stream) cudaStreamDestroy(P.stream);
+}
+
+#define TRY(x)                      \
+    do {                            \
+        int _st = (x);              \
+        if (_st != CLIQ_OK) return _st; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
+                      const int32_t* colind) {
+    const int nn = info->num_nodes;
+    if (nn <= 0 || !info->size || !info->off || !info->parent || !info->children || !info->lower_ptr || !info->lower) {
+        set_last_error("plan_create: incomplete symbolic info");
+        return CLIQ_ERR_ARG;
+    }
+    P.n = n;
+    P.nnz = rowptr[n];
+    P.num_fronts = nn;
+    const int nb = P.nb;
+    // ---- depths (post-order: parents have larger indices) ----
+    P.depth.assign(nn, 0);
+    int64_t total_size = 0;
+    for (int s = nn - 1; s >= 0; --s) {
+        const int par = info->parent[s];
+        if (par >= 0 && par < nn && par > s) P.depth[s] = P.depth[par] + 1;
+        else if (par >= 0 && par < nn) { set_last_error("plan_create: parent index not after child"); return CLIQ_ERR_ARG; }
+        total_size += info->size[s];
+        if (info->size[s] < 0) return CLIQ_ERR_ARG;
+    }
+    if (total_size != n) { set_last_error("plan_create: front sizes do not sum to n"); return CLIQ_ERR_ARG; }
+    P.max_depth = *std::max_element(P.depth.begin(), P.depth.end());
+    P.level_list.assign(P.max_depth + 1, {});
+    for (int s = 0; s < nn; ++s) P.level_list[P.depth[s]].push_back(s);
+
+    // ---- front layout ----
+    P.hfronts.assign(nn, FrontDev{});
+    const int64_t align_elems = std::max<int64_t>(1, 128 / P.elem_bytes());
+    int64_t arena = 0;
+    std::vector<int64_t> level_pool(P.max_depth + 1, 0), level_w(P.max_depth + 1, 0);
+    P.factor_flops = P.solve_flops = P.factor_entries = 0;
+    for (int s = 0; s < nn; ++s) {
+        FrontDev& f = P.hfronts[s];
+        const int64_t nlow = info->lower_ptr[s + 1] - info->lower_ptr[s];
+        f.n = info->size[s];
+        f.m = (int32_t)(f.n + nlow);
+        f.u = (int32_t)nlow;
+        f.off = info->off[s];
+        f.L = arena;
+        arena = align_up(arena + (int64_t)f.m * f.n, align_elems);
+        const int d = P.depth[s];
+        f.pool = d & 1;
+        f.U = level_pool[d];
+        level_pool[d] = align_up(level_pool[d] + (int64_t)f.u * f.u, align_elems);
+        f.W = level_w[d];
+        level_w[d] += f.u;
+        f.lower = info->lower_ptr[s];
+        f.cmap = -1;
+        f.CU[0] = f.CU[1] = -1;
+        f.CW[0] = f.CW[1] = 0;
+        f.cu[0] = f.cu[1] = 0;
+        const double m = f.m, nd = f.n;
+        P.factor_flops += nd * nd * nd / 3.0 + (m - nd) * nd * nd + (m - nd) * (m - nd) * nd;
+        P.solve_flops += nd * nd + 2.0 * (m - nd) * nd;
+        P.factor_entries += m * nd;
+    }
+    if (P.cplx()) { P.factor_flops *= 4; P.solve_flops *= 4; }
+    P.arena_elems = std::max<int64_t>(arena, 1);
+    P.pool_elems[0] = P.pool_elems[1] = 1;
+    P.wpool_elems[0] = P.wpool_elems[1] = 1;
+    for (int d = 0; d <= P.max_depth; ++d) {
+        P.pool_elems[d & 1] = std::max(P.pool_elems[d & 1], level_pool[d]);
+        P.wpool_elems[d & 1] = std::max(P.wpool_elems[d & 1], level_w[d]);
+    }
+
+    // ---- children maps (inverse relative indices) ----
+    std::vector<int32_t> cmaps;
+    const int32_t* low = info->lower;
+    for (int s = 0; s < nn; ++s) {
+        const int l = info->children[2 * s], r = info->children[2 * s + 1];
+        if (l < 0 && r < 0) continue;
+        if (l < 0 || r < 0 || l >= s || r >= s) { set_last_error("plan_create: bad children"); return CLIQ_ERR_ARG; }
+        FrontDev& f = P.hfronts[s];
+        f.cmap = (int64_t)cmaps.size();
+        cmaps.resize(cmaps.size() + 2 * (size_t)f.m, -1);
+        const int32_t* plow = low + info->lower_ptr[s];
+        const int64_t pnl = info->lower_ptr[s + 1] - info->lower_ptr[s];
+        for (int c = 0; c < 2; ++c) {
+            const int ch = c == 0 ? l : r;
+            const FrontDev& cf = P.hfronts[ch];
+            f.CU[c] = cf.U;
+            f.CW[c] = cf.W;
+            f.cu[c] = cf.u;
+            const int32_t* clow = low + info->lower_ptr[ch];
+            for (int ci = 0; ci < cf.u; ++ci) {
+                const int g = clow[ci];
+                int rel;
+                if (g >= f.off && g < f.off + f.n) rel = g - f.off;
+                else {
+                    const int32_t* it = std::lower_bound(plow, plow + pnl, g);
+                    if (it == plow + pnl || *it != g) { set_last_error("plan_create: child structure not contained in parent"); return CLIQ_ERR_ARG; }
+                    rel = f.n + (int)(it - plow);
+                }
+                cmaps[f.cmap + (int64_t)c * f.m + rel] = ci;
+            }
+        }
+    }
+
+    // ---- factor schedule ----
+    std::vector<int32_t> items;   // int4 quads
+    std::vector<GemmProb> probs;
+    std::vector<int64_t> prefix;
+    auto push_item = [&](int a, int b, int c, int d) { items.push_back(a); items.push_back(b); items.push_back(c); items.push_back(d); };
+    P.launches.clear();
+    int64_t max_slots = 1;
+    auto tiles_of = [](int M, int N) -> int64_t {
+        const int64_t Mt = (M + kTile - 1) / kTile, Nt = (N + kTile - 1) / kTile;
+        return Nt * Mt - Nt * (Nt - 1) / 2;
+    };
+    auto add_gemm = [&](std::vector<GemmProb>& lst, int depth) {
+        if (lst.empty()) return;
+        Launch ln{};
+        ln.kind = Launch::GEMM;
+        ln.items = (int64_t)probs.size();
+        ln.nitems = (int32_t)lst.size();
+        ln.prefix = (int64_t)prefix.size();
+        int64_t tot = 0;
+        for (auto& pr : lst) { prefix.push_back(tot); tot += tiles_of(pr.M, pr.N); probs.push_back(pr); }
+        ln.nblocks = tot;
+        ln.depth = depth;
+        P.launches.push_back(ln);
+    };
+    for (int d = P.max_depth; d >= 0; --d) {
+        const auto& lv = P.level_list[d];
+        // extend-add
+        {
+            Launch ln{};
+            ln.kind = Launch::EXTEND_ADD;
+            ln.items = (int64_t)items.size() / 4;
+            for (int s : lv) {
+                const FrontDev& f = P.hfronts[s];
+                const bool leaf = f.cmap < 0;
+                for (int j0 = 0; j0 < f.m; j0 += kEACols) {
+                    if (leaf && j0 + kEACols <= f.n) continue;
+                    push_item(s, j0, 0, 0);
+                }
+            }
+            ln.nitems = (int32_t)(items.size() / 4 - ln.items);
+            ln.nblocks = ln.nitems;
+            ln.depth = d;
+            if (ln.nitems) P.launches.push_back(ln);
+        }
+        int maxn = 0;
+        for (int s : lv) maxn = std::max(maxn, P.hfronts[s].n);
+        for (int k = 0; k < maxn; k += nb) {
+            Launch dg{};
+            dg.kind = Launch::DIAG;
+            dg.k = k;
+            dg.depth = d;
+            dg.items = (int64_t)items.size() / 4;
+            std::vector<std::pair<int, int>> active;
+            for (int s : lv)
+                if (P.hfronts[s].n > k) {
+                    push_item(s, (int)active.size(), 0, 0);
+                    active.push_back({s, (int)active.size()});
+                }
+            dg.nitems = (int32_t)active.size();
+            dg.nblocks = dg.nitems;
+            max_slots = std::max<int64_t>(max_slots, dg.nitems);
+            P.launches.push_back(dg);
+            Launch pn{};
+            pn.kind = Launch::PANEL;
+            pn.k = k;
+            pn.depth = d;
+            pn.items = (int64_t)items.size() / 4;
+            std::vector<GemmProb> trail;
+            for (auto& a : active) {
+                const FrontDev& f = P.hfronts[a.first];
+                const int kb = std::min(nb, f.n - k);
+                const int rows = f.m - k - kb;
+                for (int rb = 0; rb * kTile < rows; ++rb) push_item(a.first, a.second, rb, 0);
+                const int N = f.n - k - kb;
+                if (N > 0) {
+                    GemmProb pr{};
+                    pr.A = f.L + (k + kb) + (int64_t)k * f.m;
+                    pr.B = pr.A;
+                    pr.C = f.L + (k + kb) + (int64_t)(k + kb) * f.m;
+                    pr.d = f.off + k;
+                    pr.lda = f.m;
+                    pr.ldc = f.m;
+                    pr.M = rows;
+                    pr.N = N;
+                    pr.K = kb;
+                    pr.cpool = -1;
+                    trail.push_back(pr);
+                }
+            }
+            pn.nitems = (int32_t)(items.size() / 4 - pn.items);
+            pn.nblocks = pn.nitems;
+            if (pn.nitems) P.launches.push_back(pn);
+            add_gemm(trail, d);
+        }
+        std::vector<GemmProb> schur;
+        for (int s : lv) {
+            const FrontDev& f = P.hfronts[s];
+            if (f.u <= 0 || f.n <= 0) continue;
+            GemmProb pr{};
+            pr.A = f.L + f.n;
+            pr.B = pr.A;
+            pr.C = f.U;
+            pr.d = f.off;
+            pr.lda = f.m;
+            pr.ldc = f.u;
+            pr.M = f.u;
+            pr.N = f.u;
+            pr.K = f.n;
+            pr.cpool = f.pool;
+            schur.push_back(pr);
+        }
+        add_gemm(schur, d);
+    }
+    P.tinv_slots = max_slots;
+
+    // ---- solve schedule ----
+    P.solve_levels.assign(P.max_depth + 1, SolveLevel{});
+    std::vector<int32_t> level_fronts;
+    int flag = 0;
+    for (int d = 0; d <= P.max_depth; ++d) {
+        SolveLevel& sl = P.solve_levels[d];
+        sl.depth = d;
+        sl.fronts = (int64_t)level_fronts.size();
+        for (int s : P.level_list[d]) level_fronts.push_back(s);
+        sl.nfronts = (int32_t)P.level_list[d].size();
+        sl.fwd_items = (int64_t)items.size() / 4;
+        for (int s : P.level_list[d]) {
+            FrontDev& f = P.hfronts[s];
+            if (f.n <= 0 || f.m <= 0) continue;
+            f.flag_base = flag;
+            flag += (f.n + kTile - 1) / kTile;
+            for (int rb = 0; rb * kTile < f.m; ++rb) push_item(s, rb, 0, 0);
+        }
+        sl.nfwd = (int32_t)(items.size() / 4 - sl.fwd_items);
+        sl.bwd_items = (int64_t)items.size() / 4;
+        for (int s : P.level_list[d]) {
+            const FrontDev& f = P.hfronts[s];
+            if (f.n <= 0 || f.m <= 0) continue;
+            for (int rb = (f.n + kTile - 1) / kTile - 1; rb >= 0; --rb) push_item(s, rb, 0, 0);
+        }
+        sl.nbwd = (int32_t)(items.size() / 4 - sl.bwd_items);
+    }
+    P.flags_total = std::max(flag, 1);
+
+    // ---- assembly map (DistSymmFrontTree::Initialize, impl.hpp:244-297) ----
+    std::vector<int32_t> node_of(n), inv(n);
+    for (int s = 0; s < nn; ++s)
+        for (int t = 0; t < info->size[s]; ++t) node_of[info->off[s] + t] = s;
+    for (int64_t i = 0; i < n; ++i) {
+        if (map[i] < 0 || map[i] >= n) { set_last_error("plan_create: map out of range"); return CLIQ_ERR_ARG; }
+        inv[map[i]] = (int32_t)i;
+    }
+    std::vector<int64_t> dest(P.nnz, -1);
+    for (int64_t i = 0; i < n; ++i) {
+        const int p = map[i];
+        const int s = node_of[p];
+        const FrontDev& f = P.hfronts[s];
+        const int t = p - f.off;
+        const int32_t* plow = low + info->lower_ptr[s];
+        const int64_t pnl = info->lower_ptr[s + 1] - info->lower_ptr[s];
+        for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+            const int c = colind[e];
+            if (c < 0 || c >= n) { set_last_error("plan_create: column index out of range"); return CLIQ_ERR_ARG; }
+            const int target = map[c];
+            if (target < f.off + t) continue;
+            if (target < f.off + f.n) dest[e] = f.L + (target - f.off) + (int64_t)t * f.m;
+            else {
+                const int32_t* it = std::lower_bound(plow, plow + pnl, target);
+                if (it == plow + pnl || *it != target) { set_last_error("plan_create: entry outside the front structure"); return CLIQ_ERR_ARG; }
+                dest[e] = f.L + f.n + (it - plow) + (int64_t)t * f.m;
+            }
+        }
+    }
+
+    // ---- device allocations ----
+    const int eb = P.elem_bytes();
+    TRY(dev_alloc(P, &P.L, (size_t)P.arena_elems * eb));
+    TRY(dev_alloc(P, (void**)&P.D, sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)n));
+    TRY(dev_alloc(P, &P.pool[0], (size_t)P.pool_elems[0] * eb));
+    TRY(dev_alloc(P, &P.pool[1], (size_t)P.pool_elems[1] * eb));
+    TRY(dev_alloc(P, &P.tinv, (size_t)P.tinv_slots * nb * nb * eb));
+    TRY(dev_upload(P, &P.fronts, P.hfronts));
+    TRY(dev_upload(P, &P.cmaps, cmaps));
+    std::vector<int32_t> lowv(low, low + info->lower_ptr[nn]);
+    TRY(dev_upload(P, &P.lower, lowv));
+    TRY(dev_upload(P, &P.items, items));
+    TRY(dev_upload(P, &P.probs, probs));
+    TRY(dev_upload(P, &P.prefix, prefix));
+    TRY(dev_upload(P, &P.dest, dest));
+    TRY(dev_upload(P, &P.perm, inv));
+    TRY(dev_upload(P, &P.level_fronts, level_fronts));
+    std::vector<int32_t> zeros_flags(P.flags_total, 0);
+    TRY(dev_upload(P, &P.flags, zeros_flags));
+    std::vector<int32_t> zt(2 * (P.max_depth + 1) + 2, 0);
+    TRY(dev_upload(P, &P.tickets, zt));
+    std::vector<int32_t> st = {INT_MAX, 0, 0, 0};
+    TRY(dev_upload(P, &P.status, st));
+    if (P.keep_matrix) {
+        std::vector<int64_t> rp(rowptr, rowptr + n + 1);
+        std::vector<int32_t> ci(colind, colind + P.nnz);
+        TRY(dev_upload(P, &P.rowptr, rp));
+        TRY(dev_upload(P, &P.colind, ci));
+        TRY(dev_alloc(P, (void**)&P.aval, sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)std::max<int64_t>(P.nnz, 1)));
+    }
+    return CLIQ_OK;
+}
+
+static int ensure_workspace(Plan& P, int nrhs) {
+    if (nrhs <= P.ws_nrhs) return CLIQ_OK;
+    void* old[] = {P.wpool[0], P.wpool[1], P.xnodal, P.xwork, P.norms};
+    for (void* p : old)
+        if (p) cudaFree(p);
+    P.wpool[0] = P.wpool[1] = P.xnodal = nullptr;
+    P.xwork = P.norms = nullptr;
+    const int eb = P.elem_bytes();
+    const int chunk = std::min(nrhs, 16);
+    TRY(dev_alloc(P, &P.wpool[0], (size_t)P.wpool_elems[0] * chunk * eb));
+    TRY(dev_alloc(P, &P.wpool[1], (size_t)P.wpool_elems[1] * chunk * eb));
+    TRY(dev_alloc(P, &P.xnodal, (size_t)P.n * nrhs * eb));
+    TRY(dev_alloc(P, (void**)&P.xwork, sizeof(double) * (P.cplx() ? 2 : 1) * 3 * (size_t)P.n * nrhs));
+    TRY(dev_alloc(P, (void**)&P.norms, sizeof(double) * 2 * nrhs));
+    P.ws_nrhs = nrhs;
+    return CLIQ_OK;
+}
+
+static int solve_nodal_dispatch(Plan& P, void* xn, int nrhs) {
+    if (P.precision == CLIQ_FP64)
+        return P.cplx() ? run_solve_nodal<double, true>(P, xn, nrhs) : run_solve_nodal<double, false>(P, xn, nrhs);
+    return P.cplx() ? run_solve_nodal<float, true>(P, xn, nrhs) : run_solve_nodal<float, false>(P, xn, nrhs);
+}
+
+int read_status(Plan& P, int64_t* zero_pivot) {
+    int32_t st[2];
+    if (cudaMemcpyAsync(st, P.status, sizeof(st), cudaMemcpyDeviceToHost, P.stream) != cudaSuccess) return check_cuda("status");
+    if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("sync");
+    if (zero_pivot) *zero_pivot = st[0] == INT_MAX ? -1 : (int64_t)st[0] - 1;
+    if (st[1]) { set_last_error("a device-side wait timed out"); return CLIQ_ERR_TIMEOUT; }
+    return st[0] == INT_MAX ? CLIQ_OK : CLIQ_ERR_ZERO_PIVOT;
+}
+
+}  // namespace cliqgpu
+
+using namespace cliqgpu;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
+                        const int32_t* colind, const cliqgpu_options* options, void* stream, cliqgpu_plan* out) {
+    if (!info || !map || !rowptr || !colind || !out || n <= 0) return CLIQ_ERR_ARG;
+    *out = nullptr;
+    cliqgpu_plan h = new (std::nothrow) cliqgpu_plan_s;
+    if (!h) return CLIQ_ERR_OOM;
+    Plan& P = h->p;
+    if (options) {
+        P.field = options->field == CLIQ_COMPLEX ? CLIQ_COMPLEX : CLIQ_REAL;
+        P.precision = options->precision == CLIQ_FP32 ? CLIQ_FP32 : CLIQ_FP64;
+        P.conjugate = options->conjugate ? 1 : 0;
+        P.keep_matrix = options->keep_matrix ? 1 : 0;
+        if (options->block_size != 0 && options->block_size != kTile) {
+            delete h;
+            set_last_error("plan_create: only block_size 64 is supported");
+            return CLIQ_ERR_ARG;
+        }
+    }
+    P.nb = kTile;
+    if (stream) P.stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
+        P.own_stream = true;
+    }
+    int st = build_plan(P, info, n, map, rowptr, colind);
+    if (st != CLIQ_OK) {
+        free_plan(P);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CLIQ_OK;
+}
+
+int cliqgpu_assemble(cliqgpu_plan h, const void* values, int32_t values_on_device) {
+    if (!h || !values) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    const size_t bytes = sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)P.nnz;
+    const double* dvals = (const double*)values;
+    void* tmp = nullptr;
+    if (!values_on_device) {
+        if (P.keep_matrix) {
+            if (cudaMemcpyAsync(P.aval, values, bytes, cudaMemcpyHostToDevice, P.stream) != cudaSuccess) return check_cuda("copy A");
+            dvals = P.aval;
+        } else {
+            if (cudaMallocAsync(&tmp, std::max<size_t>(bytes, 16), P.stream) != cudaSuccess) return check_cuda("alloc A");
+            if (cudaMemcpyAsync(tmp, values, bytes, cudaMemcpyHostToDevice, P.stream) != cudaSuccess) return check_cuda("copy A");
+            dvals = (const double*)tmp;
+        }
+    } else if (P.keep_matrix) {
+        if (cudaMemcpyAsync(P.aval, values, bytes, cudaMemcpyDeviceToDevice, P.stream) != cudaSuccess) return check_cuda("copy A");
+    }
+    int st = launch_assemble(P, dvals);
+    if (tmp) cudaFreeAsync(tmp, P.stream);
+    if (st != CLIQ_OK) return st;
+    if (!values_on_device && cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("assemble sync");
+    P.assembled = true;
+    P.factored = false;
+    return CLIQ_OK;
+}
+
+int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
+    if (!h) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (!P.assembled) { set_last_error("factor: fronts were not assembled"); return CLIQ_ERR_STATE; }
+    if (P.factored) { set_last_error("Matrix is already factored"); return CLIQ_ERR_STATE; }
+    int32_t st0[2] = {INT_MAX, 0};
+    cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
+    int st;
+    if (P.precision == CLIQ_FP64) st = P.cplx() ? run_factor<double, true>(P) : run_factor<double, false>(P);
+    else st = P.cplx() ? run_factor<float, true>(P) : run_factor<float, false>(P);
+    if (st != CLIQ_OK) return st;
+    P.factored = true;
+    return read_status(P, zero_pivot);
+}
+
+int cliqgpu_solve(cliqgpu_plan h, void* X, int64_t ldx, int32_t nrhs, int32_t x_on_device, int32_t nodal) {
+    if (!h || !X || nrhs <= 0) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (ldx < P.n) return CLIQ_ERR_ARG;
+    if (!P.factored) { set_last_error("solve: the front tree is not factored"); return CLIQ_ERR_STATE; }
+    TRY(ensure_workspace(P, nrhs));
+    P.last_launches = 0;
+    const int w = P.cplx() ? 2 : 1;
+    const size_t colbytes = sizeof(double) * w * (size_t)P.n;
+    double* xd = (double*)X;
+    double* stage = nullptr;
+    if (!x_on_device) {
+        stage = P.xwork;   // FP64 staging, ld n
+        for (int j = 0; j < nrhs; ++j)
+            if (cudaMemcpyAsync(stage + (size_t)w * j * P.n, (const double*)X + (size_t)w * j * ldx, colbytes,
+                                cudaMemcpyHostToDevice, P.stream) != cudaSuccess)
+                return check_cuda("copy X");
+        xd = stage;
+        ldx = P.n;
+    }
+    int32_t st0[2] = {INT_MAX, 0};
+    cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
+    const int32_t* perm = nodal ? nullptr : P.perm;   // nodal: X is already in ND order
+    TRY(launch_pull(P, perm, xd, ldx, nrhs, P.xnodal, 1.0));
+    TRY(solve_nodal_dispatch(P, P.xnodal, nrhs));
+    TRY(launch_push(P, perm, P.xnodal, xd, ldx, nrhs, 1.0, 0));
+    P.last_launches += 2;
+    if (!x_on_device) {
+        for (int j = 0; j < nrhs; ++j)
+            if (cudaMemcpyAsync((double*)X + (size_t)w * j * ldx, stage + (size_t)w * j * P.n, colbytes,
+                                cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+                return check_cuda("copy X back");
+    }
+    int64_t zp;
+    int st = read_status(P, &zp);
+    if (st == CLIQ_ERR_ZERO_PIVOT) st = CLIQ_OK;   // pivots were reported by factor
+    return st;
+}
+
+int cliqgpu_multiply(cliqgpu_plan h, const double* alpha, const void* X, const double* beta, void* Y, int64_t ld, int32_t nrhs) {
+    if (!h || !alpha || !beta || !X || !Y || nrhs <= 0) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (!P.keep_matrix || !P.assembled) { set_last_error("multiply: plan holds no FP64 matrix"); return CLIQ_ERR_STATE; }
+    const bool c = P.cplx();
+    return launch_spmv(P, alpha[0], c ? alpha[1] : 0.0, (const double*)X, beta[0], c ? beta[1] : 0.0, (double*)Y, ld, nrhs);
+}
+
+int cliqgpu_refine(cliqgpu_plan h, const void* B, void* X, int64_t ld, int32_t nrhs, int32_t on_device, double tol,
+                   int32_t max_iter, int32_t* iters, double* relres) {
+    if (!h || !B || !X || nrhs <= 0 || ld <= 0) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (ld < P.n) return CLIQ_ERR_ARG;
+    if (!P.factored) { set_last_error("refine: the front tree is not factored"); return CLIQ_ERR_STATE; }
+    if (!P.keep_matrix) { set_last_error("refine: plan was created without keep_matrix"); return CLIQ_ERR_STATE; }
+    TRY(ensure_workspace(P, nrhs));
+    P.last_launches = 0;
+    const int w = P.cplx() ? 2 : 1;
+    const int64_t n = P.n;
+    const size_t colbytes = sizeof(double) * w * (size_t)n;
+    double* b = P.xwork;
+    double* x = b + (size_t)w * n * nrhs;
+    double* r = x + (size_t)w * n * nrhs;
+    const cudaMemcpyKind kin = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int j = 0; j < nrhs; ++j)
+        if (cudaMemcpyAsync(b + (size_t)w * j * n, (const double*)B + (size_t)w * j * ld, colbytes, kin, P.stream) != cudaSuccess)
+            return check_cuda("copy B");
+    cudaMemsetAsync(x, 0, colbytes * nrhs, P.stream);
+    cudaMemcpyAsync(r, b, colbytes * nrhs, cudaMemcpyDeviceToDevice, P.stream);
+    std::vector<double> hn(2 * nrhs);
+    TRY(launch_col_norms(P, b, n, nrhs, P.norms + nrhs));
+    int it = 0;
+    double rel = 0;
+    int32_t st0[2] = {INT_MAX, 0};
+    cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
+    for (;;) {
+        TRY(launch_col_norms(P, r, n, nrhs, P.norms));
+        if (cudaMemcpyAsync(hn.data(), P.norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+            return check_cuda("norms");
+        if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("refine sync");
+        rel = 0;
+        double rmax = 0;
+        for (int j = 0; j < nrhs; ++j) {
+            const double bn = std::sqrt(hn[nrhs + j]), rn = std::sqrt(hn[j]);
+            rel = std::max(rel, bn > 0 ? rn / bn : rn);
+            rmax = std::max(rmax, rn);
+        }
+        if (rel <= tol || it >= max_iter || !(rel == rel)) break;
+        const double scale = rmax > 0 ? 1.0 / rmax : 1.0;
+        TRY(launch_pull(P, P.perm, r, n, nrhs, P.xnodal, scale));
+        TRY(solve_nodal_dispatch(P, P.xnodal, nrhs));
+        TRY(launch_push(P, P.perm, P.xnodal, x, n, nrhs, 1.0 / scale, 1));
+        cudaMemcpyAsync(r, b, colbytes * nrhs, cudaMemcpyDeviceToDevice, P.stream);
+        TRY(launch_spmv(P, -1.0, 0.0, x, 1.0, 0.0, r, n, nrhs));
+        ++it;
+    }
+    const cudaMemcpyKind kout = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    for (int j = 0; j < nrhs; ++j)
+        if (cudaMemcpyAsync((double*)X + (size_t)w * j * ld, x + (size_t)w * j * n, colbytes, kout, P.stream) != cudaSuccess)
+            return check_cuda("copy X");
+    int32_t dst[2];
+    cudaMemcpyAsync(dst, P.status, sizeof(dst), cudaMemcpyDeviceToHost, P.stream);
+    if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("refine end");
+    if (iters) *iters = it;
+    if (relres) *relres = rel;
+    if (dst[1]) { set_last_error("a device-side wait timed out"); return CLIQ_ERR_TIMEOUT; }
+    return rel <= tol ? CLIQ_OK : CLIQ_ERR_NOCONV;
+}
+
+int cliqgpu_get_front(cliqgpu_plan h, int32_t s, double* Lout, double* Dout, int32_t dims[2]) {
+    if (!h) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (s < 0 || s >= P.num_fronts) return CLIQ_ERR_ARG;
+    const FrontDev& f = P.hfronts[s];
+    if (dims) { dims[0] = f.m; dims[1] = f.n; }
+    if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("sync");
+    const int w = P.cplx() ? 2 : 1;
+    if (Lout) {
+        const size_t cnt = (size_t)w * f.m * f.n;
+        if (P.precision == CLIQ_FP64) {
+            if (cudaMemcpy(Lout, (const double*)P.L + (size_t)w * f.L, sizeof(double) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess)
+                return check_cuda("get front");
+        } else {
+            std::vector<float> tmp(cnt);
+            if (cudaMemcpy(tmp.data(), (const float*)P.L + (size_t)w * f.L, sizeof(float) * cnt, cudaMemcpyDeviceToHost) != cudaSuccess)
+                return check_cuda("get front");
+            for (size_t i = 0; i < cnt; ++i) Lout[i] = tmp[i];
+        }
+    }
+    if (Dout && f.n > 0) {
+        if (cudaMemcpy(Dout, P.D + (size_t)w * f.off, sizeof(double) * w * f.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return check_cuda("get diag");
+    }
+    return CLIQ_OK;
+}
+
+int cliqgpu_plan_query(cliqgpu_plan h, int32_t key, double* value) {
+    if (!h || !value) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    switch (key) {
+        case 0: *value = P.factor_flops; break;
+        case 1: *value = P.solve_flops; break;
+        case 2: *value = P.factor_entries; break;
+        case 3: *value = (double)P.device_bytes; break;
+        case 4: *value = (double)P.last_launches; break;
+        case 5: *value = P.num_fronts; break;
+        case 6: *value = P.max_depth; break;
+        case 7: *value = (double)P.arena_elems * P.elem_bytes(); break;
+        default: return CLIQ_ERR_ARG;
+    }
+    return CLIQ_OK;
+}
+
+int cliqgpu_synchronize(cliqgpu_plan h) {
+    if (!h) return CLIQ_ERR_ARG;
+    if (cudaStreamSynchronize(h->p.stream) != cudaSuccess) return check_cuda("sync");
+    return CLIQ_OK;
+}
+
+void cliqgpu_plan_destroy(cliqgpu_plan h) {
+    if (!h) return;
+    cudaStreamSynchronize(h->p.stream);
+    free_plan(h->p);
+    delete h;
+}
+
+const char* cliqgpu_status_string(int32_t status) {
+    switch (status) {
+        case CLIQ_OK: return "ok";
+        case CLIQ_ERR_ARG: return "invalid argument";
+        case CLIQ_ERR_OOM: return "out of memory";
+        case CLIQ_ERR_ZERO_PIVOT: return "zero pivot";
+        case CLIQ_ERR_CUDA: return "CUDA error";
+        case CLIQ_ERR_TIMEOUT: return "device wait timed out";
+        case CLIQ_ERR_STATE: return "call out of order";
+        case CLIQ_ERR_NOCONV: return "refinement did not converge";
+        default: return "unknown status";
+    }
+}
+
+const char* cliqgpu_last_error(void) {
+    static thread_local std::string copy;
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    copy = g_last_error;
+    return copy.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,215 @@
+// Host-side symbolic phase: natural nested dissection and symbolic analysis
+// for a single process.  This is the product's own implementation (the CPU
+// oracle under oracle/ is a separate restatement used only to check it).
+//
+// Behaviour follows the reference:
+//   NaturalNestedDissection   include/clique/symbolic/natural_nested_dissection.hpp:447-488
+//   NaturalBisect             include/clique/symbolic/natural_nested_dissection.hpp:490-619
+//   recursion / node order    include/clique/symbolic/natural_nested_dissection.hpp:60-189, 313-445
+//   ReverseOrder              include/clique/symbolic/nested_dissection.hpp:817-886
+//   BuildMap (P=1)            include/clique/symbolic/nested_dissection.hpp:1206-1363
+//   LocalSymmetricAnalysis    src/symbolic/LocalSymmetricAnalysis.cpp:15-114
+//
+// Design: instead of materialising a child graph at every bisection (the
+// reference copies the graph into left/right children), the recursion here
+// works on index boxes only.  Every vertex of a box sub-problem is adjacent
+// only to vertices of the same box or of ancestor separators, so a node's
+// original lower structure is recovered afterwards from the global graph as
+// { ND(target) : target adjacent to the node's vertices, ND(target) >= end of
+// the node's subtree range }.  That is the same set the reference collects
+// from its child graphs (targets numbered >= numSources), computed in
+// O(nnz log) once instead of once per tree level.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "cliqgpu_internal.h"
+
+namespace cliqgpu {
+
+namespace {
+
+struct Box { int x0, y0, z0, nx, ny, nz; };
+
+struct PreNode {
+    int size = 0, off = 0, parent = -1, sep_parent = -1;
+    int nchild = 0, child[2] = {-1, -1};
+    std::vector<int> inds;      // natural indices in the node's local order
+    int subtree_end = 0;        // one past the last ND index of the node's subtree
+};
+
+struct NDBuilder {
+    int NX, NY, NZ, cutoff;
+    std::vector<PreNode> nodes;
+
+    int gidx(int x, int y, int z) const { return x + y * NX + z * NX * NY; }
+
+    // Natural order of a box (x fastest, then y, then z) -- the order in which
+    // NaturalBisect fills each child, so it is also each child's local order.
+    void box_inds(const Box& b, std::vector<int>& out) const {
+        out.clear();
+        out.reserve((size_t)b.nx * b.ny * b.nz);
+        for (int z = 0; z < b.nz; ++z)
+            for (int y = 0; y < b.ny; ++y)
+                for (int x = 0; x < b.nx; ++x) out.push_back(gidx(b.x0 + x, b.y0 + y, b.z0 + z));
+    }
+
+    void recurse(const Box& b, int parent, int off) {
+        const int n = b.nx * b.ny * b.nz;
+        const int id = (int)nodes.size();
+        nodes.emplace_back();
+        if (n <= cutoff) {
+            PreNode& nd = nodes[id];
+            nd.size = n; nd.off = off; nd.parent = parent; nd.sep_parent = parent;
+            box_inds(b, nd.inds);
+            nd.subtree_end = off + n;
+            return;
+        }
+        Box L = b, R = b;
+        std::vector<int> sep;
+        // longest axis, ties broken x > y > z (NaturalBisect)
+        if (b.nx >= b.ny && b.nx >= b.nz) {
+            const int l = (b.nx - 1) / 2;
+            L.nx = l; R.x0 = b.x0 + l + 1; R.nx = b.nx - 1 - l;
+            for (int z = 0; z < b.nz; ++z)
+                for (int y = 0; y < b.ny; ++y) sep.push_back(gidx(b.x0 + l, b.y0 + y, b.z0 + z));
+        } else if (b.ny >= b.nx && b.ny >= b.nz) {
+            const int l = (b.ny - 1) / 2;
+            L.ny = l; R.y0 = b.y0 + l + 1; R.ny = b.ny - 1 - l;
+            for (int z = 0; z < b.nz; ++z)
+                for (int x = 0; x < b.nx; ++x) sep.push_back(gidx(b.x0 + x, b.y0 + l, b.z0 + z));
+        } else {
+            const int l = (b.nz - 1) / 2;
+            L.nz = l; R.z0 = b.z0 + l + 1; R.nz = b.nz - 1 - l;
+            for (int y = 0; y < b.ny; ++y)
+                for (int x = 0; x < b.nx; ++x) sep.push_back(gidx(b.x0 + x, b.y0 + y, b.z0 + l));
+        }
+        const int nl = L.nx * L.ny * L.nz, nr = R.nx * R.ny * R.nz;
+        {
+            PreNode& nd = nodes[id];
+            nd.size = (int)sep.size();
+            nd.off = off + nl + nr;
+            nd.parent = parent; nd.sep_parent = parent;
+            nd.nchild = 2;
+            nd.inds = std::move(sep);
+            nd.subtree_end = off + n;
+        }
+        nodes[id].child[1] = (int)nodes.size();
+        recurse(R, id, off + nl);
+        nodes[id].child[0] = (int)nodes.size();
+        recurse(L, id, off);
+    }
+};
+
+// std::set_union of two sorted vectors
+static void sorted_union(const std::vector<int>& a, const std::vector<int>& b, std::vector<int>& out) {
+    out.resize(a.size() + b.size());
+    out.resize(std::set_union(a.begin(), a.end(), b.begin(), b.end(), out.begin()) - out.begin());
+}
+
+static void relative_indices(const std::vector<int>& sub, const std::vector<int>& full, std::vector<int>& rel) {
+    rel.resize(sub.size());
+    auto it = full.begin();
+    for (size_t i = 0; i < sub.size(); ++i) {
+        it = std::lower_bound(it, full.end(), sub[i]);
+        rel[i] = (int)(it - full.begin());
+    }
+}
+
+}  // namespace
+
+int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                              int cutoff, Symbolic& S) {
+    if (nx < 0 || ny < 0 || nz < 0 || (int64_t)nx * ny * nz != n || n <= 0 || !rowptr || !colind) return CLIQ_ERR_ARG;
+    if (n > INT32_MAX / 2) return CLIQ_ERR_ARG;
+    NDBuilder B{nx, ny, nz, cutoff, {}};
+    B.recurse(Box{0, 0, 0, nx, ny, nz}, -1, 0);
+
+    // ReverseOrder: new index = last - old; the root keeps parent -1 unless it is the only node.
+    const int nn = (int)B.nodes.size(), last = nn - 1;
+    S.num_nodes = nn;
+    S.n = n;
+    S.size.assign(nn, 0); S.off.assign(nn, 0); S.my_off.assign(nn, 0); S.parent.assign(nn, -1);
+    S.sep_parent.assign(nn, -1); S.children.assign(2 * (size_t)nn, -1); S.on_left.assign(nn, 0);
+    S.lower.assign(nn, {}); S.orig_lower.assign(nn, {}); S.orig_rel.assign(nn, {});
+    S.left_rel.assign(nn, {}); S.right_rel.assign(nn, {}); S.inds.assign(nn, {});
+    std::vector<int> subtree_end(nn);
+    for (int old = 0; old < nn; ++old) {
+        PreNode& p = B.nodes[old];
+        const int s = last - old;
+        S.size[s] = p.size; S.off[s] = p.off;
+        if (nn == 1) { S.parent[s] = last - p.parent; S.sep_parent[s] = last - p.sep_parent; }
+        else if (old == 0) { S.parent[s] = -1; S.sep_parent[s] = -1; }
+        else { S.parent[s] = last - p.parent; S.sep_parent[s] = last - p.sep_parent; }
+        if (p.nchild == 2) { S.children[2 * s] = last - p.child[0]; S.children[2 * s + 1] = last - p.child[1]; }
+        S.inds[s] = std::move(p.inds);
+        subtree_end[s] = p.subtree_end;
+    }
+    B.nodes.clear();
+
+    // BuildMap at P=1
+    S.map.assign(n, 0); S.inv_map.assign(n, 0);
+    for (int s = 0; s < nn; ++s)
+        for (size_t t = 0; t < S.inds[s].size(); ++t) S.map[S.inds[s][t]] = S.off[s] + (int)t;
+    for (int64_t i = 0; i < n; ++i) S.inv_map[S.map[i]] = (int)i;
+
+    // original lower structure from the global graph
+    for (int s = 0; s < nn; ++s) {
+        std::vector<int>& o = S.orig_lower[s];
+        const int end = subtree_end[s];
+        for (int v : S.inds[s])
+            for (int64_t e = rowptr[v]; e < rowptr[v + 1]; ++e) {
+                const int c = colind[e];
+                if (c < 0 || c >= n) continue;
+                const int t = S.map[c];
+                if (t >= end) o.push_back(t);
+            }
+        std::sort(o.begin(), o.end());
+        o.erase(std::unique(o.begin(), o.end()), o.end());
+    }
+
+    // LocalSymmetricAnalysis
+    int my_off = 0;
+    std::vector<int> cs, ps, fs, own;
+    for (int s = 0; s < nn; ++s) {
+        S.my_off[s] = my_off;
+        const int l = S.children[2 * s], r = S.children[2 * s + 1];
+        if (l >= 0) {
+            S.on_left[l] = 1; S.on_left[r] = 0;
+            sorted_union(S.lower[l], S.lower[r], cs);
+            sorted_union(S.orig_lower[s], cs, ps);
+            own.resize(S.size[s]);
+            for (int i = 0; i < S.size[s]; ++i) own[i] = S.off[s] + i;
+            sorted_union(ps, own, fs);
+            relative_indices(S.orig_lower[s], fs, S.orig_rel[s]);
+            relative_indices(S.lower[l], fs, S.left_rel[s]);
+            relative_indices(S.lower[r], fs, S.right_rel[s]);
+            S.lower[s].assign(fs.begin() + S.size[s], fs.end());
+        } else {
+            S.lower[s] = S.orig_lower[s];
+            S.orig_rel[s].resize(S.orig_lower[s].size());
+            for (size_t i = 0; i < S.orig_rel[s].size(); ++i) S.orig_rel[s][i] = (int)i + S.size[s];
+        }
+        my_off += S.size[s];
+    }
+    S.finalize_views();
+    return CLIQ_OK;
+}
+
+void Symbolic::finalize_views() {
+    lower_ptr.assign(num_nodes + 1, 0);
+    orig_ptr.assign(num_nodes + 1, 0);
+    for (int s = 0; s < num_nodes; ++s) {
+        lower_ptr[s + 1] = lower_ptr[s] + (int64_t)lower[s].size();
+        orig_ptr[s + 1] = orig_ptr[s] + (int64_t)orig_lower[s].size();
+    }
+    lower_flat.resize(lower_ptr[num_nodes]);
+    orig_flat.resize(orig_ptr[num_nodes]);
+    for (int s = 0; s < num_nodes; ++s) {
+        std::copy(lower[s].begin(), lower[s].end(), lower_flat.begin() + lower_ptr[s]);
+        std::copy(orig_lower[s].begin(), orig_lower[s].end(), orig_flat.begin() + orig_ptr[s]);
+    }
+}
+
+}  // namespace cliqgpu

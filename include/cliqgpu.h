@@ -1,0 +1,197 @@
+/*
+ * cliqgpu.h -- C ABI of the B200 multifrontal LDL^T engine.
+ *
+ * Plain C types only: pointers, sizes and an opaque stream (a cudaStream_t
+ * passed as void*).  Every function returns an int status (CLIQ_OK == 0).
+ * Matrices are column-major; complex values are interleaved (re, im) pairs,
+ * i.e. the memory layout of std::complex / numpy complex arrays.
+ *
+ * Clique itself has no C ABI or plugin layer: its operator interface is the
+ * C++ template API in include/clique/.  Each entry point below names the
+ * reference function whose behaviour it replaces (paths are relative to the
+ * reference project root).  include/clique_b200/clique.hpp wraps these entry
+ * points back into that C++ API (cliq::LDL, cliq::Solve, ...), converting
+ * non-zero statuses into the reference's exception types.
+ */
+#ifndef CLIQGPU_H
+#define CLIQGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define CLIQ_OK              0
+#define CLIQ_ERR_ARG         1   /* invalid argument (maps to El::LogicError)      */
+#define CLIQ_ERR_OOM         2   /* device or host allocation failed               */
+#define CLIQ_ERR_ZERO_PIVOT  3   /* an exactly-zero D pivot was met                */
+#define CLIQ_ERR_CUDA        4   /* CUDA runtime error                             */
+#define CLIQ_ERR_TIMEOUT     5   /* a bounded device-side wait gave up             */
+#define CLIQ_ERR_STATE       6   /* call out of order (e.g. solve before factor)   */
+#define CLIQ_ERR_NOCONV      7   /* iterative refinement did not reach tolerance   */
+
+/* ---- scalar / precision tags -------------------------------------------- */
+#define CLIQ_REAL     0
+#define CLIQ_COMPLEX  1
+#define CLIQ_FP64     0
+#define CLIQ_FP32     1
+
+typedef struct cliq_symbolic_s* cliq_symbolic;   /* host symbolic analysis        */
+typedef struct cliqgpu_plan_s*  cliqgpu_plan;    /* device-resident front tree    */
+
+/* Plain-array view of cliq::DistSymmInfo (single process) plus the ordering.
+ * Reference: include/clique/symbolic/dist_symm_info.hpp:17-36 (SymmNodeInfo). */
+typedef struct {
+    int32_t        num_nodes;
+    const int32_t* size;            /* [num_nodes] pivots of each front (node.size)      */
+    const int32_t* off;             /* [num_nodes] first ND index of each node           */
+    const int32_t* parent;          /* [num_nodes] parent node, -1 for the root          */
+    const int32_t* children;        /* [2*num_nodes] left, right child or -1, -1          */
+    const int64_t* lower_ptr;       /* [num_nodes+1] CSR offsets into lower               */
+    const int32_t* lower;           /* analysed lowerStruct (sorted ND indices)           */
+    const int64_t* orig_lower_ptr;  /* [num_nodes+1] CSR offsets into orig_lower          */
+    const int32_t* orig_lower;      /* origLowerStruct (sorted ND indices)                */
+} cliq_symm_info;
+
+/* ======================= host symbolic phase ============================== */
+
+/* Natural nested dissection of an nx*ny*nz grid graph followed by the
+ * symbolic analysis.  The graph is the CSR pattern of A (both triangles,
+ * natural order x + y*nx + z*nx*ny).
+ * Replaces cliq::NaturalNestedDissection,
+ * include/clique/symbolic/natural_nested_dissection.hpp:17-26,447-488 (P=1). */
+int cliq_natural_nested_dissection(int32_t nx, int32_t ny, int32_t nz, int64_t n,
+                                   const int64_t* rowptr, const int32_t* colind,
+                                   int32_t cutoff, cliq_symbolic* out);
+
+/* Views into the analysis (pointers stay valid until cliq_symbolic_destroy).
+ * Replaces reading cliq::DistSymmInfo::localNodes,
+ * include/clique/symbolic/dist_symm_info.hpp:108-113. */
+int cliq_symbolic_info(cliq_symbolic symb, cliq_symm_info* out);
+
+/* Per-node scalars: out[0..9] = size, off, myOff, parent, leftChild,
+ * rightChild, onLeft, |lowerStruct|, |origLowerStruct|, separator-tree parent.
+ * Reference: SymmNodeInfo fields (dist_symm_info.hpp:17-36) and
+ * SepOrLeaf::parent (dist_separator_tree.hpp). */
+int cliq_symbolic_node(cliq_symbolic symb, int32_t s, int32_t out[10]);
+
+/* Per-node index arrays: which = 0 lowerStruct, 1 origLowerStruct,
+ * 2 origLowerRelInds, 3 leftRelInds, 4 rightRelInds, 5 separator/leaf
+ * natural indices (SepOrLeaf::inds).  *len receives the length; out may be
+ * NULL to query it.  Reference: dist_symm_info.hpp:30-35. */
+int cliq_symbolic_node_array(cliq_symbolic symb, int32_t s, int32_t which, int32_t* out, int64_t* len);
+
+/* The reordering (natural -> ND) and its inverse.  Either pointer may be NULL.
+ * Replaces cliq::BuildMap / DistMap::FormInverse at P=1,
+ * include/clique/symbolic/nested_dissection.hpp:1206-1363. */
+int cliq_symbolic_map(cliq_symbolic symb, int32_t* map, int32_t* inverse_map);
+
+void cliq_symbolic_destroy(cliq_symbolic symb);
+
+/* ======================= device numeric phase ============================= */
+
+typedef struct {
+    int32_t field;        /* CLIQ_REAL or CLIQ_COMPLEX                                  */
+    int32_t precision;    /* factor precision: CLIQ_FP64 (plain) or CLIQ_FP32 (mixed)   */
+    int32_t conjugate;    /* 1: Hermitian (LDL^H), 0: symmetric (LDL^T)                 */
+    int32_t block_size;   /* dense panel width nb, 0 = default                           */
+    int32_t keep_matrix;  /* 1: keep A in FP64 on the device for Multiply / refinement  */
+} cliqgpu_options;
+
+/* Build the device front tree: front sizes and relative indices from the
+ * analysis, the assembly map from A's pattern, and all HBM buffers (factor
+ * arena, update stacks, workspaces).  map is natural -> ND (length n).
+ * stream: cudaStream_t to run on, or NULL for a private stream.
+ * Replaces the structural part of cliq::DistSymmFrontTree<F>::DistSymmFrontTree
+ * / Initialize, include/clique/numeric/dist_symm_front_tree/impl.hpp:24-385,
+ * plus SymmetricAnalysis's relative indices (LocalSymmetricAnalysis.cpp:84-92). */
+int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* map,
+                        const int64_t* rowptr, const int32_t* colind,
+                        const cliqgpu_options* options, void* stream, cliqgpu_plan* out);
+
+/* Scatter the values of A (CSR order of the pattern given to plan_create)
+ * into the fronts.  values: FP64 (real or interleaved complex, as the plan's
+ * field), on the host (values_on_device = 0) or the device (= 1).
+ * Replaces the value part of DistSymmFrontTree<F>::Initialize,
+ * include/clique/numeric/dist_symm_front_tree/impl.hpp:244-297. */
+int cliqgpu_assemble(cliqgpu_plan plan, const void* values, int32_t values_on_device);
+
+/* Multifrontal LDL^T (or LDL^H) of the assembled fronts, in place.
+ * *zero_pivot receives -1, or the ND index of the first exactly-zero pivot
+ * (the factorization still completes; the status is then CLIQ_ERR_ZERO_PIVOT).
+ * Replaces cliq::LDL(info, L, LDL_1D/LDL_2D), include/clique/numeric/ldl.hpp:57-75
+ * (LocalLDL ldl/local.hpp:25-122, FrontLDL ldl/local_front.hpp:30-71). */
+int cliqgpu_factor(cliqgpu_plan plan, int64_t* zero_pivot);
+
+/* Solve A X = B in place using the stored factors: forward sweep, diagonal
+ * solve, backward sweep.  X is n x nrhs column-major with leading dimension
+ * ldx, FP64 (real or interleaved complex), on the host or the device.
+ * nodal = 0: X is in natural order (Pull, Solve, Push); nodal = 1: X is
+ * already in ND order (a DistNodalMultiVec).
+ * Replaces cliq::Solve(info, L, X), include/clique/numeric/solve.hpp:41-65, with
+ * DistNodalMultiVec::Pull/Push (dist_nodal_multi_vec/impl.hpp:67-219). */
+int cliqgpu_solve(cliqgpu_plan plan, void* X, int64_t ldx, int32_t nrhs,
+                  int32_t x_on_device, int32_t nodal);
+
+/* Y := alpha A X + beta Y with the FP64 copy of A (requires keep_matrix),
+ * natural order, X/Y n x nrhs with leading dimension ld, on the device.
+ * alpha, beta point to one FP64 scalar (real) or an interleaved pair (complex).
+ * Replaces cliq::Multiply, include/clique/numeric/multiply.hpp:18-21,28-166. */
+int cliqgpu_multiply(cliqgpu_plan plan, const double* alpha, const void* X, const double* beta,
+                     void* Y, int64_t ld, int32_t nrhs);
+
+/* Mixed-precision solve: X := A^{-1} B by iterative refinement with the
+ * stored factors (any precision), FP64 residuals r = B - A X and FP64
+ * updates, until max_j ||r_j|| / ||b_j|| <= tol or max_iter refinement steps.
+ * B, X: n x nrhs, natural order, leading dimension ld, host or device.
+ * *iters receives the refinement steps taken, *relres the final max relative
+ * residual.  Returns CLIQ_ERR_NOCONV if tol was not reached.
+ * No reference counterpart (Clique has no refinement); it composes cliq::Solve
+ * and cliq::Multiply as the examples' residual check does
+ * (examples/HelmholtzPML3D.cpp:354-365). */
+int cliqgpu_refine(cliqgpu_plan plan, const void* B, void* X, int64_t ld, int32_t nrhs,
+                   int32_t on_device, double tol, int32_t max_iter, int32_t* iters, double* relres);
+
+/* Copy front s back to the host: L (m x n, column-major, in the plan's
+ * storage precision widened to FP64) and D (n entries, FP64).
+ * Either pointer may be NULL.  dims[0..1] receives m, n.
+ * Replaces reading L.localFronts[s].frontL / .diag
+ * (dist_symm_front_tree/decl.hpp:174-184). */
+int cliqgpu_get_front(cliqgpu_plan plan, int32_t s, double* L, double* D, int32_t dims[2]);
+
+/* Scalar properties: key 0 factor flops (Clique's FactorizationWork formula),
+ * 1 solve flops per right-hand side (SolveWork), 2 factor entries (sum m*n),
+ * 3 device bytes held, 4 kernel launches issued by the last call,
+ * 5 number of fronts, 6 tree depth, 7 bytes of the factor arena.
+ * Reference for 0-2: dist_symm_front_tree/impl.hpp:401-640. */
+int cliqgpu_plan_query(cliqgpu_plan plan, int32_t key, double* value);
+
+/* Wait for all work queued on the plan's stream. */
+int cliqgpu_synchronize(cliqgpu_plan plan);
+
+void cliqgpu_plan_destroy(cliqgpu_plan plan);
+
+/* Human-readable text for a status code, and the last error detail. */
+const char* cliqgpu_status_string(int32_t status);
+const char* cliqgpu_last_error(void);
+
+/* ======================= single dense front =============================== */
+
+/* Dense partial LDL^T of one front, in place on device memory:
+ * AL (m x n, ld lda) receives unit-lower L with D on its diagonal ... as
+ * FrontLDL leaves it before LocalLDL stores D separately, and ABR
+ * ((m-n) x (m-n) lower, ld ldabr) receives ABR - L_B D L_B^T.
+ * field / precision as in cliqgpu_options; data in that precision.
+ * Workspace is allocated with cudaMalloc and freed before return.
+ * Replaces cliq::FrontLDL(AL, ABR, conjugate),
+ * include/clique/numeric/ldl/local_front.hpp:17-18,30-71. */
+int cliqgpu_front_ldl(int32_t field, int32_t precision, int32_t conjugate, int32_t m, int32_t n,
+                      void* AL, int64_t lda, void* ABR, int64_t ldabr, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLIQGPU_H */

@@ -1,0 +1,259 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle and
+the dense golden factors, on the same orderings.
+
+Tolerances: FP64 factor entries within 1e-12 of the dense LDL^T (relative to
+the largest entry); FP64 solutions within 1e-10 normwise relative error of
+the oracle's with relative residual <= 1e-12; the mixed form (FP32 fronts,
+FP64 refinement) reaches relative residual <= 1e-10.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import clique_b200 as cliq
+from clique_b200 import operators as ops
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def build(A, dims, cutoff, precision="double", conjugate=False):
+    map_, sep, info = cliq.NaturalNestedDissection(*dims, A, cutoff)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, conjugate, precision=precision)
+    cliq.LDL(info, L)
+    return map_, info, L
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def residual(A, X, B):
+    return np.linalg.norm(A.to_scipy() @ X - B) / np.linalg.norm(B)
+
+
+@pytest.mark.parametrize("fx", ["ldl_lap_3x3x1.npz", "ldl_helm_3x3x1.npz", "ldl_lap_6x5x4_c8.npz", "ldl_helm_6x5x4_c8.npz"])
+def test_fronts_match_dense_golden(fx):
+    z = np.load(os.path.join(GOLD, fx))
+    A = ops.CSR(len(z["map"]), z["rowptr"], z["colind"], z["values"])
+    dims = [int(t) for t in fx[:-4].split("_")[2].split("x")]
+    cutoff = 8 if "c8" in fx else 2
+    map_, info, L = build(A, dims, cutoff)
+    assert np.array_equal(map_.array, z["map"])
+    Ld, Dd = z["L"], z["D"]
+    scale = np.abs(Ld).max()
+    for s, nd in enumerate(info.localNodes):
+        Lf, d = L.front(s)
+        rows = np.concatenate([np.arange(nd.off, nd.off + nd.size), nd.lowerStruct]).astype(int)
+        np.testing.assert_allclose(Lf, Ld[np.ix_(rows, np.arange(nd.off, nd.off + nd.size))], atol=1e-12 * scale, rtol=0)
+        np.testing.assert_allclose(d, Dd[nd.off:nd.off + nd.size], rtol=1e-12)
+    x = cliq.Solve(info, L, np.asfortranarray(z["b"].reshape(-1, 1)))[:, 0]
+    assert rel(x, z["x"]) <= 1e-12
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_fronts_match_oracle(oracle, complex_):
+    dims, cutoff = (12, 10, 9), 30
+    if complex_:
+        A = ops.helmholtz_pml_3d(*dims, omega=20.0, velocity=ops.smooth_velocity(dims, 4), b=3)
+    else:
+        A = ops.laplacian_3d(*dims, 6.1)
+    map_, info, L = build(A, dims, cutoff)
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=complex_)
+    assert F.ldl(96) == 0
+    for s in range(S.num_nodes):
+        Lg, dg = L.front(s)
+        Lo, do = F.front(s)
+        assert Lg.shape == Lo.shape
+        assert rel(Lg, Lo) <= 1e-11, s
+        assert rel(dg, do) <= 1e-11, s
+
+
+def test_cfg1_plain_fp64_30cubed(oracle):
+    """The 30^3 7-point operator (diag 6.1, cutoff 128, 1 N(0,1) RHS): GPU vs oracle on the same ordering."""
+    n = 30
+    A = ops.laplacian_3d(n, n, n, 6.1)
+    b = ops.random_rhs(A.n, 1, seed=0)
+    map_, info, L = build(A, (n, n, n), 128)
+    x = cliq.Solve(info, L, b.copy(order="F"))
+    oracle.enable_blas(0)
+    try:
+        S = oracle.Symbolic(n, n, n, A.rowptr, A.colind, cutoff=128)
+        F = oracle.Fronts(S, A.values)
+        assert F.ldl(96) == 0
+        xo = F.solve(b.copy(order="F"))
+    finally:
+        oracle.disable_blas()
+    assert rel(x, xo) <= 1e-10
+    assert residual(A, x, b) <= 1e-12
+
+
+@pytest.mark.parametrize("nrhs", [1, 4, 20])
+def test_helmholtz_fp64_solve(oracle, nrhs):
+    n = 16
+    A, omega, c = ops.helmholtz_workload_3d(n, seed=3)
+    B = ops.random_rhs(A.n, nrhs, seed=1, complex_=True)
+    map_, info, L = build(A, (n, n, n), 64)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    S = oracle.Symbolic(n, n, n, A.rowptr, A.colind, cutoff=64)
+    F = oracle.Fronts(S, A.values, is_complex=True)
+    assert F.ldl(96) == 0
+    Xo = F.solve(B.copy(order="F"))
+    assert rel(X, Xo) <= 1e-10
+    assert residual(A, X, B) <= 1e-12
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_mixed_fp32_refinement(complex_):
+    n = 20
+    if complex_:
+        A, _, _ = ops.helmholtz_workload_3d(n, seed=5)
+    else:
+        A = ops.laplacian_3d(n, n, n, 6.1)
+    B = ops.random_rhs(A.n, 3, seed=2, complex_=complex_)
+    map_, info, L = build(A, (n, n, n), 64, precision="single")
+    X, iters, rr = cliq.RefinedSolve(L, B, tol=1e-10, max_iter=30)
+    assert rr <= 1e-10, (iters, rr)
+    assert residual(A, X, B) <= 1e-10
+    Xd = np.linalg.solve(A.to_scipy().toarray(), B) if A.n <= 9000 else None
+    if Xd is not None:
+        assert rel(X, Xd) <= 1e-8
+
+
+def _magnetic(dims, shift=6.5, theta=0.3):
+    A = ops.laplacian_3d(*dims, shift)
+    vals = A.values.astype(np.complex128)
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    off = A.colind != rows
+    vals[off] = vals[off] * np.exp(1j * theta * np.sign(A.colind - rows))[off]
+    return ops.CSR(A.n, A.rowptr, A.colind, vals)
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_hermitian_ldlh(oracle, precision):
+    dims = (11, 9, 8)
+    A = _magnetic(dims)
+    B = ops.random_rhs(A.n, 2, seed=9, complex_=True)
+    map_, info, L = build(A, dims, 40, precision=precision, conjugate=True)
+    if precision == "double":
+        X = cliq.Solve(info, L, B.copy(order="F"))
+        S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=40)
+        F = oracle.Fronts(S, A.values, is_complex=True, conjugate=True)
+        assert F.ldl(96) == 0
+        assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+        assert residual(A, X, B) <= 1e-12
+    else:
+        X, it, rr = cliq.RefinedSolve(L, B, 1e-11, 20)
+        assert rr <= 1e-11
+
+
+def test_nodal_solve_equals_natural():
+    n = 14
+    A = ops.laplacian_3d(n, n, n, 6.1)
+    B = ops.random_rhs(A.n, 2, seed=3)
+    map_, info, L = build(A, (n, n, n), 50)
+    inv = map_.FormInverse()
+    Xn = cliq.DistNodalMultiVec(inv, info, B)
+    cliq.Solve(info, L, Xn)
+    X1 = np.zeros_like(B, order="F")
+    Xn.Push(inv, info, X1)
+    X2 = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(X1, X2) <= 1e-14
+    assert sum(x.shape[0] for x in Xn.localNodes) == A.n
+
+
+@pytest.mark.parametrize("dims,cutoff", [((1, 1, 1), 1), ((5, 1, 1), 1), ((2, 2, 2), 100), ((17, 3, 1), 4),
+                                         ((7, 5, 3), 6), ((65, 2, 1), 16), ((3, 70, 1), 100)])
+def test_edge_grids(oracle, dims, cutoff):
+    A = ops.laplacian_3d(*dims, 6.1)
+    B = ops.random_rhs(A.n, 2, seed=4)
+    map_, info, L = build(A, dims, cutoff)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values)
+    F.ldl(96)
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-12
+
+
+def test_zero_pivot_is_reported():
+    A = ops.laplacian_3d(3, 1, 1, 6.1)
+    vals = A.values.copy()
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    vals[(rows == 0) & (A.colind == 0)] = 0.0
+    A0 = ops.CSR(A.n, A.rowptr, A.colind, vals)
+    map_, sep, info = cliq.NaturalNestedDissection(3, 1, 1, A0, 1)
+    L = cliq.DistSymmFrontTree(A0, map_, sep, info)
+    with pytest.raises(cliq.CliqueError) as e:
+        cliq.LDL(info, L)
+    assert e.value.status == 3
+    assert L.zero_pivot == 0
+
+
+def test_ldl_twice_is_a_logic_error():
+    A = ops.laplacian_3d(4, 4, 4, 6.1)
+    map_, info, L = build(A, (4, 4, 4), 8)
+    with pytest.raises(cliq.LogicError):
+        cliq.LDL(info, L)
+
+
+def test_refactor_with_new_values_reuses_plan(oracle):
+    """tests/Refactor.cpp pattern: reassemble new values into the same front tree and factor again."""
+    n = 12
+    A = ops.laplacian_3d(n, n, n, 6.1)
+    map_, info, L = build(A, (n, n, n), 32)
+    A2 = ops.laplacian_3d(n, n, n, 7.3)
+    L.Initialize(A2.values)
+    cliq.LDL(info, L)
+    B = ops.random_rhs(A.n, 1, seed=8)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    assert residual(A2, X, B) <= 1e-12
+
+
+def test_device_resident_inputs():
+    import torch
+    n = 16
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=1)
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, 64)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
+    L.Initialize(torch.from_numpy(A.values).cuda())
+    cliq.LDL(info, L)
+    B = ops.random_rhs(A.n, 2, seed=3, complex_=True)
+    Bt = torch.from_numpy(B).cuda().t().contiguous().t()
+    X, it, rr = cliq.RefinedSolve(L, Bt, 1e-10, 30)
+    assert rr <= 1e-10
+    Xh = X.cpu().numpy()
+    assert residual(A, Xh, B) <= 1e-10
+    Y = torch.zeros_like(Bt)
+    cliq.Multiply(1.0, L, X, 0.0, Y)
+    assert rel(Y.cpu().numpy(), B) <= 1e-10
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_single_front_ldl(oracle, complex_, precision):
+    """cliqgpu_front_ldl (FrontLDL on one dense front) against the oracle's FrontLDL."""
+    import ctypes as C
+    import torch
+    from clique_b200 import _capi
+    m, n = 300, 150
+    rng = np.random.default_rng(7)
+    G = rng.standard_normal((m, m)) + (1j * rng.standard_normal((m, m)) if complex_ else 0)
+    S = G @ G.T / m + 8 * np.eye(m)      # symmetric (complex-symmetric when complex)
+    AL = np.asfortranarray(np.tril(S)[:, :n])
+    ABR = np.asfortranarray(np.tril(S[n:, n:]))
+    ALo, ABRo = AL.copy(order="F"), ABR.copy(order="F")
+    assert oracle.front_ldl(ALo, ABRo, nb=96) == 0
+    tdt = {("double", False): torch.float64, ("double", True): torch.complex128,
+           ("single", False): torch.float32, ("single", True): torch.complex64}[(precision, complex_)]
+    tAL = torch.from_numpy(AL).to(tdt).cuda().t().contiguous().t()
+    tABR = torch.from_numpy(ABR).to(tdt).cuda().t().contiguous().t()
+    st = _capi.load().cliqgpu_front_ldl(int(complex_), 0 if precision == "double" else 1, 0, m, n,
+                                        C.c_void_p(tAL.data_ptr()), m, C.c_void_p(tABR.data_ptr()), m - n, None)
+    assert st == 0
+    torch.cuda.synchronize()
+    tol = 1e-12 if precision == "double" else 1e-4
+    assert rel(tAL.cpu().numpy().astype(ALo.dtype), ALo) <= tol
+    g = np.tril(tABR.cpu().numpy().astype(ABRo.dtype))
+    assert rel(g, np.tril(ABRo)) <= tol
