@@ -92,7 +92,8 @@ void free_plan(Plan& P) {
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                       const int32_t* colind) {
     const int nn = info->num_nodes;
-    if (nn <= 0 || !info->size || !info->off || !info->parent || !info->children || !info->lower_ptr || !info->lower) {
+    if (nn <= 0 || !info->size || !info->off || !info->parent || !info->children || !info->lower_ptr ||
+        (!info->lower && info->lower_ptr[nn] > 0)) {
         set_last_error("plan_create: incomplete symbolic info");
         return CLIQ_ERR_ARG;
     }
@@ -157,7 +158,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
 
     // ---- children maps (inverse relative indices) ----
     std::vector<int32_t> cmaps;
-    const int32_t* low = info->lower;
+    static const int32_t kNoLower = 0;
+    const int32_t* low = info->lower ? info->lower : &kNoLower;
     for (int s = 0; s < nn; ++s) {
         const int l = info->children[2 * s], r = info->children[2 * s + 1];
         if (l < 0 && r < 0) continue;
