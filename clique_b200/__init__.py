@@ -254,6 +254,20 @@ class DistSymmFrontTree:
     def last_launches(self):
         return int(self.query(4))
 
+    def total_launches(self):
+        return int(self.query(8))
+
+    def set_profiling(self, on=True):
+        check(_capi.load().cliqgpu_set_profiling(self._h, int(bool(on))))
+
+    PROFILE_KEYS = ["extend_add_ms", "diag_ms", "panel_ms", "trail_ms", "schur_ms", "trail_flops", "schur_flops",
+                    "extend_add_bytes", "trail_launches", "schur_launches", "factor_ms"]
+
+    def profile(self):
+        out = np.zeros(16)
+        check(_capi.load().cliqgpu_profile_read(self._h, out.ctypes.data_as(C.c_void_p), 16))
+        return dict(zip(self.PROFILE_KEYS, out.tolist()))
+
     def front(self, s):
         """Host copies of (frontL, diag) of node s, widened to FP64."""
         lib = _capi.load()

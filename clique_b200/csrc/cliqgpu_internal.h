@@ -72,6 +72,15 @@ struct Launch {
     int64_t nblocks;      // grid size
     int32_t k;            // DIAG / PANEL: column offset of the step
     int32_t depth;
+    double work;          // GEMM: algorithmic flops; EXTEND_ADD: algorithmic bytes
+    int32_t schur;        // GEMM: 1 for the Schur-complement update, 0 for an in-panel update
+};
+
+// per-kernel-kind device time of the last profiled factorization (ms) and work
+enum ProfSlot {
+    PROF_EA_MS = 0, PROF_DIAG_MS, PROF_PANEL_MS, PROF_TRAIL_MS, PROF_SCHUR_MS,
+    PROF_TRAIL_FLOPS, PROF_SCHUR_FLOPS, PROF_EA_BYTES, PROF_TRAIL_LAUNCHES, PROF_SCHUR_LAUNCHES,
+    PROF_FACTOR_MS, PROF_SLOTS = 16
 };
 
 struct SolveLevel {
@@ -140,6 +149,18 @@ struct Plan {
     int32_t epoch = 0;
     bool assembled = false, factored = false;
     int64_t last_launches = 0;
+    int64_t total_launches = 0;   // every kernel this plan has launched
+    // FP32 updates on the tensor cores (tcgen05 3xTF32); CLIQGPU_TENSOR_CORES=0 selects the CUDA-core kernel
+    int use_tc = 1;
+    bool tensor_path() const { return use_tc && precision == CLIQ_FP32; }
+    int gemm_tile() const { return tensor_path() ? 128 : kTile; }
+    // width of the outer column block whose trailing update is deferred (multiple of nb)
+    int outer_nb = 256;
+    // optional per-launch CUDA-event timing of the factorization
+    int profile = 0;
+    bool prof_pending = false;
+    std::vector<cudaEvent_t> events;
+    double prof[PROF_SLOTS] = {0};
 
     // host-side staging for host-resident inputs/outputs
     std::vector<int32_t> hitems;
@@ -160,6 +181,8 @@ int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
 
 int check_cuda(const char* where);
+int launch_tc_update(Plan& P, const Launch& ln);
+size_t tc_update_smem(bool cplx);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);
 void free_plan(Plan& P);

@@ -22,6 +22,7 @@
 // D is kept in FP64 for every storage precision.
 #include <climits>
 #include <cstdio>
+#include <type_traits>
 
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
@@ -220,9 +221,10 @@ __global__ void __launch_bounds__(kThreads) gemm_update_kernel(const GemmProb* _
     }
     const GemmProb pr = probs[lo];
     int64_t t = bid - prefix[lo];
-    const int Mt = (pr.M + BM - 1) / BM;
+    const int Mt = (pr.M + BM - 1) / BM, Nt = (pr.N + BM - 1) / BM;
     int tj = 0;
-    while (t >= Mt - tj) { t -= Mt - tj; ++tj; }
+    while (tj < Nt && t >= Mt - tj) { t -= Mt - tj; ++tj; }
+    if (tj >= Nt) return;   // cannot happen with a consistent schedule
     const int ti = tj + (int)t;
     const int i0 = ti * BM, j0 = tj * BM;
     T* Cbase = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
@@ -299,8 +301,15 @@ static int run_factor_impl(Plan& P) {
     T* p1 = reinterpret_cast<T*>(P.pool[1]);
     const int4* items = reinterpret_cast<const int4*>(P.items);
     int64_t launches = 0;
-    for (const Launch& ln : P.launches) {
+    if (P.profile && P.events.size() < 2 * P.launches.size()) {
+        const size_t old = P.events.size();
+        P.events.resize(2 * P.launches.size());
+        for (size_t i = old; i < P.events.size(); ++i) cudaEventCreate(&P.events[i]);
+    }
+    for (size_t li = 0; li < P.launches.size(); ++li) {
+        const Launch& ln = P.launches[li];
         if (ln.nblocks <= 0) continue;
+        if (P.profile) cudaEventRecord(P.events[2 * li], P.stream);
         switch (ln.kind) {
             case Launch::EXTEND_ADD:
                 extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
@@ -314,13 +323,19 @@ static int run_factor_impl(Plan& P) {
                     P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv));
                 break;
             case Launch::GEMM:
-                gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(
-                    P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
+                if (std::is_same<T, float>::value && P.use_tc)
+                    launch_tc_update(P, ln);
+                else
+                    gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(
+                        P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
                 break;
         }
+        if (P.profile) cudaEventRecord(P.events[2 * li + 1], P.stream);
         ++launches;
     }
+    P.prof_pending = P.profile != 0;
     P.last_launches = launches;
+    P.total_launches += launches;
     return check_cuda("factor launch");
 }
 

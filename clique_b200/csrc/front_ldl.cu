@@ -4,6 +4,7 @@
 // factorization by describing the front as a one-node tree.
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <vector>
 
 #include "cliqgpu_internal.h"
@@ -33,6 +34,7 @@ extern "C" int cliqgpu_front_ldl(int32_t field, int32_t precision, int32_t conju
     P.precision = precision == CLIQ_FP32 ? CLIQ_FP32 : CLIQ_FP64;
     P.conjugate = conjugate ? 1 : 0;
     P.nb = kTile;
+    if (const char* e = getenv("CLIQGPU_TENSOR_CORES")) P.use_tc = atoi(e) != 0;
     P.stream = (cudaStream_t)stream;
     // one node: pivots 0..n-1, update rows n..m-1
     std::vector<int32_t> size{n}, off{0}, parent{-1}, children{-1, -1}, lower(m - n), map(n);
@@ -55,7 +57,7 @@ extern "C" int cliqgpu_front_ldl(int32_t field, int32_t precision, int32_t conju
     if (m > n)
         cudaMemcpy2DAsync((char*)P.pool[f.pool] + (size_t)f.U * eb, (size_t)(m - n) * eb, ABR, (size_t)ldabr * eb,
                           (size_t)(m - n) * eb, m - n, cudaMemcpyDeviceToDevice, P.stream);
-    int32_t st0[2] = {INT_MAX, 0};
+    int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
     if (P.precision == CLIQ_FP64) st = P.cplx() ? run_factor<double, true>(P) : run_factor<double, false>(P);
     else st = P.cplx() ? run_factor<float, true>(P) : run_factor<float, false>(P);

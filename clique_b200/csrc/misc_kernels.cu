@@ -34,6 +34,7 @@ static int assemble_t(Plan& P, const double* dvals) {
         assemble_kernel<T, C, true><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, dvals, P.nnz, reinterpret_cast<T*>(P.L));
     else
         assemble_kernel<T, C, false><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, dvals, P.nnz, reinterpret_cast<T*>(P.L));
+    P.total_launches += 1;
     return check_cuda("assemble");
 }
 
@@ -81,6 +82,7 @@ int launch_pull(Plan& P, const int32_t* perm, const double* X, int64_t ldx, int 
         if (P.cplx()) pull_kernel<float, true><<<g, 256, 0, P.stream>>>(X, ldx, P.n, nrhs, perm, (float*)xn, scale);
         else pull_kernel<float, false><<<g, 256, 0, P.stream>>>(X, ldx, P.n, nrhs, perm, (float*)xn, scale);
     }
+    P.total_launches += 1;
     return check_cuda("pull");
 }
 
@@ -93,6 +95,7 @@ int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t
         if (P.cplx()) push_kernel<float, true><<<g, 256, 0, P.stream>>>((const float*)xn, X, ldx, P.n, nrhs, perm, scale, accumulate);
         else push_kernel<float, false><<<g, 256, 0, P.stream>>>((const float*)xn, X, ldx, P.n, nrhs, perm, scale, accumulate);
     }
+    P.total_launches += 1;
     return check_cuda("push");
 }
 
@@ -122,6 +125,7 @@ int launch_spmv(Plan& P, double ar, double ai, const double* X, double br, doubl
         spmv_kernel<true><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.aval, P.n, cx<double>{ar, ai}, X, cx<double>{br, bi}, Y, ld, nrhs);
     else
         spmv_kernel<false><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.aval, P.n, ar, X, br, Y, ld, nrhs);
+    P.total_launches += 1;
     return check_cuda("multiply");
 }
 
@@ -147,6 +151,7 @@ __global__ void col_norms_kernel(const double* __restrict__ X, int64_t ld, int64
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out) {
     if (P.cplx()) col_norms_kernel<true><<<nrhs, 1024, 0, P.stream>>>(X, ld, P.n, out);
     else col_norms_kernel<false><<<nrhs, 1024, 0, P.stream>>>(X, ld, P.n, out);
+    P.total_launches += 1;
     return check_cuda("norms");
 }
 

@@ -16,6 +16,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -79,6 +80,8 @@ void free_plan(Plan& P) {
                     P.wpool[1], P.xnodal, P.xwork, P.norms};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (cudaEvent_t e : P.events) cudaEventDestroy(e);
+    P.events.clear();
     if (P.own_stream && P.stream) cudaStreamDestroy(P.stream);
 }
 
@@ -197,14 +200,21 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     auto push_item = [&](int a, int b, int c, int d) { items.push_back(a); items.push_back(b); items.push_back(c); items.push_back(d); };
     P.launches.clear();
     int64_t max_slots = 1;
-    auto tiles_of = [](int M, int N) -> int64_t {
-        const int64_t Mt = (M + kTile - 1) / kTile, Nt = (N + kTile - 1) / kTile;
+    // square update tiles: 128 on the tensor-core path, 64 on the CUDA-core path
+    const int gtile = P.gemm_tile();
+    auto tiles_of = [gtile](int M, int N) -> int64_t {
+        const int64_t Mt = (M + gtile - 1) / gtile, Nt = (N + gtile - 1) / gtile;
         return Nt * Mt - Nt * (Nt - 1) / 2;
     };
-    auto add_gemm = [&](std::vector<GemmProb>& lst, int depth) {
+    auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur) {
         if (lst.empty()) return;
         Launch ln{};
         ln.kind = Launch::GEMM;
+        ln.schur = schur;
+        for (auto& pr : lst) {
+            const double M = pr.M, N = pr.N;
+            ln.work += (N * M - N * (N - 1) / 2) * pr.K * (P.cplx() ? 8.0 : 2.0);
+        }
         ln.items = (int64_t)probs.size();
         ln.nitems = (int32_t)lst.size();
         ln.prefix = (int64_t)prefix.size();
@@ -232,57 +242,94 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             ln.nitems = (int32_t)(items.size() / 4 - ln.items);
             ln.nblocks = ln.nitems;
             ln.depth = d;
+            for (int s : lv) {
+                const FrontDev& f = P.hfronts[s];
+                const double m = f.m, nn2 = f.n, u = f.u, eb = P.elem_bytes();
+                double b = u * (u + 1) / 2 * eb;                                  // ABR written
+                if (f.cmap >= 0) {
+                    b += 2 * (m * nn2 - nn2 * (nn2 - 1) / 2) * eb;                // frontL read + written
+                    for (int c = 0; c < 2; ++c) b += (double)f.cu[c] * (f.cu[c] + 1) / 2 * eb;   // children read
+                }
+                ln.work += b;
+            }
             if (ln.nitems) P.launches.push_back(ln);
         }
         int maxn = 0;
         for (int s : lv) maxn = std::max(maxn, P.hfronts[s].n);
-        for (int k = 0; k < maxn; k += nb) {
-            Launch dg{};
-            dg.kind = Launch::DIAG;
-            dg.k = k;
-            dg.depth = d;
-            dg.items = (int64_t)items.size() / 4;
-            std::vector<std::pair<int, int>> active;
-            for (int s : lv)
-                if (P.hfronts[s].n > k) {
-                    push_item(s, (int)active.size(), 0, 0);
-                    active.push_back({s, (int)active.size()});
+        // Two-level blocking: inside an outer block of width nbo the nb-wide
+        // steps update only the outer block's own columns (all rows below);
+        // the columns right of the block receive the whole block's update
+        // at once (K = nbo), which the reference spreads over nbo/nb Gemm
+        // calls (ldl/local_front.hpp:67).
+        const int nbo = std::max(nb, P.outer_nb / nb * nb);
+        for (int K0 = 0; K0 < maxn; K0 += nbo) {
+            for (int k = K0; k < std::min(K0 + nbo, maxn); k += nb) {
+                Launch dg{};
+                dg.kind = Launch::DIAG;
+                dg.k = k;
+                dg.depth = d;
+                dg.items = (int64_t)items.size() / 4;
+                std::vector<std::pair<int, int>> active;
+                for (int s : lv)
+                    if (P.hfronts[s].n > k) {
+                        push_item(s, (int)active.size(), 0, 0);
+                        active.push_back({s, (int)active.size()});
+                    }
+                dg.nitems = (int32_t)active.size();
+                dg.nblocks = dg.nitems;
+                max_slots = std::max<int64_t>(max_slots, dg.nitems);
+                P.launches.push_back(dg);
+                Launch pn{};
+                pn.kind = Launch::PANEL;
+                pn.k = k;
+                pn.depth = d;
+                pn.items = (int64_t)items.size() / 4;
+                std::vector<GemmProb> trail;
+                for (auto& a : active) {
+                    const FrontDev& f = P.hfronts[a.first];
+                    const int kb = std::min(nb, f.n - k);
+                    const int rows = f.m - k - kb;
+                    for (int rb = 0; rb * kTile < rows; ++rb) push_item(a.first, a.second, rb, 0);
+                    const int N = std::min(K0 + nbo, f.n) - k - kb;
+                    if (N > 0) {
+                        GemmProb pr{};
+                        pr.A = f.L + (k + kb) + (int64_t)k * f.m;
+                        pr.B = pr.A;
+                        pr.C = f.L + (k + kb) + (int64_t)(k + kb) * f.m;
+                        pr.d = f.off + k;
+                        pr.lda = f.m;
+                        pr.ldc = f.m;
+                        pr.M = rows;
+                        pr.N = N;
+                        pr.K = kb;
+                        pr.cpool = -1;
+                        trail.push_back(pr);
+                    }
                 }
-            dg.nitems = (int32_t)active.size();
-            dg.nblocks = dg.nitems;
-            max_slots = std::max<int64_t>(max_slots, dg.nitems);
-            P.launches.push_back(dg);
-            Launch pn{};
-            pn.kind = Launch::PANEL;
-            pn.k = k;
-            pn.depth = d;
-            pn.items = (int64_t)items.size() / 4;
-            std::vector<GemmProb> trail;
-            for (auto& a : active) {
-                const FrontDev& f = P.hfronts[a.first];
-                const int kb = std::min(nb, f.n - k);
-                const int rows = f.m - k - kb;
-                for (int rb = 0; rb * kTile < rows; ++rb) push_item(a.first, a.second, rb, 0);
-                const int N = f.n - k - kb;
-                if (N > 0) {
-                    GemmProb pr{};
-                    pr.A = f.L + (k + kb) + (int64_t)k * f.m;
-                    pr.B = pr.A;
-                    pr.C = f.L + (k + kb) + (int64_t)(k + kb) * f.m;
-                    pr.d = f.off + k;
-                    pr.lda = f.m;
-                    pr.ldc = f.m;
-                    pr.M = rows;
-                    pr.N = N;
-                    pr.K = kb;
-                    pr.cpool = -1;
-                    trail.push_back(pr);
-                }
+                pn.nitems = (int32_t)(items.size() / 4 - pn.items);
+                pn.nblocks = pn.nitems;
+                if (pn.nitems) P.launches.push_back(pn);
+                add_gemm(trail, d, 0);
             }
-            pn.nitems = (int32_t)(items.size() / 4 - pn.items);
-            pn.nblocks = pn.nitems;
-            if (pn.nitems) P.launches.push_back(pn);
-            add_gemm(trail, d);
+            std::vector<GemmProb> outer;
+            for (int s : lv) {
+                const FrontDev& f = P.hfronts[s];
+                const int c1 = K0 + nbo;
+                if (f.n <= c1) continue;
+                GemmProb pr{};
+                pr.A = f.L + c1 + (int64_t)K0 * f.m;
+                pr.B = pr.A;
+                pr.C = f.L + c1 + (int64_t)c1 * f.m;
+                pr.d = f.off + K0;
+                pr.lda = f.m;
+                pr.ldc = f.m;
+                pr.M = f.m - c1;
+                pr.N = f.n - c1;
+                pr.K = nbo;
+                pr.cpool = -1;
+                outer.push_back(pr);
+            }
+            add_gemm(outer, d, 0);
         }
         std::vector<GemmProb> schur;
         for (int s : lv) {
@@ -301,7 +348,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             pr.cpool = f.pool;
             schur.push_back(pr);
         }
-        add_gemm(schur, d);
+        add_gemm(schur, d, 1);
     }
     P.tinv_slots = max_slots;
 
@@ -422,11 +469,16 @@ static int solve_nodal_dispatch(Plan& P, void* xn, int nrhs) {
 }
 
 int read_status(Plan& P, int64_t* zero_pivot) {
-    int32_t st[2];
+    int32_t st[4];
     if (cudaMemcpyAsync(st, P.status, sizeof(st), cudaMemcpyDeviceToHost, P.stream) != cudaSuccess) return check_cuda("status");
     if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("sync");
     if (zero_pivot) *zero_pivot = st[0] == INT_MAX ? -1 : (int64_t)st[0] - 1;
-    if (st[1]) { set_last_error("a device-side wait timed out"); return CLIQ_ERR_TIMEOUT; }
+    if (st[1]) {
+        static const char* sites[] = {"?", "update: stage full", "update: stage empty", "update: accumulator", "solve: block flag",
+                                      "update: tile outside the schedule"};
+        set_last_error(std::string("a device-side wait timed out at ") + sites[(st[2] >= 0 && st[2] <= 5) ? st[2] : 0]);
+        return CLIQ_ERR_TIMEOUT;
+    }
     return st[0] == INT_MAX ? CLIQ_OK : CLIQ_ERR_ZERO_PIVOT;
 }
 
@@ -458,6 +510,8 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
     }
     P.nb = kTile;
+    if (const char* e = getenv("CLIQGPU_TENSOR_CORES")) P.use_tc = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_OUTER_BLOCK")) P.outer_nb = std::max(kTile, atoi(e));
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
@@ -505,7 +559,7 @@ int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
     Plan& P = h->p;
     if (!P.assembled) { set_last_error("factor: fronts were not assembled"); return CLIQ_ERR_STATE; }
     if (P.factored) { set_last_error("Matrix is already factored"); return CLIQ_ERR_STATE; }
-    int32_t st0[2] = {INT_MAX, 0};
+    int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
     int st;
     if (P.precision == CLIQ_FP64) st = P.cplx() ? run_factor<double, true>(P) : run_factor<double, false>(P);
@@ -535,7 +589,7 @@ int cliqgpu_solve(cliqgpu_plan h, void* X, int64_t ldx, int32_t nrhs, int32_t x_
         xd = stage;
         ldx = P.n;
     }
-    int32_t st0[2] = {INT_MAX, 0};
+    int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
     const int32_t* perm = nodal ? nullptr : P.perm;   // nodal: X is already in ND order
     TRY(launch_pull(P, perm, xd, ldx, nrhs, P.xnodal, 1.0));
@@ -587,7 +641,7 @@ int cliqgpu_refine(cliqgpu_plan h, const void* B, void* X, int64_t ld, int32_t n
     TRY(launch_col_norms(P, b, n, nrhs, P.norms + nrhs));
     int it = 0;
     double rel = 0;
-    int32_t st0[2] = {INT_MAX, 0};
+    int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
     for (;;) {
         TRY(launch_col_norms(P, r, n, nrhs, P.norms));
@@ -662,8 +716,51 @@ int cliqgpu_plan_query(cliqgpu_plan h, int32_t key, double* value) {
         case 5: *value = P.num_fronts; break;
         case 6: *value = P.max_depth; break;
         case 7: *value = (double)P.arena_elems * P.elem_bytes(); break;
+        case 8: *value = (double)P.total_launches; break;
         default: return CLIQ_ERR_ARG;
     }
+    return CLIQ_OK;
+}
+
+int cliqgpu_set_profiling(cliqgpu_plan h, int32_t enable) {
+    if (!h) return CLIQ_ERR_ARG;
+    h->p.profile = enable ? 1 : 0;
+    return CLIQ_OK;
+}
+
+int cliqgpu_profile_read(cliqgpu_plan h, double* out, int32_t nout) {
+    if (!h || !out || nout <= 0) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (P.prof_pending) {
+        if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("profile sync");
+        for (double& v : P.prof) v = 0;
+        int first = -1, last = -1;
+        for (size_t li = 0; li < P.launches.size(); ++li) {
+            const Launch& ln = P.launches[li];
+            if (ln.nblocks <= 0) continue;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, P.events[2 * li], P.events[2 * li + 1]);
+            if (first < 0) first = (int)li;
+            last = (int)li;
+            switch (ln.kind) {
+                case Launch::EXTEND_ADD: P.prof[PROF_EA_MS] += ms; P.prof[PROF_EA_BYTES] += ln.work; break;
+                case Launch::DIAG: P.prof[PROF_DIAG_MS] += ms; break;
+                case Launch::PANEL: P.prof[PROF_PANEL_MS] += ms; break;
+                case Launch::GEMM:
+                    if (ln.schur) { P.prof[PROF_SCHUR_MS] += ms; P.prof[PROF_SCHUR_FLOPS] += ln.work; P.prof[PROF_SCHUR_LAUNCHES] += 1; }
+                    else { P.prof[PROF_TRAIL_MS] += ms; P.prof[PROF_TRAIL_FLOPS] += ln.work; P.prof[PROF_TRAIL_LAUNCHES] += 1; }
+                    break;
+            }
+        }
+        if (first >= 0) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, P.events[2 * first], P.events[2 * last + 1]);
+            P.prof[PROF_FACTOR_MS] = ms;
+        }
+        cudaGetLastError();
+        P.prof_pending = false;
+    }
+    for (int i = 0; i < nout && i < PROF_SLOTS; ++i) out[i] = P.prof[i];
     return CLIQ_OK;
 }
 

@@ -28,7 +28,7 @@ namespace cliqgpu {
 
 constexpr int kSolveThreads = 256;
 constexpr int kMaxRhsChunk = 16;     // right-hand sides per sweep
-constexpr long long kSpinLimit = 1LL << 22;   // ~0.5-2 s with backoff
+constexpr uint64_t kSpinNs = 500000000ull;   // 0.5 s bound on any single wait
 
 __device__ __forceinline__ int ld_acquire(const int32_t* p) {
     int v;
@@ -36,15 +36,24 @@ __device__ __forceinline__ int ld_acquire(const int32_t* p) {
     return v;
 }
 
-// thread 0 waits for flag == epoch; returns false (and records a timeout) on expiry
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// thread 0 waits for flag == epoch; returns false (and records a timeout,
+// wait site 4) once the wall-clock bound expires
 __device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_t* status) {
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
-        long long it = 0;
         int ok = 1;
-        while (ld_acquire(flag) != epoch) {
-            if (++it > kSpinLimit) { atomicExch(&status[1], 1); ok = 0; break; }
-            __nanosleep(128);
+        if (ld_acquire(flag) != epoch) {
+            const uint64_t t0 = global_ns();
+            while (ld_acquire(flag) != epoch) {
+                if (global_ns() - t0 > kSpinNs) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 4); ok = 0; break; }
+                __nanosleep(64);
+            }
         }
         s_ok = ok;
     }
@@ -107,6 +116,7 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_chain_kernel(const FrontDev
     __shared__ int s_item;
     if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
     __syncthreads();
+    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
     const int4 it = items[s_item];
     const FrontDev f = F[it.x];
     const int rb = it.y;
@@ -231,6 +241,7 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev
     __shared__ int s_item;
     if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
     __syncthreads();
+    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
     const int4 it = items[s_item];
     const FrontDev f = F[it.x];
     const int rb = it.y;
@@ -368,6 +379,7 @@ static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
         }
     }
     P.last_launches += launches;
+    P.total_launches += launches;
     return check_cuda("solve launch");
 }
 

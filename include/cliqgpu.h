@@ -164,9 +164,22 @@ int cliqgpu_get_front(cliqgpu_plan plan, int32_t s, double* L, double* D, int32_
 /* Scalar properties: key 0 factor flops (Clique's FactorizationWork formula),
  * 1 solve flops per right-hand side (SolveWork), 2 factor entries (sum m*n),
  * 3 device bytes held, 4 kernel launches issued by the last call,
- * 5 number of fronts, 6 tree depth, 7 bytes of the factor arena.
+ * 5 number of fronts, 6 tree depth, 7 bytes of the factor arena,
+ * 8 kernels launched by this plan since creation (all calls).
  * Reference for 0-2: dist_symm_front_tree/impl.hpp:401-640. */
 int cliqgpu_plan_query(cliqgpu_plan plan, int32_t key, double* value);
+
+/* Per-kernel timing of the factorization with CUDA events recorded around
+ * every launch of cliqgpu_factor on the plan's stream (enable = 1 / 0).
+ * cliqgpu_profile_read waits for the stream and fills out[0..nout-1]:
+ * 0 extend-add ms, 1 diagonal-block ms, 2 panel ms, 3 in-panel update ms,
+ * 4 Schur update ms, 5 in-panel update flops, 6 Schur update flops (Clique's
+ * counting: 2 per real multiply-add, x4 complex), 7 extend-add bytes moved,
+ * 8 in-panel update launches, 9 Schur launches, 10 factor ms (first to last
+ * launch).  No reference counterpart: the reference times phases with
+ * mpi::Time (tests/Solve.cpp:224-251). */
+int cliqgpu_set_profiling(cliqgpu_plan plan, int32_t enable);
+int cliqgpu_profile_read(cliqgpu_plan plan, double* out, int32_t nout);
 
 /* Wait for all work queued on the plan's stream. */
 int cliqgpu_synchronize(cliqgpu_plan plan);

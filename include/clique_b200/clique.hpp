@@ -1,0 +1,366 @@
+// clique.hpp -- single-process drop-in for Clique's numeric API on one B200.
+//
+// Header-only C++ layer over the C ABI in cliqgpu.h.  The class and function
+// names, argument order and error behaviour follow the reference:
+//   DistSparseMatrix        include/clique/core/dist_sparse_matrix/decl.hpp:32-100
+//   DistMultiVec            include/clique/core/dist_multi_vec/decl.hpp:20-64
+//   DistMap                 include/clique/core/dist_map/decl.hpp:21-82
+//   NaturalNestedDissection include/clique/symbolic/natural_nested_dissection.hpp:17-26
+//   DistSymmFrontTree       include/clique/numeric/dist_symm_front_tree/decl.hpp:206-249
+//   LDL                     include/clique/numeric/ldl.hpp:23-26
+//   DistNodalMultiVec       include/clique/numeric/dist_nodal_multi_vec/decl.hpp:20-51
+//   Solve                   include/clique/numeric/solve.hpp:17-20
+//   Multiply                include/clique/numeric/multiply.hpp:18-21
+// A program written against those headers for a single process compiles
+// against this one after replacing `#include "clique.hpp"`.  Errors from the
+// device are raised as LogicError / RuntimeError (std::logic_error /
+// std::runtime_error), as El::LogicError / El::RuntimeError do.
+//
+// Scalar types: double and Complex<double> factor in FP64; float and
+// Complex<float> factor in FP32 (values pass through the ABI as FP64).
+// Multiply is the reference's host-side CSR product; LDL and Solve run on
+// the device only.
+#pragma once
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdlib>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../cliqgpu.h"
+
+namespace cliq {
+
+template <class T>
+using Complex = std::complex<T>;
+
+struct LogicError : std::logic_error {
+    explicit LogicError(const std::string& s) : std::logic_error(s) {}
+};
+struct RuntimeError : std::runtime_error {
+    explicit RuntimeError(const std::string& s) : std::runtime_error(s) {}
+};
+
+inline void Check(int status, const char* where) {
+    if (status == CLIQ_OK) return;
+    std::string msg = std::string(where) + ": " + cliqgpu_status_string(status);
+    const char* d = cliqgpu_last_error();
+    if (d && *d) msg += std::string(" (") + d + ")";
+    if (status == CLIQ_ERR_ARG || status == CLIQ_ERR_STATE) throw LogicError(msg);
+    throw RuntimeError(msg);
+}
+
+// ---- environment (one process, no MPI) -------------------------------------
+namespace mpi {
+struct Comm {};
+static const Comm COMM_WORLD{};
+inline int Rank(Comm = COMM_WORLD) { return 0; }
+inline int Size(Comm = COMM_WORLD) { return 1; }
+inline void Barrier(Comm = COMM_WORLD) {}
+inline double Time() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace mpi
+inline void Initialize(int&, char**&) {}
+inline void Finalize() {}
+// El::SetBlocksize: accepted for source compatibility; the device kernels use 64.
+inline void SetBlocksize(int) {}
+
+template <class F> struct Traits { static constexpr bool complex = false; static constexpr bool single = false; };
+template <> struct Traits<float> { static constexpr bool complex = false; static constexpr bool single = true; };
+template <> struct Traits<Complex<double>> { static constexpr bool complex = true; static constexpr bool single = false; };
+template <> struct Traits<Complex<float>> { static constexpr bool complex = true; static constexpr bool single = true; };
+
+// ---- sparse matrix ---------------------------------------------------------
+class DistGraph;
+class DistGraph {
+public:
+    int NumSources() const { return n_; }
+    const std::vector<int64_t>& RowPtr() const { return rowptr_; }
+    const std::vector<int32_t>& ColInd() const { return colind_; }
+    int n_ = 0;
+    std::vector<int64_t> rowptr_;
+    std::vector<int32_t> colind_;
+};
+
+template <class F>
+class DistSparseMatrix {
+public:
+    DistSparseMatrix(int height, mpi::Comm = mpi::COMM_WORLD) { graph_.n_ = height; }
+    int Height() const { return graph_.n_; }
+    int FirstLocalRow() const { return 0; }
+    int LocalHeight() const { return graph_.n_; }
+    void StartAssembly() { tri_.clear(); assembling_ = true; }
+    void Reserve(int cap) { tri_.reserve(cap); }
+    void Update(int i, int j, F v) {
+        if (!assembling_) throw LogicError("Update outside of assembly");
+        tri_.push_back({i, j, v});
+    }
+    // sort and sum duplicates (core/dist_sparse_matrix/impl.hpp:209-257)
+    void StopAssembly() {
+        if (!assembling_) throw LogicError("Cannot stop assembly without starting");
+        assembling_ = false;
+        std::stable_sort(tri_.begin(), tri_.end(), [](const Trip& a, const Trip& b) {
+            return a.i < b.i || (a.i == b.i && a.j < b.j);
+        });
+        const int n = graph_.n_;
+        graph_.rowptr_.assign(n + 1, 0);
+        graph_.colind_.clear();
+        vals_.clear();
+        for (size_t e = 0; e < tri_.size(); ++e) {
+            if (!vals_.empty() && e > 0 && tri_[e].i == tri_[e - 1].i && tri_[e].j == tri_[e - 1].j) {
+                vals_.back() += tri_[e].v;
+                continue;
+            }
+            graph_.colind_.push_back(tri_[e].j);
+            vals_.push_back(tri_[e].v);
+            graph_.rowptr_[tri_[e].i + 1]++;
+        }
+        for (int i = 0; i < n; ++i) graph_.rowptr_[i + 1] += graph_.rowptr_[i];
+        tri_.clear();
+    }
+    const ::cliq::DistGraph& LockedDistGraph() const { return graph_; }
+    const ::cliq::DistGraph& DistGraph() const { return graph_; }
+    const std::vector<F>& Values() const { return vals_; }
+
+private:
+    struct Trip { int i, j; F v; };
+    ::cliq::DistGraph graph_;
+    std::vector<Trip> tri_;
+    std::vector<F> vals_;
+    bool assembling_ = false;
+};
+
+// ---- dense multivector ------------------------------------------------------
+template <class F>
+class DistMultiVec {
+public:
+    DistMultiVec(int height = 0, int width = 1, mpi::Comm = mpi::COMM_WORLD) { Resize(height, width); }
+    void Resize(int h, int w) { h_ = h; w_ = w; d_.assign((size_t)h * w, F(0)); }
+    int Height() const { return h_; }
+    int Width() const { return w_; }
+    int LocalHeight() const { return h_; }
+    int FirstLocalRow() const { return 0; }
+    F GetLocal(int i, int j) const { return d_[i + (size_t)j * h_]; }
+    void SetLocal(int i, int j, F v) { d_[i + (size_t)j * h_] = v; }
+    void UpdateLocal(int i, int j, F v) { d_[i + (size_t)j * h_] += v; }
+    F* Buffer() { return d_.data(); }
+    const F* LockedBuffer() const { return d_.data(); }
+
+private:
+    int h_ = 0, w_ = 1;
+    std::vector<F> d_;
+};
+
+template <class F>
+void Zero(DistMultiVec<F>& X) {
+    for (int j = 0; j < X.Width(); ++j)
+        for (int i = 0; i < X.Height(); ++i) X.SetLocal(i, j, F(0));
+}
+
+// MakeUniform: entries drawn uniformly from the unit ball (El::SampleBall)
+template <class F>
+void MakeUniform(DistMultiVec<F>& X, unsigned seed = 0) {
+    std::mt19937_64 g(seed);
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    for (int j = 0; j < X.Width(); ++j)
+        for (int i = 0; i < X.Height(); ++i) {
+            if constexpr (Traits<F>::complex) {
+                const double r = std::sqrt(u(g)), t = 2 * M_PI * u(g);
+                X.SetLocal(i, j, F(r * std::cos(t), r * std::sin(t)));
+            } else {
+                X.SetLocal(i, j, F(2 * u(g) - 1));
+            }
+        }
+}
+
+template <class F>
+void Norms(const DistMultiVec<F>& X, std::vector<double>& norms) {
+    norms.assign(X.Width(), 0.0);
+    for (int j = 0; j < X.Width(); ++j) {
+        double s = 0;
+        for (int i = 0; i < X.Height(); ++i) s += std::norm(X.GetLocal(i, j));
+        norms[j] = std::sqrt(s);
+    }
+}
+
+// Y := alpha A X + beta Y (host CSR product, multiply.hpp:28-166 at P=1)
+template <class F>
+void Multiply(F alpha, const DistSparseMatrix<F>& A, const DistMultiVec<F>& X, F beta, DistMultiVec<F>& Y) {
+    const auto& g = A.LockedDistGraph();
+    const auto& v = A.Values();
+    for (int j = 0; j < Y.Width(); ++j)
+        for (int i = 0; i < Y.Height(); ++i) Y.SetLocal(i, j, beta * Y.GetLocal(i, j));
+    for (int i = 0; i < g.n_; ++i)
+        for (int64_t e = g.rowptr_[i]; e < g.rowptr_[i + 1]; ++e)
+            for (int j = 0; j < X.Width(); ++j) Y.UpdateLocal(i, j, alpha * v[e] * X.GetLocal(g.colind_[e], j));
+}
+
+// ---- symbolic --------------------------------------------------------------
+class DistMap {
+public:
+    std::vector<int32_t> map;
+    int Translate(int i) const { return map[i]; }
+    void FormInverse(DistMap& inv) const {
+        inv.map.assign(map.size(), 0);
+        for (size_t i = 0; i < map.size(); ++i) inv.map[map[i]] = (int32_t)i;
+    }
+};
+
+struct SymmNodeInfo {
+    int size, off, myOff, parent;
+    std::vector<int> children;
+    bool onLeft;
+    std::vector<int> lowerStruct, origLowerStruct, origLowerRelInds, leftRelInds, rightRelInds;
+};
+
+class DistSymmInfo {
+public:
+    std::vector<SymmNodeInfo> localNodes;
+    std::shared_ptr<std::remove_pointer<cliq_symbolic>::type> handle;
+    cliq_symm_info view{};
+};
+
+class DistSeparatorTree {
+public:
+    std::vector<std::vector<int>> inds;   // natural indices of each separator / leaf (post-order)
+};
+
+inline void NaturalNestedDissection(int nx, int ny, int nz, const DistGraph& graph, DistMap& map, DistSeparatorTree& sepTree,
+                                    DistSymmInfo& info, int cutoff = 128, bool /*storeFactRecvInds*/ = false) {
+    cliq_symbolic h = nullptr;
+    Check(cliq_natural_nested_dissection(nx, ny, nz, graph.n_, graph.rowptr_.data(), graph.colind_.data(), cutoff, &h),
+          "NaturalNestedDissection");
+    info.handle.reset(h, cliq_symbolic_destroy);
+    Check(cliq_symbolic_info(h, &info.view), "NaturalNestedDissection");
+    const int nn = info.view.num_nodes;
+    info.localNodes.assign(nn, SymmNodeInfo{});
+    sepTree.inds.assign(nn, {});
+    auto arr = [&](int s, int which, std::vector<int>& out) {
+        int64_t len = 0;
+        Check(cliq_symbolic_node_array(h, s, which, nullptr, &len), "NaturalNestedDissection");
+        std::vector<int32_t> tmp(len);
+        Check(cliq_symbolic_node_array(h, s, which, tmp.data(), &len), "NaturalNestedDissection");
+        out.assign(tmp.begin(), tmp.end());
+    };
+    for (int s = 0; s < nn; ++s) {
+        int32_t v[10];
+        Check(cliq_symbolic_node(h, s, v), "NaturalNestedDissection");
+        SymmNodeInfo& nd = info.localNodes[s];
+        nd.size = v[0]; nd.off = v[1]; nd.myOff = v[2]; nd.parent = v[3];
+        if (v[4] >= 0) nd.children = {v[4], v[5]};
+        nd.onLeft = v[6] != 0;
+        arr(s, 0, nd.lowerStruct); arr(s, 1, nd.origLowerStruct); arr(s, 2, nd.origLowerRelInds);
+        arr(s, 3, nd.leftRelInds); arr(s, 4, nd.rightRelInds); arr(s, 5, sepTree.inds[s]);
+    }
+    map.map.assign(graph.n_, 0);
+    Check(cliq_symbolic_map(h, map.map.data(), nullptr), "NaturalNestedDissection");
+}
+
+// ---- numeric ---------------------------------------------------------------
+enum SymmFrontType { SYMM_1D, SYMM_2D, LDL_1D, LDL_2D };
+
+template <class F>
+class DistSymmFrontTree {
+public:
+    bool isHermitian = false;
+    SymmFrontType frontType = SYMM_2D;
+
+    DistSymmFrontTree(const DistSparseMatrix<F>& A, const DistMap& map, const DistSeparatorTree&, const DistSymmInfo& info,
+                      bool conjugate = false)
+        : isHermitian(conjugate), n_(A.Height()) {
+        cliqgpu_options opt{Traits<F>::complex ? CLIQ_COMPLEX : CLIQ_REAL, Traits<F>::single ? CLIQ_FP32 : CLIQ_FP64,
+                            conjugate ? 1 : 0, 0, 1};
+        const auto& g = A.LockedDistGraph();
+        cliqgpu_plan p = nullptr;
+        Check(cliqgpu_plan_create(&info.view, n_, map.map.data(), g.rowptr_.data(), g.colind_.data(), &opt, nullptr, &p),
+              "DistSymmFrontTree");
+        plan_.reset(p, cliqgpu_plan_destroy);
+        Initialize(A);
+    }
+    void Initialize(const DistSparseMatrix<F>& A) {
+        const auto& v = A.Values();
+        if constexpr (Traits<F>::complex) {
+            std::vector<std::complex<double>> w(v.begin(), v.end());
+            Check(cliqgpu_assemble(plan_.get(), w.data(), 0), "DistSymmFrontTree::Initialize");
+        } else {
+            std::vector<double> w(v.begin(), v.end());
+            Check(cliqgpu_assemble(plan_.get(), w.data(), 0), "DistSymmFrontTree::Initialize");
+        }
+        frontType = SYMM_2D;
+    }
+    // FactorizationWork / SolveWork (dist_symm_front_tree/impl.hpp:542-640), P = 1
+    void FactorizationWork(double& local, double& mn, double& mx, double& global, bool = false) const {
+        cliqgpu_plan_query(plan_.get(), 0, &local);
+        mn = mx = global = local;
+    }
+    void SolveWork(double& local, double& mn, double& mx, double& global, int numRhs = 1) const {
+        cliqgpu_plan_query(plan_.get(), 1, &local);
+        local *= numRhs;
+        mn = mx = global = local;
+    }
+    cliqgpu_plan Plan() const { return plan_.get(); }
+    int Height() const { return n_; }
+
+private:
+    std::shared_ptr<std::remove_pointer<cliqgpu_plan>::type> plan_;
+    int n_;
+};
+
+template <class F>
+void LDL(DistSymmInfo&, DistSymmFrontTree<F>& L, SymmFrontType newFrontType = LDL_2D) {
+    if (L.frontType == LDL_1D || L.frontType == LDL_2D) throw LogicError("Matrix is already factored");
+    if (newFrontType != LDL_1D && newFrontType != LDL_2D) throw LogicError("Only unpivoted LDL_1D / LDL_2D are provided");
+    int64_t zp = -1;
+    Check(cliqgpu_factor(L.Plan(), &zp), "LDL");
+    L.frontType = newFrontType;
+}
+
+template <class F>
+class DistNodalMultiVec {
+public:
+    std::vector<F> data;   // ND-ordered, n x width column-major
+    DistNodalMultiVec() = default;
+    DistNodalMultiVec(const DistMap& inverseMap, const DistSymmInfo& info, const DistMultiVec<F>& X) { Pull(inverseMap, info, X); }
+    // Pull / Push at P=1 (dist_nodal_multi_vec/impl.hpp:67-219)
+    void Pull(const DistMap& inverseMap, const DistSymmInfo&, const DistMultiVec<F>& X) {
+        h_ = X.Height(); w_ = X.Width();
+        data.assign((size_t)h_ * w_, F(0));
+        for (int j = 0; j < w_; ++j)
+            for (int p = 0; p < h_; ++p) data[p + (size_t)j * h_] = X.GetLocal(inverseMap.map[p], j);
+    }
+    void Push(const DistMap& inverseMap, const DistSymmInfo&, DistMultiVec<F>& X) const {
+        for (int j = 0; j < w_; ++j)
+            for (int p = 0; p < h_; ++p) X.SetLocal(inverseMap.map[p], j, data[p + (size_t)j * h_]);
+    }
+    int Height() const { return h_; }
+    int Width() const { return w_; }
+
+private:
+    int h_ = 0, w_ = 0;
+};
+
+template <class F>
+void Solve(const DistSymmInfo&, const DistSymmFrontTree<F>& L, DistNodalMultiVec<F>& X) {
+    if (L.frontType != LDL_1D && L.frontType != LDL_2D) throw LogicError("Invalid front type for solve");
+    const int n = X.Height(), w = X.Width();
+    if constexpr (std::is_same<F, double>::value || std::is_same<F, Complex<double>>::value) {
+        Check(cliqgpu_solve(L.Plan(), X.data.data(), n, w, 0, 1), "Solve");
+    } else {
+        using D = typename std::conditional<Traits<F>::complex, std::complex<double>, double>::type;
+        std::vector<D> tmp(X.data.begin(), X.data.end());
+        Check(cliqgpu_solve(L.Plan(), tmp.data(), n, w, 0, 1), "Solve");
+        for (size_t i = 0; i < tmp.size(); ++i) X.data[i] = F(tmp[i]);
+    }
+}
+
+}  // namespace cliq

@@ -1,0 +1,88 @@
+// The flow of the reference's tests/Solve.cpp written against the drop-in
+// header: 3D 7-point Laplacian (diagonal 6 + shift), manufactured solution
+// X, Y := A X, natural nested dissection, front tree, LDL, Pull / Solve /
+// Push, and the error || X - X_hat || / || X || per right-hand side.
+// Exit status 0 when every error is below the tolerance.
+#include <cstdio>
+#include <cstdlib>
+
+#include "clique_b200/clique.hpp"
+
+using namespace cliq;
+
+template <class F>
+int run(int n1, int n2, int n3, int numRhs, int cutoff, double shift, double tol) {
+    const int N = n1 * n2 * n3;
+    DistSparseMatrix<F> A(N, mpi::COMM_WORLD);
+    A.StartAssembly();
+    A.Reserve(7 * N);
+    for (int i = 0; i < N; ++i) {
+        const int x = i % n1, y = (i / n1) % n2, z = i / (n1 * n2);
+        A.Update(i, i, F(6. + shift));
+        if (x != 0) A.Update(i, i - 1, F(-1));
+        if (x != n1 - 1) A.Update(i, i + 1, F(-1));
+        if (y != 0) A.Update(i, i - n1, F(-1));
+        if (y != n2 - 1) A.Update(i, i + n1, F(-1));
+        if (z != 0) A.Update(i, i - n1 * n2, F(-1));
+        if (z != n3 - 1) A.Update(i, i + n1 * n2, F(-1));
+    }
+    A.StopAssembly();
+    DistMultiVec<F> X(N, numRhs), Y(N, numRhs);
+    MakeUniform(X, 7);
+    Zero(Y);
+    Multiply(F(1), A, X, F(0), Y);
+
+    DistSymmInfo info;
+    DistSeparatorTree sepTree;
+    DistMap map, inverseMap;
+    NaturalNestedDissection(n1, n2, n3, A.DistGraph(), map, sepTree, info, cutoff);
+    map.FormInverse(inverseMap);
+    DistSymmFrontTree<F> frontTree(A, map, sepTree, info, false);
+    const double t0 = mpi::Time();
+    LDL(info, frontTree, LDL_2D);
+    const double t1 = mpi::Time();
+    DistNodalMultiVec<F> YNodal;
+    YNodal.Pull(inverseMap, info, Y);
+    Solve(info, frontTree, YNodal);
+    YNodal.Push(inverseMap, info, Y);
+    const double t2 = mpi::Time();
+    double local, mn, mx, flops;
+    frontTree.FactorizationWork(local, mn, mx, flops);
+    std::printf("N=%d fronts=%zu factor %.3f s (%.1f GFlop/s) solve %.3f s\n", N, info.localNodes.size(), t1 - t0,
+                flops / (t1 - t0) / 1e9, t2 - t1);
+    int bad = 0;
+    for (int j = 0; j < numRhs; ++j) {
+        double e = 0, x = 0;
+        for (int i = 0; i < N; ++i) {
+            e += std::norm(Y.GetLocal(i, j) - X.GetLocal(i, j));
+            x += std::norm(X.GetLocal(i, j));
+        }
+        const double rel = std::sqrt(e / x);
+        std::printf("||X - X_hat|| / ||X|| (rhs %d) = %.3e\n", j, rel);
+        if (!(rel <= tol)) bad = 1;
+    }
+    // a second LDL on the factored tree is a logic error, as in the reference
+    try {
+        LDL(info, frontTree, LDL_2D);
+        std::printf("missing LogicError\n");
+        bad = 1;
+    } catch (const LogicError&) {
+    }
+    return bad;
+}
+
+int main(int argc, char* argv[]) {
+    Initialize(argc, argv);
+    const int n = argc > 1 ? std::atoi(argv[1]) : 30;
+    int rc = 0;
+    try {
+        rc |= run<double>(n, n, n, 5, 128, 0.1, 1e-10);
+        rc |= run<Complex<double>>(n / 2 + 3, n / 2, n / 2 + 1, 3, 64, 0.1, 1e-10);
+        rc |= run<float>(n / 2, n / 2, n / 2, 2, 64, 0.1, 1e-4);
+    } catch (const std::exception& e) {
+        std::printf("exception: %s\n", e.what());
+        rc = 1;
+    }
+    Finalize();
+    return rc;
+}

@@ -257,3 +257,34 @@ def test_single_front_ldl(oracle, complex_, precision):
     assert rel(tAL.cpu().numpy().astype(ALo.dtype), ALo) <= tol
     g = np.tril(tABR.cpu().numpy().astype(ABRo.dtype))
     assert rel(g, np.tril(ABRo)) <= tol
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_fp32_tensor_core_fronts(oracle, complex_, monkeypatch):
+    """FP32 fronts from the tcgen05 (3xTF32) update kernel agree with the FP64
+    oracle to FP32-level accuracy, and with the CUDA-core FP32 kernel."""
+    dims, cutoff = (14, 13, 12), 40
+    if complex_:
+        A = ops.helmholtz_pml_3d(*dims, omega=25.0, velocity=ops.smooth_velocity(dims, 6), b=3)
+    else:
+        A = ops.laplacian_3d(*dims, 6.1)
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=complex_)
+    assert F.ldl(96) == 0
+    fronts = {}
+    for tc in ("1", "0"):
+        monkeypatch.setenv("CLIQGPU_TENSOR_CORES", tc)
+        map_, info, L = build(A, dims, cutoff, precision="single")
+        fronts[tc] = [L.front(s) for s in range(S.num_nodes)]
+    worst_tc = worst_cc = 0.0
+    for s in range(S.num_nodes):
+        Lo, do = F.front(s)
+        Lt, dt = fronts["1"][s]
+        Ls, ds = fronts["0"][s]
+        worst_tc = max(worst_tc, rel(Lt, Lo), rel(dt, do))
+        worst_cc = max(worst_cc, rel(Ls, Lo), rel(ds, do))
+    # 3xTF32 products are as accurate as FP32 CUDA-core arithmetic (the
+    # absolute level reflects unpivoted FP32 LDL^T of an indefinite operator)
+    print(f"worst front error: tensor cores {worst_tc:.2e}, CUDA cores {worst_cc:.2e}")
+    assert worst_tc <= 4 * worst_cc + 1e-6, (worst_tc, worst_cc)
+    assert worst_tc <= 1e-3
