@@ -100,6 +100,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
 def workload(n, nrhs, seed):
     from clique_b200 import operators as ops
     A, omega, c = ops.helmholtz_workload_3d(n, seed=seed)
@@ -203,11 +212,15 @@ def run_ours(args):
     B_d = torch.from_numpy(B).cuda().t().contiguous().t()
 
     L32 = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single", stream=stream.cuda_stream)
+    phase_ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
 
     def step32():
+        phase_ev[0].record()
         L32.Initialize(vals_d)
         cliq.LDL(info, L32)
+        phase_ev[1].record()
         X, it, rr = cliq.RefinedSolve(L32, B_d, args.tol, 30)
+        phase_ev[2].record()
         return it, rr
 
     def barrier():
@@ -218,6 +231,9 @@ def run_ours(args):
         it, rr = step32()
     torch.cuda.synchronize()
     barrier()
+    # CUDA events around every factorization launch during the timed steps
+    L32.set_profiling(True)
+    launches0 = L32.total_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
@@ -236,7 +252,24 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     factor_flops = L32.FactorizationWork()
-    launches = L32.last_launches()
+    launches = (L32.total_launches() - launches0) // args.steps
+    prof = L32.profile()
+    L32.set_profiling(False)
+    factor_phase_ms = phase_ev[0].elapsed_time(phase_ev[1])
+    solve_phase_ms = phase_ev[1].elapsed_time(phase_ev[2])
+    peaks = measured_peaks()
+    upd_ms = prof["trail_ms"] + prof["schur_ms"]
+    upd_flops = prof["trail_flops"] + prof["schur_flops"]
+    achieved = upd_flops / (upd_ms * 1e-3) / 1e12 if upd_ms > 0 else 0.0
+    tf32_peak = peaks["bf16_tflops"] / 2.0 if peaks else 1590.0 / 2.0
+    roofline = {"kernel": "tc_update_kernel (tcgen05 kind::tf32, 3xTF32; Schur + in-panel updates)",
+                "bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
+                "frac": achieved / tf32_peak,
+                "peak_source": ("measured bf16 burst / 2 (dense TF32 rate is half of BF16), MEASURED_PEAKS.json"
+                                if peaks else "fallback 1.59 PFLOP/s bf16 / 2"),
+                "numerator": "Clique FactorizationWork counting (complex x4) of the update GEMMs; the three TF32 "
+                             "products per split count against the fraction, not in the numerator",
+                "traffic": None}
 
     # end-to-end through the C ABI with host buffers
     L32h = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
@@ -264,6 +297,7 @@ def run_ours(args):
         for _ in range(max(1, args.warmup)):
             step64()
         torch.cuda.synchronize()
+        L64.set_profiling(True)
         ev0.record()
         for _ in range(args.steps):
             step64()
@@ -272,8 +306,12 @@ def run_ours(args):
         fp64_ms = ev0.elapsed_time(ev1) / args.steps
         Xc = X64.cpu().numpy()
         res64 = float(np.linalg.norm(A.to_scipy() @ Xc - B) / np.linalg.norm(B))
+        p64 = L64.profile()
         fp64 = {"fp64_plain_s": fp64_ms / 1e3, "fp64_residual": res64,
-                "speedup_vs_fp64": fp64_ms / ms}
+                "speedup_vs_fp64": fp64_ms / ms,
+                "fp64_factor_profile_ms": {k: v for k, v in p64.items() if k.endswith("_ms")},
+                "fp64_update_tflops": (p64["trail_flops"] + p64["schur_flops"]) /
+                                      max(1e-9, (p64["trail_ms"] + p64["schur_ms"]) * 1e-3) / 1e12}
         del L64
 
     line = {"metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -286,6 +324,9 @@ def run_ours(args):
             "refine_iters": its, "relres": max(rrs), "factor_gflop": factor_flops / 1e9,
             "factor_tflops_effective": factor_flops / (ms / 1e3) / 1e12,
             "gpu_launches": launches,
+            "phases_ms": {"assemble+factor": factor_phase_ms, "refined_solve": solve_phase_ms},
+            "factor_profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")},
+            "roofline": roofline,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(A.values.nbytes + B.nbytes),
                     "d2h_bytes_per_step": int(B.nbytes)},
             "clocks": clk.summary()}

@@ -56,6 +56,7 @@ struct FrontDev {
     int32_t cu[2];      // children's update sizes
     int32_t pool;       // parity of the depth
     int32_t flag_base;  // first chain-solve flag of this front
+    int64_t dinv;       // inverse diagonal blocks (ceil(n/64) blocks of 64 x 64) in the dinv store
 };
 
 // One GEMM update problem: C -= A diag(d) op(B)^T restricted to i >= j.
@@ -122,7 +123,9 @@ struct Plan {
     void* L = nullptr;            // factor arena (storage precision)
     double* D = nullptr;          // pivots, FP64 (complex: interleaved), length n
     void* pool[2] = {nullptr, nullptr};
-    void* tinv = nullptr;         // per-front inverse diagonal blocks, FP64 storage
+    void* tinv = nullptr;         // U = op(L11^{-1})^T of each front of one panel step (storage precision)
+    void* dinv = nullptr;         // L11^{-1} of every 64-block of every front, kept for the solves
+    int64_t dinv_elems = 0;
     FrontDev* fronts = nullptr;
     int32_t* cmaps = nullptr;
     int32_t* lower = nullptr;     // flattened lowerStruct (ND indices)

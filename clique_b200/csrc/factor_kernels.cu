@@ -73,17 +73,26 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
 
 // ---------------------------------------------------------------------------
 // 2a. LDL of the diagonal block (one CTA per front), FP64 in shared memory
+//
+// Right-looking elimination of the kb x kb block; the same row operations
+// are applied to an identity block, which therefore ends as L11^{-1}
+// (Gaussian elimination on [A | I]).  Two barriers per pivot.  Outputs:
+// L11 (unit diagonal) and D back to global memory, U = op(L11^{-1})^T for the
+// panel kernel, and L11^{-1} itself into the per-front inverse store used by
+// the triangular solves.
 // ---------------------------------------------------------------------------
 template <class T, bool C, bool CJ>
 __global__ void __launch_bounds__(kThreads) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
                                                             T* __restrict__ L, double* __restrict__ D, T* __restrict__ tinv,
-                                                            int32_t* __restrict__ status) {
+                                                            T* __restrict__ dinv, int32_t* __restrict__ status) {
     using W = DV<C>;
     using X = V<T, C>;
     constexpr int nb = kTile, ld = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    W* sA = reinterpret_cast<W*>(smem_raw);
-    W* sX = sA + nb * ld;
+    W* sA = reinterpret_cast<W*>(smem_raw);          // nb x ld, row-major
+    W* sX = sA + nb * ld;                              // inverse, nb x ld
+    W* sa = sX + nb * ld;                              // pivot column before scaling
+    W* sl = sa + nb;                                   // pivot column after scaling
     const int4 it = items[blockIdx.x];
     const FrontDev f = F[it.x];
     const int slot = it.y;
@@ -93,41 +102,47 @@ __global__ void __launch_bounds__(kThreads) diag_ldl_kernel(const FrontDev* __re
         W v{};
         if (i >= j) v = conv<W>(ldv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m));
         sA[i * ld + j] = v;
-        sX[i * ld + j] = W{};
+        sX[i * ld + j] = (i == j) ? vone<W>() : W{};
     }
     __syncthreads();
     for (int j = 0; j < kb; ++j) {
         const W d = sA[j * ld + j];
         if (threadIdx.x == 0 && is_zero(d)) atomicMin(&status[0], f.off + k + j + 1);
-        const int r = kb - j - 1;
-        for (int idx = threadIdx.x; idx < r * r; idx += blockDim.x) {
-            const int ii = idx % r, cc = idx / r;
-            if (ii >= cc) {
-                const int i = j + 1 + ii, c = j + 1 + cc;
-                sA[i * ld + c] -= sA[i * ld + j] * (opc<CJ>(sA[c * ld + j]) / d);
+        const W rd = vone<W>() / d;
+        for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) {
+            const W a = sA[i * ld + j];
+            const W l = a * rd;
+            sa[i] = a;
+            sl[i] = l;
+            sA[i * ld + j] = l;
+        }
+        __syncthreads();
+        const int r = kb - 1 - j;            // rows below the pivot
+        for (int idx = threadIdx.x; idx < r * kb; idx += blockDim.x) {
+            const int i = j + 1 + idx % r, c = idx / r;
+            if (c > j) {
+                if (i >= c) sA[i * ld + c] -= sl[i] * opc<CJ>(sa[c]);
+            } else {
+                sX[i * ld + c] -= sl[i] * sX[j * ld + c];
             }
         }
         __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) sA[i * ld + j] = sA[i * ld + j] / d;
     }
-    __syncthreads();
-    // Linv = L11^{-1} (unit lower), one column per thread
-    for (int c = threadIdx.x; c < kb; c += blockDim.x) {
-        sX[c * ld + c] = vone<W>();
-        for (int i = c + 1; i < kb; ++i) {
-            W acc = sA[i * ld + c];
-            for (int t = c + 1; t < i; ++t) mac(acc, sA[i * ld + t], sX[t * ld + c]);
-            sX[i * ld + c] = W{} - acc;
-        }
-    }
-    __syncthreads();
-    // U = op(Linv)^T, row-major kb x kb (upper unit) into the slot; L11 and D back to global
+    // U = op(L11^{-1})^T row-major (upper unit) into the step's slot
     X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
     for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
         const int t = idx / nb, c = idx % nb;
         X v{};
         if (t < kb && c < kb && t <= c) v = conv<X>(opc<CJ>(sX[c * ld + t]));
         U[idx] = v;
+    }
+    // L11^{-1} (column-major nb x nb) for the solves
+    X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)(k / nb) * nb * nb;
+    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+        const int i = idx % nb, c = idx / nb;
+        X v{};
+        if (i < kb && c < kb && i >= c) v = conv<X>(sX[i * ld + c]);
+        Dv[idx] = v;
     }
     for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
         const int i = idx % kb, j = idx / kb;
@@ -288,7 +303,7 @@ template <class T, bool C, bool CJ>
 static int run_factor_impl(Plan& P) {
     using X = V<T, C>;
     using W = DV<C>;
-    const size_t smem_diag = 2 * sizeof(W) * kTile * (kTile + 1);
+    const size_t smem_diag = sizeof(W) * (2 * kTile * (kTile + 1) + 2 * kTile);
     const size_t smem_panel = sizeof(X) * (kTile * kTile + kTile * (kTile + 1) + kTile);
     static bool attr_done = false;
     if (!attr_done) {
@@ -316,7 +331,8 @@ static int run_factor_impl(Plan& P) {
                 break;
             case Launch::DIAG:
                 diag_ldl_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, smem_diag, P.stream>>>(
-                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), P.status);
+                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), reinterpret_cast<T*>(P.dinv),
+                    P.status);
                 break;
             case Launch::PANEL:
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(

@@ -75,7 +75,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 }
 
 void free_plan(Plan& P) {
-    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.prefix, P.dest,
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
                     P.wpool[1], P.xnodal, P.xwork, P.norms};
     for (void* p : ptrs)
@@ -125,6 +125,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     int64_t arena = 0;
     std::vector<int64_t> level_pool(P.max_depth + 1, 0), level_w(P.max_depth + 1, 0);
     P.factor_flops = P.solve_flops = P.factor_entries = 0;
+    P.dinv_elems = 0;
     for (int s = 0; s < nn; ++s) {
         FrontDev& f = P.hfronts[s];
         const int64_t nlow = info->lower_ptr[s + 1] - info->lower_ptr[s];
@@ -141,6 +142,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         f.W = level_w[d];
         level_w[d] += f.u;
         f.lower = info->lower_ptr[s];
+        f.dinv = P.dinv_elems;
+        P.dinv_elems += (int64_t)((f.n + kTile - 1) / kTile) * kTile * kTile;
         f.cmap = -1;
         f.CU[0] = f.CU[1] = -1;
         f.CW[0] = f.CW[1] = 0;
@@ -418,6 +421,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.pool[0], (size_t)P.pool_elems[0] * eb));
     TRY(dev_alloc(P, &P.pool[1], (size_t)P.pool_elems[1] * eb));
     TRY(dev_alloc(P, &P.tinv, (size_t)P.tinv_slots * nb * nb * eb));
+    TRY(dev_alloc(P, &P.dinv, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_upload(P, &P.fronts, P.hfronts));
     TRY(dev_upload(P, &P.cmaps, cmaps));
     std::vector<int32_t> lowv(low, low + info->lower_ptr[nn]);

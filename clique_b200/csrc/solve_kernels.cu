@@ -105,14 +105,16 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_gather_kernel(const FrontDe
 template <class T, bool C>
 __global__ void __launch_bounds__(kSolveThreads) fwd_chain_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
                                                                   int32_t* __restrict__ ticket, int32_t* __restrict__ flags, int epoch,
-                                                                  const T* __restrict__ L, T* __restrict__ X, int64_t ldx,
+                                                                  const T* __restrict__ L, const T* __restrict__ dinv,
+                                                                  T* __restrict__ X, int64_t ldx,
                                                                   T* __restrict__ w0, T* __restrict__ w1, int nrhs,
                                                                   int32_t* __restrict__ status) {
     using Xv = V<T, C>;
     constexpr int ldl = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Xv* sL = reinterpret_cast<Xv*>(smem_raw);         // 64 x 65
-    Xv* sx = sL + kTile * ldl;                          // 64 x kMaxRhsChunk
+    Xv* sD = sL + kTile * ldl;                          // 64 x 65: inverse of the diagonal block, sD[r*65+c] = Linv[r][c]
+    Xv* sx = sD + kTile * ldl;                          // 64 x kMaxRhsChunk
     __shared__ int s_item;
     if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
     __syncthreads();
@@ -153,9 +155,11 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_chain_kernel(const FrontDev
     }
     if (rb < nT) {
         const int dcols = min(kTile, f.n - r0);
+        const Xv* Dv = reinterpret_cast<const Xv*>(dinv) + f.dinv + (int64_t)rb * kTile * kTile;
         for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
             const int rr = idx % kTile, cc = idx / kTile;
             sL[rr * ldl + cc] = (rr < rows && cc < dcols) ? ldv<T, C>(L, f.L + (r0 + rr) + (int64_t)(r0 + cc) * f.m) : Xv{};
+            sD[rr * ldl + cc] = Dv[idx];
         }
 #pragma unroll
         for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
@@ -163,18 +167,23 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_chain_kernel(const FrontDev
             if (j < nrhs && r < dcols) sx[r * kMaxRhsChunk + j] = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * ldx) - acc[a];
         }
         __syncthreads();
-        // unit lower forward substitution on the diagonal block
-        for (int c = 0; c < dcols; ++c) {
-            if (r > c && r < dcols) {
-                const Xv l = sL[r * ldl + c];
+        // x = L11^{-1} b with the inverse kept by the factorization
+        Xv y[kMaxRhsChunk / 4];
 #pragma unroll
-                for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-                    const int j = q + 4 * a;
-                    if (j < nrhs) sx[r * kMaxRhsChunk + j] -= l * sx[c * kMaxRhsChunk + j];
-                }
-            }
-            __syncthreads();
+        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
+            const int j = q + 4 * a;
+            Xv sacc{};
+            if (j < nrhs && r < dcols)
+                for (int cc = 0; cc <= r; ++cc) mac(sacc, sD[r * ldl + cc], sx[cc * kMaxRhsChunk + j]);
+            y[a] = sacc;
         }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
+            const int j = q + 4 * a;
+            if (j < nrhs && r < dcols) sx[r * kMaxRhsChunk + j] = y[a];
+        }
+        __syncthreads();
 #pragma unroll
         for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
             const int j = q + 4 * a;
@@ -230,14 +239,16 @@ __global__ void diag_scale_kernel(T* __restrict__ X, int64_t ldx, int64_t n, int
 template <class T, bool C, bool CJ>
 __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
                                                                   int32_t* __restrict__ ticket, int32_t* __restrict__ flags, int epoch,
-                                                                  const T* __restrict__ L, T* __restrict__ X, int64_t ldx,
+                                                                  const T* __restrict__ L, const T* __restrict__ dinv,
+                                                                  T* __restrict__ X, int64_t ldx,
                                                                   const int32_t* __restrict__ lower, int nrhs,
                                                                   int32_t* __restrict__ status) {
     using Xv = V<T, C>;
     constexpr int ldl = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Xv* sL = reinterpret_cast<Xv*>(smem_raw);
-    Xv* sx = sL + kTile * ldl;
+    Xv* sD = sL + kTile * ldl;
+    Xv* sx = sD + kTile * ldl;
     __shared__ int s_item;
     if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
     __syncthreads();
@@ -301,10 +312,11 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev
         }
         __syncthreads();
     }
-    // diagonal block, transposed
+    // diagonal block, transposed: x = op(L11^{-1})^T b
+    const Xv* Dv = reinterpret_cast<const Xv*>(dinv) + f.dinv + (int64_t)rb * kTile * kTile;
     for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
         const int rr = idx % kTile, cc = idx / kTile;
-        sL[rr * ldl + cc] = (rr < dcols && cc < dcols) ? ldv<T, C>(L, f.L + (c0 + rr) + (int64_t)(c0 + cc) * f.m) : Xv{};
+        sD[rr * ldl + cc] = Dv[idx];
     }
 #pragma unroll
     for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
@@ -312,17 +324,22 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev
         if (j < nrhs && c < dcols) sx[c * kMaxRhsChunk + j] = ldv<T, C>(X, f.off + c0 + c + (int64_t)j * ldx) - acc[a];
     }
     __syncthreads();
-    for (int cc = dcols - 1; cc >= 0; --cc) {
-        if (c < cc) {
-            const Xv l = opc<CJ>(sL[cc * ldl + c]);   // (L^T)[c][cc] = L[cc][c]
+    Xv y[kMaxRhsChunk / 4];
 #pragma unroll
-            for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-                const int j = q + 4 * a;
-                if (j < nrhs) sx[c * kMaxRhsChunk + j] -= l * sx[cc * kMaxRhsChunk + j];
-            }
-        }
-        __syncthreads();
+    for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
+        const int j = q + 4 * a;
+        Xv sacc{};
+        if (j < nrhs && c < dcols)
+            for (int rr = c; rr < dcols; ++rr) mac(sacc, opc<CJ>(sD[rr * ldl + c]), sx[rr * kMaxRhsChunk + j]);
+        y[a] = sacc;
     }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
+        const int j = q + 4 * a;
+        if (j < nrhs && c < dcols) sx[c * kMaxRhsChunk + j] = y[a];
+    }
+    __syncthreads();
 #pragma unroll
     for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
         const int j = q + 4 * a;
@@ -337,7 +354,7 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev
 template <class T, bool C, bool CJ>
 static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
     using Xv = V<T, C>;
-    const size_t smem = sizeof(Xv) * (kTile * (kTile + 1) + kTile * kMaxRhsChunk);
+    const size_t smem = sizeof(Xv) * (2 * kTile * (kTile + 1) + kTile * kMaxRhsChunk);
     static bool attr_done = false;
     if (!attr_done) {
         cudaFuncSetAttribute(fwd_chain_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -363,7 +380,7 @@ static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
             if (lv.nfwd > 0) {
                 const int epoch = ++P.epoch;
                 fwd_chain_kernel<T, C><<<lv.nfwd, kSolveThreads, smem, P.stream>>>(P.fronts, items + lv.fwd_items, P.tickets + 2 * d,
-                                                                                   P.flags, epoch, L, X, P.n, w0, w1, nrhs, P.status);
+                                                                                   P.flags, epoch, L, reinterpret_cast<const T*>(P.dinv), X, P.n, w0, w1, nrhs, P.status);
                 ++launches;
             }
         }
@@ -374,7 +391,7 @@ static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
             if (lv.nbwd == 0) continue;
             const int epoch = ++P.epoch;
             bwd_chain_kernel<T, C, CJ><<<lv.nbwd, kSolveThreads, smem, P.stream>>>(P.fronts, items + lv.bwd_items, P.tickets + 2 * d + 1,
-                                                                                    P.flags, epoch, L, X, P.n, P.lower, nrhs, P.status);
+                                                                                    P.flags, epoch, L, reinterpret_cast<const T*>(P.dinv), X, P.n, P.lower, nrhs, P.status);
             ++launches;
         }
     }
