@@ -63,6 +63,15 @@ struct FrontDev {
 struct GemmProb {
     int64_t A, B, C, d;   // A, B in the arena; C in the arena (cpool < 0) or a pool; d in the D array
     int32_t lda, ldc, M, N, K, cpool;
+    int64_t packA, packB; // tensor-core path: float offsets of the packed operands in the pack buffer
+};
+
+// One operand panel to pack for the tensor cores: R rows x K columns of the
+// arena at src (leading dimension ld), scaled by d[k] when d >= 0, written
+// as (row tile, k step) blocks of tile_rows rows at float offset dst.
+struct PackJob {
+    int64_t src, dst, d;
+    int32_t R, K, ld, tile_rows;
 };
 
 struct Launch {
@@ -75,6 +84,9 @@ struct Launch {
     int32_t depth;
     double work;          // GEMM: algorithmic flops; EXTEND_ADD: algorithmic bytes
     int32_t schur;        // GEMM: 1 for the Schur-complement update, 0 for an in-panel update
+    // tensor-core path: operand packing for this GEMM
+    int64_t pack_items = 0, pack_prefix = 0, pack_blocks = 0;
+    int32_t pack_njobs = 0;
 };
 
 // per-kernel-kind device time of the last profiled factorization (ms) and work
@@ -131,6 +143,9 @@ struct Plan {
     int32_t* lower = nullptr;     // flattened lowerStruct (ND indices)
     int32_t* items = nullptr;     // int2 items for extend-add / diag / panel / chain solves
     GemmProb* probs = nullptr;
+    PackJob* packjobs = nullptr;
+    void* pack = nullptr;         // packed tensor-core operands of one GEMM launch
+    int64_t pack_floats = 0;
     int64_t* prefix = nullptr;
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
@@ -156,7 +171,6 @@ struct Plan {
     // FP32 updates on the tensor cores (tcgen05 3xTF32); CLIQGPU_TENSOR_CORES=0 selects the CUDA-core kernel
     int use_tc = 1;
     bool tensor_path() const { return use_tc && precision == CLIQ_FP32; }
-    int gemm_tile() const { return tensor_path() ? 128 : kTile; }
     // width of the outer column block whose trailing update is deferred (multiple of nb)
     int outer_nb = 256;
     // optional per-launch CUDA-event timing of the factorization
@@ -184,8 +198,8 @@ int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
 
 int check_cuda(const char* where);
-int launch_tc_update(Plan& P, const Launch& ln);
-size_t tc_update_smem(bool cplx);
+int launch_tc2(Plan& P, const Launch& ln);
+size_t tc2_smem(bool cplx);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);
 void free_plan(Plan& P);

@@ -339,8 +339,8 @@ static int run_factor_impl(Plan& P) {
                     P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv));
                 break;
             case Launch::GEMM:
-                if (std::is_same<T, float>::value && P.use_tc)
-                    launch_tc_update(P, ln);
+                if (std::is_same<T, float>::value && P.tensor_path())
+                    launch_tc2(P, ln);
                 else
                     gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(
                         P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);

@@ -75,7 +75,8 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 }
 
 void free_plan(Plan& P) {
-    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.prefix, P.dest,
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
+                    P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
                     P.wpool[1], P.xnodal, P.xwork, P.norms};
     for (void* p : ptrs)
@@ -203,12 +204,21 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     auto push_item = [&](int a, int b, int c, int d) { items.push_back(a); items.push_back(b); items.push_back(c); items.push_back(d); };
     P.launches.clear();
     int64_t max_slots = 1;
-    // square update tiles: 128 on the tensor-core path, 64 on the CUDA-core path
-    const int gtile = P.gemm_tile();
-    auto tiles_of = [gtile](int M, int N) -> int64_t {
-        const int64_t Mt = (M + gtile - 1) / gtile, Nt = (N + gtile - 1) / gtile;
+    // update tiles over the lower trapezoid i >= j: 64 x 64 on the CUDA cores,
+    // 128 x 256 (row tile ti needed when ti >= 2 tj) on the tensor cores
+    const bool tcp = P.tensor_path();
+    auto tiles_of = [tcp](int M, int N) -> int64_t {
+        if (tcp) {
+            const int64_t Mt = (M + 127) / 128, Nt = (N + 255) / 256;
+            return Nt * Mt - Nt * (Nt - 1);
+        }
+        const int64_t Mt = (M + kTile - 1) / kTile, Nt = (N + kTile - 1) / kTile;
         return Nt * Mt - Nt * (Nt - 1) / 2;
     };
+    std::vector<PackJob> packjobs;
+    const int planes = P.cplx() ? 4 : 2;
+    const int64_t blkA = (int64_t)planes * 128 * 8, blkB = (int64_t)planes * 256 * 8;   // floats per packed block
+    int64_t pack_max = 1;
     auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur) {
         if (lst.empty()) return;
         Launch ln{};
@@ -220,6 +230,29 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
         ln.items = (int64_t)probs.size();
         ln.nitems = (int32_t)lst.size();
+        if (tcp) {
+            // pack jobs: A (128-row tiles) and S = d op(B) (256-row tiles) of every problem
+            int64_t off = 0, blocks = 0;
+            ln.pack_items = (int64_t)packjobs.size();
+            ln.pack_prefix = (int64_t)prefix.size();
+            for (auto& pr : lst) {
+                const int64_t nk = (pr.K + 7) / 8;
+                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, 128};
+                pr.packA = off;
+                off += (pr.M + 127) / 128 * nk * blkA;
+                PackJob b{pr.B, off, pr.d, pr.N, pr.K, pr.lda, 256};
+                pr.packB = off;
+                off += (pr.N + 255) / 256 * nk * blkB;
+                for (const PackJob& j : {a, b}) {
+                    prefix.push_back(blocks);
+                    blocks += (int64_t)((j.R + j.tile_rows - 1) / j.tile_rows) * nk;
+                    packjobs.push_back(j);
+                }
+            }
+            ln.pack_njobs = (int32_t)(packjobs.size() - ln.pack_items);
+            ln.pack_blocks = blocks;
+            pack_max = std::max(pack_max, off);
+        }
         ln.prefix = (int64_t)prefix.size();
         int64_t tot = 0;
         for (auto& pr : lst) { prefix.push_back(tot); tot += tiles_of(pr.M, pr.N); probs.push_back(pr); }
@@ -354,6 +387,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         add_gemm(schur, d, 1);
     }
     P.tinv_slots = max_slots;
+    P.pack_floats = tcp ? pack_max : 0;
 
     // ---- solve schedule ----
     P.solve_levels.assign(P.max_depth + 1, SolveLevel{});
@@ -428,6 +462,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.lower, lowv));
     TRY(dev_upload(P, &P.items, items));
     TRY(dev_upload(P, &P.probs, probs));
+    TRY(dev_upload(P, &P.packjobs, packjobs));
+    if (P.pack_floats > 0) TRY(dev_alloc(P, &P.pack, (size_t)P.pack_floats * sizeof(float)));
     TRY(dev_upload(P, &P.prefix, prefix));
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));

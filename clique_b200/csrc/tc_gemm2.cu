@@ -1,0 +1,341 @@
+// Tensor-core update for FP32 / complex-FP32 fronts, fed by TMA bulk copies:
+//     C[i, j] -= sum_k A[i, k] * d[k] * op(B[j, k])      for i >= j
+// (FrontLDL's in-panel Gemm and Schur-complement Trrk,
+// include/clique/numeric/ldl/local_front.hpp:67-69).
+//
+// Two kernels per schedule entry:
+//  * pack_kernel writes every operand panel once into a scratch buffer in
+//    exactly the shared-memory layout tcgen05.mma reads: planes (Re, Im)
+//    x (hi, lo) of the 3xTF32 split, K-major canonical no-swizzle layout
+//    (8-row x 16-byte core matrices; K-adjacent cores 128 B apart; 8-row
+//    groups 256 B apart), one contiguous block per (row tile, 8-wide k step).
+//    The B operand is packed already scaled, S = d * op(B).
+//  * tc_gemm_kernel streams those blocks with cp.async.bulk (one elected
+//    producer thread, mbarrier transaction counts) through a 4-stage ring,
+//    one elected thread issues 12 (complex) or 3 (real) tcgen05.mma
+//    kind::tf32 128 x 256 x 8 per k step into two 256-column TMEM
+//    accumulators (Re, Im), and four epilogue warps read them back with
+//    tcgen05.ld and update C.
+// The 3xTF32 split: X = X_hi + X_lo, X_hi = X with the low 13 mantissa bits
+// cleared; A B ~= A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32.
+// Complex: Re C -= Ar Sr^T - Ai Si^T (negate-A bit), Im C -= Ar Si^T + Ai Sr^T.
+// All waits are bounded by wall-clock time and report a wait site.
+#include "cliqgpu_internal.h"
+#include "device_common.cuh"
+
+namespace cliqgpu {
+namespace tc2 {
+
+constexpr int kBM = 128, kBN = 256, kKS = 8;
+constexpr int kStages = 4;
+constexpr int kThreads = 192;                 // warps 0-3 epilogue, 4 TMA producer, 5 MMA issuer
+constexpr uint64_t kWaitNs = 200000000ull;
+
+template <bool C>
+struct Cfg {
+    static constexpr int kPlanes = C ? 4 : 2;                  // (re_hi, re_lo, im_hi, im_lo) or (hi, lo)
+    static constexpr int kABytes = kPlanes * kBM * kKS * 4;    // one A block: 128 rows
+    static constexpr int kBBytes = kPlanes * kBN * kKS * 4;    // one S block: 256 rows
+    static constexpr int kStage = kABytes + kBBytes;
+    static constexpr int kTmem = C ? 512 : 256;
+};
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t gns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t c) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(c) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int32_t* status, int site) {
+    if (mbar_try(b, parity)) return true;
+    const uint64_t t0 = gns();
+    while (!mbar_try(b, parity)) {
+        if (gns() - t0 > kWaitNs) {
+            atomicExch(&status[1], 1);
+            atomicCAS(&status[2], 0, site);
+            return false;
+        }
+    }
+    return true;
+}
+// 1-D bulk copy global -> shared, completion counted on the mbarrier
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(su32(dst)), "l"(src), "r"(bytes), "r"(su32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ uint64_t sdesc(uint32_t a, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool negA) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((negA ? 1u : 0u) << 13) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d), "l"(a), "l"(b), "r"(id), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* b) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+__device__ __forceinline__ uint32_t core_off(int row, int chunk) { return (row >> 3) * 256 + chunk * 128 + (row & 7) * 16; }
+
+// ---------------------------------------------------------------------------
+// pack: one CTA per (row tile, k step) block of one job; thread = row
+// ---------------------------------------------------------------------------
+template <bool C, bool CJ>
+__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+                                                   const float* __restrict__ L, const double* __restrict__ D,
+                                                   float* __restrict__ out) {
+    using X = V<float, C>;
+    using W = DV<C>;
+    const int64_t bid = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const PackJob jb = jobs[lo];
+    const int64_t blk = bid - prefix[lo];
+    const int nks = (jb.K + kKS - 1) / kKS;
+    const int tile = (int)(blk / nks), ks = (int)(blk % nks);
+    const int row = threadIdx.x;
+    if (row >= jb.tile_rows) return;
+    const int r = tile * jb.tile_rows + row;
+    float re[kKS], im[kKS];
+#pragma unroll
+    for (int q = 0; q < kKS; ++q) {
+        const int k = ks * kKS + q;
+        X v{};
+        if (r < jb.R && k < jb.K) {
+            v = ldv<float, C>(L, jb.src + r + (int64_t)k * jb.ld);
+            if (jb.d >= 0) v = conv<X>(reinterpret_cast<const W*>(D)[jb.d + k]) * opc<CJ>(v);
+        }
+        if constexpr (C) { re[q] = v.r; im[q] = v.i; } else { re[q] = v; im[q] = 0.f; }
+    }
+    const int planes = C ? 4 : 2;
+    const int64_t plane_bytes = (int64_t)jb.tile_rows * kKS * 4;
+    uint8_t* base = reinterpret_cast<uint8_t*>(out + jb.dst) + blk * plane_bytes * planes;
+    float h[kKS], l[kKS];
+#pragma unroll
+    for (int q = 0; q < kKS; ++q) { h[q] = tf32_hi(re[q]); l[q] = re[q] - h[q]; }
+    *reinterpret_cast<float4*>(base + 0 * plane_bytes + core_off(row, 0)) = make_float4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<float4*>(base + 0 * plane_bytes + core_off(row, 1)) = make_float4(h[4], h[5], h[6], h[7]);
+    *reinterpret_cast<float4*>(base + 1 * plane_bytes + core_off(row, 0)) = make_float4(l[0], l[1], l[2], l[3]);
+    *reinterpret_cast<float4*>(base + 1 * plane_bytes + core_off(row, 1)) = make_float4(l[4], l[5], l[6], l[7]);
+    if constexpr (C) {
+#pragma unroll
+        for (int q = 0; q < kKS; ++q) { h[q] = tf32_hi(im[q]); l[q] = im[q] - h[q]; }
+        *reinterpret_cast<float4*>(base + 2 * plane_bytes + core_off(row, 0)) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(base + 2 * plane_bytes + core_off(row, 1)) = make_float4(h[4], h[5], h[6], h[7]);
+        *reinterpret_cast<float4*>(base + 3 * plane_bytes + core_off(row, 0)) = make_float4(l[0], l[1], l[2], l[3]);
+        *reinterpret_cast<float4*>(base + 3 * plane_bytes + core_off(row, 1)) = make_float4(l[4], l[5], l[6], l[7]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// GEMM on packed operands
+// ---------------------------------------------------------------------------
+template <bool C>
+__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
+                                                              int nprobs, const float* __restrict__ pack, float* __restrict__ L,
+                                                              float* __restrict__ pool0, float* __restrict__ pool1,
+                                                              int32_t* __restrict__ status) {
+    using CF = Cfg<C>;
+    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * CF::kStage);
+    uint64_t* empty = full + kStages;
+    uint64_t* done = empty + kStages;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+
+    // tile of this CTA: 128-row tiles ti, 256-column tiles tj, needed when ti >= 2 tj
+    const int64_t bid = blockIdx.x;
+    int lo = 0, hi = nprobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const GemmProb pr = probs[lo];
+    int64_t t = bid - prefix[lo];
+    const int Mt = (pr.M + kBM - 1) / kBM, Nt = (pr.N + kBN - 1) / kBN;
+    int tj = 0;
+    while (tj < Nt && t >= Mt - 2 * tj) { t -= Mt - 2 * tj; ++tj; }
+    if (tj >= Nt) {
+        if (threadIdx.x == 0) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 5); }
+        return;
+    }
+    const int ti = 2 * tj + (int)t;
+    const int i0 = ti * kBM, j0 = tj * kBN;
+    const int nk = (pr.K + kKS - 1) / kKS;
+    const uint8_t* packA = reinterpret_cast<const uint8_t*>(pack + pr.packA) + (int64_t)ti * nk * CF::kABytes;
+    const uint8_t* packB = reinterpret_cast<const uint8_t*>(pack + pr.packB) + (int64_t)tj * nk * CF::kBBytes;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)), "r"(CF::kTmem) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 4) {
+        // ---- TMA producer ----
+        if (lane == 0) {
+            for (int it = 0; it < nk; ++it) {
+                const int s = it % kStages;
+                if (it >= kStages && !mbar_wait(&empty[s], ((it / kStages) - 1) & 1, status, 2)) break;
+                uint8_t* st = smem + s * CF::kStage;
+                mbar_expect_tx(&full[s], CF::kStage);
+                bulk_g2s(st, packA + (int64_t)it * CF::kABytes, CF::kABytes, &full[s]);
+                bulk_g2s(st + CF::kABytes, packB + (int64_t)it * CF::kBBytes, CF::kBBytes, &full[s]);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 5) {
+        // ---- MMA issuer ----
+        const uint32_t idp = idesc_tf32(kBM, kBN, false), idn = idesc_tf32(kBM, kBN, true);
+        const uint32_t dre = tmem, dim = tmem + kBN;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % kStages;
+            if (!mbar_wait(&full[s], (it / kStages) & 1, status, 1)) break;
+            tc_fence_after();
+            if (lane == 0) {
+                const uint32_t a = su32(smem + s * CF::kStage), b = a + CF::kABytes;
+                const uint32_t pa = kBM * kKS * 4, pb = kBN * kKS * 4;   // plane strides
+                auto A = [&](int p) { return sdesc(a + p * pa, 128, 256); };
+                auto B = [&](int p) { return sdesc(b + p * pb, 128, 256); };
+                const uint32_t acc = it > 0 ? 1u : 0u;
+                mma_tf32(dre, A(0), B(0), idp, acc);
+                mma_tf32(dre, A(0), B(1), idp, 1u);
+                mma_tf32(dre, A(1), B(0), idp, 1u);
+                if constexpr (C) {
+                    mma_tf32(dre, A(2), B(2), idn, 1u);
+                    mma_tf32(dre, A(2), B(3), idn, 1u);
+                    mma_tf32(dre, A(3), B(2), idn, 1u);
+                    mma_tf32(dim, A(0), B(2), idp, acc);
+                    mma_tf32(dim, A(0), B(3), idp, 1u);
+                    mma_tf32(dim, A(1), B(2), idp, 1u);
+                    mma_tf32(dim, A(2), B(0), idp, 1u);
+                    mma_tf32(dim, A(2), B(1), idp, 1u);
+                    mma_tf32(dim, A(3), B(0), idp, 1u);
+                }
+                mma_commit(&empty[s]);
+                if (it == nk - 1) mma_commit(done);
+            }
+            __syncwarp();
+        }
+    } else {
+        // ---- epilogue (warps 0-3 own TMEM lanes 32w .. 32w+31) ----
+        const bool ok = mbar_wait(done, 0, status, 3);
+        tc_fence_after();
+        if (ok) {
+            using X = V<float, C>;
+            float* Cb = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
+            const int i = i0 + warp * 32 + lane;
+            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+            const bool vrow = i < pr.M;
+#pragma unroll 1
+            for (int c0 = 0; c0 < kBN; c0 += 16) {
+                if (j0 + c0 >= pr.N || j0 + c0 > i0 + kBM - 1) break;   // warp-uniform: nothing left in this tile row block
+                float re[16], im[16];
+                tmem_ld16(lane_base + c0, re);
+                if constexpr (C) tmem_ld16(lane_base + kBN + c0, im);
+                if (vrow) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int j = j0 + c0 + q;
+                        if (j < pr.N && i >= j) {
+                            const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
+                            X cv = ldv<float, C>(Cb, e);
+                            if constexpr (C) { cv.r -= re[q]; cv.i -= im[q]; } else { cv -= re[q]; }
+                            stv<float, C>(Cb, e, cv);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(CF::kTmem) : "memory");
+    }
+}
+
+}  // namespace tc2
+
+size_t tc2_smem(bool cplx) {
+    return (size_t)tc2::kStages * (cplx ? tc2::Cfg<true>::kStage : tc2::Cfg<false>::kStage) + 1024 + 256;
+}
+
+// pack the launch's operands, then run the tensor-core GEMM
+int launch_tc2(Plan& P, const Launch& ln) {
+    float* L = reinterpret_cast<float*>(P.L);
+    float* p0 = reinterpret_cast<float*>(P.pool[0]);
+    float* p1 = reinterpret_cast<float*>(P.pool[1]);
+    float* pk = reinterpret_cast<float*>(P.pack);
+    const size_t smem = tc2_smem(P.cplx());
+    static bool attr[2] = {false, false};
+    const PackJob* jobs = P.packjobs + ln.pack_items;
+    const int64_t* jpre = P.prefix + ln.pack_prefix;
+    if (P.cplx()) {
+        if (P.conjugate)
+            tc2::pack_kernel<true, true><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+        else
+            tc2::pack_kernel<true, false><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+        if (!attr[1]) { cudaFuncSetAttribute(tc2::tc_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[1] = true; }
+        tc2::tc_gemm_kernel<true><<<(unsigned)ln.nblocks, tc2::kThreads, smem, P.stream>>>(
+            P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
+    } else {
+        tc2::pack_kernel<false, false><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+        if (!attr[0]) { cudaFuncSetAttribute(tc2::tc_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[0] = true; }
+        tc2::tc_gemm_kernel<false><<<(unsigned)ln.nblocks, tc2::kThreads, smem, P.stream>>>(
+            P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
+    }
+    P.total_launches += 1;   // the pack kernel (the caller counts the GEMM)
+    return CLIQ_OK;
+}
+
+}  // namespace cliqgpu
