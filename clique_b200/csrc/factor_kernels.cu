@@ -82,76 +82,100 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
 // the triangular solves.
 // ---------------------------------------------------------------------------
 template <class T, bool C, bool CJ>
-__global__ void __launch_bounds__(kThreads) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
-                                                            T* __restrict__ L, double* __restrict__ D, T* __restrict__ tinv,
-                                                            T* __restrict__ dinv, int32_t* __restrict__ status) {
+__global__ void __launch_bounds__(kThreads, 1) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
+                                                               T* __restrict__ L, double* __restrict__ D, T* __restrict__ tinv,
+                                                               T* __restrict__ dinv, int32_t* __restrict__ status) {
     using W = DV<C>;
     using X = V<T, C>;
-    constexpr int nb = kTile, ld = kTile + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    W* sA = reinterpret_cast<W*>(smem_raw);          // nb x ld, row-major
-    W* sX = sA + nb * ld;                              // inverse, nb x ld
-    W* sa = sX + nb * ld;                              // pivot column before scaling
-    W* sl = sa + nb;                                   // pivot column after scaling
+    constexpr int nb = kTile;
+    // thread (tr, tc) owns rows tr + 16a and columns tc + 16b (a, b < 4) of the
+    // block A and of the running inverse Xm, both held in registers
+    __shared__ W s_a[nb], s_l[nb], s_xr[nb], s_d[nb];
     const int4 it = items[blockIdx.x];
     const FrontDev f = F[it.x];
     const int slot = it.y;
     const int kb = min(nb, f.n - k);
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-        const int i = idx % kb, j = idx / kb;
-        W v{};
-        if (i >= j) v = conv<W>(ldv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m));
-        sA[i * ld + j] = v;
-        sX[i * ld + j] = (i == j) ? vone<W>() : W{};
-    }
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    W A[4][4], Xm[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int i = tr + 16 * a, c = tc + 16 * b;
+            W v{};
+            if (i < kb && c < kb && i >= c) v = conv<W>(ldv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m));
+            A[a][b] = v;
+            Xm[a][b] = (i == c) ? vone<W>() : W{};
+            if (i == c && i < kb) s_d[i] = v;
+        }
     __syncthreads();
     for (int j = 0; j < kb; ++j) {
-        const W d = sA[j * ld + j];
+        const W d = s_d[j];
         if (threadIdx.x == 0 && is_zero(d)) atomicMin(&status[0], f.off + k + j + 1);
         const W rd = vone<W>() / d;
-        for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) {
-            const W a = sA[i * ld + j];
-            const W l = a * rd;
-            sa[i] = a;
-            sl[i] = l;
-            sA[i * ld + j] = l;
-        }
+        // publish the pivot column (scaled and unscaled) and row j of the inverse
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int i = tr + 16 * a, c = tc + 16 * b;
+                if (c == j && i > j && i < kb) {
+                    const W l = A[a][b] * rd;
+                    s_a[i] = A[a][b];
+                    s_l[i] = l;
+                    A[a][b] = l;
+                }
+                if (i == j && c <= j) s_xr[c] = Xm[a][b];
+            }
         __syncthreads();
-        const int r = kb - 1 - j;            // rows below the pivot
-        for (int idx = threadIdx.x; idx < r * kb; idx += blockDim.x) {
-            const int i = j + 1 + idx % r, c = idx / r;
-            if (c > j) {
-                if (i >= c) sA[i * ld + c] -= sl[i] * opc<CJ>(sa[c]);
-            } else {
-                sX[i * ld + c] -= sl[i] * sX[j * ld + c];
+        W la[4], ab[4], xb[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = tr + 16 * a;
+            la[a] = (i > j && i < kb) ? s_l[i] : W{};
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int c = tc + 16 * b;
+            ab[b] = (c > j && c < kb) ? opc<CJ>(s_a[c]) : W{};
+            xb[b] = (c <= j) ? s_xr[c] : W{};
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int i = tr + 16 * a, c = tc + 16 * b;
+                if (i > j && i < kb) {
+                    if (c > j) {
+                        if (i >= c) A[a][b] -= la[a] * ab[b];
+                    } else {
+                        Xm[a][b] -= la[a] * xb[b];
+                    }
+                    if (i == j + 1 && c == j + 1) s_d[j + 1] = A[a][b];
+                }
+            }
+        __syncthreads();
+    }
+    // outputs: U = op(L11^{-1})^T (row-major, for the panel), L11^{-1}
+    // (column-major, for the solves), L11 with unit diagonal, and D
+    X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
+    X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)(k / nb) * nb * nb;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int i = tr + 16 * a, c = tc + 16 * b;
+            const bool in = i < kb && c < kb && i >= c;
+            U[c * nb + i] = in ? conv<X>(opc<CJ>(Xm[a][b])) : X{};
+            Dv[i + c * nb] = in ? conv<X>(Xm[a][b]) : X{};
+            if (in) {
+                if (i > c) stv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m, conv<X>(A[a][b]));
+                else {
+                    stv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m, vone<X>());
+                    reinterpret_cast<W*>(D)[f.off + k + i] = A[a][b];
+                }
             }
         }
-        __syncthreads();
-    }
-    // U = op(L11^{-1})^T row-major (upper unit) into the step's slot
-    X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
-    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-        const int t = idx / nb, c = idx % nb;
-        X v{};
-        if (t < kb && c < kb && t <= c) v = conv<X>(opc<CJ>(sX[c * ld + t]));
-        U[idx] = v;
-    }
-    // L11^{-1} (column-major nb x nb) for the solves
-    X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)(k / nb) * nb * nb;
-    for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-        const int i = idx % nb, c = idx / nb;
-        X v{};
-        if (i < kb && c < kb && i >= c) v = conv<X>(sX[i * ld + c]);
-        Dv[idx] = v;
-    }
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-        const int i = idx % kb, j = idx / kb;
-        if (i > j) stv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m, conv<X>(sA[i * ld + j]));
-        else if (i == j) {
-            stv<T, C>(L, f.L + (k + i) + (int64_t)(k + j) * f.m, vone<X>());
-            reinterpret_cast<W*>(D)[f.off + k + j] = sA[j * ld + j];
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -289,8 +313,14 @@ __global__ void __launch_bounds__(kThreads) gemm_update_kernel(const GemmProb* _
         for (int a = 0; a < 4; ++a) {
             const int i = i0 + ty + 16 * a;
             if (i < pr.M && i >= j) {
+                // one reduction per element per launch: same result as load-subtract-store
                 const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
-                stv<T, C>(Cbase, e, ldv<T, C>(Cbase, e) - acc[a][b]);
+                if constexpr (C) {
+                    atomicAdd(Cbase + 2 * e, -acc[a][b].r);
+                    atomicAdd(Cbase + 2 * e + 1, -acc[a][b].i);
+                } else {
+                    atomicAdd(Cbase + e, -acc[a][b]);
+                }
             }
         }
     }
@@ -303,11 +333,10 @@ template <class T, bool C, bool CJ>
 static int run_factor_impl(Plan& P) {
     using X = V<T, C>;
     using W = DV<C>;
-    const size_t smem_diag = sizeof(W) * (2 * kTile * (kTile + 1) + 2 * kTile);
+    const size_t smem_diag = 0;
     const size_t smem_panel = sizeof(X) * (kTile * kTile + kTile * (kTile + 1) + kTile);
     static bool attr_done = false;
     if (!attr_done) {
-        cudaFuncSetAttribute(diag_ldl_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag);
         cudaFuncSetAttribute(panel_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel);
         attr_done = true;
     }

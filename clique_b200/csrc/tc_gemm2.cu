@@ -109,6 +109,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
+// C -= v without reading C: one reduction per element per launch, so the
+// result equals the load-subtract-store it replaces (same rounding, no race)
+__device__ __forceinline__ void red_sub(float* p, float v) {
+    asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(-v) : "memory");
+}
+__device__ __forceinline__ void red_sub2(float* p, float re, float im) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(-re), "f"(-im) : "memory");
+}
+
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 __device__ __forceinline__ uint32_t core_off(int row, int chunk) { return (row >> 3) * 256 + chunk * 128 + (row & 7) * 16; }
 
@@ -270,7 +279,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
         const bool ok = mbar_wait(done, 0, status, 3);
         tc_fence_after();
         if (ok) {
-            using X = V<float, C>;
             float* Cb = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
             const int i = i0 + warp * 32 + lane;
             const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
@@ -287,9 +295,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
                         const int j = j0 + c0 + q;
                         if (j < pr.N && i >= j) {
                             const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
-                            X cv = ldv<float, C>(Cb, e);
-                            if constexpr (C) { cv.r -= re[q]; cv.i -= im[q]; } else { cv -= re[q]; }
-                            stv<float, C>(Cb, e, cv);
+                            if constexpr (C) red_sub2(Cb + 2 * e, re[q], im[q]);
+                            else red_sub(Cb + e, re[q]);
                         }
                     }
                 }
