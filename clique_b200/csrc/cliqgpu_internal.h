@@ -104,6 +104,7 @@ struct SolveLevel {
     int64_t bwd_items;
     int32_t nbwd;
     int32_t depth;
+    int32_t gather_chunks;   // 1024-row chunks of the level's tallest front (gather grid y)
 };
 
 // ---------------------------------------------------------------------------

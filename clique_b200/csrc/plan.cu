@@ -399,6 +399,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         sl.fronts = (int64_t)level_fronts.size();
         for (int s : P.level_list[d]) level_fronts.push_back(s);
         sl.nfronts = (int32_t)P.level_list[d].size();
+        sl.gather_chunks = 1;
+        for (int s : P.level_list[d]) sl.gather_chunks = std::max(sl.gather_chunks, (P.hfronts[s].m + 1023) / 1024);
         sl.fwd_items = (int64_t)items.size() / 4;
         for (int s : P.level_list[d]) {
             FrontDev& f = P.hfronts[s];

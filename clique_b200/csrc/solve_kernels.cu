@@ -28,6 +28,7 @@ namespace cliqgpu {
 
 constexpr int kSolveThreads = 256;
 constexpr int kMaxRhsChunk = 16;     // right-hand sides per sweep
+constexpr int kGatherRows = 1024;    // front rows per gather CTA (grid y of the gather launch)
 constexpr uint64_t kSpinNs = 500000000ull;   // 0.5 s bound on any single wait
 
 __device__ __forceinline__ int ld_acquire(const int32_t* p) {
@@ -67,6 +68,27 @@ __device__ __forceinline__ void publish_flag(int32_t* flag, int epoch) {
     if (threadIdx.x == 0) atomicExch(flag, epoch);
 }
 
+// A 64 x 64 tile of a front, loaded into registers one step ahead of its use
+// (L does not depend on the chain flags, so its load overlaps the waits).
+constexpr int kPre = kTile * kTile / kSolveThreads;   // 16 elements per thread
+template <class T, bool C>
+__device__ __forceinline__ void tile_fetch(V<T, C>* pre, const T* L, const FrontDev& f, int r0, int nr, int c0, int nc) {
+#pragma unroll
+    for (int q = 0; q < kPre; ++q) {
+        const int idx = threadIdx.x + kSolveThreads * q;
+        const int rr = idx % kTile, cc = idx / kTile;
+        pre[q] = (rr < nr && cc < nc) ? ldv<T, C>(L, f.L + (r0 + rr) + (int64_t)(c0 + cc) * f.m) : V<T, C>{};
+    }
+}
+template <class X>
+__device__ __forceinline__ void tile_store(X* sL, const X* pre) {
+#pragma unroll
+    for (int q = 0; q < kPre; ++q) {
+        const int idx = threadIdx.x + kSolveThreads * q;
+        sL[(idx % kTile) * (kTile + 1) + idx / kTile] = pre[q];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // forward gather: X_T += children's W_B (rows < n), W_B := children's W_B
 // ---------------------------------------------------------------------------
@@ -76,13 +98,16 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_gather_kernel(const FrontDe
                                                                    const int32_t* __restrict__ cmaps, int nrhs) {
     using Xv = V<T, C>;
     const FrontDev f = F[fl[blockIdx.x]];
+    const int i0 = blockIdx.y * kGatherRows;       // this CTA's chunk of the front's rows
+    if (i0 >= f.m) return;
+    const int ni = min(kGatherRows, f.m - i0);
     T* wb = f.pool == 0 ? w0 : w1;
     const T* cw = f.pool == 0 ? w1 : w0;
     const int32_t* lm = f.cmap >= 0 ? cmaps + f.cmap : nullptr;
     const int32_t* rm = lm ? lm + f.m : nullptr;
-    const int64_t total = (int64_t)f.m * nrhs;
+    const int64_t total = (int64_t)ni * nrhs;
     for (int64_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int i = (int)(idx % f.m), j = (int)(idx / f.m);
+        const int i = i0 + (int)(idx % ni), j = (int)(idx / ni);
         if (i < f.n && !lm) continue;
         Xv v{};
         if (lm) {
@@ -130,13 +155,13 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_chain_kernel(const FrontDev
 #pragma unroll
     for (int a = 0; a < kMaxRhsChunk / 4; ++a) acc[a] = Xv{};
     const int cb_end = min(rb, nT);
+    Xv pre[kPre];
+    if (cb_end > 0) tile_fetch<T, C>(pre, L, f, r0, rows, 0, min(kTile, f.n));
     for (int cb = 0; cb < cb_end; ++cb) {
-        if (!wait_flag(&flags[f.flag_base + cb], epoch, status)) break;
         const int c0 = kTile * cb, ncols = min(kTile, f.n - c0);
-        for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
-            const int rr = idx % kTile, cc = idx / kTile;
-            sL[rr * ldl + cc] = (rr < rows && cc < ncols) ? ldv<T, C>(L, f.L + (r0 + rr) + (int64_t)(c0 + cc) * f.m) : Xv{};
-        }
+        tile_store(sL, pre);
+        if (cb + 1 < cb_end) tile_fetch<T, C>(pre, L, f, r0, rows, c0 + kTile, min(kTile, f.n - c0 - kTile));
+        if (!wait_flag(&flags[f.flag_base + cb], epoch, status)) break;
         for (int idx = threadIdx.x; idx < kTile * nrhs; idx += blockDim.x) {
             const int cc = idx % kTile, j = idx / kTile;
             sx[cc * kMaxRhsChunk + j] = cc < ncols ? ldv_cg<T, C>(X, f.off + c0 + cc + (int64_t)j * ldx) : Xv{};
@@ -264,12 +289,13 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev
 #pragma unroll
     for (int a = 0; a < kMaxRhsChunk / 4; ++a) acc[a] = Xv{};
     // rows below the pivots: x gathered from the (final) ancestor entries
+    Xv pre[kPre];
+    if (f.n < f.m) tile_fetch<T, C>(pre, L, f, f.n, min(kTile, f.m - f.n), c0, dcols);
     for (int rr0 = f.n; rr0 < f.m; rr0 += kTile) {
         const int nr = min(kTile, f.m - rr0);
-        for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
-            const int rr = idx % kTile, cc = idx / kTile;
-            sL[rr * ldl + cc] = (rr < nr && cc < dcols) ? ldv<T, C>(L, f.L + (rr0 + rr) + (int64_t)(c0 + cc) * f.m) : Xv{};
-        }
+        tile_store(sL, pre);
+        if (rr0 + kTile < f.m) tile_fetch<T, C>(pre, L, f, rr0 + kTile, min(kTile, f.m - rr0 - kTile), c0, dcols);
+        else if (nT - 1 > rb) tile_fetch<T, C>(pre, L, f, kTile * (nT - 1), min(kTile, f.n - kTile * (nT - 1)), c0, dcols);
         for (int idx = threadIdx.x; idx < kTile * nrhs; idx += blockDim.x) {
             const int rr = idx % kTile, j = idx / kTile;
             Xv v{};
@@ -288,14 +314,13 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev
         }
         __syncthreads();
     }
+    if (f.n >= f.m && nT - 1 > rb) tile_fetch<T, C>(pre, L, f, kTile * (nT - 1), min(kTile, f.n - kTile * (nT - 1)), c0, dcols);
     // later pivot blocks of this front
     for (int ib = nT - 1; ib > rb; --ib) {
-        if (!wait_flag(&flags[f.flag_base + ib], epoch, status)) break;
         const int rr0 = kTile * ib, nr = min(kTile, f.n - rr0);
-        for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
-            const int rr = idx % kTile, cc = idx / kTile;
-            sL[rr * ldl + cc] = (rr < nr && cc < dcols) ? ldv<T, C>(L, f.L + (rr0 + rr) + (int64_t)(c0 + cc) * f.m) : Xv{};
-        }
+        tile_store(sL, pre);
+        if (ib - 1 > rb) tile_fetch<T, C>(pre, L, f, rr0 - kTile, kTile, c0, dcols);
+        if (!wait_flag(&flags[f.flag_base + ib], epoch, status)) break;
         for (int idx = threadIdx.x; idx < kTile * nrhs; idx += blockDim.x) {
             const int rr = idx % kTile, j = idx / kTile;
             sx[rr * kMaxRhsChunk + j] = rr < nr ? ldv_cg<T, C>(X, f.off + rr0 + rr + (int64_t)j * ldx) : Xv{};
@@ -374,7 +399,7 @@ static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
         for (int d = P.max_depth; d >= 0; --d) {
             const SolveLevel& lv = P.solve_levels[d];
             if (lv.nfronts == 0) continue;
-            fwd_gather_kernel<T, C><<<lv.nfronts, kSolveThreads, 0, P.stream>>>(P.fronts, P.level_fronts + lv.fronts, X, P.n, w0, w1,
+            fwd_gather_kernel<T, C><<<dim3(lv.nfronts, lv.gather_chunks), kSolveThreads, 0, P.stream>>>(P.fronts, P.level_fronts + lv.fronts, X, P.n, w0, w1,
                                                                                P.cmaps, nrhs);
             ++launches;
             if (lv.nfwd > 0) {
