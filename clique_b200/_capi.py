@@ -61,6 +61,8 @@ _SIGS = {
     "cliqgpu_last_error": (C.c_char_p, []),
     "cliqgpu_front_ldl": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
                                     C.c_void_p, C.c_int64, C.c_void_p]),
+    "cliqgpu_front_ldl_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                            C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]),
 }
 
 _lib = None

@@ -21,6 +21,9 @@
 //      reference's n/nb rank-nb Trrk passes (same sum, one pass over ABR).
 // D is kept in FP64 for every storage precision.
 #include <climits>
+#include <mutex>
+#include <string>
+#include <vector>
 #include <cstdio>
 #include <type_traits>
 
@@ -396,3 +399,230 @@ template int run_factor<double, false>(Plan&);
 template int run_factor<double, true>(Plan&);
 
 }  // namespace cliqgpu
+
+
+// ===========================================================================
+// cliqgpu_front_ldl_noalloc: FrontLDL on one dense front without any device
+// allocation.
+//
+// Some callers cannot allocate device memory while they run: code that owns
+// its memory pool and forbids cudaMalloc / cudaFree during a solve phase (a
+// cudaFree synchronises the whole device), or code running inside another
+// library's critical section.  For them this entry point keeps all of its
+// scratch -- D, the inverse diagonal blocks, the work descriptors and the
+// status word -- in one file-scope device array of fixed size, and otherwise
+// runs the same diagonal-block, panel and CUDA-core update kernels as the
+// tree factorization (plain right-looking 64-column steps, Schur update with
+// K = n).  The caller passes the front in place: AL (m x n, leading dimension
+// exactly m) and ABR ((m-n) x (m-n), leading dimension >= m-n).
+//
+// Limits: n <= 1024 pivots and m <= 16384 rows.  The array (about 1.2 MB)
+// is held by every GPU that loads the library until the process exits.  The
+// first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that
+// first call before any stream capture.  All calls share the array and it
+// keeps the previous call's contents, so calls that overlap on the GPU (other
+// streams, other host threads) race: serialise them.
+// ===========================================================================
+namespace cliqgpu {
+namespace noalloc {
+
+constexpr int kMaxN = 1024;
+constexpr int kMaxM = 16384;
+constexpr int kMaxSteps = kMaxN / kTile;
+constexpr int kMaxItems = kMaxSteps * (1 + (kMaxM + kTile - 1) / kTile);
+constexpr int kMaxProbs = kMaxSteps + 1;
+constexpr size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+// byte offsets inside the scratch array (sized for complex FP64, the widest element)
+constexpr size_t kOffStatus = 0;
+constexpr size_t kOffFront = align256(kOffStatus + 4 * sizeof(int32_t));
+constexpr size_t kOffD = align256(kOffFront + sizeof(FrontDev));
+constexpr size_t kOffTinv = align256(kOffD + (size_t)kMaxN * 16);
+constexpr size_t kOffDinv = align256(kOffTinv + (size_t)kTile * kTile * 16);
+constexpr size_t kOffItems = align256(kOffDinv + (size_t)kMaxSteps * kTile * kTile * 16);
+constexpr size_t kOffProbs = align256(kOffItems + (size_t)kMaxItems * sizeof(int4));
+constexpr size_t kOffPrefix = align256(kOffProbs + (size_t)kMaxProbs * sizeof(GemmProb));
+constexpr size_t kBytes = align256(kOffPrefix + (size_t)kMaxProbs * sizeof(int64_t));
+
+static __device__ __align__(256) unsigned char g_scratch[kBytes];
+
+// device address of g_scratch per device, looked up once with that device current
+static std::mutex g_mu;
+static void* g_addr[64] = {nullptr};
+
+static int scratch_address(void** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda("front_ldl_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= 64) {
+        set_last_error("front_ldl_noalloc: device ordinal out of range");
+        return CLIQ_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            set_last_error(std::string("front_ldl_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+            return CLIQ_ERR_CUDA;
+        }
+        g_addr[dev] = p;
+    }
+    *out = g_addr[dev];
+    return CLIQ_OK;
+}
+
+template <class T, bool C>
+__global__ void put_diag(T* __restrict__ A, int64_t lda, int n, const double* __restrict__ D) {
+    using W = DV<C>;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        stv<T, C>(A, j + (int64_t)j * lda, conv<V<T, C>>(reinterpret_cast<const W*>(D)[j]));
+}
+
+// one 64-column step: diagonal block, panel row blocks, trailing update (if any)
+struct Step {
+    int k;
+    int64_t diag_item, panel_item;
+    int panel_blocks;
+    int prob;            // index of the trailing update problem, -1 if none
+    int64_t tiles;
+};
+
+template <class T, bool C, bool CJ>
+static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const std::vector<Step>& steps, int schur_prob,
+                       int64_t schur_tiles, cudaStream_t st) {
+    using X = V<T, C>;
+    const size_t smem_panel = sizeof(X) * (kTile * kTile + kTile * (kTile + 1) + kTile);
+    cudaFuncSetAttribute(panel_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel);
+    const FrontDev* F = reinterpret_cast<const FrontDev*>(base + kOffFront);
+    double* D = reinterpret_cast<double*>(base + kOffD);
+    T* tinv = reinterpret_cast<T*>(base + kOffTinv);
+    T* dinv = reinterpret_cast<T*>(base + kOffDinv);
+    const int4* items = reinterpret_cast<const int4*>(base + kOffItems);
+    const GemmProb* probs = reinterpret_cast<const GemmProb*>(base + kOffProbs);
+    const int64_t* prefix = reinterpret_cast<const int64_t*>(base + kOffPrefix);
+    int32_t* status = reinterpret_cast<int32_t*>(base + kOffStatus);
+    for (const Step& s : steps) {
+        diag_ldl_kernel<T, C, CJ><<<1, kThreads, 0, st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, status);
+        if (s.panel_blocks > 0)
+            panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv);
+        if (s.prob >= 0)
+            gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, AL, ABR,
+                                                                               ABR, D);
+    }
+    if (schur_prob >= 0)
+        gemm_update_kernel<T, C, CJ><<<(unsigned)schur_tiles, kThreads, 0, st>>>(probs + schur_prob, prefix + schur_prob, 1, AL,
+                                                                               ABR, ABR, D);
+    put_diag<T, C><<<(n + 255) / 256, 256, 0, st>>>(AL, (int64_t)m, n, D);
+}
+
+}  // namespace noalloc
+}  // namespace cliqgpu
+
+using namespace cliqgpu;
+
+extern "C" int cliqgpu_front_ldl_noalloc(int32_t field, int32_t precision, int32_t conjugate, int32_t m, int32_t n, void* AL,
+                                         int64_t lda, void* ABR, int64_t ldabr, void* stream) {
+    using namespace noalloc;
+    if (m < 0 || n < 0 || n > m || !AL || (m > n && (!ABR || ldabr < m - n))) {
+        set_last_error("front_ldl_noalloc: invalid sizes or pointers");
+        return CLIQ_ERR_ARG;
+    }
+    if (n > kMaxN || m > kMaxM) {
+        set_last_error("front_ldl_noalloc: front too large for the fixed scratch (n <= " + std::to_string(kMaxN) +
+                       ", m <= " + std::to_string(kMaxM) + ")");
+        return CLIQ_ERR_ARG;
+    }
+    if (lda != m) {
+        set_last_error("front_ldl_noalloc: AL must be stored with leading dimension m");
+        return CLIQ_ERR_ARG;
+    }
+    if (n == 0) return CLIQ_OK;
+    void* scratch = nullptr;
+    int st = scratch_address(&scratch);
+    if (st != CLIQ_OK) return st;
+    unsigned char* base = reinterpret_cast<unsigned char*>(scratch);
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool cplx = field == CLIQ_COMPLEX;
+    const bool fp32 = precision == CLIQ_FP32;
+    const int u = m - n;
+
+    // host-side schedule for the single front (the whole tree has one node)
+    FrontDev f{};
+    f.L = 0; f.U = 0; f.CU[0] = f.CU[1] = -1; f.cmap = -1; f.lower = 0; f.W = 0;
+    f.m = m; f.n = n; f.off = 0; f.u = u; f.pool = 0; f.flag_base = 0; f.dinv = 0;
+    std::vector<int4> items;
+    std::vector<GemmProb> probs;
+    std::vector<int64_t> prefix;
+    std::vector<Step> steps;
+    auto tiles_of = [](int M, int N) -> int64_t {
+        const int64_t Mt = (M + kTile - 1) / kTile, Nt = (N + kTile - 1) / kTile;
+        return Nt * Mt - Nt * (Nt - 1) / 2;
+    };
+    for (int k = 0; k < n; k += kTile) {
+        Step sp{};
+        sp.k = k;
+        const int kb = std::min(kTile, n - k);
+        sp.diag_item = (int64_t)items.size();
+        items.push_back(make_int4(0, 0, 0, 0));
+        sp.panel_item = (int64_t)items.size();
+        const int rows = m - k - kb;
+        for (int rb = 0; rb * kTile < rows; ++rb) items.push_back(make_int4(0, 0, rb, 0));
+        sp.panel_blocks = (int)(items.size() - sp.panel_item);
+        const int N = n - k - kb;
+        sp.prob = -1;
+        if (N > 0) {
+            GemmProb pr{};
+            pr.A = (k + kb) + (int64_t)k * m;
+            pr.B = pr.A;
+            pr.C = (k + kb) + (int64_t)(k + kb) * m;
+            pr.d = k;
+            pr.lda = m; pr.ldc = m; pr.M = rows; pr.N = N; pr.K = kb; pr.cpool = -1;
+            sp.prob = (int)probs.size();
+            sp.tiles = tiles_of(pr.M, pr.N);
+            probs.push_back(pr);
+            prefix.push_back(0);
+        }
+        steps.push_back(sp);
+    }
+    int schur_prob = -1;
+    int64_t schur_tiles = 0;
+    if (u > 0) {
+        GemmProb pr{};
+        pr.A = n; pr.B = n; pr.C = 0; pr.d = 0;
+        pr.lda = m; pr.ldc = (int32_t)ldabr; pr.M = u; pr.N = u; pr.K = n; pr.cpool = 0;
+        schur_prob = (int)probs.size();
+        schur_tiles = tiles_of(u, u);
+        probs.push_back(pr);
+        prefix.push_back(0);
+    }
+    // descriptors and a cleared status word into the scratch array (no allocation)
+    const int32_t st0[4] = {INT_MAX, 0, 0, 0};
+    cudaMemcpyAsync(base + kOffStatus, st0, sizeof(st0), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(base + kOffFront, &f, sizeof(f), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(base + kOffItems, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, s);
+    if (!probs.empty()) {
+        cudaMemcpyAsync(base + kOffProbs, probs.data(), sizeof(GemmProb) * probs.size(), cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(base + kOffPrefix, prefix.data(), sizeof(int64_t) * prefix.size(), cudaMemcpyHostToDevice, s);
+    }
+    if (fp32) {
+        if (cplx && conjugate) launch_all<float, true, true>(base, m, n, (float*)AL, (float*)ABR, steps, schur_prob, schur_tiles, s);
+        else if (cplx) launch_all<float, true, false>(base, m, n, (float*)AL, (float*)ABR, steps, schur_prob, schur_tiles, s);
+        else launch_all<float, false, false>(base, m, n, (float*)AL, (float*)ABR, steps, schur_prob, schur_tiles, s);
+    } else {
+        if (cplx && conjugate) launch_all<double, true, true>(base, m, n, (double*)AL, (double*)ABR, steps, schur_prob, schur_tiles, s);
+        else if (cplx) launch_all<double, true, false>(base, m, n, (double*)AL, (double*)ABR, steps, schur_prob, schur_tiles, s);
+        else launch_all<double, false, false>(base, m, n, (double*)AL, (double*)ABR, steps, schur_prob, schur_tiles, s);
+    }
+    st = check_cuda("front_ldl_noalloc");
+    if (st != CLIQ_OK) return st;
+    int32_t out[4];
+    if (cudaMemcpyAsync(out, base + kOffStatus, sizeof(out), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return check_cuda("front_ldl_noalloc: status");
+    if (out[1]) {
+        set_last_error("front_ldl_noalloc: a device-side wait timed out");
+        return CLIQ_ERR_TIMEOUT;
+    }
+    return out[0] == INT_MAX ? CLIQ_OK : CLIQ_ERR_ZERO_PIVOT;
+}

@@ -203,6 +203,21 @@ const char* cliqgpu_last_error(void);
 int cliqgpu_front_ldl(int32_t field, int32_t precision, int32_t conjugate, int32_t m, int32_t n,
                       void* AL, int64_t lda, void* ABR, int64_t ldabr, void* stream);
 
+/* The same dense partial LDL^T of one front for callers that must not
+ * allocate device memory during the call -- for example an application that
+ * manages its own memory pool and bans cudaMalloc/cudaFree inside its solve
+ * phase (cudaFree synchronises the whole device), or code running under
+ * another library's allocation lock.  All scratch lives in one fixed device
+ * array inside the library (about 1.2 MB, held on every GPU that loads the
+ * library until exit); nothing is allocated or freed.  Limits: n <= 1024,
+ * m <= 16384, lda == m, ldabr >= m - n; larger fronts return CLIQ_ERR_ARG.
+ * The first call on a device looks up the array's address (do it before any
+ * stream capture).  Calls share the array, so calls that overlap on the GPU
+ * race; serialise them.  Uses the CUDA-core update kernel in every precision.
+ * No counterpart in the reference (Clique allocates freely in FrontLDL). */
+int cliqgpu_front_ldl_noalloc(int32_t field, int32_t precision, int32_t conjugate, int32_t m, int32_t n,
+                              void* AL, int64_t lda, void* ABR, int64_t ldabr, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
