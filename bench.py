@@ -37,7 +37,7 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--n", type=int, default=100)
+    p.add_argument("--grid", dest="n", type=int, default=100, help="grid points per axis")
     p.add_argument("--nrhs", type=int, default=4)
     p.add_argument("--cutoff", type=int, default=128)
     p.add_argument("--tol", type=float, default=1e-10)
@@ -100,6 +100,39 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def rank_env():
+    """(rank, world, local_rank) from the torchrun environment (1 process when absent)."""
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def dist_init(backend):
+    """Process group for a multi-rank launch (None for one process).  Every rank
+    solves its own replica; the group carries only barriers and the timing max."""
+    _, world, _ = rank_env()
+    if world == 1:
+        return None
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(value, dist, device="cpu"):
+    """Slowest rank's value: the job's time is set by its last replica."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -150,7 +183,7 @@ def cpu_run(n, nrhs, cutoff, seed, threads):
 
 def cpu_baseline(args, target_n):
     threads = os.cpu_count() or 1
-    n0 = 30
+    n0 = min(30, target_n)
     t0, _ = cpu_run(n0, args.nrhs, args.cutoff, args.seed, threads)
     rate = cpu_flops(n0, args.cutoff) / t0
     # largest sample grid whose estimated time fits the budget (flops grow like n^6)
@@ -167,8 +200,8 @@ def cpu_baseline(args, target_n):
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    # rank 0 alone runs the CPU arm; the other ranks of a torchrun launch exit 0 without work
+    if rank_env()[0] != 0:
         return
     vals = []
     cb = None
@@ -194,15 +227,9 @@ def run_ours(args):
     import torch
     import clique_b200 as cliq
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = rank_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dist = dist_init("nccl")
 
     A, B, omega = workload(args.n, args.nrhs, args.seed)
     n = args.n
@@ -223,21 +250,17 @@ def run_ours(args):
         phase_ev[2].record()
         return it, rr
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
     for _ in range(args.warmup):
         it, rr = step32()
     torch.cuda.synchronize()
-    barrier()
+    barrier(dist)
     # CUDA events around every factorization launch during the timed steps
     L32.set_profiling(True)
     launches0 = L32.total_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
-        barrier()
+        barrier(dist)
         ev0.record()
         its, rrs = [], []
         for _ in range(args.steps):
@@ -245,12 +268,9 @@ def run_ours(args):
             its.append(it); rrs.append(rr)
         ev1.record()
         torch.cuda.synchronize()
-    barrier()
+    barrier(dist)
     ms = ev0.elapsed_time(ev1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     factor_flops = L32.FactorizationWork()
     launches = (L32.total_launches() - launches0) // args.steps
     prof = L32.profile()
@@ -282,6 +302,7 @@ def run_ours(args):
     for _ in range(args.steps):
         Xh, ith, rrh = step_host()
     e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = max_over_ranks(e2e_s, dist, "cuda")
     del L32h
 
     fp64 = None
@@ -304,6 +325,7 @@ def run_ours(args):
         ev1.record()
         torch.cuda.synchronize()
         fp64_ms = ev0.elapsed_time(ev1) / args.steps
+        fp64_ms = max_over_ranks(fp64_ms, dist, "cuda")
         Xc = X64.cpu().numpy()
         res64 = float(np.linalg.norm(A.to_scipy() @ Xc - B) / np.linalg.norm(B))
         p64 = L64.profile()
