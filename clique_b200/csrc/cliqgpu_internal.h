@@ -41,6 +41,12 @@ void set_last_error(const std::string& msg);
 // ---------------------------------------------------------------------------
 constexpr int kTile = 64;        // rows per solve block, GEMM tile edge
 constexpr int kEACols = 16;      // columns per extend-add work item
+// Triangular sweeps: the chain CTA of a front adds the contributions of the
+// kSolveLag newest solved blocks itself; workers add the older ones.
+constexpr int kSolveLag = 1;
+constexpr int kSolveRhsChunk = 16;   // right-hand sides per sweep (partial-sum stride)
+// sweep work items {front, kind, block, 0}
+enum SweepItem : int { kItemChain = 0, kItemPivotRows = 1, kItemLowerRows = 2, kItemColumns = 1 };
 
 // One front as the kernels see it.  Offsets are in elements (a complex
 // element is two scalars).
@@ -138,6 +144,9 @@ struct Plan {
     void* pool[2] = {nullptr, nullptr};
     void* tinv = nullptr;         // U = op(L11^{-1})^T of each front of one panel step (storage precision)
     void* dinv = nullptr;         // L11^{-1} of every 64-block of every front, kept for the solves
+    void* dinvT = nullptr;        // the same blocks row-major (backward sweep)
+    void* subT = nullptr;         // per pivot block b: tile (b+1, b) of the front's L, row-major (backward sweep)
+    void* partial = nullptr;      // per pivot block: 64 x kSolveRhsChunk partial sums from the sweep workers
     int64_t dinv_elems = 0;
     FrontDev* fronts = nullptr;
     int32_t* cmaps = nullptr;
@@ -151,7 +160,7 @@ struct Plan {
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;
-    int32_t* flags = nullptr;
+    int32_t* flags = nullptr;     // 2 * flags_total: solved-block flags, then partial-sum flags
     int32_t* tickets = nullptr;
     int32_t* status = nullptr;    // [0] first zero pivot + 1 (min), [1] timeout flag
     int64_t* rowptr = nullptr;    // FP64 matrix (keep_matrix)

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
 template <class T, bool C, bool CJ>
 __global__ void __launch_bounds__(kThreads, 1) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
                                                                T* __restrict__ L, double* __restrict__ D, T* __restrict__ tinv,
-                                                               T* __restrict__ dinv, int32_t* __restrict__ status) {
+                                                               T* __restrict__ dinv, T* __restrict__ dinvT, int32_t* __restrict__ status) {
     using W = DV<C>;
     using X = V<T, C>;
     constexpr int nb = kTile;
@@ -160,9 +160,11 @@ __global__ void __launch_bounds__(kThreads, 1) diag_ldl_kernel(const FrontDev* _
         __syncthreads();
     }
     // outputs: U = op(L11^{-1})^T (row-major, for the panel), L11^{-1}
-    // (column-major, for the solves), L11 with unit diagonal, and D
+    // (column-major for the forward sweep, row-major for the backward sweep),
+    // L11 with unit diagonal, and D
     X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
     X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)(k / nb) * nb * nb;
+    X* DvT = dinvT ? reinterpret_cast<X*>(dinvT) + f.dinv + (int64_t)(k / nb) * nb * nb : nullptr;
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(kThreads, 1) diag_ldl_kernel(const FrontDev* _
             const bool in = i < kb && c < kb && i >= c;
             U[c * nb + i] = in ? conv<X>(opc<CJ>(Xm[a][b])) : X{};
             Dv[i + c * nb] = in ? conv<X>(Xm[a][b]) : X{};
+            if (DvT) DvT[i * nb + c] = in ? conv<X>(Xm[a][b]) : X{};
             if (in) {
                 if (i > c) stv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m, conv<X>(A[a][b]));
                 else {
@@ -186,7 +189,8 @@ __global__ void __launch_bounds__(kThreads, 1) diag_ldl_kernel(const FrontDev* _
 // ---------------------------------------------------------------------------
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
-                                                         T* __restrict__ L, const double* __restrict__ D, const T* __restrict__ tinv) {
+                                                         T* __restrict__ L, const double* __restrict__ D, const T* __restrict__ tinv,
+                                                         T* __restrict__ subT) {
     using X = V<T, C>;
     using W = DV<C>;
     constexpr int nb = kTile, ldA = kTile + 1;
@@ -240,6 +244,20 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restr
             const int r = ty + 16 * a;
             if (r < rows) stv<T, C>(L, f.L + (r0 + r) + (int64_t)(k + c) * f.m, acc[a][b] * rd);
         }
+    }
+    // the first row block under a full diagonal block is tile (b+1, b) of the
+    // pivot rows: keep a row-major copy (zero outside the pivot rows) for the
+    // backward sweep
+    if (subT && rb == 0 && kb == nb && r0 < f.n) {
+        X* S = reinterpret_cast<X*>(subT) + f.dinv + (int64_t)(k / nb) * nb * nb;
+        const int prow = min(rows, f.n - r0);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = ty + 16 * a, c = tx + 16 * b;
+                S[r * nb + c] = r < prow ? acc[a][b] * sR[c] : X{};
+            }
     }
 }
 
@@ -364,11 +382,11 @@ static int run_factor_impl(Plan& P) {
             case Launch::DIAG:
                 diag_ldl_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, smem_diag, P.stream>>>(
                     P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), reinterpret_cast<T*>(P.dinv),
-                    P.status);
+                    reinterpret_cast<T*>(P.dinvT), P.status);
                 break;
             case Launch::PANEL:
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
-                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv));
+                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), reinterpret_cast<T*>(P.subT));
                 break;
             case Launch::GEMM:
                 if (std::is_same<T, float>::value && P.tensor_path())
@@ -503,9 +521,9 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
     const int64_t* prefix = reinterpret_cast<const int64_t*>(base + kOffPrefix);
     int32_t* status = reinterpret_cast<int32_t*>(base + kOffStatus);
     for (const Step& s : steps) {
-        diag_ldl_kernel<T, C, CJ><<<1, kThreads, 0, st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, status);
+        diag_ldl_kernel<T, C, CJ><<<1, kThreads, 0, st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, nullptr, status);
         if (s.panel_blocks > 0)
-            panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv);
+            panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr);
         if (s.prob >= 0)
             gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, AL, ABR,
                                                                                ABR, D);

@@ -75,7 +75,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 }
 
 void free_plan(Plan& P) {
-    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.partial, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
                     P.wpool[1], P.xnodal, P.xwork, P.norms};
@@ -401,20 +401,34 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         sl.nfronts = (int32_t)P.level_list[d].size();
         sl.gather_chunks = 1;
         for (int s : P.level_list[d]) sl.gather_chunks = std::max(sl.gather_chunks, (P.hfronts[s].m + 1023) / 1024);
+        // forward: each front's chain followed by its pivot-row workers in the
+        // order the chain consumes their partial sums, then the workers for the
+        // rows below the pivots (they only wait on chains, all issued before)
         sl.fwd_items = (int64_t)items.size() / 4;
         for (int s : P.level_list[d]) {
             FrontDev& f = P.hfronts[s];
             if (f.n <= 0 || f.m <= 0) continue;
+            const int nT = (f.n + kTile - 1) / kTile;
             f.flag_base = flag;
-            flag += (f.n + kTile - 1) / kTile;
-            for (int rb = 0; rb * kTile < f.m; ++rb) push_item(s, rb, 0, 0);
+            flag += nT;
+            push_item(s, kItemChain, 0, 0);
+            for (int rb = kSolveLag + 1; rb < nT; ++rb) push_item(s, kItemPivotRows, rb, 0);
+        }
+        for (int s : P.level_list[d]) {
+            const FrontDev& f = P.hfronts[s];
+            if (f.n <= 0 || f.m <= 0) continue;
+            for (int i = 0; f.n + i * kTile < f.m; ++i) push_item(s, kItemLowerRows, i, 0);
         }
         sl.nfwd = (int32_t)(items.size() / 4 - sl.fwd_items);
+        // backward: each front's chain followed by its column workers, last block first
         sl.bwd_items = (int64_t)items.size() / 4;
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
             if (f.n <= 0 || f.m <= 0) continue;
-            for (int rb = (f.n + kTile - 1) / kTile - 1; rb >= 0; --rb) push_item(s, rb, 0, 0);
+            const int nT = (f.n + kTile - 1) / kTile;
+            push_item(s, kItemChain, 0, 0);
+            for (int c = nT - 1; c >= 0; --c)
+                if (f.m > f.n || c + kSolveLag + 1 <= nT - 1) push_item(s, kItemColumns, c, 0);
         }
         sl.nbwd = (int32_t)(items.size() / 4 - sl.bwd_items);
     }
@@ -458,6 +472,9 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.pool[1], (size_t)P.pool_elems[1] * eb));
     TRY(dev_alloc(P, &P.tinv, (size_t)P.tinv_slots * nb * nb * eb));
     TRY(dev_alloc(P, &P.dinv, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.dinvT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.subT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.partial, (size_t)P.flags_total * kTile * kSolveRhsChunk * eb));
     TRY(dev_upload(P, &P.fronts, P.hfronts));
     TRY(dev_upload(P, &P.cmaps, cmaps));
     std::vector<int32_t> lowv(low, low + info->lower_ptr[nn]);
@@ -470,7 +487,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));
     TRY(dev_upload(P, &P.level_fronts, level_fronts));
-    std::vector<int32_t> zeros_flags(P.flags_total, 0);
+    std::vector<int32_t> zeros_flags(2 * P.flags_total, 0);
     TRY(dev_upload(P, &P.flags, zeros_flags));
     std::vector<int32_t> zt(2 * (P.max_depth + 1) + 2, 0);
     TRY(dev_upload(P, &P.tickets, zt));

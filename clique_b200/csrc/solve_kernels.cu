@@ -7,29 +7,43 @@
 // LocalLowerBackwardSolve, lower_solve/local.hpp:203-277).  Per front the
 // reference calls Trsm + Gemm (lower_solve/local_front.hpp:36-82).
 //
-// Here each tree level is one pair of launches:
-//   forward:  gather (children's W_B into this front's rows)  then
-//             fwd_chain: the front's rows in 64-row blocks.  Each block
-//             accumulates L[rows, T-block] * x[T-block] over the already
-//             solved blocks, then either solves its own diagonal block and
-//             publishes it, or subtracts into W_B.  One pass over L.
-//   backward: bwd_chain: per 64-column block of L_T, reduce L_B^T x_B (x_B
-//             gathered straight from the solution at the front's lowerStruct
-//             indices, which the ancestors have finished) and the later
-//             T-blocks, then solve the transposed diagonal block.
-// Blocks of one front depend on earlier blocks; CTAs take work items from
-// an atomic ticket counter in order, so every block a CTA waits for was
-// taken by a CTA that is already running.  Waits are bounded: on expiry the
-// kernel records a timeout in the status word and finishes without hanging.
+// Each tree level is one gather launch plus one sweep launch (forward), or
+// one sweep launch (backward).  Inside a sweep launch every front gets
+//   * one chain CTA, which walks the front's 64-wide pivot blocks in order.
+//     Step s needs the block's right-hand side minus the contributions of
+//     all solved blocks; the chain adds the newest block's contribution
+//     itself (x_{s-1} stays in its shared memory, the 64x64 tile it needs
+//     was prefetched into registers during the previous step) and takes the
+//     older ones from a worker as one finished 64 x nrhs partial sum.  Then
+//     it applies the stored inverse of the diagonal block and publishes
+//     x_s.  The critical path per step is therefore two 64x64 products and
+//     one flag, with no global-memory round trip for x.
+//   * workers, which stream the rest of the front's L tiles as the chain
+//     publishes solved blocks: forward, one per 64-row block of pivot rows
+//     (its partial feeds the chain) and one per 64-row block below the
+//     pivots (subtracts into the update vector W_B); backward, one per
+//     pivot column block (lower rows first, which need no wait, then the
+//     later pivot blocks).
+// Work items are taken from an atomic ticket counter in the order chain,
+// then that chain's workers in the order the chain consumes them, so every
+// CTA a resident CTA waits for was either issued before it or is a worker
+// whose own waits only reach back to earlier tickets: the sweep finishes
+// with any number of resident CTAs >= 2.  Waits are bounded: on expiry a
+// CTA records a timeout in the status word and returns, and every other
+// wait gives up as soon as it sees that word set.
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
 
 namespace cliqgpu {
 
 constexpr int kSolveThreads = 256;
-constexpr int kMaxRhsChunk = 16;     // right-hand sides per sweep
-constexpr int kGatherRows = 1024;    // front rows per gather CTA (grid y of the gather launch)
-constexpr uint64_t kSpinNs = 500000000ull;   // 0.5 s bound on any single wait
+constexpr int kQ = kSolveThreads / kTile;   // slices per tile row (4)
+constexpr int kE = kTile / kQ;              // tile elements per thread and slice (16)
+constexpr int kLag = kSolveLag;             // blocks the chain adds itself (the newest one)
+constexpr int kMaxRhsChunk = kSolveRhsChunk;   // right-hand sides per sweep
+constexpr int kPartialStride = kTile * kMaxRhsChunk;   // elements per pivot block in the partial store
+constexpr int kGatherRows = 1024;           // front rows per gather CTA (grid y of the gather launch)
+constexpr uint64_t kSpinNs = 500000000ull;  // 0.5 s bound on any single wait
 
 __device__ __forceinline__ int ld_acquire(const int32_t* p) {
     int v;
@@ -44,7 +58,8 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // thread 0 waits for flag == epoch; returns false (and records a timeout,
-// wait site 4) once the wall-clock bound expires
+// wait site 4) once the wall-clock bound expires, or at once when another
+// CTA has recorded one
 __device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_t* status) {
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
@@ -52,8 +67,9 @@ __device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_
         if (ld_acquire(flag) != epoch) {
             const uint64_t t0 = global_ns();
             while (ld_acquire(flag) != epoch) {
+                if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) { ok = 0; break; }
                 if (global_ns() - t0 > kSpinNs) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 4); ok = 0; break; }
-                __nanosleep(64);
+                __nanosleep(100);
             }
         }
         s_ok = ok;
@@ -68,24 +84,58 @@ __device__ __forceinline__ void publish_flag(int32_t* flag, int epoch) {
     if (threadIdx.x == 0) atomicExch(flag, epoch);
 }
 
-// A 64 x 64 tile of a front, loaded into registers one step ahead of its use
-// (L does not depend on the chain flags, so its load overlaps the waits).
-constexpr int kPre = kTile * kTile / kSolveThreads;   // 16 elements per thread
+// v[k] = A(r, q*kE + k) of a column-major tile at element offset a0 with
+// leading dimension ld, zero outside nr rows / nc columns.  With ld = 64 on
+// a row-major tile this reads element (q*kE + k, r) instead.
 template <class T, bool C>
-__device__ __forceinline__ void tile_fetch(V<T, C>* pre, const T* L, const FrontDev& f, int r0, int nr, int c0, int nc) {
+__device__ __forceinline__ void row_slice(V<T, C>* v, const T* __restrict__ A, int64_t a0, int64_t ld, int r, int q, int nr,
+                                          int nc) {
 #pragma unroll
-    for (int q = 0; q < kPre; ++q) {
-        const int idx = threadIdx.x + kSolveThreads * q;
-        const int rr = idx % kTile, cc = idx / kTile;
-        pre[q] = (rr < nr && cc < nc) ? ldv<T, C>(L, f.L + (r0 + rr) + (int64_t)(c0 + cc) * f.m) : V<T, C>{};
+    for (int k = 0; k < kE; ++k) {
+        const int c = q * kE + k;
+        v[k] = (r < nr && c < nc) ? ldv<T, C>(A, a0 + r + (int64_t)c * ld) : V<T, C>{};
     }
 }
-template <class X>
-__device__ __forceinline__ void tile_store(X* sL, const X* pre) {
+
+// acc[j] += sum_k op(v[k]) * s[(q*kE + k) * NR + j]; s is a 64 x NR tile in
+// shared memory, read as a broadcast by the 32 threads of a warp (same q)
+template <bool CJ, int NR, class Xv>
+__device__ __forceinline__ void slice_mac(Xv (&acc)[NR], const Xv* v, const Xv* s, int q) {
 #pragma unroll
-    for (int q = 0; q < kPre; ++q) {
-        const int idx = threadIdx.x + kSolveThreads * q;
-        sL[(idx % kTile) * (kTile + 1) + idx / kTile] = pre[q];
+    for (int k = 0; k < kE; ++k) {
+        const Xv a = opc<CJ>(v[k]);
+        const Xv* sr = s + (q * kE + k) * NR;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) mac(acc[j], a, sr[j]);
+    }
+}
+
+// Sum the kQ slice partials of each (row, rhs): thread (r, q) gets the
+// totals for rhs j = q + kQ*a.  Ends with red still being read: the caller
+// synchronises before red is written again.
+template <int NR, class Xv>
+__device__ __forceinline__ void reduce_slices(const Xv (&acc)[NR], Xv* red, Xv (&out)[NR / kQ], int r, int q) {
+#pragma unroll
+    for (int j = 0; j < NR; ++j) red[(q * NR + j) * kTile + r] = acc[j];
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < NR / kQ; ++a) {
+        const int j = q + kQ * a;
+        Xv s{};
+#pragma unroll
+        for (int qq = 0; qq < kQ; ++qq) s += red[(qq * NR + j) * kTile + r];
+        out[a] = s;
+    }
+}
+
+// 64 x NR tile of right-hand sides from X (column-major, ldx) starting at
+// row x0, zero beyond nr rows or nrhs columns; L2-coherent loads for values
+// another CTA of this launch published
+template <class T, bool C, int NR>
+__device__ __forceinline__ void load_x_tile(V<T, C>* s, const T* X, int64_t x0, int64_t ldx, int nr, int nrhs) {
+    for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
+        const int rr = idx % kTile, j = idx / kTile;
+        s[rr * NR + j] = (rr < nr && j < nrhs) ? ldv_cg<T, C>(X, x0 + rr + (int64_t)j * ldx) : V<T, C>{};
     }
 }
 
@@ -125,123 +175,6 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_gather_kernel(const FrontDe
 }
 
 // ---------------------------------------------------------------------------
-// forward chain
-// ---------------------------------------------------------------------------
-template <class T, bool C>
-__global__ void __launch_bounds__(kSolveThreads) fwd_chain_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
-                                                                  int32_t* __restrict__ ticket, int32_t* __restrict__ flags, int epoch,
-                                                                  const T* __restrict__ L, const T* __restrict__ dinv,
-                                                                  T* __restrict__ X, int64_t ldx,
-                                                                  T* __restrict__ w0, T* __restrict__ w1, int nrhs,
-                                                                  int32_t* __restrict__ status) {
-    using Xv = V<T, C>;
-    constexpr int ldl = kTile + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Xv* sL = reinterpret_cast<Xv*>(smem_raw);         // 64 x 65
-    Xv* sD = sL + kTile * ldl;                          // 64 x 65: inverse of the diagonal block, sD[r*65+c] = Linv[r][c]
-    Xv* sx = sD + kTile * ldl;                          // 64 x kMaxRhsChunk
-    __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
-    __syncthreads();
-    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
-    const int4 it = items[s_item];
-    const FrontDev f = F[it.x];
-    const int rb = it.y;
-    const int r0 = kTile * rb;
-    const int rows = min(kTile, f.m - r0);
-    const int nT = (f.n + kTile - 1) / kTile;
-    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;   // row, rhs lane
-    Xv acc[kMaxRhsChunk / 4];
-#pragma unroll
-    for (int a = 0; a < kMaxRhsChunk / 4; ++a) acc[a] = Xv{};
-    const int cb_end = min(rb, nT);
-    Xv pre[kPre];
-    if (cb_end > 0) tile_fetch<T, C>(pre, L, f, r0, rows, 0, min(kTile, f.n));
-    for (int cb = 0; cb < cb_end; ++cb) {
-        const int c0 = kTile * cb, ncols = min(kTile, f.n - c0);
-        tile_store(sL, pre);
-        if (cb + 1 < cb_end) tile_fetch<T, C>(pre, L, f, r0, rows, c0 + kTile, min(kTile, f.n - c0 - kTile));
-        if (!wait_flag(&flags[f.flag_base + cb], epoch, status)) break;
-        for (int idx = threadIdx.x; idx < kTile * nrhs; idx += blockDim.x) {
-            const int cc = idx % kTile, j = idx / kTile;
-            sx[cc * kMaxRhsChunk + j] = cc < ncols ? ldv_cg<T, C>(X, f.off + c0 + cc + (int64_t)j * ldx) : Xv{};
-        }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs) {
-                Xv s = acc[a];
-                for (int cc = 0; cc < ncols; ++cc) mac(s, sL[r * ldl + cc], sx[cc * kMaxRhsChunk + j]);
-                acc[a] = s;
-            }
-        }
-        __syncthreads();
-    }
-    if (rb < nT) {
-        const int dcols = min(kTile, f.n - r0);
-        const Xv* Dv = reinterpret_cast<const Xv*>(dinv) + f.dinv + (int64_t)rb * kTile * kTile;
-        for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
-            const int rr = idx % kTile, cc = idx / kTile;
-            sL[rr * ldl + cc] = (rr < rows && cc < dcols) ? ldv<T, C>(L, f.L + (r0 + rr) + (int64_t)(r0 + cc) * f.m) : Xv{};
-            sD[rr * ldl + cc] = Dv[idx];
-        }
-#pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs && r < dcols) sx[r * kMaxRhsChunk + j] = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * ldx) - acc[a];
-        }
-        __syncthreads();
-        // x = L11^{-1} b with the inverse kept by the factorization
-        Xv y[kMaxRhsChunk / 4];
-#pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            Xv sacc{};
-            if (j < nrhs && r < dcols)
-                for (int cc = 0; cc <= r; ++cc) mac(sacc, sD[r * ldl + cc], sx[cc * kMaxRhsChunk + j]);
-            y[a] = sacc;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs && r < dcols) sx[r * kMaxRhsChunk + j] = y[a];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs && r < dcols) stv<T, C>(X, f.off + r0 + r + (int64_t)j * ldx, sx[r * kMaxRhsChunk + j]);
-        }
-        publish_flag(&flags[f.flag_base + rb], epoch);
-        // rows of this block below the pivots (rows >= n) take this block's contribution
-        if (r >= dcols && r < rows) {
-#pragma unroll
-            for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-                const int j = q + 4 * a;
-                if (j < nrhs) {
-                    Xv s = acc[a];
-                    for (int cc = 0; cc < dcols; ++cc) mac(s, sL[r * ldl + cc], sx[cc * kMaxRhsChunk + j]);
-                    acc[a] = s;
-                }
-            }
-        }
-    }
-    if (r0 + r >= f.n && r < rows) {
-        T* wb = f.pool == 0 ? w0 : w1;
-#pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs) {
-                const int64_t e = f.W * nrhs + (r0 + r - f.n) + (int64_t)j * f.u;
-                stv<T, C>(wb, e, ldv<T, C>(wb, e) - acc[a]);
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // diagonal solve X := D^{-1} X (FP64 pivots)
 // ---------------------------------------------------------------------------
 template <class T, bool C>
@@ -259,166 +192,390 @@ __global__ void diag_scale_kernel(T* __restrict__ X, int64_t ldx, int64_t n, int
 }
 
 // ---------------------------------------------------------------------------
-// backward chain
+// sweep launches
 // ---------------------------------------------------------------------------
-template <class T, bool C, bool CJ>
-__global__ void __launch_bounds__(kSolveThreads) bwd_chain_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
-                                                                  int32_t* __restrict__ ticket, int32_t* __restrict__ flags, int epoch,
-                                                                  const T* __restrict__ L, const T* __restrict__ dinv,
-                                                                  T* __restrict__ X, int64_t ldx,
-                                                                  const int32_t* __restrict__ lower, int nrhs,
-                                                                  int32_t* __restrict__ status) {
+struct SweepArgs {
+    const FrontDev* F;
+    const int4* items;      // {front, kind, block, 0}
+    int32_t* ticket;
+    int32_t* xflags;        // per pivot block: x_b published (chain)
+    int32_t* pflags;        // per pivot block: partial sum published (worker)
+    int epoch;
+    const void* L;
+    const void* dinv;       // L11^{-1} per 64-block, column-major
+    const void* dinvT;      // the same, row-major
+    const void* subT;       // tile (b+1, b) of L per pivot block, row-major
+    void* partial;          // kPartialStride elements per pivot block
+    void* X;                // n x nrhs, ND order, ld ldx
+    int64_t ldx;
+    void* w0;
+    void* w1;
+    const int32_t* lower;
+    int nrhs;
+    int32_t* status;
+};
+
+// One L tile of a forward worker: wait for x_t, stage it, accumulate.
+template <class T, bool C, int NR>
+__device__ __forceinline__ bool fwd_tile(const SweepArgs& a, const FrontDev& f, int t, const V<T, C>* lt, V<T, C> (&acc)[NR],
+                                         V<T, C>* sx, int q) {
+    V<T, C>* sb = sx + (t & 1) * kTile * NR;
+    if (!wait_flag(&a.xflags[f.flag_base + t], a.epoch, a.status)) return false;
+    load_x_tile<T, C, NR>(sb, reinterpret_cast<const T*>(a.X), f.off + (int64_t)t * kTile, a.ldx, min(kTile, f.n - t * kTile), a.nrhs);
+    __syncthreads();
+    slice_mac<false, NR>(acc, lt, sb, q);
+    return true;
+}
+
+// Forward chain of one front: x_s = L_ss^{-1} (b_s - partial_s - L_{s,s-1} x_{s-1}).
+template <class T, bool C, int NR>
+__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+    using Xv = V<T, C>;
+    const T* L = reinterpret_cast<const T*>(a.L);
+    const T* Dinv = reinterpret_cast<const T*>(a.dinv);
+    const T* Part = reinterpret_cast<const T*>(a.partial);
+    T* X = reinterpret_cast<T*>(a.X);
+    Xv* sprev = sx;                 // x_{s-1}
+    Xv* st = sx + kTile * NR;       // right-hand side of the diagonal block
+    Xv lp[kE], dv[kE];
+    row_slice<T, C>(dv, Dinv, f.dinv, kTile, r, q, kTile, kTile);
+    for (int s = 0; s < nT; ++s) {
+        const int r0 = s * kTile, ds = min(kTile, f.n - r0);
+        const bool fed = s > kLag;  // a worker holds the contributions of blocks < s - kLag
+        if (fed && !wait_flag(&a.pflags[f.flag_base + s], a.epoch, a.status)) return;
+        Xv tv[NR / kQ];
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            Xv v{};
+            if (r < ds && j < a.nrhs) {
+                v = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx);
+                if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s) * kPartialStride + j * kTile + r);
+            }
+            tv[b] = v;
+        }
+        if (s > 0) {
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, lp, sprev, q);
+            Xv u[NR / kQ];
+            reduce_slices<NR>(acc, red, u, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) tv[b] -= u[b];
+        }
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = tv[b];
+        __syncthreads();
+        {
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, dv, st, q);
+            Xv xs[NR / kQ];
+            reduce_slices<NR>(acc, red, xs, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                const bool in = r < ds && j < a.nrhs;
+                if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, xs[b]);
+                sprev[r * NR + j] = in ? xs[b] : Xv{};
+            }
+        }
+        if (s + 1 < nT) {
+            row_slice<T, C>(lp, L, f.L + (r0 + kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - kTile), kTile);
+            row_slice<T, C>(dv, Dinv, f.dinv + (int64_t)(s + 1) * kTile * kTile, kTile, r, q, kTile, kTile);
+        }
+        publish_flag(&a.xflags[f.flag_base + s], a.epoch);
+    }
+}
+
+template <class T, bool C, int NR>
+__global__ void __launch_bounds__(kSolveThreads) fwd_sweep_kernel(SweepArgs a) {
+    using Xv = V<T, C>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
+    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
+    __shared__ int s_item;
+    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
+    __syncthreads();
+    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
+    const int4 it = a.items[s_item];
+    const FrontDev f = a.F[it.x];
+    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
+    const int nT = (f.n + kTile - 1) / kTile;
+    if (it.y == kItemChain) {
+        fwd_chain<T, C, NR>(a, f, nT, r, q, sx, red);
+        return;
+    }
+    // worker: rows [R0, R0 + nr) against the pivot blocks t < t_end
+    const T* L = reinterpret_cast<const T*>(a.L);
+    int R0, nr, t_end;
+    if (it.y == kItemPivotRows) { R0 = kTile * it.z; nr = min(kTile, f.n - R0); t_end = it.z - kLag; }
+    else { R0 = f.n + kTile * it.z; nr = min(kTile, f.m - R0); t_end = nT; }
+    Xv acc[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+    Xv la[kE], lb[kE];
+    row_slice<T, C>(la, L, f.L + R0, f.m, r, q, nr, min(kTile, f.n));
+    for (int t = 0; t < t_end; t += 2) {
+        // two tiles in flight: the next one loads while this one waits for its x block
+        if (t + 1 < t_end)
+            row_slice<T, C>(lb, L, f.L + R0 + (int64_t)(t + 1) * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - (t + 1) * kTile));
+        if (!fwd_tile<T, C, NR>(a, f, t, la, acc, sx, q)) return;
+        if (t + 1 >= t_end) break;
+        if (t + 2 < t_end)
+            row_slice<T, C>(la, L, f.L + R0 + (int64_t)(t + 2) * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - (t + 2) * kTile));
+        if (!fwd_tile<T, C, NR>(a, f, t + 1, lb, acc, sx, q)) return;
+    }
+    Xv out[NR / kQ];
+    reduce_slices<NR>(acc, red, out, r, q);
+    if (it.y == kItemPivotRows) {
+        T* Part = reinterpret_cast<T*>(a.partial);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + it.z) * kPartialStride + j * kTile + r, out[b]);
+        }
+        publish_flag(&a.pflags[f.flag_base + it.z], a.epoch);
+    } else if (r < nr) {
+        T* wb = reinterpret_cast<T*>(f.pool == 0 ? a.w0 : a.w1);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            if (j < a.nrhs) {
+                const int64_t e = f.W * a.nrhs + (R0 - f.n + r) + (int64_t)j * f.u;
+                stv<T, C>(wb, e, ldv<T, C>(wb, e) - out[b]);
+            }
+        }
+    }
+}
+
+// Backward chain of one front, last pivot block first:
+// x_c = op(L_cc^{-1})^T (y_c - partial_c - op(L_{c+1,c})^T x_{c+1}).
+template <class T, bool C, bool CJ, int NR>
+__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+    using Xv = V<T, C>;
+    const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
+    const T* SubT = reinterpret_cast<const T*>(a.subT);
+    const T* Part = reinterpret_cast<const T*>(a.partial);
+    T* X = reinterpret_cast<T*>(a.X);
+    Xv* sprev = sx;                 // x_{c+1}
+    Xv* st = sx + kTile * NR;
+    // thread (r, q) holds column r, rows q*kE .. q*kE+kE-1 of the row-major tiles
+    Xv lp[kE], dv[kE];
+    row_slice<T, C>(dv, DinvT, f.dinv + (int64_t)(nT - 1) * kTile * kTile, kTile, r, q, kTile, kTile);
+    for (int c = nT - 1; c >= 0; --c) {
+        const int c0 = c * kTile, dc = min(kTile, f.n - c0);
+        const bool fed = f.m > f.n || c + kLag + 1 <= nT - 1;
+        if (fed && !wait_flag(&a.pflags[f.flag_base + c], a.epoch, a.status)) return;
+        Xv tv[NR / kQ];
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            Xv v{};
+            if (r < dc && j < a.nrhs) {
+                v = ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx);
+                if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r);
+            }
+            tv[b] = v;
+        }
+        if (c + 1 < nT) {
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<CJ, NR>(acc, lp, sprev, q);
+            Xv u[NR / kQ];
+            reduce_slices<NR>(acc, red, u, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) tv[b] -= u[b];
+        }
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = tv[b];
+        __syncthreads();
+        {
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<CJ, NR>(acc, dv, st, q);
+            Xv xs[NR / kQ];
+            reduce_slices<NR>(acc, red, xs, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                const bool in = r < dc && j < a.nrhs;
+                if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xs[b]);
+                sprev[r * NR + j] = in ? xs[b] : Xv{};
+            }
+        }
+        if (c > 0) {
+            const int64_t blk = f.dinv + (int64_t)(c - 1) * kTile * kTile;
+            row_slice<T, C>(lp, SubT, blk, kTile, r, q, kTile, kTile);
+            row_slice<T, C>(dv, DinvT, blk, kTile, r, q, kTile, kTile);
+        }
+        publish_flag(&a.xflags[f.flag_base + c], a.epoch);
+    }
+}
+
+template <class T, bool C, bool CJ, int NR>
+__global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
     using Xv = V<T, C>;
     constexpr int ldl = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Xv* sL = reinterpret_cast<Xv*>(smem_raw);
-    Xv* sD = sL + kTile * ldl;
-    Xv* sx = sD + kTile * ldl;
+    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
+    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
+    Xv* sL = red + kQ * NR * kTile;               // [64 columns][65]
     __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
+    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
     __syncthreads();
-    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
-    const int4 it = items[s_item];
-    const FrontDev f = F[it.x];
-    const int rb = it.y;
-    const int c0 = kTile * rb;
-    const int dcols = min(kTile, f.n - c0);
+    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
+    const int4 it = a.items[s_item];
+    const FrontDev f = a.F[it.x];
+    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
     const int nT = (f.n + kTile - 1) / kTile;
-    const int c = threadIdx.x % kTile, q = threadIdx.x / kTile;
-    Xv acc[kMaxRhsChunk / 4];
+    if (it.y == kItemChain) {
+        bwd_chain<T, C, CJ, NR>(a, f, nT, r, q, sx, red);
+        return;
+    }
+    // column worker: op(L[R, c-block])^T x_R over the rows below the pivots
+    // (x gathered at lowerStruct, final since the ancestors are solved), then
+    // over the pivot blocks after c + kLag as the chain publishes them
+    const T* L = reinterpret_cast<const T*>(a.L);
+    const T* X = reinterpret_cast<const T*>(a.X);
+    const int c = it.z, c0 = c * kTile, dc = min(kTile, f.n - c0);
+    const int nlow = (f.m - f.n + kTile - 1) / kTile;
+    const int npiv = max(0, nT - 1 - (c + kLag));
+    const int ntiles = nlow + npiv;
+    // coalesced staging: element p of this thread is (row r, column q + kQ*p)
+    auto tile_of = [&](int i, int& R0, int& nr) {
+        if (i < nlow) { R0 = f.n + kTile * i; nr = min(kTile, f.m - R0); }
+        else { R0 = kTile * (nT - 1 - (i - nlow)); nr = min(kTile, f.n - R0); }
+    };
+    Xv pre[kE];
+    auto fetch = [&](int i) {
+        int R0, nr;
+        tile_of(i, R0, nr);
 #pragma unroll
-    for (int a = 0; a < kMaxRhsChunk / 4; ++a) acc[a] = Xv{};
-    // rows below the pivots: x gathered from the (final) ancestor entries
-    Xv pre[kPre];
-    if (f.n < f.m) tile_fetch<T, C>(pre, L, f, f.n, min(kTile, f.m - f.n), c0, dcols);
-    for (int rr0 = f.n; rr0 < f.m; rr0 += kTile) {
-        const int nr = min(kTile, f.m - rr0);
-        tile_store(sL, pre);
-        if (rr0 + kTile < f.m) tile_fetch<T, C>(pre, L, f, rr0 + kTile, min(kTile, f.m - rr0 - kTile), c0, dcols);
-        else if (nT - 1 > rb) tile_fetch<T, C>(pre, L, f, kTile * (nT - 1), min(kTile, f.n - kTile * (nT - 1)), c0, dcols);
-        for (int idx = threadIdx.x; idx < kTile * nrhs; idx += blockDim.x) {
-            const int rr = idx % kTile, j = idx / kTile;
-            Xv v{};
-            if (rr < nr) v = ldv<T, C>(X, (int64_t)lower[f.lower + rr0 + rr - f.n] + (int64_t)j * ldx);
-            sx[rr * kMaxRhsChunk + j] = v;
+        for (int p = 0; p < kE; ++p) {
+            const int cc = q + kQ * p;
+            pre[p] = (r < nr && cc < dc) ? ldv<T, C>(L, f.L + R0 + r + (int64_t)(c0 + cc) * f.m) : Xv{};
         }
-        __syncthreads();
+    };
+    Xv acc[NR];
 #pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs) {
-                Xv s = acc[a];
-                for (int rr = 0; rr < nr; ++rr) mac(s, opc<CJ>(sL[rr * ldl + c]), sx[rr * kMaxRhsChunk + j]);
-                acc[a] = s;
+    for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+    if (ntiles > 0) fetch(0);
+    for (int i = 0; i < ntiles; ++i) {
+        int R0, nr;
+        tile_of(i, R0, nr);
+        __syncthreads();   // the previous tile's readers are done with sL and sx
+#pragma unroll
+        for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
+        if (i + 1 < ntiles) fetch(i + 1);
+        if (i >= nlow) {
+            if (!wait_flag(&a.xflags[f.flag_base + R0 / kTile], a.epoch, a.status)) return;
+            load_x_tile<T, C, NR>(sx, X, f.off + R0, a.ldx, nr, a.nrhs);
+        } else {
+            for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
+                const int rr = idx % kTile, j = idx / kTile;
+                sx[rr * NR + j] = (rr < nr && j < a.nrhs)
+                                      ? ldv<T, C>(X, (int64_t)a.lower[f.lower + R0 - f.n + rr] + (int64_t)j * a.ldx) : Xv{};
             }
         }
         __syncthreads();
-    }
-    if (f.n >= f.m && nT - 1 > rb) tile_fetch<T, C>(pre, L, f, kTile * (nT - 1), min(kTile, f.n - kTile * (nT - 1)), c0, dcols);
-    // later pivot blocks of this front
-    for (int ib = nT - 1; ib > rb; --ib) {
-        const int rr0 = kTile * ib, nr = min(kTile, f.n - rr0);
-        tile_store(sL, pre);
-        if (ib - 1 > rb) tile_fetch<T, C>(pre, L, f, rr0 - kTile, kTile, c0, dcols);
-        if (!wait_flag(&flags[f.flag_base + ib], epoch, status)) break;
-        for (int idx = threadIdx.x; idx < kTile * nrhs; idx += blockDim.x) {
-            const int rr = idx % kTile, j = idx / kTile;
-            sx[rr * kMaxRhsChunk + j] = rr < nr ? ldv_cg<T, C>(X, f.off + rr0 + rr + (int64_t)j * ldx) : Xv{};
-        }
-        __syncthreads();
+        Xv v[kE];
 #pragma unroll
-        for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-            const int j = q + 4 * a;
-            if (j < nrhs) {
-                Xv s = acc[a];
-                for (int rr = 0; rr < nr; ++rr) mac(s, opc<CJ>(sL[rr * ldl + c]), sx[rr * kMaxRhsChunk + j]);
-                acc[a] = s;
-            }
-        }
-        __syncthreads();
+        for (int k = 0; k < kE; ++k) v[k] = sL[r * ldl + q * kE + k];
+        slice_mac<CJ, NR>(acc, v, sx, q);
     }
-    // diagonal block, transposed: x = op(L11^{-1})^T b
-    const Xv* Dv = reinterpret_cast<const Xv*>(dinv) + f.dinv + (int64_t)rb * kTile * kTile;
-    for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
-        const int rr = idx % kTile, cc = idx / kTile;
-        sD[rr * ldl + cc] = Dv[idx];
-    }
+    Xv out[NR / kQ];
+    reduce_slices<NR>(acc, red, out, r, q);
+    T* Part = reinterpret_cast<T*>(a.partial);
 #pragma unroll
-    for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-        const int j = q + 4 * a;
-        if (j < nrhs && c < dcols) sx[c * kMaxRhsChunk + j] = ldv<T, C>(X, f.off + c0 + c + (int64_t)j * ldx) - acc[a];
+    for (int b = 0; b < NR / kQ; ++b) {
+        const int j = q + kQ * b;
+        if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r, out[b]);
     }
-    __syncthreads();
-    Xv y[kMaxRhsChunk / 4];
-#pragma unroll
-    for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-        const int j = q + 4 * a;
-        Xv sacc{};
-        if (j < nrhs && c < dcols)
-            for (int rr = c; rr < dcols; ++rr) mac(sacc, opc<CJ>(sD[rr * ldl + c]), sx[rr * kMaxRhsChunk + j]);
-        y[a] = sacc;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-        const int j = q + 4 * a;
-        if (j < nrhs && c < dcols) sx[c * kMaxRhsChunk + j] = y[a];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int a = 0; a < kMaxRhsChunk / 4; ++a) {
-        const int j = q + 4 * a;
-        if (j < nrhs && c < dcols) stv<T, C>(X, f.off + c0 + c + (int64_t)j * ldx, sx[c * kMaxRhsChunk + j]);
-    }
-    publish_flag(&flags[f.flag_base + rb], epoch);
+    publish_flag(&a.pflags[f.flag_base + c], a.epoch);
 }
 
 // ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
-template <class T, bool C, bool CJ>
-static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
+template <class T, bool C, bool CJ, int NR>
+static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     using Xv = V<T, C>;
-    const size_t smem = sizeof(Xv) * (2 * kTile * (kTile + 1) + kTile * kMaxRhsChunk);
+    const size_t smem_fwd = sizeof(Xv) * (2 + kQ) * kTile * NR;
+    const size_t smem_bwd = smem_fwd + sizeof(Xv) * kTile * (kTile + 1);
     static bool attr_done = false;
     if (!attr_done) {
-        cudaFuncSetAttribute(fwd_chain_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(bwd_chain_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(fwd_sweep_kernel<T, C, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fwd);
+        cudaFuncSetAttribute(bwd_sweep_kernel<T, C, CJ, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bwd);
         attr_done = true;
     }
     const int4* items = reinterpret_cast<const int4*>(P.items);
-    T* L = reinterpret_cast<T*>(P.L);
+    SweepArgs a{};
+    a.F = P.fronts;
+    a.xflags = P.flags;
+    a.pflags = P.flags + P.flags_total;
+    a.L = P.L;
+    a.dinv = P.dinv;
+    a.dinvT = P.dinvT;
+    a.subT = P.subT;
+    a.partial = P.partial;
+    a.X = X;
+    a.ldx = P.n;
+    a.w0 = P.wpool[0];
+    a.w1 = P.wpool[1];
+    a.lower = P.lower;
+    a.nrhs = nrhs;
+    a.status = P.status;
     T* w0 = reinterpret_cast<T*>(P.wpool[0]);
     T* w1 = reinterpret_cast<T*>(P.wpool[1]);
     const int nlev = P.max_depth + 1;
     int64_t launches = 0;
-    for (int j0 = 0; j0 < nrhs_total; j0 += kMaxRhsChunk) {
-        const int nrhs = nrhs_total - j0 < kMaxRhsChunk ? nrhs_total - j0 : kMaxRhsChunk;
-        T* X = xn + (C ? 2 : 1) * (int64_t)j0 * P.n;
-        cudaMemsetAsync(P.tickets, 0, sizeof(int32_t) * 2 * nlev, P.stream);
-        for (int d = P.max_depth; d >= 0; --d) {
-            const SolveLevel& lv = P.solve_levels[d];
-            if (lv.nfronts == 0) continue;
-            fwd_gather_kernel<T, C><<<dim3(lv.nfronts, lv.gather_chunks), kSolveThreads, 0, P.stream>>>(P.fronts, P.level_fronts + lv.fronts, X, P.n, w0, w1,
-                                                                               P.cmaps, nrhs);
-            ++launches;
-            if (lv.nfwd > 0) {
-                const int epoch = ++P.epoch;
-                fwd_chain_kernel<T, C><<<lv.nfwd, kSolveThreads, smem, P.stream>>>(P.fronts, items + lv.fwd_items, P.tickets + 2 * d,
-                                                                                   P.flags, epoch, L, reinterpret_cast<const T*>(P.dinv), X, P.n, w0, w1, nrhs, P.status);
-                ++launches;
-            }
-        }
-        diag_scale_kernel<T, C><<<1184, 256, 0, P.stream>>>(X, P.n, P.n, nrhs, P.D);
+    cudaMemsetAsync(P.tickets, 0, sizeof(int32_t) * 2 * nlev, P.stream);
+    for (int d = P.max_depth; d >= 0; --d) {
+        const SolveLevel& lv = P.solve_levels[d];
+        if (lv.nfronts == 0) continue;
+        fwd_gather_kernel<T, C><<<dim3(lv.nfronts, lv.gather_chunks), kSolveThreads, 0, P.stream>>>(
+            P.fronts, P.level_fronts + lv.fronts, X, P.n, w0, w1, P.cmaps, nrhs);
         ++launches;
-        for (int d = 0; d <= P.max_depth; ++d) {
-            const SolveLevel& lv = P.solve_levels[d];
-            if (lv.nbwd == 0) continue;
-            const int epoch = ++P.epoch;
-            bwd_chain_kernel<T, C, CJ><<<lv.nbwd, kSolveThreads, smem, P.stream>>>(P.fronts, items + lv.bwd_items, P.tickets + 2 * d + 1,
-                                                                                    P.flags, epoch, L, reinterpret_cast<const T*>(P.dinv), X, P.n, P.lower, nrhs, P.status);
+        if (lv.nfwd > 0) {
+            a.items = items + lv.fwd_items;
+            a.ticket = P.tickets + 2 * d;
+            a.epoch = ++P.epoch;
+            fwd_sweep_kernel<T, C, NR><<<lv.nfwd, kSolveThreads, smem_fwd, P.stream>>>(a);
             ++launches;
         }
+    }
+    diag_scale_kernel<T, C><<<1184, 256, 0, P.stream>>>(X, P.n, P.n, nrhs, P.D);
+    ++launches;
+    for (int d = 0; d <= P.max_depth; ++d) {
+        const SolveLevel& lv = P.solve_levels[d];
+        if (lv.nbwd == 0) continue;
+        a.items = items + lv.bwd_items;
+        a.ticket = P.tickets + 2 * d + 1;
+        a.epoch = ++P.epoch;
+        bwd_sweep_kernel<T, C, CJ, NR><<<lv.nbwd, kSolveThreads, smem_bwd, P.stream>>>(a);
+        ++launches;
+    }
+    return launches;
+}
+
+template <class T, bool C, bool CJ>
+static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
+    // complex double sweeps take at most 8 right-hand sides at a time (the
+    // 16-wide accumulators would not fit in registers)
+    constexpr int kChunk = (C && sizeof(T) == 8) ? 8 : kMaxRhsChunk;
+    int64_t launches = 0;
+    for (int j0 = 0; j0 < nrhs_total; j0 += kChunk) {
+        const int nrhs = nrhs_total - j0 < kChunk ? nrhs_total - j0 : kChunk;
+        T* X = xn + (C ? 2 : 1) * (int64_t)j0 * P.n;
+        if (nrhs <= 4) launches += run_sweeps<T, C, CJ, 4>(P, X, nrhs);
+        else if constexpr (kChunk == 8) launches += run_sweeps<T, C, CJ, 8>(P, X, nrhs);
+        else if (nrhs <= 8) launches += run_sweeps<T, C, CJ, 8>(P, X, nrhs);
+        else launches += run_sweeps<T, C, CJ, 16>(P, X, nrhs);
     }
     P.last_launches += launches;
     P.total_launches += launches;
