@@ -41,6 +41,7 @@ void set_last_error(const std::string& msg);
 // ---------------------------------------------------------------------------
 constexpr int kTile = 64;        // rows per solve block, GEMM tile edge
 constexpr int kEACols = 16;      // columns per extend-add work item
+constexpr int kEARows = 2048;    // rows per extend-add work item
 // Triangular sweeps: the chain CTA of a front adds the contributions of the
 // kSolveLag newest solved blocks itself; workers add the older ones.
 constexpr int kSolveLag = 1;
@@ -180,6 +181,8 @@ struct Plan {
     int64_t total_launches = 0;   // every kernel this plan has launched
     // FP32 updates on the tensor cores (tcgen05 3xTF32); CLIQGPU_TENSOR_CORES=0 selects the CUDA-core kernel
     int use_tc = 1;
+    // FP32 storage: diagonal-block LDL in FP64 arithmetic (CLIQGPU_DIAG_FP64=1) instead of FP32
+    int diag_fp64 = 0;
     bool tensor_path() const { return use_tc && precision == CLIQ_FP32; }
     // width of the outer column block whose trailing update is deferred (multiple of nb)
     int outer_nb = 256;

@@ -14,7 +14,9 @@
 //      ABR := children), using per-front inverse maps of the relative indices.
 //   2. for k in steps of nb over the level's widest front:
 //        diag_ldl_kernel  -- LDL of the kb x kb diagonal block in shared memory
-//                            in FP64, writes L11, D (FP64) and U = L11^{-T}.
+//                            (FP64 arithmetic for FP64 storage, FP32 for FP32
+//                            storage), writes L11, D (FP64), U = L11^{-T} and
+//                            L11^{-1} for the solves.
 //        panel_kernel     -- S21 = A21 U, L21 = S21 D^{-1} (row blocks of 64).
 //        gemm (trailing)  -- A22 -= L21 D L21^T over the remaining panel columns.
 //   3. gemm (Schur)       -- ABR -= L_B D L_B^T once with K = n, instead of the
@@ -36,6 +38,10 @@ constexpr int kThreads = 256;
 
 // ---------------------------------------------------------------------------
 // 1. extend-add (gather form)
+//
+// Work item (front, j0, i0): columns j0 .. j0+15, rows i0 .. i0+kEARows-1 on
+// or below the diagonal; the CTA sweeps each column down a contiguous run of
+// rows (consecutive threads, consecutive rows).
 // ---------------------------------------------------------------------------
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
@@ -49,12 +55,13 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
     const T* cp = f.pool == 0 ? pool1 : pool0;
     const int32_t* lm = f.cmap >= 0 ? cmaps + f.cmap : nullptr;
     const int32_t* rm = lm ? lm + f.m : nullptr;
+    const int i_end = min(f.m, it.z + kEARows);
     for (int jj = 0; jj < kEACols; ++jj) {
         const int j = j0 + jj;
         if (j >= f.m) break;
         const int lj = lm ? lm[j] : -1, rj = rm ? rm[j] : -1;
         if (j < f.n && lj < 0 && rj < 0) continue;
-        for (int i = j + threadIdx.x; i < f.m; i += blockDim.x) {
+        for (int i = max(j, it.z) + threadIdx.x; i < i_end; i += blockDim.x) {
             X v = X{};
             if (lj >= 0) {
                 const int li = lm[i];
@@ -77,111 +84,245 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
 // ---------------------------------------------------------------------------
 // 2a. LDL of the diagonal block (one CTA per front), FP64 in shared memory
 //
-// Right-looking elimination of the kb x kb block; the same row operations
-// are applied to an identity block, which therefore ends as L11^{-1}
-// (Gaussian elimination on [A | I]).  Two barriers per pivot.  Outputs:
-// L11 (unit diagonal) and D back to global memory, U = op(L11^{-1})^T for the
-// panel kernel, and L11^{-1} itself into the per-front inverse store used by
-// the triangular solves.
+// The kb x kb block (padded to 64 with an identity block) is factored in
+// four 16-column steps p.  In each step the 256 threads hold the 16 x 16
+// diagonal sub-block one entry each (full symmetric copy) together with the
+// matching entry of a running inverse (Gaussian elimination on [P | I]);
+// one barrier per pivot, the working copies double-buffered by pivot
+// parity, and the reciprocal of the next pivot computed by its owner right
+// after its own update, so the per-pivot critical path is one update, one
+// reciprocal and one barrier.  Then G = A_ip op(L_pp^{-1})^T,
+// L_ip = G D_p^{-1} and the rank-16 update A_22 -= G op(L_2p)^T (2 x 2
+// register tiles).  Finally the off-diagonal 16 x 16 blocks of L^{-1}:
+//   Linv_ij = -Linv_ii * sum_{k=j}^{i-1} L_ik Linv_kj,   i > j.
+// Storage: sA holds A / L column-major in its lower triangle and, once
+// formed, Linv(r, c) (r > c) at the mirrored position sA[r * 65 + c].
+// Outputs: L11 (unit diagonal) and D to global memory, U = op(L11^{-1})^T
+// for the panel kernel, and L11^{-1} column-major (forward sweep) and
+// row-major (backward sweep).
 // ---------------------------------------------------------------------------
-template <class T, bool C, bool CJ>
-__global__ void __launch_bounds__(kThreads, 1) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
+constexpr int kDiagLd = kTile + 1;
+constexpr int kSub = 16;
+constexpr int kSubLd = kSub + 1;
+
+// working type of the diagonal-block factorization: WT real or complex
+template <class WT, bool C>
+using DiagW = typename std::conditional<C, cx<WT>, WT>::type;
+
+template <class WT, bool C>
+__host__ __device__ constexpr size_t diag_smem_bytes() {
+    // sA, sG, 2 x (P, X) sub-block buffers, d, 1/d
+    return sizeof(DiagW<WT, C>) * (size_t)(kTile * kDiagLd + kTile * kSub + 4 * kSub * kSubLd + 2 * kTile);
+}
+
+// Reciprocal of a pivot, on the critical path of every elimination step.
+// 1/x for x within float range: Newton-Raphson iteration y <- y (2 - x y)
+// from the single-precision reciprocal (about 23 correct bits, two steps
+// give full double precision); outside that range the IEEE reciprocal.
+// Complex: conj(d) / |d|^2, with d scaled by a power of two when |d|^2
+// would leave the range.
+__device__ __forceinline__ double recip_nr(double x) {
+    const double ax = fabs(x);
+    if (!(ax > 1e-30 && ax < 1e30)) return __drcp_rn(x);
+    double y = (double)__frcp_rn((float)x);
+    y = y * fma(-x, y, 2.0);
+    y = y * fma(-x, y, 2.0);
+    return y;
+}
+__device__ __forceinline__ float pivot_recip(float d) { return __frcp_rn(d); }
+__device__ __forceinline__ cx<float> pivot_recip(cx<float> d) {
+    const float n2 = fmaf(d.r, d.r, d.i * d.i);
+    if (n2 > 1e-36f && n2 < 1e36f) {
+        const float s = __frcp_rn(n2);
+        return {d.r * s, -d.i * s};
+    }
+    const float mx = fmaxf(fabsf(d.r), fabsf(d.i));
+    const int e = ((__float_as_int(mx) >> 23) & 0xff) - 127;
+    const float sc = __int_as_float((127 - e) << 23);   // 2^-e
+    const float xr = d.r * sc, xi = d.i * sc;
+    const float s = __frcp_rn(fmaf(xr, xr, xi * xi)) * sc;
+    return {xr * s, -xi * s};
+}
+__device__ __forceinline__ double pivot_recip(double d) { return recip_nr(d); }
+__device__ __forceinline__ cx<double> pivot_recip(cx<double> d) {
+    const double n2 = fma(d.r, d.r, d.i * d.i);
+    if (n2 > 1e-30 && n2 < 1e30) {
+        const double s = recip_nr(n2);
+        return {d.r * s, -d.i * s};
+    }
+    const double mx = fmax(fabs(d.r), fabs(d.i));
+    const int e = ((__double2hiint(mx) >> 20) & 0x7ff) - 1023;
+    const double sc = __hiloint2double((1023 - e) << 20, 0);   // 2^-e
+    const double xr = d.r * sc, xi = d.i * sc;
+    const double s = __drcp_rn(fma(xr, xr, xi * xi)) * sc;
+    return {xr * s, -xi * s};
+}
+
+template <class T, bool C, bool CJ, class WT>
+__global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
                                                                T* __restrict__ L, double* __restrict__ D, T* __restrict__ tinv,
                                                                T* __restrict__ dinv, T* __restrict__ dinvT, int32_t* __restrict__ status) {
-    using W = DV<C>;
+    using W = DiagW<WT, C>;
     using X = V<T, C>;
-    constexpr int nb = kTile;
-    // thread (tr, tc) owns rows tr + 16a and columns tc + 16b (a, b < 4) of the
-    // block A and of the running inverse Xm, both held in registers
-    __shared__ W s_a[nb], s_l[nb], s_xr[nb], s_d[nb];
+    constexpr int nb = kTile, ld = kDiagLd;
+    static_assert(kThreads == kSub * kSub, "one thread per sub-block entry");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    W* sA = reinterpret_cast<W*>(smem_raw);        // 64 x 65, column-major
+    W* sG = sA + nb * ld;                           // 64 x 16 scratch
+    W* sP = sG + nb * kSub;                         // 2 x 16 x 17: sub-block working copy (by pivot parity)
+    W* sX = sP + 2 * kSub * kSubLd;                 // 2 x 16 x 17: running inverse
+    W* s_d = sX + 2 * kSub * kSubLd;
+    W* s_rd = s_d + nb;
     const int4 it = items[blockIdx.x];
     const FrontDev f = F[it.x];
     const int slot = it.y;
     const int kb = min(nb, f.n - k);
-    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
-    W A[4][4], Xm[4][4];
+    const int tid = threadIdx.x;
+    // lower triangle of the block, identity beyond kb; all 16 loads of a
+    // thread are issued before the first one is used
+    {
+        constexpr int kPer = nb * nb / kThreads;
+        X v[kPer];
+        const int r = tid % nb;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int i = tr + 16 * a, c = tc + 16 * b;
-            W v{};
-            if (i < kb && c < kb && i >= c) v = conv<W>(ldv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m));
-            A[a][b] = v;
-            Xm[a][b] = (i == c) ? vone<W>() : W{};
-            if (i == c && i < kb) s_d[i] = v;
+        for (int q = 0; q < kPer; ++q) {
+            const int c = tid / nb + (kThreads / nb) * q;
+            v[q] = (r < kb && c < kb && r >= c) ? ldv<T, C>(L, f.L + (k + r) + (int64_t)(k + c) * f.m) : X{};
         }
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int c = tid / nb + (kThreads / nb) * q;
+            if (r < c) continue;
+            W w = conv<W>(v[q]);
+            if (r >= kb && r == c) w = vone<W>();
+            sA[c * ld + r] = w;
+        }
+    }
     __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        const W d = s_d[j];
-        if (threadIdx.x == 0 && is_zero(d)) atomicMin(&status[0], f.off + k + j + 1);
-        const W rd = vone<W>() / d;
-        // publish the pivot column (scaled and unscaled) and row j of the inverse
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int i = tr + 16 * a, c = tc + 16 * b;
-                if (c == j && i > j && i < kb) {
-                    const W l = A[a][b] * rd;
-                    s_a[i] = A[a][b];
-                    s_l[i] = l;
-                    A[a][b] = l;
-                }
-                if (i == j && c <= j) s_xr[c] = Xm[a][b];
-            }
+    const int sr = tid % kSub, sc = tid / kSub;    // this thread's sub-block entry
+    for (int p = 0; p < nb / kSub; ++p) {
+        const int b0 = kSub * p;
+        // ---- 16 x 16 sub-block: LDL and inverse ----
+        W a = sr >= sc ? sA[(b0 + sc) * ld + b0 + sr] : opc<CJ>(sA[(b0 + sr) * ld + b0 + sc]);
+        W x = sr == sc ? vone<W>() : W{};
+        sP[sc * kSubLd + sr] = a;
+        sX[sc * kSubLd + sr] = x;
+        if (tid == 0) {
+            s_d[b0] = a;
+            s_rd[b0] = pivot_recip(a);
+            if (b0 < kb && is_zero(a)) atomicMin(&status[0], f.off + k + b0 + 1);
+        }
         __syncthreads();
-        W la[4], ab[4], xb[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = tr + 16 * a;
-            la[a] = (i > j && i < kb) ? s_l[i] : W{};
-        }
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int c = tc + 16 * b;
-            ab[b] = (c > j && c < kb) ? opc<CJ>(s_a[c]) : W{};
-            xb[b] = (c <= j) ? s_xr[c] : W{};
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int i = tr + 16 * a, c = tc + 16 * b;
-                if (i > j && i < kb) {
-                    if (c > j) {
-                        if (i >= c) A[a][b] -= la[a] * ab[b];
-                    } else {
-                        Xm[a][b] -= la[a] * xb[b];
-                    }
-                    if (i == j + 1 && c == j + 1) s_d[j + 1] = A[a][b];
-                }
+#pragma unroll 1
+        for (int j = 0; j < kSub; ++j) {
+            const W* P0 = sP + (j & 1) * kSub * kSubLd;
+            const W* X0 = sX + (j & 1) * kSub * kSubLd;
+            W* P1 = sP + ((j + 1) & 1) * kSub * kSubLd;
+            W* X1 = sX + ((j + 1) & 1) * kSub * kSubLd;
+            if (sr > j) {
+                const W rd = s_rd[b0 + j];
+                const W prj = P0[j * kSubLd + sr];                  // P[r][j]
+                const W lrj = prj * rd;
+                if (sc > j) a -= lrj * P0[sc * kSubLd + j];          // P[r][c] -= L[r][j] P[j][c]
+                else if (sc == j) a = lrj;
+                x -= lrj * X0[sc * kSubLd + j];                      // row r -= L[r][j] row j
             }
+            P1[sc * kSubLd + sr] = a;
+            X1[sc * kSubLd + sr] = x;
+            if (sr == j + 1 && sc == j + 1) {
+                s_d[b0 + j + 1] = a;
+                s_rd[b0 + j + 1] = pivot_recip(a);
+                if (b0 + j + 1 < kb && is_zero(a)) atomicMin(&status[0], f.off + k + b0 + j + 2);
+            }
+            __syncthreads();
+        }
+        if (sr > sc) {
+            sA[(b0 + sc) * ld + b0 + sr] = a;      // L_pp
+            sA[(b0 + sr) * ld + b0 + sc] = x;      // Linv_pp, mirrored
+        }
+        __syncthreads();
+        const int R = nb - b0 - kSub;     // rows below the sub-block
+        if (R == 0) break;
+        const int i0 = b0 + kSub;
+        // ---- panel: G = A_ip op(Linv_pp)^T, then L_ip = G D_p^{-1} ----
+        for (int idx = tid; idx < R * kSub; idx += kThreads) {
+            const int i = i0 + idx % R, c = idx / R;
+            W g = sA[(b0 + c) * ld + i];
+            for (int t = 0; t < c; ++t) g += sA[(b0 + t) * ld + i] * opc<CJ>(sA[(b0 + c) * ld + b0 + t]);
+            sG[c * nb + i] = g;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < R * kSub; idx += kThreads) {
+            const int i = i0 + idx % R, c = idx / R;
+            sA[(b0 + c) * ld + i] = sG[c * nb + i] * s_rd[b0 + c];
+        }
+        __syncthreads();
+        // ---- A_22 -= G op(L_2p)^T on the lower triangle, 2 x 2 tiles ----
+        const int T2 = R / 2, ntile = T2 * (T2 + 1) / 2;
+        for (int tt = tid; tt < ntile; tt += kThreads) {
+            int ti = (int)((sqrtf(8.f * tt + 1.f) - 1.f) * 0.5f);
+            while (ti * (ti + 1) / 2 > tt) --ti;
+            while ((ti + 1) * (ti + 2) / 2 <= tt) ++ti;
+            const int tj = tt - ti * (ti + 1) / 2;
+            const int ri = i0 + 2 * ti, cj = i0 + 2 * tj;
+            W a00{}, a01{}, a10{}, a11{};
+#pragma unroll 4
+            for (int t = 0; t < kSub; ++t) {
+                const W g0 = sG[t * nb + ri], g1 = sG[t * nb + ri + 1];
+                const W l0 = opc<CJ>(sA[(b0 + t) * ld + cj]), l1 = opc<CJ>(sA[(b0 + t) * ld + cj + 1]);
+                a00 += g0 * l0; a01 += g0 * l1; a10 += g1 * l0; a11 += g1 * l1;
+            }
+            sA[cj * ld + ri] -= a00;
+            sA[cj * ld + ri + 1] -= a10;
+            sA[(cj + 1) * ld + ri + 1] -= a11;
+            if (ri > cj) sA[(cj + 1) * ld + ri] -= a01;
+        }
         __syncthreads();
     }
-    // outputs: U = op(L11^{-1})^T (row-major, for the panel), L11^{-1}
-    // (column-major for the forward sweep, row-major for the backward sweep),
-    // L11 with unit diagonal, and D
+    // ---- off-diagonal blocks of L^{-1}, one block row at a time ----
+    for (int i = 1; i < nb / kSub; ++i) {
+        for (int idx = tid; idx < i * kSub * kSub; idx += kThreads) {
+            const int j = idx / (kSub * kSub), e = idx % (kSub * kSub), r = e % kSub, c = e / kSub;
+            const int R = kSub * i + r;
+            // k = j: Linv_jj is unit lower triangular
+            W tsum = sA[(kSub * j + c) * ld + R];
+            for (int t = c + 1; t < kSub; ++t) tsum += sA[(kSub * j + t) * ld + R] * sA[(kSub * j + t) * ld + kSub * j + c];
+            for (int kk = j + 1; kk < i; ++kk)
+#pragma unroll 4
+                for (int t = 0; t < kSub; ++t) tsum += sA[(kSub * kk + t) * ld + R] * sA[(kSub * kk + t) * ld + kSub * j + c];
+            sG[(j * kSub + c) * kSub + r] = tsum;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < i * kSub * kSub; idx += kThreads) {
+            const int j = idx / (kSub * kSub), e = idx % (kSub * kSub), r = e % kSub, c = e / kSub;
+            const int R = kSub * i + r;
+            W v = sG[(j * kSub + c) * kSub + r];
+            for (int t = 0; t < r; ++t) v += sA[R * ld + kSub * i + t] * sG[(j * kSub + c) * kSub + t];
+            sA[R * ld + kSub * j + c] = W{} - v;
+        }
+        __syncthreads();
+    }
+    // ---- outputs, each written with consecutive threads on consecutive addresses ----
     X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
     X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)(k / nb) * nb * nb;
-    X* DvT = dinvT ? reinterpret_cast<X*>(dinvT) + f.dinv + (int64_t)(k / nb) * nb * nb : nullptr;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int i = tr + 16 * a, c = tc + 16 * b;
+    for (int idx = tid; idx < nb * nb; idx += kThreads) {
+        const int i = idx % nb, c = idx / nb;
+        const bool in = i < kb && c < kb && i >= c;
+        const W linv = i == c ? vone<W>() : (i > c ? sA[i * ld + c] : W{});
+        U[c * nb + i] = in ? conv<X>(opc<CJ>(linv)) : X{};
+        Dv[i + c * nb] = in ? conv<X>(linv) : X{};
+        if (in) stv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m, i == c ? vone<X>() : conv<X>(sA[c * ld + i]));
+    }
+    if (dinvT) {
+        X* DvT = reinterpret_cast<X*>(dinvT) + f.dinv + (int64_t)(k / nb) * nb * nb;
+        for (int idx = tid; idx < nb * nb; idx += kThreads) {
+            const int c = idx % nb, i = idx / nb;
             const bool in = i < kb && c < kb && i >= c;
-            U[c * nb + i] = in ? conv<X>(opc<CJ>(Xm[a][b])) : X{};
-            Dv[i + c * nb] = in ? conv<X>(Xm[a][b]) : X{};
-            if (DvT) DvT[i * nb + c] = in ? conv<X>(Xm[a][b]) : X{};
-            if (in) {
-                if (i > c) stv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m, conv<X>(A[a][b]));
-                else {
-                    stv<T, C>(L, f.L + (k + i) + (int64_t)(k + c) * f.m, vone<X>());
-                    reinterpret_cast<W*>(D)[f.off + k + i] = A[a][b];
-                }
-            }
+            const W linv = i == c ? vone<W>() : (i > c ? sA[i * ld + c] : W{});
+            DvT[c + i * nb] = in ? conv<X>(linv) : X{};
         }
+    }
+    if (tid < kb) reinterpret_cast<DV<C>*>(D)[f.off + k + tid] = conv<DV<C>>(s_d[tid]);
 }
 
 // ---------------------------------------------------------------------------
@@ -350,14 +491,27 @@ __global__ void __launch_bounds__(kThreads) gemm_update_kernel(const GemmProb* _
 // ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
+// Working precision of the diagonal-block LDL: FP64 for FP64 storage; for
+// FP32 storage FP32 unless the plan asks for FP64 (CLIQGPU_DIAG_FP64=1).
+// The pivots are stored in FP64 either way.
+template <class T, bool C, bool CJ, class WT>
+static void launch_diag(const Plan& P, const Launch& ln, T* L, const int4* items) {
+    diag_ldl_kernel<T, C, CJ, WT><<<(unsigned)ln.nblocks, kThreads, diag_smem_bytes<WT, C>(), P.stream>>>(
+        P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), reinterpret_cast<T*>(P.dinv),
+        reinterpret_cast<T*>(P.dinvT), P.status);
+}
+
 template <class T, bool C, bool CJ>
 static int run_factor_impl(Plan& P) {
     using X = V<T, C>;
     using W = DV<C>;
-    const size_t smem_diag = 0;
+    const size_t smem_diag = diag_smem_bytes<double, C>();
     const size_t smem_panel = sizeof(X) * (kTile * kTile + kTile * (kTile + 1) + kTile);
     static bool attr_done = false;
     if (!attr_done) {
+        cudaFuncSetAttribute(diag_ldl_kernel<T, C, CJ, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_diag);
+        cudaFuncSetAttribute(diag_ldl_kernel<T, C, CJ, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)diag_smem_bytes<T, C>());
         cudaFuncSetAttribute(panel_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel);
         attr_done = true;
     }
@@ -380,9 +534,8 @@ static int run_factor_impl(Plan& P) {
                 extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
                 break;
             case Launch::DIAG:
-                diag_ldl_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, smem_diag, P.stream>>>(
-                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), reinterpret_cast<T*>(P.dinv),
-                    reinterpret_cast<T*>(P.dinvT), P.status);
+                if (std::is_same<T, float>::value && !P.diag_fp64) launch_diag<T, C, CJ, T>(P, ln, L, items);
+                else launch_diag<T, C, CJ, double>(P, ln, L, items);
                 break;
             case Launch::PANEL:
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
@@ -512,6 +665,7 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
     using X = V<T, C>;
     const size_t smem_panel = sizeof(X) * (kTile * kTile + kTile * (kTile + 1) + kTile);
     cudaFuncSetAttribute(panel_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_panel);
+    cudaFuncSetAttribute(diag_ldl_kernel<T, C, CJ, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem_bytes<T, C>());
     const FrontDev* F = reinterpret_cast<const FrontDev*>(base + kOffFront);
     double* D = reinterpret_cast<double*>(base + kOffD);
     T* tinv = reinterpret_cast<T*>(base + kOffTinv);
@@ -521,7 +675,7 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
     const int64_t* prefix = reinterpret_cast<const int64_t*>(base + kOffPrefix);
     int32_t* status = reinterpret_cast<int32_t*>(base + kOffStatus);
     for (const Step& s : steps) {
-        diag_ldl_kernel<T, C, CJ><<<1, kThreads, 0, st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, nullptr, status);
+        diag_ldl_kernel<T, C, CJ, T><<<1, kThreads, diag_smem_bytes<T, C>(), st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, nullptr, status);
         if (s.panel_blocks > 0)
             panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr);
         if (s.prob >= 0)

@@ -272,7 +272,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 const bool leaf = f.cmap < 0;
                 for (int j0 = 0; j0 < f.m; j0 += kEACols) {
                     if (leaf && j0 + kEACols <= f.n) continue;
-                    push_item(s, j0, 0, 0);
+                    for (int i0 = j0 / kEARows * kEARows; i0 < f.m; i0 += kEARows) push_item(s, j0, i0, 0);
                 }
             }
             ln.nitems = (int32_t)(items.size() / 4 - ln.items);
@@ -571,6 +571,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     P.nb = kTile;
     if (const char* e = getenv("CLIQGPU_TENSOR_CORES")) P.use_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_OUTER_BLOCK")) P.outer_nb = std::max(kTile, atoi(e));
+    if (const char* e = getenv("CLIQGPU_DIAG_FP64")) P.diag_fp64 = atoi(e) != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
