@@ -261,7 +261,7 @@ class DistSymmFrontTree:
         check(_capi.load().cliqgpu_set_profiling(self._h, int(bool(on))))
 
     PROFILE_KEYS = ["extend_add_ms", "diag_ms", "panel_ms", "trail_ms", "schur_ms", "trail_flops", "schur_flops",
-                    "extend_add_bytes", "trail_launches", "schur_launches", "factor_ms"]
+                    "extend_add_bytes", "trail_launches", "schur_launches", "factor_ms", "pack_ms"]
 
     def profile(self):
         out = np.zeros(16)

@@ -64,6 +64,8 @@ struct FrontDev {
     int32_t pool;       // parity of the depth
     int32_t flag_base;  // first chain-solve flag of this front
     int64_t dinv;       // inverse diagonal blocks (ceil(n/64) blocks of 64 x 64) in the dinv store
+    int64_t eblk;       // 2xFP16 split: per (row, 64-column block) largest |component| of L and of D op(L), m x nT
+    int64_t erow;       // 2xFP16 split: per row, the same over all blocks so far (m)
 };
 
 // One GEMM update problem: C -= A diag(d) op(B)^T restricted to i >= j.
@@ -71,6 +73,8 @@ struct GemmProb {
     int64_t A, B, C, d;   // A, B in the arena; C in the arena (cpool < 0) or a pool; d in the D array
     int32_t lda, ldc, M, N, K, cpool;
     int64_t packA, packB; // tensor-core path: float offsets of the packed operands in the pack buffer
+    int64_t scaleA, scaleB;   // FP16 split: float offsets of the per-row inverse scales (A rows, S rows)
+    int32_t front, row0, kb0, nkb;   // operand rows start at front row row0; K covers 64-blocks kb0 .. kb0+nkb-1 (0: all)
 };
 
 // One operand panel to pack for the tensor cores: R rows x K columns of the
@@ -79,6 +83,9 @@ struct GemmProb {
 struct PackJob {
     int64_t src, dst, d;
     int32_t R, K, ld, tile_rows;
+    int64_t dst_scale;    // FP16 split: float offset of the R (padded to tiles) inverse row scales
+    int64_t emax;         // FP16 split: row maxima of the job's first row (block kb0), in the eblk / erow arrays
+    int32_t enT, nkb;     // row stride of eblk (blocks per row); blocks in K (0: use erow)
 };
 
 struct Launch {
@@ -96,11 +103,13 @@ struct Launch {
     int32_t pack_njobs = 0;
 };
 
-// per-kernel-kind device time of the last profiled factorization (ms) and work
+// per-kernel-kind device time of the last profiled factorization (ms) and
+// work; on the tensor path trail / schur time is the GEMM alone and the
+// operand packing is PROF_PACK_MS
 enum ProfSlot {
     PROF_EA_MS = 0, PROF_DIAG_MS, PROF_PANEL_MS, PROF_TRAIL_MS, PROF_SCHUR_MS,
     PROF_TRAIL_FLOPS, PROF_SCHUR_FLOPS, PROF_EA_BYTES, PROF_TRAIL_LAUNCHES, PROF_SCHUR_LAUNCHES,
-    PROF_FACTOR_MS, PROF_SLOTS = 16
+    PROF_FACTOR_MS, PROF_PACK_MS, PROF_SLOTS = 16
 };
 
 struct SolveLevel {
@@ -148,6 +157,12 @@ struct Plan {
     void* dinvT = nullptr;        // the same blocks row-major (backward sweep)
     void* subT = nullptr;         // per pivot block b: tile (b+1, b) of the front's L, row-major (backward sweep)
     void* partial = nullptr;      // per pivot block: 64 x kSolveRhsChunk partial sums from the sweep workers
+    // 2xFP16 split: row maxima (float bits) of L panels and of D op(L) panels,
+    // [A | S] halves of eblk_total and erow_total entries
+    uint32_t* eblk = nullptr;
+    uint32_t* erow = nullptr;
+    int64_t eblk_total = 0, erow_total = 0;
+    bool f16_scales() const { return tensor_path() && split_f16; }
     int64_t dinv_elems = 0;
     FrontDev* fronts = nullptr;
     int32_t* cmaps = nullptr;
@@ -184,6 +199,9 @@ struct Plan {
     // FP32 storage: diagonal-block LDL in FP64 arithmetic (CLIQGPU_DIAG_FP64=1) instead of FP32
     int diag_fp64 = 0;
     bool tensor_path() const { return use_tc && precision == CLIQ_FP32; }
+    // operand split on the tensor path: 2 x FP16 with per-row power-of-two
+    // scales (default) or 3 x TF32 (CLIQGPU_SPLIT=tf32)
+    int split_f16 = 1;
     // width of the outer column block whose trailing update is deferred (multiple of nb)
     int outer_nb = 256;
     // optional per-launch CUDA-event timing of the factorization
@@ -211,7 +229,8 @@ int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
 
 int check_cuda(const char* where);
-int launch_tc2(Plan& P, const Launch& ln);
+// packs the launch's operands, records `between` (if given), runs the GEMM
+int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between);
 size_t tc2_smem(bool cplx);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);

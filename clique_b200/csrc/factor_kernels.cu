@@ -36,6 +36,11 @@ namespace cliqgpu {
 
 constexpr int kThreads = 256;
 
+__device__ __forceinline__ float cabsmax(float v) { return fabsf(v); }
+__device__ __forceinline__ float cabsmax(double v) { return (float)fabs(v); }
+__device__ __forceinline__ float cabsmax(cx<float> v) { return fmaxf(fabsf(v.r), fabsf(v.i)); }
+__device__ __forceinline__ float cabsmax(cx<double> v) { return (float)fmax(fabs(v.r), fabs(v.i)); }
+
 // ---------------------------------------------------------------------------
 // 1. extend-add (gather form)
 //
@@ -331,7 +336,8 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
                                                          T* __restrict__ L, const double* __restrict__ D, const T* __restrict__ tinv,
-                                                         T* __restrict__ subT) {
+                                                         T* __restrict__ subT, uint32_t* __restrict__ eblk, uint32_t* __restrict__ erow,
+                                                         int64_t eblk_total, int64_t erow_total) {
     using X = V<T, C>;
     using W = DV<C>;
     constexpr int nb = kTile, ldA = kTile + 1;
@@ -384,6 +390,39 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restr
         for (int a = 0; a < 4; ++a) {
             const int r = ty + 16 * a;
             if (r < rows) stv<T, C>(L, f.L + (r0 + r) + (int64_t)(k + c) * f.m, acc[a][b] * rd);
+        }
+    }
+    // 2xFP16 split: largest |component| of each row of L21 and of S21 = D L21
+    // over this block's columns (float bits, order-preserving for >= 0), per
+    // block and as a running maximum over the front's blocks
+    if (eblk) {
+        const int nT = (f.n + nb - 1) / nb;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            float ml = 0.f, ms = 0.f;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int c = tx + 16 * b;
+                if (c < kb) {
+                    const X v = acc[a][b];
+                    ms = fmaxf(ms, cabsmax(v));
+                    ml = fmaxf(ml, cabsmax(v * sR[c]));
+                }
+            }
+#pragma unroll
+            for (int o = 8; o >= 1; o >>= 1) {
+                ml = fmaxf(ml, __shfl_xor_sync(0xffffffffu, ml, o, 16));
+                ms = fmaxf(ms, __shfl_xor_sync(0xffffffffu, ms, o, 16));
+            }
+            const int r = ty + 16 * a;
+            if (tx == 0 && r < rows) {
+                const int64_t row = r0 + r;
+                const int64_t eb = f.eblk + row * nT + k / nb;
+                eblk[eb] = __float_as_uint(ml);
+                eblk[eblk_total + eb] = __float_as_uint(ms);
+                atomicMax(&erow[f.erow + row], __float_as_uint(ml));
+                atomicMax(&erow[erow_total + f.erow + row], __float_as_uint(ms));
+            }
         }
     }
     // the first row block under a full diagonal block is tile (b+1, b) of the
@@ -520,15 +559,16 @@ static int run_factor_impl(Plan& P) {
     T* p1 = reinterpret_cast<T*>(P.pool[1]);
     const int4* items = reinterpret_cast<const int4*>(P.items);
     int64_t launches = 0;
-    if (P.profile && P.events.size() < 2 * P.launches.size()) {
+    if (P.profile && P.events.size() < 3 * P.launches.size()) {
         const size_t old = P.events.size();
-        P.events.resize(2 * P.launches.size());
+        P.events.resize(3 * P.launches.size());
         for (size_t i = old; i < P.events.size(); ++i) cudaEventCreate(&P.events[i]);
     }
+    if (P.erow) cudaMemsetAsync(P.erow, 0, sizeof(uint32_t) * 2 * (size_t)P.erow_total, P.stream);
     for (size_t li = 0; li < P.launches.size(); ++li) {
         const Launch& ln = P.launches[li];
         if (ln.nblocks <= 0) continue;
-        if (P.profile) cudaEventRecord(P.events[2 * li], P.stream);
+        if (P.profile) cudaEventRecord(P.events[3 * li], P.stream);
         switch (ln.kind) {
             case Launch::EXTEND_ADD:
                 extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
@@ -539,17 +579,18 @@ static int run_factor_impl(Plan& P) {
                 break;
             case Launch::PANEL:
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
-                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), reinterpret_cast<T*>(P.subT));
+                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), reinterpret_cast<T*>(P.subT),
+                    P.eblk, P.erow, P.eblk_total, P.erow_total);
                 break;
             case Launch::GEMM:
                 if (std::is_same<T, float>::value && P.tensor_path())
-                    launch_tc2(P, ln);
+                    launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr);
                 else
                     gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(
                         P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
                 break;
         }
-        if (P.profile) cudaEventRecord(P.events[2 * li + 1], P.stream);
+        if (P.profile) cudaEventRecord(P.events[3 * li + 1], P.stream);
         ++launches;
     }
     P.prof_pending = P.profile != 0;
@@ -677,7 +718,8 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
     for (const Step& s : steps) {
         diag_ldl_kernel<T, C, CJ, T><<<1, kThreads, diag_smem_bytes<T, C>(), st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, nullptr, status);
         if (s.panel_blocks > 0)
-            panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr);
+            panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr,
+                                                                               nullptr, nullptr, 0, 0);
         if (s.prob >= 0)
             gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, AL, ABR,
                                                                                ABR, D);

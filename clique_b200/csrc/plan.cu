@@ -75,7 +75,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 }
 
 void free_plan(Plan& P) {
-    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.partial, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
                     P.wpool[1], P.xnodal, P.xwork, P.norms};
@@ -127,6 +127,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     std::vector<int64_t> level_pool(P.max_depth + 1, 0), level_w(P.max_depth + 1, 0);
     P.factor_flops = P.solve_flops = P.factor_entries = 0;
     P.dinv_elems = 0;
+    P.eblk_total = P.erow_total = 0;
     for (int s = 0; s < nn; ++s) {
         FrontDev& f = P.hfronts[s];
         const int64_t nlow = info->lower_ptr[s + 1] - info->lower_ptr[s];
@@ -145,6 +146,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         f.lower = info->lower_ptr[s];
         f.dinv = P.dinv_elems;
         P.dinv_elems += (int64_t)((f.n + kTile - 1) / kTile) * kTile * kTile;
+        f.eblk = P.eblk_total;
+        P.eblk_total += (int64_t)f.m * ((f.n + kTile - 1) / kTile);
+        f.erow = P.erow_total;
+        P.erow_total += f.m;
         f.cmap = -1;
         f.CU[0] = f.CU[1] = -1;
         f.CW[0] = f.CW[1] = 0;
@@ -235,14 +240,33 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             int64_t off = 0, blocks = 0;
             ln.pack_items = (int64_t)packjobs.size();
             ln.pack_prefix = (int64_t)prefix.size();
+            // 3xTF32: one pack CTA per (row tile, 8-wide k step); 2xFP16: one
+            // pack CTA per row tile (16-wide k steps, same bytes per block),
+            // followed by the tile's inverse row scales
+            const bool f16 = P.split_f16 != 0;
+            const int kstep = f16 ? 16 : 8;
             for (auto& pr : lst) {
-                const int64_t nk = (pr.K + 7) / 8;
-                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, 128};
+                const int64_t nk = (pr.K + kstep - 1) / kstep;
+                const int64_t tA = (pr.M + 127) / 128, tB = (pr.N + 255) / 256;
+                const FrontDev& fr = P.hfronts[pr.front];
+                const int nT = (fr.n + kTile - 1) / kTile;
+                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, 128, 0, 0, nT, pr.nkb};
+                a.emax = pr.nkb > 0 ? fr.eblk + (int64_t)pr.row0 * nT + pr.kb0 : fr.erow + pr.row0;
                 pr.packA = off;
-                off += (pr.M + 127) / 128 * nk * blkA;
-                PackJob b{pr.B, off, pr.d, pr.N, pr.K, pr.lda, 256};
+                off += tA * nk * blkA;
+                a.dst_scale = pr.scaleA = off;
+                if (f16) off += tA * 128;
+                PackJob b = a;
+                b.src = pr.B;
+                b.dst = off;
+                b.d = pr.d;
+                b.R = pr.N;
+                b.tile_rows = 256;
+                b.emax += pr.nkb > 0 ? P.eblk_total : P.erow_total;   // the D op(L) half
                 pr.packB = off;
-                off += (pr.N + 255) / 256 * nk * blkB;
+                off += tB * nk * blkB;
+                b.dst_scale = pr.scaleB = off;
+                if (f16) off += tB * 256;
                 for (const PackJob& j : {a, b}) {
                     prefix.push_back(blocks);
                     blocks += (int64_t)((j.R + j.tile_rows - 1) / j.tile_rows) * nk;
@@ -329,6 +353,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                     const int N = std::min(K0 + nbo, f.n) - k - kb;
                     if (N > 0) {
                         GemmProb pr{};
+                        pr.front = a.first;
+                        pr.row0 = k + kb;
+                        pr.kb0 = k / kTile;
+                        pr.nkb = 1;
                         pr.A = f.L + (k + kb) + (int64_t)k * f.m;
                         pr.B = pr.A;
                         pr.C = f.L + (k + kb) + (int64_t)(k + kb) * f.m;
@@ -353,6 +381,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 const int c1 = K0 + nbo;
                 if (f.n <= c1) continue;
                 GemmProb pr{};
+                pr.front = s;
+                pr.row0 = c1;
+                pr.kb0 = K0 / kTile;
+                pr.nkb = nbo / kTile;
                 pr.A = f.L + c1 + (int64_t)K0 * f.m;
                 pr.B = pr.A;
                 pr.C = f.L + c1 + (int64_t)c1 * f.m;
@@ -372,6 +404,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             const FrontDev& f = P.hfronts[s];
             if (f.u <= 0 || f.n <= 0) continue;
             GemmProb pr{};
+            pr.front = s;
+            pr.row0 = f.n;
+            pr.kb0 = 0;
+            pr.nkb = 0;
             pr.A = f.L + f.n;
             pr.B = pr.A;
             pr.C = f.U;
@@ -475,6 +511,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.dinvT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.subT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.partial, (size_t)P.flags_total * kTile * kSolveRhsChunk * eb));
+    if (P.f16_scales()) {
+        TRY(dev_alloc(P, (void**)&P.eblk, sizeof(uint32_t) * 2 * (size_t)std::max<int64_t>(P.eblk_total, 1)));
+        TRY(dev_alloc(P, (void**)&P.erow, sizeof(uint32_t) * 2 * (size_t)std::max<int64_t>(P.erow_total, 1)));
+    }
     TRY(dev_upload(P, &P.fronts, P.hfronts));
     TRY(dev_upload(P, &P.cmaps, cmaps));
     std::vector<int32_t> lowv(low, low + info->lower_ptr[nn]);
@@ -572,6 +612,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_TENSOR_CORES")) P.use_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_OUTER_BLOCK")) P.outer_nb = std::max(kTile, atoi(e));
     if (const char* e = getenv("CLIQGPU_DIAG_FP64")) P.diag_fp64 = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_SPLIT")) P.split_f16 = strcmp(e, "tf32") != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
@@ -799,7 +840,13 @@ int cliqgpu_profile_read(cliqgpu_plan h, double* out, int32_t nout) {
             const Launch& ln = P.launches[li];
             if (ln.nblocks <= 0) continue;
             float ms = 0;
-            cudaEventElapsedTime(&ms, P.events[2 * li], P.events[2 * li + 1]);
+            cudaEventElapsedTime(&ms, P.events[3 * li], P.events[3 * li + 1]);
+            if (ln.kind == Launch::GEMM && P.tensor_path()) {
+                float pk = 0;
+                cudaEventElapsedTime(&pk, P.events[3 * li], P.events[3 * li + 2]);
+                P.prof[PROF_PACK_MS] += pk;
+                ms -= pk;
+            }
             if (first < 0) first = (int)li;
             last = (int)li;
             switch (ln.kind) {
@@ -814,7 +861,7 @@ int cliqgpu_profile_read(cliqgpu_plan h, double* out, int32_t nout) {
         }
         if (first >= 0) {
             float ms = 0;
-            cudaEventElapsedTime(&ms, P.events[2 * first], P.events[2 * last + 1]);
+            cudaEventElapsedTime(&ms, P.events[3 * first], P.events[3 * last + 1]);
             P.prof[PROF_FACTOR_MS] = ms;
         }
         cudaGetLastError();

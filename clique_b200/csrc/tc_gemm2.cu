@@ -18,15 +18,26 @@
 //    tcgen05.ld and update C.
 // The 3xTF32 split: X = X_hi + X_lo, X_hi = X with the low 13 mantissa bits
 // cleared; A B ~= A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32.
+// The 2xFP16 split (default) keeps the same three products at twice the
+// tensor rate: each operand row r is scaled by a power of two s_r that puts
+// its largest |Re|, |Im| over the GEMM's K range in [2^14, 2^15), then
+// X_hi = fp16(s X), X_lo = fp16(s X - X_hi): 22 significant bits like the
+// TF32 pair (FP16 and TF32 both carry 10 explicit mantissa bits), and only
+// entries below 2^-38 of their row's largest lose relative precision.  The
+// blocks hold 16-wide k steps in the same bytes as the 8-wide TF32 steps;
+// tcgen05.mma kind::f16 (K = 16, FP32 accumulation) replaces kind::tf32 and
+// the epilogue multiplies by 1 / (s_i s_j).
 // Complex: Re C -= Ar Sr^T - Ai Si^T (negate-A bit), Im C -= Ar Si^T + Ai Sr^T.
 // All waits are bounded by wall-clock time and report a wait site.
+#include <cuda_fp16.h>
+
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
 
 namespace cliqgpu {
 namespace tc2 {
 
-constexpr int kBM = 128, kBN = 256, kKS = 8;
+constexpr int kBM = 128, kBN = 256, kKS = 8;   // kKS: TF32 k step (an FP16 step is 2 * kKS wide, same bytes)
 constexpr int kStages = 4;
 constexpr int kThreads = 192;                 // warps 0-3 epilogue, 4 TMA producer, 5 MMA issuer
 constexpr uint64_t kWaitNs = 200000000ull;
@@ -92,6 +103,18 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool negA) {
 __device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d), "l"(a), "l"(b), "r"(id), "r"(acc)
+        : "memory");
+}
+// kind::f16 instruction descriptor: F32 accumulator (bits 4-5 = 1), A and B
+// FP16 (format 0 at bits 7-9 and 10-12), negate-A bit 13, N >> 3 at bit 17,
+// M >> 4 at bit 24
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool negA) {
+    return (1u << 4) | ((negA ? 1u : 0u) << 13) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(d), "l"(a), "l"(b), "r"(id), "r"(acc)
         : "memory");
 }
@@ -175,9 +198,111 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ j
 }
 
 // ---------------------------------------------------------------------------
+// 2xFP16 pack: one CTA per (row tile, 16-wide k step) block of one job;
+// thread = row.  The row's scale comes from the largest |component| over the
+// job's K columns, which the panel kernel recorded per (row, 64-column
+// block) and as a running maximum per row; the CTA of the first k step also
+// stores the row's inverse scale for the GEMM epilogue.
+// ---------------------------------------------------------------------------
+constexpr int kKS16 = 2 * kKS;
+
+template <bool C, bool CJ>
+__device__ __forceinline__ V<float, C> pack_load(const PackJob& jb, const float* __restrict__ L, const double* __restrict__ D, int r,
+                                                 int k) {
+    using X = V<float, C>;
+    using W = DV<C>;
+    X v{};
+    if (r < jb.R && k < jb.K) {
+        v = ldv<float, C>(L, jb.src + r + (int64_t)k * jb.ld);
+        if (jb.d >= 0) v = conv<X>(reinterpret_cast<const W*>(D)[jb.d + k]) * opc<CJ>(v);
+    }
+    return v;
+}
+__device__ __forceinline__ float absmax(float v) { return fabsf(v); }
+__device__ __forceinline__ float absmax(cx<float> v) { return fmaxf(fabsf(v.r), fabsf(v.i)); }
+
+__device__ __forceinline__ uint32_t h2pack(__half a, __half b) {
+    return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+// one plane chunk: 8 consecutive k of one row as fp16 hi and lo
+__device__ __forceinline__ void split8(const float* y, uint4& hi, uint4& lo) {
+    __half h[8], l[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        h[q] = __float2half_rn(y[q]);
+        l[q] = __float2half_rn(y[q] - __half2float(h[q]));
+    }
+    hi = make_uint4(h2pack(h[0], h[1]), h2pack(h[2], h[3]), h2pack(h[4], h[5]), h2pack(h[6], h[7]));
+    lo = make_uint4(h2pack(l[0], l[1]), h2pack(l[2], l[3]), h2pack(l[4], l[5]), h2pack(l[6], l[7]));
+}
+
+template <bool C, bool CJ>
+__global__ void __launch_bounds__(256) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+                                                       const float* __restrict__ L, const double* __restrict__ D,
+                                                       const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
+                                                       float* __restrict__ out) {
+    using X = V<float, C>;
+    const int64_t bid = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const PackJob jb = jobs[lo];
+    const int64_t blk = bid - prefix[lo];
+    const int nks = (jb.K + kKS16 - 1) / kKS16;
+    const int tile = (int)(blk / nks), ks = (int)(blk % nks);
+    const int row = threadIdx.x;
+    if (row >= jb.tile_rows) return;
+    const int r = tile * jb.tile_rows + row;
+    X v[kKS16];
+#pragma unroll
+    for (int q = 0; q < kKS16; ++q) v[q] = pack_load<C, CJ>(jb, L, D, r, ks * kKS16 + q);
+    float mx = 0.f;
+    if (r < jb.R) {
+        if (jb.nkb > 0) {
+            for (int b = 0; b < jb.nkb; ++b) mx = fmaxf(mx, __uint_as_float(eblk[jb.emax + (int64_t)r * jb.enT + b]));
+        } else {
+            mx = __uint_as_float(erow[jb.emax + r]);
+        }
+    }
+    // s = 2^(14 - e) for mx in [2^e, 2^(e+1)): s * mx in [2^14, 2^15)
+    int e = mx > 0.f ? ((__float_as_int(mx) >> 23) & 0xff) - 127 : 0;
+    e = max(-100, min(100, e));
+    const float s = __int_as_float((127 + 14 - e) << 23);
+    if (ks == 0) out[jb.dst_scale + r] = __int_as_float((127 - 14 + e) << 23);
+    // planes (re_hi, re_lo, im_hi, im_lo) of this k step
+    constexpr int planes = C ? 4 : 2;
+    const int64_t plane_bytes = (int64_t)jb.tile_rows * kKS16 * 2;
+    uint8_t* base = reinterpret_cast<uint8_t*>(out + jb.dst) + blk * plane_bytes * planes;
+    float y[kKS16];
+    uint4 h, l;
+#pragma unroll
+    for (int q = 0; q < kKS16; ++q) {
+        if constexpr (C) y[q] = v[q].r * s; else y[q] = v[q] * s;
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        split8(y + 8 * c, h, l);
+        *reinterpret_cast<uint4*>(base + 0 * plane_bytes + core_off(row, c)) = h;
+        *reinterpret_cast<uint4*>(base + 1 * plane_bytes + core_off(row, c)) = l;
+    }
+    if constexpr (C) {
+#pragma unroll
+        for (int q = 0; q < kKS16; ++q) y[q] = v[q].i * s;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            split8(y + 8 * c, h, l);
+            *reinterpret_cast<uint4*>(base + 2 * plane_bytes + core_off(row, c)) = h;
+            *reinterpret_cast<uint4*>(base + 3 * plane_bytes + core_off(row, c)) = l;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // GEMM on packed operands
 // ---------------------------------------------------------------------------
-template <bool C>
+template <bool C, bool F16>
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
                                                               int nprobs, const float* __restrict__ pack, float* __restrict__ L,
                                                               float* __restrict__ pool0, float* __restrict__ pool1,
@@ -209,7 +334,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
     }
     const int ti = 2 * tj + (int)t;
     const int i0 = ti * kBM, j0 = tj * kBN;
-    const int nk = (pr.K + kKS - 1) / kKS;
+    constexpr int kstep = F16 ? 2 * kKS : kKS;
+    const int nk = (pr.K + kstep - 1) / kstep;
     const uint8_t* packA = reinterpret_cast<const uint8_t*>(pack + pr.packA) + (int64_t)ti * nk * CF::kABytes;
     const uint8_t* packB = reinterpret_cast<const uint8_t*>(pack + pr.packB) + (int64_t)tj * nk * CF::kBBytes;
 
@@ -243,7 +369,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
         __syncwarp();
     } else if (warp == 5) {
         // ---- MMA issuer ----
-        const uint32_t idp = idesc_tf32(kBM, kBN, false), idn = idesc_tf32(kBM, kBN, true);
+        const uint32_t idp = F16 ? idesc_f16(kBM, kBN, false) : idesc_tf32(kBM, kBN, false);
+        const uint32_t idn = F16 ? idesc_f16(kBM, kBN, true) : idesc_tf32(kBM, kBN, true);
+        auto mma = [](uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+            if constexpr (F16) mma_f16(d, a, b, id, acc); else mma_tf32(d, a, b, id, acc);
+        };
         const uint32_t dre = tmem, dim = tmem + kBN;
         for (int it = 0; it < nk; ++it) {
             const int s = it % kStages;
@@ -255,19 +385,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
                 auto A = [&](int p) { return sdesc(a + p * pa, 128, 256); };
                 auto B = [&](int p) { return sdesc(b + p * pb, 128, 256); };
                 const uint32_t acc = it > 0 ? 1u : 0u;
-                mma_tf32(dre, A(0), B(0), idp, acc);
-                mma_tf32(dre, A(0), B(1), idp, 1u);
-                mma_tf32(dre, A(1), B(0), idp, 1u);
+                mma(dre, A(0), B(0), idp, acc);
+                mma(dre, A(0), B(1), idp, 1u);
+                mma(dre, A(1), B(0), idp, 1u);
                 if constexpr (C) {
-                    mma_tf32(dre, A(2), B(2), idn, 1u);
-                    mma_tf32(dre, A(2), B(3), idn, 1u);
-                    mma_tf32(dre, A(3), B(2), idn, 1u);
-                    mma_tf32(dim, A(0), B(2), idp, acc);
-                    mma_tf32(dim, A(0), B(3), idp, 1u);
-                    mma_tf32(dim, A(1), B(2), idp, 1u);
-                    mma_tf32(dim, A(2), B(0), idp, 1u);
-                    mma_tf32(dim, A(2), B(1), idp, 1u);
-                    mma_tf32(dim, A(3), B(0), idp, 1u);
+                    mma(dre, A(2), B(2), idn, 1u);
+                    mma(dre, A(2), B(3), idn, 1u);
+                    mma(dre, A(3), B(2), idn, 1u);
+                    mma(dim, A(0), B(2), idp, acc);
+                    mma(dim, A(0), B(3), idp, 1u);
+                    mma(dim, A(1), B(2), idp, 1u);
+                    mma(dim, A(2), B(0), idp, 1u);
+                    mma(dim, A(2), B(1), idp, 1u);
+                    mma(dim, A(3), B(0), idp, 1u);
                 }
                 mma_commit(&empty[s]);
                 if (it == nk - 1) mma_commit(done);
@@ -283,6 +413,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
             const int i = i0 + warp * 32 + lane;
             const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
             const bool vrow = i < pr.M;
+            // 2xFP16: undo the row scales of A (this thread's row) and S (columns)
+            const float sa = F16 && vrow ? pack[pr.scaleA + i] : 1.f;
 #pragma unroll 1
             for (int c0 = 0; c0 < kBN; c0 += 16) {
                 if (j0 + c0 >= pr.N || j0 + c0 > i0 + kBM - 1) break;   // warp-uniform: nothing left in this tile row block
@@ -295,8 +427,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
                         const int j = j0 + c0 + q;
                         if (j < pr.N && i >= j) {
                             const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
-                            if constexpr (C) red_sub2(Cb + 2 * e, re[q], im[q]);
-                            else red_sub(Cb + e, re[q]);
+                            float f = 1.f;
+                            if constexpr (F16) f = sa * __ldg(pack + pr.scaleB + j);
+                            if constexpr (C) red_sub2(Cb + 2 * e, re[q] * f, im[q] * f);
+                            else red_sub(Cb + e, re[q] * f);
                         }
                     }
                 }
@@ -318,28 +452,37 @@ size_t tc2_smem(bool cplx) {
 }
 
 // pack the launch's operands, then run the tensor-core GEMM
-int launch_tc2(Plan& P, const Launch& ln) {
+template <bool C, bool CJ, bool F16>
+static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between) {
     float* L = reinterpret_cast<float*>(P.L);
     float* p0 = reinterpret_cast<float*>(P.pool[0]);
     float* p1 = reinterpret_cast<float*>(P.pool[1]);
     float* pk = reinterpret_cast<float*>(P.pack);
-    const size_t smem = tc2_smem(P.cplx());
-    static bool attr[2] = {false, false};
     const PackJob* jobs = P.packjobs + ln.pack_items;
     const int64_t* jpre = P.prefix + ln.pack_prefix;
+    if constexpr (F16)
+        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
+                                                                                   pk);
+    else
+        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+    if (between) cudaEventRecord(between, P.stream);
+    const size_t smem = tc2_smem(C);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tc2::tc_gemm_kernel<C, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    tc2::tc_gemm_kernel<C, F16><<<(unsigned)ln.nblocks, tc2::kThreads, smem, P.stream>>>(
+        P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
+}
+
+int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between) {
+    const bool f16 = P.split_f16 != 0;
     if (P.cplx()) {
-        if (P.conjugate)
-            tc2::pack_kernel<true, true><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
-        else
-            tc2::pack_kernel<true, false><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
-        if (!attr[1]) { cudaFuncSetAttribute(tc2::tc_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[1] = true; }
-        tc2::tc_gemm_kernel<true><<<(unsigned)ln.nblocks, tc2::kThreads, smem, P.stream>>>(
-            P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
+        if (P.conjugate) { if (f16) launch_pair<true, true, true>(P, ln, between); else launch_pair<true, true, false>(P, ln, between); }
+        else { if (f16) launch_pair<true, false, true>(P, ln, between); else launch_pair<true, false, false>(P, ln, between); }
     } else {
-        tc2::pack_kernel<false, false><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
-        if (!attr[0]) { cudaFuncSetAttribute(tc2::tc_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[0] = true; }
-        tc2::tc_gemm_kernel<false><<<(unsigned)ln.nblocks, tc2::kThreads, smem, P.stream>>>(
-            P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
+        if (f16) launch_pair<false, false, true>(P, ln, between); else launch_pair<false, false, false>(P, ln, between);
     }
     P.total_launches += 1;   // the pack kernel (the caller counts the GEMM)
     return CLIQ_OK;

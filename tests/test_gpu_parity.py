@@ -259,10 +259,13 @@ def test_single_front_ldl(oracle, complex_, precision):
     assert rel(g, np.tril(ABRo)) <= tol
 
 
+@pytest.mark.parametrize("split", ["f16", "tf32"])
 @pytest.mark.parametrize("complex_", [False, True])
-def test_fp32_tensor_core_fronts(oracle, complex_, monkeypatch):
-    """FP32 fronts from the tcgen05 (3xTF32) update kernel agree with the FP64
-    oracle to FP32-level accuracy, and with the CUDA-core FP32 kernel."""
+def test_fp32_tensor_core_fronts(oracle, complex_, split, monkeypatch):
+    """FP32 fronts from the tcgen05 update kernel (2xFP16 split with per-row
+    scales, or 3xTF32) agree with the FP64 oracle to FP32-level accuracy, and
+    with the CUDA-core FP32 kernel."""
+    monkeypatch.setenv("CLIQGPU_SPLIT", split)
     dims, cutoff = (14, 13, 12), 40
     if complex_:
         A = ops.helmholtz_pml_3d(*dims, omega=25.0, velocity=ops.smooth_velocity(dims, 6), b=3)
@@ -283,7 +286,7 @@ def test_fp32_tensor_core_fronts(oracle, complex_, monkeypatch):
         Ls, ds = fronts["0"][s]
         worst_tc = max(worst_tc, rel(Lt, Lo), rel(dt, do))
         worst_cc = max(worst_cc, rel(Ls, Lo), rel(ds, do))
-    # 3xTF32 products are as accurate as FP32 CUDA-core arithmetic (the
+    # the split products are as accurate as FP32 CUDA-core arithmetic (the
     # absolute level reflects unpivoted FP32 LDL^T of an indefinite operator)
     print(f"worst front error: tensor cores {worst_tc:.2e}, CUDA cores {worst_cc:.2e}")
     assert worst_tc <= 4 * worst_cc + 1e-6, (worst_tc, worst_cc)
