@@ -98,6 +98,7 @@ struct Launch {
     int32_t depth;
     double work;          // GEMM: algorithmic flops; EXTEND_ADD: algorithmic bytes
     int32_t schur;        // GEMM: 1 for the Schur-complement update, 0 for an in-panel update
+    int32_t simt = 0;     // GEMM: CUDA-core kernel (64 x 64 tiles) even on the tensor path
     // tensor-core path: operand packing for this GEMM
     int64_t pack_items = 0, pack_prefix = 0, pack_blocks = 0;
     int32_t pack_njobs = 0;
@@ -202,6 +203,9 @@ struct Plan {
     // operand split on the tensor path: 2 x FP16 with per-row power-of-two
     // scales (default) or 3 x TF32 (CLIQGPU_SPLIT=tf32)
     int split_f16 = 1;
+    // in-panel updates (K = 64) on the tensor cores (default) or on the CUDA
+    // cores without operand packing (CLIQGPU_INPANEL_TC=0)
+    int inpanel_tc = 1;
     // width of the outer column block whose trailing update is deferred (multiple of nb)
     int outer_nb = 256;
     // optional per-launch CUDA-event timing of the factorization

@@ -583,7 +583,7 @@ static int run_factor_impl(Plan& P) {
                     P.eblk, P.erow, P.eblk_total, P.erow_total);
                 break;
             case Launch::GEMM:
-                if (std::is_same<T, float>::value && P.tensor_path())
+                if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
                     launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr);
                 else
                     gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(

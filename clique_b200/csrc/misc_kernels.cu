@@ -130,13 +130,21 @@ int launch_spmv(Plan& P, double ar, double ai, const double* X, double br, doubl
 }
 
 // out[j] = sum_i |X[i, j]|^2 (FP64), one block per column
+// Squared 2-norms of the nrhs columns of X (FP64; complex: |re|^2 + |im|^2).
+// Stage 1: kNormChunks CTAs per column write partial sums; stage 2 adds
+// them in a fixed order, so the result does not depend on scheduling.
+constexpr int kNormChunks = 128;
+
 template <bool C>
-__global__ void col_norms_kernel(const double* __restrict__ X, int64_t ld, int64_t n, double* __restrict__ out) {
-    const int j = blockIdx.x;
+__global__ void col_norms_partial_kernel(const double* __restrict__ X, int64_t ld, int64_t n, double* __restrict__ part) {
+    const int j = blockIdx.y;
     const int w = C ? 2 : 1;
     const double* x = X + (int64_t)w * j * ld;
+    const int64_t len = n * w;
+    const int64_t per = (len + kNormChunks - 1) / kNormChunks;
+    const int64_t b = per * blockIdx.x, e = min(len, b + per);
     double s = 0;
-    for (int64_t i = threadIdx.x; i < n * w; i += blockDim.x) s = fma(x[i], x[i], s);
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) s = fma(x[i], x[i], s);
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -144,14 +152,31 @@ __global__ void col_norms_kernel(const double* __restrict__ X, int64_t ld, int64
     if (threadIdx.x < 32) {
         s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (threadIdx.x == 0) out[j] = s;
+        if (threadIdx.x == 0) part[(int64_t)j * kNormChunks + blockIdx.x] = s;
+    }
+}
+
+__global__ void col_norms_final_kernel(const double* __restrict__ part, double* __restrict__ out) {
+    const int j = blockIdx.x;
+    double s = part[(int64_t)j * kNormChunks + threadIdx.x];
+    __shared__ double red[kNormChunks / 32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int q = 0; q < kNormChunks / 32; ++q) t += red[q];
+        out[j] = t;
     }
 }
 
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out) {
-    if (P.cplx()) col_norms_kernel<true><<<nrhs, 1024, 0, P.stream>>>(X, ld, P.n, out);
-    else col_norms_kernel<false><<<nrhs, 1024, 0, P.stream>>>(X, ld, P.n, out);
-    P.total_launches += 1;
+    double* part = P.norms + 2 * P.ws_nrhs;   // kNormChunks * nrhs scratch after the two norm vectors
+    const dim3 grid(kNormChunks, nrhs);
+    if (P.cplx()) col_norms_partial_kernel<true><<<grid, 256, 0, P.stream>>>(X, ld, P.n, part);
+    else col_norms_partial_kernel<false><<<grid, 256, 0, P.stream>>>(X, ld, P.n, part);
+    col_norms_final_kernel<<<nrhs, kNormChunks, 0, P.stream>>>(part, out);
+    P.total_launches += 2;
     return check_cuda("norms");
 }
 

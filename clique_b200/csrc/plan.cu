@@ -212,8 +212,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     // update tiles over the lower trapezoid i >= j: 64 x 64 on the CUDA cores,
     // 128 x 256 (row tile ti needed when ti >= 2 tj) on the tensor cores
     const bool tcp = P.tensor_path();
-    auto tiles_of = [tcp](int M, int N) -> int64_t {
-        if (tcp) {
+    auto tiles_of = [](bool tc, int M, int N) -> int64_t {
+        if (tc) {
             const int64_t Mt = (M + 127) / 128, Nt = (N + 255) / 256;
             return Nt * Mt - Nt * (Nt - 1);
         }
@@ -224,18 +224,20 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     const int planes = P.cplx() ? 4 : 2;
     const int64_t blkA = (int64_t)planes * 128 * 8, blkB = (int64_t)planes * 256 * 8;   // floats per packed block
     int64_t pack_max = 1;
-    auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur) {
+    auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur, bool inpanel) {
         if (lst.empty()) return;
         Launch ln{};
         ln.kind = Launch::GEMM;
         ln.schur = schur;
+        const bool tc = tcp && !(inpanel && !P.inpanel_tc);
+        ln.simt = tcp && !tc;
         for (auto& pr : lst) {
             const double M = pr.M, N = pr.N;
             ln.work += (N * M - N * (N - 1) / 2) * pr.K * (P.cplx() ? 8.0 : 2.0);
         }
         ln.items = (int64_t)probs.size();
         ln.nitems = (int32_t)lst.size();
-        if (tcp) {
+        if (tc) {
             // pack jobs: A (128-row tiles) and S = d op(B) (256-row tiles) of every problem
             int64_t off = 0, blocks = 0;
             ln.pack_items = (int64_t)packjobs.size();
@@ -279,7 +281,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
         ln.prefix = (int64_t)prefix.size();
         int64_t tot = 0;
-        for (auto& pr : lst) { prefix.push_back(tot); tot += tiles_of(pr.M, pr.N); probs.push_back(pr); }
+        for (auto& pr : lst) { prefix.push_back(tot); tot += tiles_of(tc, pr.M, pr.N); probs.push_back(pr); }
         ln.nblocks = tot;
         ln.depth = depth;
         P.launches.push_back(ln);
@@ -373,7 +375,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 pn.nitems = (int32_t)(items.size() / 4 - pn.items);
                 pn.nblocks = pn.nitems;
                 if (pn.nitems) P.launches.push_back(pn);
-                add_gemm(trail, d, 0);
+                add_gemm(trail, d, 0, true);
             }
             std::vector<GemmProb> outer;
             for (int s : lv) {
@@ -397,7 +399,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 pr.cpool = -1;
                 outer.push_back(pr);
             }
-            add_gemm(outer, d, 0);
+            add_gemm(outer, d, 0, false);
         }
         std::vector<GemmProb> schur;
         for (int s : lv) {
@@ -420,7 +422,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             pr.cpool = f.pool;
             schur.push_back(pr);
         }
-        add_gemm(schur, d, 1);
+        add_gemm(schur, d, 1, false);
     }
     P.tinv_slots = max_slots;
     P.pack_floats = tcp ? pack_max : 0;
@@ -556,7 +558,7 @@ static int ensure_workspace(Plan& P, int nrhs) {
     TRY(dev_alloc(P, &P.wpool[1], (size_t)P.wpool_elems[1] * chunk * eb));
     TRY(dev_alloc(P, &P.xnodal, (size_t)P.n * nrhs * eb));
     TRY(dev_alloc(P, (void**)&P.xwork, sizeof(double) * (P.cplx() ? 2 : 1) * 3 * (size_t)P.n * nrhs));
-    TRY(dev_alloc(P, (void**)&P.norms, sizeof(double) * 2 * nrhs));
+    TRY(dev_alloc(P, (void**)&P.norms, sizeof(double) * (2 + 128) * nrhs));   // two norm vectors + partial sums
     P.ws_nrhs = nrhs;
     return CLIQ_OK;
 }
@@ -613,6 +615,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_OUTER_BLOCK")) P.outer_nb = std::max(kTile, atoi(e));
     if (const char* e = getenv("CLIQGPU_DIAG_FP64")) P.diag_fp64 = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_SPLIT")) P.split_f16 = strcmp(e, "tf32") != 0;
+    if (const char* e = getenv("CLIQGPU_INPANEL_TC")) P.inpanel_tc = atoi(e) != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
@@ -841,7 +844,7 @@ int cliqgpu_profile_read(cliqgpu_plan h, double* out, int32_t nout) {
             if (ln.nblocks <= 0) continue;
             float ms = 0;
             cudaEventElapsedTime(&ms, P.events[3 * li], P.events[3 * li + 1]);
-            if (ln.kind == Launch::GEMM && P.tensor_path()) {
+            if (ln.kind == Launch::GEMM && P.tensor_path() && !ln.simt) {
                 float pk = 0;
                 cudaEventElapsedTime(&pk, P.events[3 * li], P.events[3 * li + 2]);
                 P.prof[PROF_PACK_MS] += pk;
