@@ -44,10 +44,13 @@ constexpr int kEACols = 16;      // columns per extend-add work item
 constexpr int kEARows = 2048;    // rows per extend-add work item
 // Triangular sweeps: the chain CTA of a front adds the contributions of the
 // kSolveLag newest solved blocks itself; workers add the older ones.
-constexpr int kSolveLag = 1;
+// The chain computes the newest block's contribution on its critical path and
+// the second newest right after publishing each block, off that path.
+constexpr int kSolveLag = 2;
 constexpr int kSolveRhsChunk = 16;   // right-hand sides per sweep (partial-sum stride)
-// sweep work items {front, kind, block, 0}
-enum SweepItem : int { kItemChain = 0, kItemPivotRows = 1, kItemLowerRows = 2, kItemColumns = 1 };
+constexpr int kLowerChunkTiles = 16; // backward: 64-row tiles below the pivots per helper
+// sweep work items {front, kind, block, chunk}
+enum SweepItem : int { kItemChain = 0, kItemPivotRows = 1, kItemLowerRows = 2, kItemColumns = 1, kItemLowerChunk = 2 };
 
 // One front as the kernels see it.  Offsets are in elements (a complex
 // element is two scalars).
@@ -64,6 +67,8 @@ struct FrontDev {
     int32_t pool;       // parity of the depth
     int32_t flag_base;  // first chain-solve flag of this front
     int64_t dinv;       // inverse diagonal blocks (ceil(n/64) blocks of 64 x 64) in the dinv store
+    int32_t hbase;      // backward sweep: first helper slot ((nch - 1) per pivot block)
+    int32_t nch;        // backward sweep: 16-tile chunks of the rows below the pivots
     int64_t eblk;       // 2xFP16 split: per (row, 64-column block) largest |component| of L and of D op(L), m x nT
     int64_t erow;       // 2xFP16 split: per row, the same over all blocks so far (m)
 };
@@ -157,6 +162,9 @@ struct Plan {
     void* dinv = nullptr;         // L11^{-1} of every 64-block of every front, kept for the solves
     void* dinvT = nullptr;        // the same blocks row-major (backward sweep)
     void* subT = nullptr;         // per pivot block b: tile (b+1, b) of the front's L, row-major (backward sweep)
+    void* subT2 = nullptr;        // per pivot block b: tile (b+2, b), row-major
+    void* hpart = nullptr;        // backward helpers' partial sums (kSolveRhsChunk x 64 per helper)
+    int64_t helpers_total = 0;
     void* partial = nullptr;      // per pivot block: 64 x kSolveRhsChunk partial sums from the sweep workers
     // 2xFP16 split: row maxima (float bits) of L panels and of D op(L) panels,
     // [A | S] halves of eblk_total and erow_total entries
@@ -177,7 +185,7 @@ struct Plan {
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;
-    int32_t* flags = nullptr;     // 2 * flags_total: solved-block flags, then partial-sum flags
+    int32_t* flags = nullptr;     // solved-block flags, partial-sum flags (flags_total each), helper flags
     int32_t* tickets = nullptr;
     int32_t* status = nullptr;    // [0] first zero pivot + 1 (min), [1] timeout flag
     int64_t* rowptr = nullptr;    // FP64 matrix (keep_matrix)

@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
                                                          T* __restrict__ L, const double* __restrict__ D, const T* __restrict__ tinv,
-                                                         T* __restrict__ subT, uint32_t* __restrict__ eblk, uint32_t* __restrict__ erow,
+                                                         T* __restrict__ subT, T* __restrict__ subT2, uint32_t* __restrict__ eblk,
+                                                         uint32_t* __restrict__ erow,
                                                          int64_t eblk_total, int64_t erow_total) {
     using X = V<T, C>;
     using W = DV<C>;
@@ -425,11 +426,12 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restr
             }
         }
     }
-    // the first row block under a full diagonal block is tile (b+1, b) of the
-    // pivot rows: keep a row-major copy (zero outside the pivot rows) for the
-    // backward sweep
-    if (subT && rb == 0 && kb == nb && r0 < f.n) {
-        X* S = reinterpret_cast<X*>(subT) + f.dinv + (int64_t)(k / nb) * nb * nb;
+    // the first two row blocks under a full diagonal block are tiles (b+1, b)
+    // and (b+2, b) of the pivot rows: keep row-major copies (zero outside the
+    // pivot rows) for the backward sweep's chain
+    T* sub = rb == 0 ? subT : (rb == 1 ? subT2 : nullptr);
+    if (sub && kb == nb && r0 < f.n) {
+        X* S = reinterpret_cast<X*>(sub) + f.dinv + (int64_t)(k / nb) * nb * nb;
         const int prow = min(rows, f.n - r0);
 #pragma unroll
         for (int a = 0; a < 4; ++a)
@@ -580,7 +582,7 @@ static int run_factor_impl(Plan& P) {
             case Launch::PANEL:
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
                     P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), reinterpret_cast<T*>(P.subT),
-                    P.eblk, P.erow, P.eblk_total, P.erow_total);
+                    reinterpret_cast<T*>(P.subT2), P.eblk, P.erow, P.eblk_total, P.erow_total);
                 break;
             case Launch::GEMM:
                 if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
@@ -719,7 +721,7 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
         diag_ldl_kernel<T, C, CJ, T><<<1, kThreads, diag_smem_bytes<T, C>(), st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, nullptr, status);
         if (s.panel_blocks > 0)
             panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr,
-                                                                               nullptr, nullptr, 0, 0);
+                                                                               nullptr, nullptr, nullptr, 0, 0);
         if (s.prob >= 0)
             gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, AL, ABR,
                                                                                ABR, D);

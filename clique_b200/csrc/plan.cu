@@ -75,7 +75,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 }
 
 void free_plan(Plan& P) {
-    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.subT2, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
                     P.wpool[1], P.xnodal, P.xwork, P.norms};
@@ -429,6 +429,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
 
     // ---- solve schedule ----
     P.solve_levels.assign(P.max_depth + 1, SolveLevel{});
+    P.helpers_total = 0;
     std::vector<int32_t> level_fronts;
     int flag = 0;
     for (int d = 0; d <= P.max_depth; ++d) {
@@ -458,8 +459,21 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             for (int i = 0; f.n + i * kTile < f.m; ++i) push_item(s, kItemLowerRows, i, 0);
         }
         sl.nfwd = (int32_t)(items.size() / 4 - sl.fwd_items);
-        // backward: each front's chain followed by its column workers, last block first
+        // backward: first the helpers (rows below the pivots beyond the first
+        // 16-tile chunk, no waits), then each front's chain followed by its
+        // column workers, last block first
         sl.bwd_items = (int64_t)items.size() / 4;
+        for (int s : P.level_list[d]) {
+            FrontDev& f = P.hfronts[s];
+            if (f.n <= 0 || f.m <= 0) continue;
+            const int nT = (f.n + kTile - 1) / kTile;
+            const int low_tiles = (f.m - f.n + kTile - 1) / kTile;
+            f.nch = std::max(1, (low_tiles + kLowerChunkTiles - 1) / kLowerChunkTiles);
+            f.hbase = (int32_t)P.helpers_total;
+            P.helpers_total += (int64_t)nT * (f.nch - 1);
+            for (int c = nT - 1; c >= 0; --c)
+                for (int ch = 1; ch < f.nch; ++ch) push_item(s, kItemLowerChunk, c, ch);
+        }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
             if (f.n <= 0 || f.m <= 0) continue;
@@ -512,6 +526,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.dinv, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.dinvT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.subT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.subT2, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.hpart, (size_t)std::max<int64_t>(P.helpers_total, 1) * kTile * kSolveRhsChunk * eb));
     TRY(dev_alloc(P, &P.partial, (size_t)P.flags_total * kTile * kSolveRhsChunk * eb));
     if (P.f16_scales()) {
         TRY(dev_alloc(P, (void**)&P.eblk, sizeof(uint32_t) * 2 * (size_t)std::max<int64_t>(P.eblk_total, 1)));
@@ -529,7 +545,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));
     TRY(dev_upload(P, &P.level_fronts, level_fronts));
-    std::vector<int32_t> zeros_flags(2 * P.flags_total, 0);
+    std::vector<int32_t> zeros_flags(2 * P.flags_total + P.helpers_total, 0);
     TRY(dev_upload(P, &P.flags, zeros_flags));
     std::vector<int32_t> zt(2 * (P.max_depth + 1) + 2, 0);
     TRY(dev_upload(P, &P.tickets, zt));

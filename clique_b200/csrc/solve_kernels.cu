@@ -11,26 +11,30 @@
 // one sweep launch (backward).  Inside a sweep launch every front gets
 //   * one chain CTA, which walks the front's 64-wide pivot blocks in order.
 //     Step s needs the block's right-hand side minus the contributions of
-//     all solved blocks; the chain adds the newest block's contribution
-//     itself (x_{s-1} stays in its shared memory, the 64x64 tile it needs
-//     was prefetched into registers during the previous step) and takes the
-//     older ones from a worker as one finished 64 x nrhs partial sum.  Then
-//     it applies the stored inverse of the diagonal block and publishes
-//     x_s.  The critical path per step is therefore two 64x64 products and
-//     one flag, with no global-memory round trip for x.
+//     all solved blocks.  The newest block's contribution is the only
+//     product on the chain's critical path (x_{s-1} stays in its shared
+//     memory, the 64x64 tile was prefetched into registers during the
+//     previous step); the second newest, q_s, the chain formed right after
+//     publishing x_{s-2}; the older ones arrive from a worker as one
+//     finished 64 x nrhs partial sum, which the worker had two chain steps
+//     to produce.  Then the chain applies the stored inverse of the diagonal
+//     block and publishes x_s: two 64x64 products and one flag per step, with
+//     no global-memory round trip for x.
 //   * workers, which stream the rest of the front's L tiles as the chain
 //     publishes solved blocks: forward, one per 64-row block of pivot rows
 //     (its partial feeds the chain) and one per 64-row block below the
 //     pivots (subtracts into the update vector W_B); backward, one per
-//     pivot column block (lower rows first, which need no wait, then the
-//     later pivot blocks).
-// Work items are taken from an atomic ticket counter in the order chain,
-// then that chain's workers in the order the chain consumes them, so every
-// CTA a resident CTA waits for was either issued before it or is a worker
-// whose own waits only reach back to earlier tickets: the sweep finishes
-// with any number of resident CTAs >= 2.  Waits are bounded: on expiry a
-// CTA records a timeout in the status word and returns, and every other
-// wait gives up as soon as it sees that word set.
+//     pivot column block (the first 16 tiles of rows below the pivots, the
+//     sums of its helpers in chunk order, then the later pivot blocks), and
+//     helpers for the further 16-tile chunks of rows below the pivots.
+// Work items are taken from an atomic ticket counter in the order helpers
+// (which wait for nothing), then each chain followed by its workers in the
+// order the chain consumes them, so every CTA a resident CTA waits for was
+// either issued before it or is a worker whose own waits only reach back to
+// earlier tickets: the sweep finishes with any number of resident CTAs >= 2.
+// Waits are bounded: on expiry a CTA records a timeout in the status word
+// and returns, and every other wait gives up as soon as it sees that word
+// set.
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
 
@@ -39,7 +43,7 @@ namespace cliqgpu {
 constexpr int kSolveThreads = 256;
 constexpr int kQ = kSolveThreads / kTile;   // slices per tile row (4)
 constexpr int kE = kTile / kQ;              // tile elements per thread and slice (16)
-constexpr int kLag = kSolveLag;             // blocks the chain adds itself (the newest one)
+constexpr int kLag = kSolveLag;             // blocks the chain adds itself (the two newest)
 constexpr int kMaxRhsChunk = kSolveRhsChunk;   // right-hand sides per sweep
 constexpr int kPartialStride = kTile * kMaxRhsChunk;   // elements per pivot block in the partial store
 constexpr int kGatherRows = 1024;           // front rows per gather CTA (grid y of the gather launch)
@@ -205,7 +209,10 @@ struct SweepArgs {
     const void* dinv;       // L11^{-1} per 64-block, column-major
     const void* dinvT;      // the same, row-major
     const void* subT;       // tile (b+1, b) of L per pivot block, row-major
+    const void* subT2;      // tile (b+2, b) of L per pivot block, row-major
     void* partial;          // kPartialStride elements per pivot block
+    void* hpart;            // backward helpers' partial sums, kPartialStride each
+    int32_t* hflags;        // backward helpers' flags
     void* X;                // n x nrhs, ND order, ld ldx
     int64_t ldx;
     void* w0;
@@ -227,10 +234,14 @@ __device__ __forceinline__ bool fwd_tile(const SweepArgs& a, const FrontDev& f, 
     return true;
 }
 
-// Forward chain of one front: x_s = L_ss^{-1} (b_s - partial_s - L_{s,s-1} x_{s-1}).
+// Forward chain of one front:
+//   x_s = L_ss^{-1} (b_s - partial_s - q_s - L_{s,s-1} x_{s-1}),
+// partial_s from the pivot-row worker (blocks < s - 2), q_s = L_{s,s-2} x_{s-2}
+// formed by the chain right after it published x_{s-2}.
 template <class T, bool C, int NR>
-__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq) {
     using Xv = V<T, C>;
+    static_assert(kLag == 2, "the chain adds the two newest blocks");
     const T* L = reinterpret_cast<const T*>(a.L);
     const T* Dinv = reinterpret_cast<const T*>(a.dinv);
     const T* Part = reinterpret_cast<const T*>(a.partial);
@@ -251,6 +262,7 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             if (r < ds && j < a.nrhs) {
                 v = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx);
                 if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s) * kPartialStride + j * kTile + r);
+                if (s >= 2) v -= sq[(s & 1) * kTile * NR + r * NR + j];
             }
             tv[b] = v;
         }
@@ -287,6 +299,20 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             row_slice<T, C>(dv, Dinv, f.dinv + (int64_t)(s + 1) * kTile * kTile, kTile, r, q, kTile, kTile);
         }
         publish_flag(&a.xflags[f.flag_base + s], a.epoch);
+        // off the critical path: q_{s+2} = L_{s+2,s} x_s
+        if (s + 2 < nT) {
+            Xv lq[kE];
+            row_slice<T, C>(lq, L, f.L + (r0 + 2 * kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - 2 * kTile), kTile);
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, lq, sprev, q);
+            Xv qv[NR / kQ];
+            reduce_slices<NR>(acc, red, qv, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) sq[(s & 1) * kTile * NR + r * NR + q + kQ * b] = qv[b];
+            __syncthreads();
+        }
     }
 }
 
@@ -296,6 +322,7 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
     Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
+    Xv* sq = red + kQ * NR * kTile;               // 2 x [64][NR]: the chain's off-path products
     __shared__ int s_item;
     if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
     __syncthreads();
@@ -305,7 +332,7 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_sweep_kernel(SweepArgs a) {
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
     const int nT = (f.n + kTile - 1) / kTile;
     if (it.y == kItemChain) {
-        fwd_chain<T, C, NR>(a, f, nT, r, q, sx, red);
+        fwd_chain<T, C, NR>(a, f, nT, r, q, sx, red, sq);
         return;
     }
     // worker: rows [R0, R0 + nr) against the pivot blocks t < t_end
@@ -352,12 +379,16 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_sweep_kernel(SweepArgs a) {
 }
 
 // Backward chain of one front, last pivot block first:
-// x_c = op(L_cc^{-1})^T (y_c - partial_c - op(L_{c+1,c})^T x_{c+1}).
+//   x_c = op(L_cc^{-1})^T (y_c - partial_c - q_c - op(L_{c+1,c})^T x_{c+1}),
+// partial_c from the column worker (rows below the pivots and pivot blocks
+// after c + 2), q_c = op(L_{c+2,c})^T x_{c+2} formed right after x_{c+2}.
 template <class T, bool C, bool CJ, int NR>
-__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq) {
     using Xv = V<T, C>;
+    static_assert(kLag == 2, "the chain adds the two newest blocks");
     const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
     const T* SubT = reinterpret_cast<const T*>(a.subT);
+    const T* SubT2 = reinterpret_cast<const T*>(a.subT2);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
     Xv* sprev = sx;                 // x_{c+1}
@@ -377,6 +408,7 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             if (r < dc && j < a.nrhs) {
                 v = ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx);
                 if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r);
+                if (c + 2 < nT) v -= sq[(c & 1) * kTile * NR + r * NR + j];
             }
             tv[b] = v;
         }
@@ -414,6 +446,20 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             row_slice<T, C>(dv, DinvT, blk, kTile, r, q, kTile, kTile);
         }
         publish_flag(&a.xflags[f.flag_base + c], a.epoch);
+        // off the critical path: q_{c-2} = op(L_{c,c-2})^T x_c
+        if (c >= 2) {
+            Xv lq[kE];
+            row_slice<T, C>(lq, SubT2, f.dinv + (int64_t)(c - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<CJ, NR>(acc, lq, sprev, q);
+            Xv qv[NR / kQ];
+            reduce_slices<NR>(acc, red, qv, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) sq[(c & 1) * kTile * NR + r * NR + q + kQ * b] = qv[b];
+            __syncthreads();
+        }
     }
 }
 
@@ -424,7 +470,8 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
     Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
-    Xv* sL = red + kQ * NR * kTile;               // [64 columns][65]
+    Xv* sq = red + kQ * NR * kTile;               // 2 x [64][NR]: the chain's off-path products
+    Xv* sL = sq + 2 * kTile * NR;                 // [64 columns][65]
     __shared__ int s_item;
     if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
     __syncthreads();
@@ -434,22 +481,28 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
     const int nT = (f.n + kTile - 1) / kTile;
     if (it.y == kItemChain) {
-        bwd_chain<T, C, CJ, NR>(a, f, nT, r, q, sx, red);
+        bwd_chain<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sq);
         return;
     }
-    // column worker: op(L[R, c-block])^T x_R over the rows below the pivots
-    // (x gathered at lowerStruct, final since the ancestors are solved), then
-    // over the pivot blocks after c + kLag as the chain publishes them
+    // column worker (kItemColumns) or helper (kItemLowerChunk, chunk it.w >= 1):
+    // op(L[R, c-block])^T x_R over rows R below the pivots (x gathered at
+    // lowerStruct, final since the ancestors are solved); the worker then adds
+    // the helpers' sums and the pivot blocks after c + kLag as the chain
+    // publishes them
+    const bool helper = it.y == kItemLowerChunk;
     const T* L = reinterpret_cast<const T*>(a.L);
     const T* X = reinterpret_cast<const T*>(a.X);
     const int c = it.z, c0 = c * kTile, dc = min(kTile, f.n - c0);
     const int nlow = (f.m - f.n + kTile - 1) / kTile;
-    const int npiv = max(0, nT - 1 - (c + kLag));
-    const int ntiles = nlow + npiv;
+    const int low0 = helper ? it.w * kLowerChunkTiles : 0;
+    const int low1 = min(nlow, low0 + kLowerChunkTiles);
+    const int nl = max(0, low1 - low0);
+    const int npiv = helper ? 0 : max(0, nT - 1 - (c + kLag));
+    const int ntiles = nl + npiv;
     // coalesced staging: element p of this thread is (row r, column q + kQ*p)
     auto tile_of = [&](int i, int& R0, int& nr) {
-        if (i < nlow) { R0 = f.n + kTile * i; nr = min(kTile, f.m - R0); }
-        else { R0 = kTile * (nT - 1 - (i - nlow)); nr = min(kTile, f.n - R0); }
+        if (i < nl) { R0 = f.n + kTile * (low0 + i); nr = min(kTile, f.m - R0); }
+        else { R0 = kTile * (nT - 1 - (i - nl)); nr = min(kTile, f.n - R0); }
     };
     Xv pre[kE];
     auto fetch = [&](int i) {
@@ -472,7 +525,7 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
 #pragma unroll
         for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
         if (i + 1 < ntiles) fetch(i + 1);
-        if (i >= nlow) {
+        if (i >= nl) {
             if (!wait_flag(&a.xflags[f.flag_base + R0 / kTile], a.epoch, a.status)) return;
             load_x_tile<T, C, NR>(sx, X, f.off + R0, a.ldx, nr, a.nrhs);
         } else {
@@ -490,6 +543,29 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
     }
     Xv out[NR / kQ];
     reduce_slices<NR>(acc, red, out, r, q);
+    if (helper) {
+        T* HP = reinterpret_cast<T*>(a.hpart);
+        const int64_t h = f.hbase + (int64_t)c * (f.nch - 1) + (it.w - 1);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            if (j < a.nrhs) stv<T, C>(HP, h * kPartialStride + j * kTile + r, out[b]);
+        }
+        publish_flag(&a.hflags[h], a.epoch);
+        return;
+    }
+    // the helpers of this column block were issued before this CTA; add
+    // their sums in chunk order
+    const T* HP = reinterpret_cast<const T*>(a.hpart);
+    for (int ch = 1; ch < f.nch; ++ch) {
+        const int64_t h = f.hbase + (int64_t)c * (f.nch - 1) + (ch - 1);
+        if (!wait_flag(&a.hflags[h], a.epoch, a.status)) return;
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            if (j < a.nrhs) out[b] += ldv_cg<T, C>(HP, h * kPartialStride + j * kTile + r);
+        }
+    }
     T* Part = reinterpret_cast<T*>(a.partial);
 #pragma unroll
     for (int b = 0; b < NR / kQ; ++b) {
@@ -505,7 +581,7 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
 template <class T, bool C, bool CJ, int NR>
 static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     using Xv = V<T, C>;
-    const size_t smem_fwd = sizeof(Xv) * (2 + kQ) * kTile * NR;
+    const size_t smem_fwd = sizeof(Xv) * (4 + kQ) * kTile * NR;
     const size_t smem_bwd = smem_fwd + sizeof(Xv) * kTile * (kTile + 1);
     static bool attr_done = false;
     if (!attr_done) {
@@ -522,7 +598,10 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     a.dinv = P.dinv;
     a.dinvT = P.dinvT;
     a.subT = P.subT;
+    a.subT2 = P.subT2;
     a.partial = P.partial;
+    a.hpart = P.hpart;
+    a.hflags = P.flags + 2 * P.flags_total;
     a.X = X;
     a.ldx = P.n;
     a.w0 = P.wpool[0];
