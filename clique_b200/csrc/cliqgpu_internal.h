@@ -244,6 +244,7 @@ int check_cuda(const char* where);
 // packs the launch's operands, records `between` (if given), runs the GEMM
 int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between);
 size_t tc2_smem(bool cplx);
+int launch_panel_tc(Plan& P, const Launch& ln);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);
 void free_plan(Plan& P);

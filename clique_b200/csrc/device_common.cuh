@@ -20,6 +20,7 @@ template <class T> __host__ __device__ __forceinline__ cx<T> operator-(cx<T> a, 
 template <class T> __host__ __device__ __forceinline__ cx<T> operator*(cx<T> a, cx<T> b) {
     return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r};
 }
+template <class T> __host__ __device__ __forceinline__ cx<T> operator*(cx<T> a, T s) { return {a.r * s, a.i * s}; }
 template <class T> __host__ __device__ __forceinline__ cx<T> operator/(cx<T> a, cx<T> b) {
     // Smith's algorithm for complex division
     if (fabs(b.r) >= fabs(b.i)) {

@@ -580,6 +580,10 @@ static int run_factor_impl(Plan& P) {
                 else launch_diag<T, C, CJ, double>(P, ln, L, items);
                 break;
             case Launch::PANEL:
+                if (std::is_same<T, float>::value && P.f16_scales()) {
+                    launch_panel_tc(P, ln);
+                    break;
+                }
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
                     P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), reinterpret_cast<T*>(P.subT),
                     reinterpret_cast<T*>(P.subT2), P.eblk, P.erow, P.eblk_total, P.erow_total);

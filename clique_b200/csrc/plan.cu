@@ -351,7 +351,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                     const FrontDev& f = P.hfronts[a.first];
                     const int kb = std::min(nb, f.n - k);
                     const int rows = f.m - k - kb;
-                    for (int rb = 0; rb * kTile < rows; ++rb) push_item(a.first, a.second, rb, 0);
+                    const int prows = P.f16_scales() ? 128 : kTile;   // tensor-core panel: 128-row tiles
+                    for (int rb = 0; rb * prows < rows; ++rb) push_item(a.first, a.second, rb, 0);
                     const int N = std::min(K0 + nbo, f.n) - k - kb;
                     if (N > 0) {
                         GemmProb pr{};
@@ -592,8 +593,8 @@ int read_status(Plan& P, int64_t* zero_pivot) {
     if (zero_pivot) *zero_pivot = st[0] == INT_MAX ? -1 : (int64_t)st[0] - 1;
     if (st[1]) {
         static const char* sites[] = {"?", "update: stage full", "update: stage empty", "update: accumulator", "solve: block flag",
-                                      "update: tile outside the schedule"};
-        set_last_error(std::string("a device-side wait timed out at ") + sites[(st[2] >= 0 && st[2] <= 5) ? st[2] : 0]);
+                                      "update: tile outside the schedule", "panel: tensor-core products"};
+        set_last_error(std::string("a device-side wait timed out at ") + sites[(st[2] >= 0 && st[2] <= 6) ? st[2] : 0]);
         return CLIQ_ERR_TIMEOUT;
     }
     return st[0] == INT_MAX ? CLIQ_OK : CLIQ_ERR_ZERO_PIVOT;
