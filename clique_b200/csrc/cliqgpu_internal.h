@@ -195,7 +195,10 @@ struct Plan {
     void* wpool[2] = {nullptr, nullptr};
     void* xnodal = nullptr;       // n x nrhs in storage precision
     double* xwork = nullptr;      // FP64 workspaces for refinement (3 * n * nrhs)
-    double* norms = nullptr;      // 2 * nrhs
+    double* norms = nullptr;      // 2 * nrhs norms + partial sums
+    double* krylov = nullptr;     // Krylov refinement: basis V, preconditioned Z, dots scratch
+    int64_t krylov_doubles = 0;
+    int refine_gmres = 1;         // FGMRES refinement (default) or classical (CLIQGPU_REFINE=ir)
     int32_t ws_nrhs = 0;
     int64_t device_bytes = 0;
 
@@ -239,6 +242,10 @@ int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t
 int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double beta_r, double beta_i,
                 double* Y, int64_t ld, int nrhs);
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
+// Krylov refinement: out[i][j] = <V_i[:, j], w[:, j]> (pairs), w += sign * sum_i h[i][j] V_i, v = s_j w
+int launch_multi_dot(Plan& P, const double* V, int64_t vstride, int nv, const double* w, int nrhs, double* part, double* out);
+int launch_multi_axpy(Plan& P, const double* V, int64_t vstride, int nv, const double* h, double* w, int nrhs, double sign);
+int launch_col_scale(Plan& P, const double* w, double* v, int nrhs, const double* s);
 
 int check_cuda(const char* where);
 // packs the launch's operands, records `between` (if given), runs the GEMM

@@ -114,7 +114,7 @@ __global__ void spmv_kernel(const int64_t* __restrict__ rowptr, const int32_t* _
             W s{};
             for (int64_t e = e0; e < e1; ++e) mac(s, A[e], x[colind[e] + j * ld]);
             const int64_t o = i + j * ld;
-            y[o] = beta * y[o] + alpha * s;
+            y[o] = is_zero(beta) ? alpha * s : beta * y[o] + alpha * s;   // beta = 0: Y is not read (BLAS semantics)
         }
     }
 }
@@ -129,7 +129,6 @@ int launch_spmv(Plan& P, double ar, double ai, const double* X, double br, doubl
     return check_cuda("multiply");
 }
 
-// out[j] = sum_i |X[i, j]|^2 (FP64), one block per column
 // Squared 2-norms of the nrhs columns of X (FP64; complex: |re|^2 + |im|^2).
 // Stage 1: kNormChunks CTAs per column write partial sums; stage 2 adds
 // them in a fixed order, so the result does not depend on scheduling.
@@ -178,6 +177,117 @@ int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out
     col_norms_final_kernel<<<nrhs, kNormChunks, 0, P.stream>>>(part, out);
     P.total_launches += 2;
     return check_cuda("norms");
+}
+
+// ---------------------------------------------------------------------------
+// FP64 block-vector operations for the Krylov refinement.  A block vector
+// holds nrhs columns of length n (complex: interleaved), column j at
+// j * n * w doubles; a basis is nv block vectors vstride doubles apart.
+// ---------------------------------------------------------------------------
+constexpr int kDotChunks = 128;
+
+// part[(i * nrhs + j) * kDotChunks + chunk] = partial of <V_i[:, j], w[:, j]>
+// (conjugate-linear in V); fixed-order second stage below
+template <bool C>
+__global__ void multi_dot_partial_kernel(const double* __restrict__ V, int64_t vstride, const double* __restrict__ w, int64_t n,
+                                         int nrhs, double* __restrict__ part) {
+    const int i = blockIdx.z, j = blockIdx.y;
+    constexpr int ww = C ? 2 : 1;
+    const double* v = V + (int64_t)i * vstride + (int64_t)j * n * ww;
+    const double* x = w + (int64_t)j * n * ww;
+    const int64_t per = (n + kDotChunks - 1) / kDotChunks;
+    const int64_t b = per * blockIdx.x, e = min(n, b + per);
+    double sr = 0, si = 0;
+    for (int64_t p = b + threadIdx.x; p < e; p += blockDim.x) {
+        if constexpr (C) {
+            const double vr = v[2 * p], vi = v[2 * p + 1], xr = x[2 * p], xi = x[2 * p + 1];
+            sr = fma(vr, xr, fma(vi, xi, sr));
+            si = fma(vr, xi, fma(-vi, xr, si));
+        } else {
+            sr = fma(v[p], x[p], sr);
+        }
+    }
+    __shared__ double rr[32], ri[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_down_sync(0xffffffffu, sr, o);
+        si += __shfl_down_sync(0xffffffffu, si, o);
+    }
+    if ((threadIdx.x & 31) == 0) { rr[threadIdx.x >> 5] = sr; ri[threadIdx.x >> 5] = si; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tr = 0, ti = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { tr += rr[q]; ti += ri[q]; }
+        const int64_t o = ((int64_t)i * nrhs + j) * kDotChunks + blockIdx.x;
+        part[2 * o] = tr;
+        part[2 * o + 1] = ti;
+    }
+}
+
+__global__ void multi_dot_final_kernel(const double* __restrict__ part, double* __restrict__ out) {
+    const int o = blockIdx.x;
+    if (threadIdx.x == 0) {
+        double tr = 0, ti = 0;
+        for (int c = 0; c < kDotChunks; ++c) { tr += part[2 * ((int64_t)o * kDotChunks + c)]; ti += part[2 * ((int64_t)o * kDotChunks + c) + 1]; }
+        out[2 * o] = tr;
+        out[2 * o + 1] = ti;
+    }
+}
+
+// w[:, j] += sign * sum_i h[i][j] V_i[:, j]   (h complex pairs, or reals in the first slot)
+template <bool C>
+__global__ void multi_axpy_kernel(const double* __restrict__ V, int64_t vstride, int nv, const double* __restrict__ h,
+                                  double* __restrict__ w, int64_t n, int nrhs, double sign) {
+    constexpr int ww = C ? 2 : 1;
+    const int64_t total = n * nrhs;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = idx % n, j = idx / n;
+        const int64_t e = (j * n + p) * ww;
+        if constexpr (C) {
+            double ar = 0, ai = 0;
+            for (int i = 0; i < nv; ++i) {
+                const double hr = h[2 * (i * nrhs + j)], hi = h[2 * (i * nrhs + j) + 1];
+                const double vr = V[(int64_t)i * vstride + e], vi = V[(int64_t)i * vstride + e + 1];
+                ar = fma(hr, vr, fma(-hi, vi, ar));
+                ai = fma(hr, vi, fma(hi, vr, ai));
+            }
+            w[e] += sign * ar;
+            w[e + 1] += sign * ai;
+        } else {
+            double a = 0;
+            for (int i = 0; i < nv; ++i) a = fma(h[2 * (i * nrhs + j)], V[(int64_t)i * vstride + e], a);
+            w[e] += sign * a;
+        }
+    }
+}
+
+// v[:, j] = s_j * w[:, j], s real
+__global__ void col_scale_kernel(const double* __restrict__ w, double* __restrict__ v, int64_t len_per_col, int nrhs,
+                                 const double* __restrict__ s) {
+    const int64_t total = len_per_col * nrhs;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x)
+        v[idx] = w[idx] * s[idx / len_per_col];
+}
+
+int launch_multi_dot(Plan& P, const double* V, int64_t vstride, int nv, const double* w, int nrhs, double* part, double* out) {
+    const dim3 grid(kDotChunks, nrhs, nv);
+    if (P.cplx()) multi_dot_partial_kernel<true><<<grid, 256, 0, P.stream>>>(V, vstride, w, P.n, nrhs, part);
+    else multi_dot_partial_kernel<false><<<grid, 256, 0, P.stream>>>(V, vstride, w, P.n, nrhs, part);
+    multi_dot_final_kernel<<<nv * nrhs, 32, 0, P.stream>>>(part, out);
+    P.total_launches += 2;
+    return check_cuda("multi_dot");
+}
+
+int launch_multi_axpy(Plan& P, const double* V, int64_t vstride, int nv, const double* h, double* w, int nrhs, double sign) {
+    if (P.cplx()) multi_axpy_kernel<true><<<1184, 256, 0, P.stream>>>(V, vstride, nv, h, w, P.n, nrhs, sign);
+    else multi_axpy_kernel<false><<<1184, 256, 0, P.stream>>>(V, vstride, nv, h, w, P.n, nrhs, sign);
+    P.total_launches += 1;
+    return check_cuda("multi_axpy");
+}
+
+int launch_col_scale(Plan& P, const double* w, double* v, int nrhs, const double* s) {
+    col_scale_kernel<<<1184, 256, 0, P.stream>>>(w, v, P.n * (P.cplx() ? 2 : 1), nrhs, s);
+    P.total_launches += 1;
+    return check_cuda("col_scale");
 }
 
 }  // namespace cliqgpu

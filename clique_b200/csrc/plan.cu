@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <complex>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -78,7 +79,7 @@ void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.subT2, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
-                    P.wpool[1], P.xnodal, P.xwork, P.norms};
+                    P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : P.events) cudaEventDestroy(e);
@@ -633,6 +634,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_DIAG_FP64")) P.diag_fp64 = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_SPLIT")) P.split_f16 = strcmp(e, "tf32") != 0;
     if (const char* e = getenv("CLIQGPU_INPANEL_TC")) P.inpanel_tc = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_REFINE")) P.refine_gmres = strcmp(e, "ir") != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
@@ -737,6 +739,156 @@ int cliqgpu_multiply(cliqgpu_plan h, const double* alpha, const void* X, const d
     return launch_spmv(P, alpha[0], c ? alpha[1] : 0.0, (const double*)X, beta[0], c ? beta[1] : 0.0, (double*)Y, ld, nrhs);
 }
 
+// ---------------------------------------------------------------------------
+// Krylov refinement: right-preconditioned FGMRES (restart length up to
+// kKrylovMax) with the stored factorization as the preconditioner, FP64
+// residuals and basis.  x_k minimises ||b - A x|| over x0 + span(Z), which
+// contains the classical refinement iterate after the same number of
+// solves, so it never needs more solves than classical refinement.  Each
+// right-hand side runs its own Arnoldi process (complex Givens rotations on
+// the host); the basis vectors of all right-hand sides are processed
+// together (one solve per step).  Orthogonalisation: classical Gram-Schmidt,
+// applied twice.  The relative residual returned is recomputed from x.
+// ---------------------------------------------------------------------------
+constexpr int kKrylovMax = 8;
+
+static int ensure_krylov(Plan& P, int nrhs) {
+    const int w = P.cplx() ? 2 : 1;
+    const int64_t vec = (int64_t)w * P.n * nrhs;
+    const int64_t need = (2 * kKrylovMax + 2) * vec + 2 * (int64_t)(kKrylovMax + 1) * nrhs * (128 + 4) + 8 * nrhs;
+    if (need <= P.krylov_doubles) return CLIQ_OK;
+    if (P.krylov) cudaFree(P.krylov);
+    P.krylov = nullptr;
+    P.krylov_doubles = 0;
+    TRY(dev_alloc(P, (void**)&P.krylov, sizeof(double) * (size_t)need));
+    P.krylov_doubles = need;
+    return CLIQ_OK;
+}
+
+static int refine_fgmres(Plan& P, const double* b, double* x, double* r, int nrhs, double tol, int max_iter, int* iters,
+                         double* relres) {
+    using cd = std::complex<double>;
+    const bool cplx = P.cplx();
+    const int w = cplx ? 2 : 1;
+    const int64_t n = P.n;
+    const int64_t vec = (int64_t)w * n * nrhs;
+    TRY(ensure_krylov(P, nrhs));
+    double* V = P.krylov;                              // kKrylovMax + 1 basis block vectors
+    double* Z = V + (kKrylovMax + 1) * vec;             // kKrylovMax preconditioned block vectors
+    double* wv = Z + kKrylovMax * vec;                  // work block vector
+    double* part = wv + vec;                            // dot partial sums
+    double* hdev = part + 2 * (int64_t)(kKrylovMax + 1) * nrhs * 128;   // (k+1) x nrhs complex coefficients
+    double* sdev = hdev + 2 * (int64_t)(kKrylovMax + 1) * nrhs * 2;     // per-column scales / solution coefficients
+    std::vector<double> bn(nrhs), hn(2 * nrhs);
+    // ||b_j|| (norms[nrhs..] were filled by the caller)
+    if (cudaMemcpyAsync(hn.data(), P.norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+        return check_cuda("norms");
+    if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("refine sync");
+    for (int j = 0; j < nrhs; ++j) bn[j] = std::sqrt(hn[nrhs + j]);
+    int it = 0;
+    double rel = 0;
+    std::vector<double> hbuf(2 * (kKrylovMax + 1) * nrhs), h2(2 * (kKrylovMax + 1) * nrhs), sc(2 * nrhs);
+    auto residual = [&](double* relp, std::vector<double>& beta) -> int {
+        cudaMemcpyAsync(r, b, sizeof(double) * vec, cudaMemcpyDeviceToDevice, P.stream);
+        TRY(launch_spmv(P, -1.0, 0.0, x, 1.0, 0.0, r, n, nrhs));
+        TRY(launch_col_norms(P, r, n, nrhs, P.norms));
+        if (cudaMemcpyAsync(hn.data(), P.norms, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+            return check_cuda("norms");
+        if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("refine sync");
+        double rl = 0;
+        for (int j = 0; j < nrhs; ++j) {
+            beta[j] = std::sqrt(hn[j]);
+            rl = std::max(rl, bn[j] > 0 ? beta[j] / bn[j] : beta[j]);
+        }
+        *relp = rl;
+        return CLIQ_OK;
+    };
+    std::vector<double> beta(nrhs);
+    TRY(residual(&rel, beta));
+    while (rel > tol && it < max_iter && rel == rel) {
+        // v_0 = r / beta
+        for (int j = 0; j < nrhs; ++j) sc[j] = beta[j] > 0 ? 1.0 / beta[j] : 0.0;
+        cudaMemcpyAsync(sdev, sc.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, P.stream);
+        TRY(launch_col_scale(P, r, V, nrhs, sdev));
+        // per right-hand side: rotated Hessenberg R, rotations, right-hand side g
+        std::vector<std::vector<cd>> R(nrhs, std::vector<cd>((kKrylovMax + 1) * kKrylovMax)), g(nrhs, std::vector<cd>(kKrylovMax + 1));
+        std::vector<std::vector<double>> cs(nrhs, std::vector<double>(kKrylovMax));
+        std::vector<std::vector<cd>> sn(nrhs, std::vector<cd>(kKrylovMax));
+        for (int j = 0; j < nrhs; ++j) g[j][0] = beta[j];
+        int k = 0;
+        double est = rel;
+        for (; k < kKrylovMax && it < max_iter; ++k) {
+            // z_k = M^{-1} v_k (natural order FP64 -> nodal storage precision -> solve -> back)
+            TRY(launch_pull(P, P.perm, V + k * vec, n, nrhs, P.xnodal, 1.0));
+            TRY(solve_nodal_dispatch(P, P.xnodal, nrhs));
+            TRY(launch_push(P, P.perm, P.xnodal, Z + k * vec, n, nrhs, 1.0, 0));
+            ++it;
+            // w = A z_k, orthogonalised twice against v_0 .. v_k
+            TRY(launch_spmv(P, 1.0, 0.0, Z + k * vec, 0.0, 0.0, wv, n, nrhs));
+            TRY(launch_multi_dot(P, V, vec, k + 1, wv, nrhs, part, hdev));
+            TRY(launch_multi_axpy(P, V, vec, k + 1, hdev, wv, nrhs, -1.0));
+            if (cudaMemcpyAsync(hbuf.data(), hdev, sizeof(double) * 2 * (k + 1) * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+                return check_cuda("dots");
+            TRY(launch_multi_dot(P, V, vec, k + 1, wv, nrhs, part, hdev));
+            TRY(launch_multi_axpy(P, V, vec, k + 1, hdev, wv, nrhs, -1.0));
+            if (cudaMemcpyAsync(h2.data(), hdev, sizeof(double) * 2 * (k + 1) * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+                return check_cuda("dots");
+            TRY(launch_col_norms(P, wv, n, nrhs, P.norms));
+            if (cudaMemcpyAsync(hn.data(), P.norms, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
+                return check_cuda("norms");
+            if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("refine sync");
+            for (int j = 0; j < nrhs; ++j) sc[j] = hn[j] > 0 ? 1.0 / std::sqrt(hn[j]) : 0.0;
+            cudaMemcpyAsync(sdev, sc.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, P.stream);
+            TRY(launch_col_scale(P, wv, V + (k + 1) * vec, nrhs, sdev));
+            est = 0;
+            for (int j = 0; j < nrhs; ++j) {
+                cd* col = &R[j][(kKrylovMax + 1) * k];
+                for (int i = 0; i <= k; ++i)
+                    col[i] = cd(hbuf[2 * (i * nrhs + j)] + h2[2 * (i * nrhs + j)],
+                                cplx ? hbuf[2 * (i * nrhs + j) + 1] + h2[2 * (i * nrhs + j) + 1] : 0.0);
+                col[k + 1] = std::sqrt(hn[j]);
+                for (int i = 0; i < k; ++i) {   // earlier rotations
+                    const cd a = col[i], bb = col[i + 1];
+                    col[i] = cs[j][i] * a + sn[j][i] * bb;
+                    col[i + 1] = -std::conj(sn[j][i]) * a + cs[j][i] * bb;
+                }
+                const double ha = std::abs(col[k]), hb = std::abs(col[k + 1]), rr = std::hypot(ha, hb);
+                if (rr == 0) { cs[j][k] = 1; sn[j][k] = 0; }
+                else if (ha == 0) { cs[j][k] = 0; sn[j][k] = std::conj(col[k + 1]) / hb; }
+                else {
+                    const cd al = col[k] / ha;
+                    cs[j][k] = ha / rr;
+                    sn[j][k] = al * std::conj(col[k + 1]) / rr;
+                }
+                col[k] = cs[j][k] * col[k] + sn[j][k] * col[k + 1];
+                col[k + 1] = 0;
+                g[j][k + 1] = -std::conj(sn[j][k]) * g[j][k];
+                g[j][k] = cs[j][k] * g[j][k];
+                est = std::max(est, bn[j] > 0 ? std::abs(g[j][k + 1]) / bn[j] : std::abs(g[j][k + 1]));
+            }
+            if (est <= tol) { ++k; break; }
+        }
+        // x += Z y, R y = g (back substitution per right-hand side)
+        std::vector<double> ycoef(2 * kKrylovMax * nrhs, 0.0);
+        for (int j = 0; j < nrhs; ++j) {
+            std::vector<cd> y(k);
+            for (int i = k - 1; i >= 0; --i) {
+                cd t = g[j][i];
+                for (int l = i + 1; l < k; ++l) t -= R[j][(kKrylovMax + 1) * l + i] * y[l];
+                const cd d = R[j][(kKrylovMax + 1) * i + i];
+                y[i] = d != cd(0) ? t / d : cd(0);
+            }
+            for (int i = 0; i < k; ++i) { ycoef[2 * (i * nrhs + j)] = y[i].real(); ycoef[2 * (i * nrhs + j) + 1] = y[i].imag(); }
+        }
+        cudaMemcpyAsync(hdev, ycoef.data(), sizeof(double) * 2 * k * nrhs, cudaMemcpyHostToDevice, P.stream);
+        TRY(launch_multi_axpy(P, Z, vec, k, hdev, x, nrhs, 1.0));
+        TRY(residual(&rel, beta));
+    }
+    *iters = it;
+    *relres = rel;
+    return CLIQ_OK;
+}
+
 int cliqgpu_refine(cliqgpu_plan h, const void* B, void* X, int64_t ld, int32_t nrhs, int32_t on_device, double tol,
                    int32_t max_iter, int32_t* iters, double* relres) {
     if (!h || !B || !X || nrhs <= 0 || ld <= 0) return CLIQ_ERR_ARG;
@@ -764,6 +916,10 @@ int cliqgpu_refine(cliqgpu_plan h, const void* B, void* X, int64_t ld, int32_t n
     double rel = 0;
     int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
+    if (P.refine_gmres) {
+        TRY(refine_fgmres(P, b, x, r, nrhs, tol, max_iter, &it, &rel));
+        goto done;
+    }
     for (;;) {
         TRY(launch_col_norms(P, r, n, nrhs, P.norms));
         if (cudaMemcpyAsync(hn.data(), P.norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, P.stream) != cudaSuccess)
@@ -785,6 +941,7 @@ int cliqgpu_refine(cliqgpu_plan h, const void* B, void* X, int64_t ld, int32_t n
         TRY(launch_spmv(P, -1.0, 0.0, x, 1.0, 0.0, r, n, nrhs));
         ++it;
     }
+done:
     const cudaMemcpyKind kout = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     for (int j = 0; j < nrhs; ++j)
         if (cudaMemcpyAsync((double*)X + (size_t)w * j * ld, x + (size_t)w * j * n, colbytes, kout, P.stream) != cudaSuccess)

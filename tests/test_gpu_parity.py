@@ -122,6 +122,31 @@ def test_mixed_fp32_refinement(complex_):
         assert rel(X, Xd) <= 1e-8
 
 
+@pytest.mark.parametrize("complex_", [False, True])
+def test_refinement_fgmres_vs_classical(complex_, monkeypatch):
+    """FGMRES refinement (default) reaches the tolerance in no more solves
+    than classical refinement over the same FP32 factors, and both converge
+    to the same solution."""
+    n = 24
+    if complex_:
+        A, _, _ = ops.helmholtz_workload_3d(n, seed=7)
+    else:
+        A = ops.laplacian_3d(n, n, n, 6.1)
+    B = ops.random_rhs(A.n, 4, seed=3, complex_=complex_)
+    out = {}
+    for mode in ("gmres", "ir"):
+        monkeypatch.setenv("CLIQGPU_REFINE", mode)
+        map_, info, L = build(A, (n, n, n), 64, precision="single")
+        out[mode] = cliq.RefinedSolve(L, B, tol=1e-11, max_iter=30)
+        del L
+    (Xg, itg, rrg), (Xi, iti, rri) = out["gmres"], out["ir"]
+    print(f"solves: FGMRES {itg} (relres {rrg:.1e}), classical {iti} (relres {rri:.1e})")
+    assert rrg <= 1e-11 and rri <= 1e-11
+    assert residual(A, Xg, B) <= 1e-11
+    assert itg <= iti
+    assert rel(Xg, Xi) <= 1e-8
+
+
 def _magnetic(dims, shift=6.5, theta=0.3):
     A = ops.laplacian_3d(*dims, shift)
     vals = A.values.astype(np.complex128)
