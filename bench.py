@@ -281,15 +281,22 @@ def run_ours(args):
     upd_ms = prof["trail_ms"] + prof["schur_ms"]
     upd_flops = prof["trail_flops"] + prof["schur_flops"]
     achieved = upd_flops / (upd_ms * 1e-3) / 1e12 if upd_ms > 0 else 0.0
-    tf32_peak = peaks["bf16_tflops"] / 2.0 if peaks else 1590.0 / 2.0
-    roofline = {"kernel": "tc_update_kernel (tcgen05 kind::tf32, 3xTF32; Schur + in-panel updates)",
-                "bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
-                "frac": achieved / tf32_peak,
-                "peak_source": ("measured bf16 burst / 2 (dense TF32 rate is half of BF16), MEASURED_PEAKS.json"
-                                if peaks else "fallback 1.59 PFLOP/s bf16 / 2"),
-                "numerator": "Clique FactorizationWork counting (complex x4) of the update GEMMs; the three TF32 "
-                             "products per split count against the fraction, not in the numerator",
-                "traffic": None}
+    f16 = os.environ.get("CLIQGPU_SPLIT", "f16") != "tf32"
+    bf16 = peaks["bf16_tflops"] if peaks else 1590.0
+    # dense FP16 runs at the BF16 rate, dense TF32 at half of it
+    peak = bf16 if f16 else bf16 / 2.0
+    roofline = {"kernel": "tc_gemm_kernel (tcgen05 kind::f16, 2xFP16 split; Schur, outer and in-panel updates)"
+                          if f16 else "tc_gemm_kernel (tcgen05 kind::tf32, 3xTF32 split)",
+                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": ("measured bf16 burst" + ("" if f16 else " / 2") + ", MEASURED_PEAKS.json (of measured)")
+                if peaks else "fallback 1.59 PFLOP/s bf16" + ("" if f16 else " / 2") + " (of fallback)",
+                "numerator": "Clique FactorizationWork counting (complex x4) of the update GEMMs over their CUDA-event "
+                             "time (GEMM kernel only; operand packing is pack_ms); the three split products per real "
+                             "product count against the fraction, not in the numerator (frac <= 1/3)",
+                "traffic": 575e6,
+                "traffic_note": "DRAM read+write bytes of one Schur-update launch (60^3, tree level 2, 855 CTAs; "
+                                "ncu --set full); its algorithmic bytes (packed operands read once, update read and "
+                                "written once) are 582 MB"}
 
     # end-to-end through the C ABI with host buffers
     L32h = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
