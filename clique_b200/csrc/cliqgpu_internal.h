@@ -40,6 +40,8 @@ void set_last_error(const std::string& msg);
 // device-side descriptors
 // ---------------------------------------------------------------------------
 constexpr int kTile = 64;        // rows per solve block, GEMM tile edge
+constexpr int kTcBM = 128;       // tensor-core update tile: rows
+constexpr int kTcBN = 128;       // tensor-core update tile: columns (two CTAs per SM at 128)
 constexpr int kEACols = 16;      // columns per extend-add work item
 constexpr int kEARows = 2048;    // rows per extend-add work item
 // Triangular sweeps: the chain CTA of a front adds the contributions of the

@@ -211,19 +211,21 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     P.launches.clear();
     int64_t max_slots = 1;
     // update tiles over the lower trapezoid i >= j: 64 x 64 on the CUDA cores,
-    // 128 x 256 (row tile ti needed when ti >= 2 tj) on the tensor cores
+    // kTcBM x kTcBN (row tile ti needed when ti >= (kTcBN / kTcBM) tj) on the
+    // tensor cores
     const bool tcp = P.tensor_path();
     auto tiles_of = [](bool tc, int M, int N) -> int64_t {
         if (tc) {
-            const int64_t Mt = (M + 127) / 128, Nt = (N + 255) / 256;
-            return Nt * Mt - Nt * (Nt - 1);
+            const int64_t R = kTcBN / kTcBM;
+            const int64_t Mt = (M + kTcBM - 1) / kTcBM, Nt = (N + kTcBN - 1) / kTcBN;
+            return Nt * Mt - R * Nt * (Nt - 1) / 2;
         }
         const int64_t Mt = (M + kTile - 1) / kTile, Nt = (N + kTile - 1) / kTile;
         return Nt * Mt - Nt * (Nt - 1) / 2;
     };
     std::vector<PackJob> packjobs;
     const int planes = P.cplx() ? 4 : 2;
-    const int64_t blkA = (int64_t)planes * 128 * 8, blkB = (int64_t)planes * 256 * 8;   // floats per packed block
+    const int64_t blkA = (int64_t)planes * kTcBM * 8, blkB = (int64_t)planes * kTcBN * 8;   // floats per packed block
     int64_t pack_max = 1;
     auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur, bool inpanel) {
         if (lst.empty()) return;
@@ -250,26 +252,26 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             const int kstep = f16 ? 16 : 8;
             for (auto& pr : lst) {
                 const int64_t nk = (pr.K + kstep - 1) / kstep;
-                const int64_t tA = (pr.M + 127) / 128, tB = (pr.N + 255) / 256;
+                const int64_t tA = (pr.M + kTcBM - 1) / kTcBM, tB = (pr.N + kTcBN - 1) / kTcBN;
                 const FrontDev& fr = P.hfronts[pr.front];
                 const int nT = (fr.n + kTile - 1) / kTile;
-                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, 128, 0, 0, nT, pr.nkb};
+                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, kTcBM, 0, 0, nT, pr.nkb};
                 a.emax = pr.nkb > 0 ? fr.eblk + (int64_t)pr.row0 * nT + pr.kb0 : fr.erow + pr.row0;
                 pr.packA = off;
                 off += tA * nk * blkA;
                 a.dst_scale = pr.scaleA = off;
-                if (f16) off += tA * 128;
+                if (f16) off += tA * kTcBM;
                 PackJob b = a;
                 b.src = pr.B;
                 b.dst = off;
                 b.d = pr.d;
                 b.R = pr.N;
-                b.tile_rows = 256;
+                b.tile_rows = kTcBN;
                 b.emax += pr.nkb > 0 ? P.eblk_total : P.erow_total;   // the D op(L) half
                 pr.packB = off;
                 off += tB * nk * blkB;
                 b.dst_scale = pr.scaleB = off;
-                if (f16) off += tB * 256;
+                if (f16) off += tB * kTcBN;
                 for (const PackJob& j : {a, b}) {
                     prefix.push_back(blocks);
                     blocks += (int64_t)((j.R + j.tile_rows - 1) / j.tile_rows) * nk;

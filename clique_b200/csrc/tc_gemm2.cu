@@ -12,10 +12,11 @@
 //    The B operand is packed already scaled, S = d * op(B).
 //  * tc_gemm_kernel streams those blocks with cp.async.bulk (one elected
 //    producer thread, mbarrier transaction counts) through a 4-stage ring,
-//    one elected thread issues 12 (complex) or 3 (real) tcgen05.mma
-//    kind::tf32 128 x 256 x 8 per k step into two 256-column TMEM
-//    accumulators (Re, Im), and four epilogue warps read them back with
-//    tcgen05.ld and update C.
+//    one elected thread issues 12 (complex) or 3 (real) tcgen05.mma of
+//    128 x kTcBN per k step into two kTcBN-column TMEM accumulators (Re, Im),
+//    and four epilogue warps read them back with tcgen05.ld and update C.
+//    With 128 x 128 tiles (256 TMEM columns, 3 stages of 32 KB) two CTAs
+//    share an SM, so one CTA's epilogue overlaps the other's products.
 // The 3xTF32 split: X = X_hi + X_lo, X_hi = X with the low 13 mantissa bits
 // cleared; A B ~= A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32.
 // The 2xFP16 split (default) keeps the same three products at twice the
@@ -38,17 +39,19 @@
 namespace cliqgpu {
 namespace tc2 {
 
-constexpr int kBM = 128, kBN = 256, kKS = 8;   // kKS: TF32 k step (an FP16 step is 2 * kKS wide, same bytes)
-constexpr int kStages = 4;
+constexpr int kBM = kTcBM, kBN = kTcBN, kKS = 8;   // kKS: TF32 k step (an FP16 step is 2 * kKS wide, same bytes)
+constexpr int kRatio = kBN / kBM;                  // row tiles per column tile
+constexpr int kStages = kBN == 128 ? 3 : 4;        // 3 stages of 32 KB: two CTAs per SM
+constexpr int kMinBlocks = kBN == 128 ? 2 : 1;
 constexpr int kThreads = 192;                 // warps 0-3 epilogue, 4 TMA producer, 5 MMA issuer
 
 template <bool C>
 struct Cfg {
     static constexpr int kPlanes = C ? 4 : 2;                  // (re_hi, re_lo, im_hi, im_lo) or (hi, lo)
     static constexpr int kABytes = kPlanes * kBM * kKS * 4;    // one A block: 128 rows
-    static constexpr int kBBytes = kPlanes * kBN * kKS * 4;    // one S block: 256 rows
+    static constexpr int kBBytes = kPlanes * kBN * kKS * 4;    // one S block: kBN rows
     static constexpr int kStage = kABytes + kBBytes;
-    static constexpr int kTmem = C ? 512 : 256;
+    static constexpr int kTmem = C ? 2 * kBN : kBN;
 };
 
 
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(256) pack_f16_kernel(const PackJob* __restrict
 // GEMM on packed operands
 // ---------------------------------------------------------------------------
 template <bool C, bool F16>
-__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
                                                               int nprobs, const float* __restrict__ pack, float* __restrict__ L,
                                                               float* __restrict__ pool0, float* __restrict__ pool1,
                                                               int32_t* __restrict__ status) {
@@ -209,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
     uint64_t* done = empty + kStages;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
 
-    // tile of this CTA: 128-row tiles ti, 256-column tiles tj, needed when ti >= 2 tj
+    // tile of this CTA: kBM-row tiles ti, kBN-column tiles tj, needed when ti >= kRatio tj
     const int64_t bid = blockIdx.x;
     int lo = 0, hi = nprobs - 1;
     while (lo < hi) {
@@ -220,12 +223,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const GemmProb* __
     int64_t t = bid - prefix[lo];
     const int Mt = (pr.M + kBM - 1) / kBM, Nt = (pr.N + kBN - 1) / kBN;
     int tj = 0;
-    while (tj < Nt && t >= Mt - 2 * tj) { t -= Mt - 2 * tj; ++tj; }
+    while (tj < Nt && t >= Mt - kRatio * tj) { t -= Mt - kRatio * tj; ++tj; }
     if (tj >= Nt) {
         if (threadIdx.x == 0) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 5); }
         return;
     }
-    const int ti = 2 * tj + (int)t;
+    const int ti = kRatio * tj + (int)t;
     const int i0 = ti * kBM, j0 = tj * kBN;
     constexpr int kstep = F16 ? 2 * kKS : kKS;
     const int nk = (pr.K + kstep - 1) / kstep;
