@@ -52,7 +52,11 @@ constexpr int kSolveLag = 2;
 constexpr int kSolveRhsChunk = 16;   // right-hand sides per sweep (partial-sum stride)
 constexpr int kLowerChunkTiles = 16; // backward: 64-row tiles below the pivots per helper
 // sweep work items {front, kind, block, chunk}
-enum SweepItem : int { kItemChain = 0, kItemPivotRows = 1, kItemLowerRows = 2, kItemColumns = 1, kItemLowerChunk = 2 };
+enum SweepItem : int { kItemChain = 0, kItemPivotRows = 1, kItemLowerRows = 2, kItemColumns = 1, kItemLowerChunk = 2,
+                       kItemWhole = 3 };
+// fronts solved by one CTA per sweep (no flags): at most two pivot blocks
+// and kWholeLowerRows rows below the pivots
+constexpr int kWholeLowerRows = 512;
 
 // One front as the kernels see it.  Offsets are in elements (a complex
 // element is two scalars).

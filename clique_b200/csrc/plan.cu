@@ -447,6 +447,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         // forward: each front's chain followed by its pivot-row workers in the
         // order the chain consumes their partial sums, then the workers for the
         // rows below the pivots (they only wait on chains, all issued before)
+        // Small fronts (whole()) get one CTA that solves the front alone, last.
+        auto whole = [](const FrontDev& f) { return f.n <= 2 * kTile && f.m - f.n <= kWholeLowerRows; };
         sl.fwd_items = (int64_t)items.size() / 4;
         for (int s : P.level_list[d]) {
             FrontDev& f = P.hfronts[s];
@@ -454,13 +456,18 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             const int nT = (f.n + kTile - 1) / kTile;
             f.flag_base = flag;
             flag += nT;
+            if (whole(f)) continue;
             push_item(s, kItemChain, 0, 0);
             for (int rb = kSolveLag + 1; rb < nT; ++rb) push_item(s, kItemPivotRows, rb, 0);
         }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
-            if (f.n <= 0 || f.m <= 0) continue;
+            if (f.n <= 0 || f.m <= 0 || whole(f)) continue;
             for (int i = 0; f.n + i * kTile < f.m; ++i) push_item(s, kItemLowerRows, i, 0);
+        }
+        for (int s : P.level_list[d]) {
+            const FrontDev& f = P.hfronts[s];
+            if (f.n > 0 && f.m > 0 && whole(f)) push_item(s, kItemWhole, 0, 0);
         }
         sl.nfwd = (int32_t)(items.size() / 4 - sl.fwd_items);
         // backward: first the helpers (rows below the pivots beyond the first
@@ -474,17 +481,22 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             const int low_tiles = (f.m - f.n + kTile - 1) / kTile;
             f.nch = std::max(1, (low_tiles + kLowerChunkTiles - 1) / kLowerChunkTiles);
             f.hbase = (int32_t)P.helpers_total;
+            if (whole(f)) { f.nch = 1; continue; }
             P.helpers_total += (int64_t)nT * (f.nch - 1);
             for (int c = nT - 1; c >= 0; --c)
                 for (int ch = 1; ch < f.nch; ++ch) push_item(s, kItemLowerChunk, c, ch);
         }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
-            if (f.n <= 0 || f.m <= 0) continue;
+            if (f.n <= 0 || f.m <= 0 || whole(f)) continue;
             const int nT = (f.n + kTile - 1) / kTile;
             push_item(s, kItemChain, 0, 0);
             for (int c = nT - 1; c >= 0; --c)
                 if (f.m > f.n || c + kSolveLag + 1 <= nT - 1) push_item(s, kItemColumns, c, 0);
+        }
+        for (int s : P.level_list[d]) {
+            const FrontDev& f = P.hfronts[s];
+            if (f.n > 0 && f.m > 0 && whole(f)) push_item(s, kItemWhole, 0, 0);
         }
         sl.nbwd = (int32_t)(items.size() / 4 - sl.bwd_items);
     }

@@ -82,6 +82,14 @@ __device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_
     return s_ok != 0;
 }
 
+// thread 0 reads the flag once (no wait); the CTA learns whether it is set
+__device__ __forceinline__ bool test_flag(const int32_t* flag, int epoch) {
+    __shared__ int s_set;
+    if (threadIdx.x == 0) s_set = ld_acquire(flag) == epoch;
+    __syncthreads();
+    return s_set != 0;
+}
+
 __device__ __forceinline__ void publish_flag(int32_t* flag, int epoch) {
     __threadfence();
     __syncthreads();
@@ -250,21 +258,35 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
     Xv* st = sx + kTile * NR;       // right-hand side of the diagonal block
     Xv lp[kE], dv[kE];
     row_slice<T, C>(dv, Dinv, f.dinv, kTile, r, q, kTile, kTile);
+    // b_s - partial_s for the next step, gathered after each publish when the
+    // worker has already finished (then the step starts without a global
+    // round trip)
+    Xv nxt[NR / kQ];
+    bool have_next = false;
     for (int s = 0; s < nT; ++s) {
         const int r0 = s * kTile, ds = min(kTile, f.n - r0);
         const bool fed = s > kLag;  // a worker holds the contributions of blocks < s - kLag
-        if (fed && !wait_flag(&a.pflags[f.flag_base + s], a.epoch, a.status)) return;
         Xv tv[NR / kQ];
+        if (have_next) {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) tv[b] = nxt[b];
+        } else {
+            if (fed && !wait_flag(&a.pflags[f.flag_base + s], a.epoch, a.status)) return;
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                Xv v{};
+                if (r < ds && j < a.nrhs) {
+                    v = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx);
+                    if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s) * kPartialStride + j * kTile + r);
+                }
+                tv[b] = v;
+            }
+        }
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            Xv v{};
-            if (r < ds && j < a.nrhs) {
-                v = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx);
-                if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s) * kPartialStride + j * kTile + r);
-                if (s >= 2) v -= sq[(s & 1) * kTile * NR + r * NR + j];
-            }
-            tv[b] = v;
+            if (s >= 2 && r < ds && j < a.nrhs) tv[b] -= sq[(s & 1) * kTile * NR + r * NR + j];
         }
         if (s > 0) {
             Xv acc[NR];
@@ -298,11 +320,31 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             row_slice<T, C>(lp, L, f.L + (r0 + kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - kTile), kTile);
             row_slice<T, C>(dv, Dinv, f.dinv + (int64_t)(s + 1) * kTile * kTile, kTile, r, q, kTile, kTile);
         }
+        // tile of the off-path product, in flight during the publish
+        Xv lq[kE];
+        if (s + 2 < nT)
+            row_slice<T, C>(lq, L, f.L + (r0 + 2 * kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - 2 * kTile), kTile);
         publish_flag(&a.xflags[f.flag_base + s], a.epoch);
+        have_next = false;
+        if (s + 1 < nT) {
+            const int s1 = s + 1, r1 = s1 * kTile, d1 = min(kTile, f.n - r1);
+            const bool fed1 = s1 > kLag;
+            if (!fed1 || test_flag(&a.pflags[f.flag_base + s1], a.epoch)) {
+#pragma unroll
+                for (int b = 0; b < NR / kQ; ++b) {
+                    const int j = q + kQ * b;
+                    Xv v{};
+                    if (r < d1 && j < a.nrhs) {
+                        v = ldv<T, C>(X, f.off + r1 + r + (int64_t)j * a.ldx);
+                        if (fed1) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s1) * kPartialStride + j * kTile + r);
+                    }
+                    nxt[b] = v;
+                }
+                have_next = true;
+            }
+        }
         // off the critical path: q_{s+2} = L_{s+2,s} x_s
         if (s + 2 < nT) {
-            Xv lq[kE];
-            row_slice<T, C>(lq, L, f.L + (r0 + 2 * kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - 2 * kTile), kTile);
             Xv acc[NR];
 #pragma unroll
             for (int j = 0; j < NR; ++j) acc[j] = Xv{};
@@ -316,8 +358,87 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
     }
 }
 
+// Forward sweep of a small front (at most two pivot blocks, kWholeLowerRows
+// rows below) by one CTA: both blocks, then every 64-row tile below the
+// pivots, with the solved blocks kept in shared memory (no flags).
 template <class T, bool C, int NR>
-__global__ void __launch_bounds__(kSolveThreads) fwd_sweep_kernel(SweepArgs a) {
+__device__ void fwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq) {
+    using Xv = V<T, C>;
+    const T* L = reinterpret_cast<const T*>(a.L);
+    const T* Dinv = reinterpret_cast<const T*>(a.dinv);
+    T* X = reinterpret_cast<T*>(a.X);
+    Xv* st = sx;                     // right-hand side of the diagonal block
+    Xv* xb = sq;                     // x_0, x_1
+    for (int s = 0; s < nT; ++s) {
+        const int r0 = s * kTile, ds = min(kTile, f.n - r0);
+        Xv tv[NR / kQ];
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            tv[b] = (r < ds && j < a.nrhs) ? ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx) : Xv{};
+        }
+        Xv dv[kE];
+        row_slice<T, C>(dv, Dinv, f.dinv + (int64_t)s * kTile * kTile, kTile, r, q, kTile, kTile);
+        if (s == 1) {
+            Xv lp[kE];
+            row_slice<T, C>(lp, L, f.L + kTile, f.m, r, q, ds, kTile);   // L_{1,0}
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, lp, xb, q);
+            Xv u[NR / kQ];
+            reduce_slices<NR>(acc, red, u, r, q);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) tv[b] -= u[b];
+        }
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = tv[b];
+        __syncthreads();
+        Xv acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+        slice_mac<false, NR>(acc, dv, st, q);
+        Xv xs[NR / kQ];
+        reduce_slices<NR>(acc, red, xs, r, q);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            const bool in = r < ds && j < a.nrhs;
+            if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, xs[b]);
+            xb[s * kTile * NR + r * NR + j] = in ? xs[b] : Xv{};
+        }
+        __syncthreads();
+    }
+    // rows below the pivots: W_B -= L_B x_T
+    T* wb = reinterpret_cast<T*>(f.pool == 0 ? a.w0 : a.w1);
+    for (int R0 = f.n; R0 < f.m; R0 += kTile) {
+        const int nr = min(kTile, f.m - R0);
+        Xv acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+        for (int t = 0; t < nT; ++t) {
+            Xv lt[kE];
+            row_slice<T, C>(lt, L, f.L + R0 + (int64_t)t * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - t * kTile));
+            slice_mac<false, NR>(acc, lt, xb + t * kTile * NR, q);
+        }
+        Xv out[NR / kQ];
+        reduce_slices<NR>(acc, red, out, r, q);
+        if (r < nr) {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                if (j < a.nrhs) {
+                    const int64_t e = f.W * a.nrhs + (R0 - f.n + r) + (int64_t)j * f.u;
+                    stv<T, C>(wb, e, ldv<T, C>(wb, e) - out[b]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <class T, bool C, int NR>
+__global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) fwd_sweep_kernel(SweepArgs a) {
     using Xv = V<T, C>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
@@ -333,6 +454,10 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_sweep_kernel(SweepArgs a) {
     const int nT = (f.n + kTile - 1) / kTile;
     if (it.y == kItemChain) {
         fwd_chain<T, C, NR>(a, f, nT, r, q, sx, red, sq);
+        return;
+    }
+    if (it.y == kItemWhole) {
+        fwd_whole<T, C, NR>(a, f, nT, r, q, sx, red, sq);
         return;
     }
     // worker: rows [R0, R0 + nr) against the pivot blocks t < t_end
@@ -396,21 +521,34 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
     // thread (r, q) holds column r, rows q*kE .. q*kE+kE-1 of the row-major tiles
     Xv lp[kE], dv[kE];
     row_slice<T, C>(dv, DinvT, f.dinv + (int64_t)(nT - 1) * kTile * kTile, kTile, r, q, kTile, kTile);
+    // y_c - partial_c for the next step, gathered after each publish when the
+    // worker has already finished
+    Xv nxt[NR / kQ];
+    bool have_next = false;
     for (int c = nT - 1; c >= 0; --c) {
         const int c0 = c * kTile, dc = min(kTile, f.n - c0);
         const bool fed = f.m > f.n || c + kLag + 1 <= nT - 1;
-        if (fed && !wait_flag(&a.pflags[f.flag_base + c], a.epoch, a.status)) return;
         Xv tv[NR / kQ];
+        if (have_next) {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) tv[b] = nxt[b];
+        } else {
+            if (fed && !wait_flag(&a.pflags[f.flag_base + c], a.epoch, a.status)) return;
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                Xv v{};
+                if (r < dc && j < a.nrhs) {
+                    v = ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx);
+                    if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r);
+                }
+                tv[b] = v;
+            }
+        }
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            Xv v{};
-            if (r < dc && j < a.nrhs) {
-                v = ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx);
-                if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r);
-                if (c + 2 < nT) v -= sq[(c & 1) * kTile * NR + r * NR + j];
-            }
-            tv[b] = v;
+            if (c + 2 < nT && r < dc && j < a.nrhs) tv[b] -= sq[(c & 1) * kTile * NR + r * NR + j];
         }
         if (c + 1 < nT) {
             Xv acc[NR];
@@ -445,11 +583,30 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             row_slice<T, C>(lp, SubT, blk, kTile, r, q, kTile, kTile);
             row_slice<T, C>(dv, DinvT, blk, kTile, r, q, kTile, kTile);
         }
+        // tile of the off-path product, in flight during the publish
+        Xv lq[kE];
+        if (c >= 2) row_slice<T, C>(lq, SubT2, f.dinv + (int64_t)(c - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
         publish_flag(&a.xflags[f.flag_base + c], a.epoch);
+        have_next = false;
+        if (c >= 1) {
+            const int c1 = c - 1, o1 = c1 * kTile;
+            const bool fed1 = f.m > f.n || c1 + kLag + 1 <= nT - 1;
+            if (!fed1 || test_flag(&a.pflags[f.flag_base + c1], a.epoch)) {
+#pragma unroll
+                for (int b = 0; b < NR / kQ; ++b) {
+                    const int j = q + kQ * b;
+                    Xv v{};
+                    if (j < a.nrhs) {   // blocks before the last are full
+                        v = ldv<T, C>(X, f.off + o1 + r + (int64_t)j * a.ldx);
+                        if (fed1) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c1) * kPartialStride + j * kTile + r);
+                    }
+                    nxt[b] = v;
+                }
+                have_next = true;
+            }
+        }
         // off the critical path: q_{c-2} = op(L_{c,c-2})^T x_c
         if (c >= 2) {
-            Xv lq[kE];
-            row_slice<T, C>(lq, SubT2, f.dinv + (int64_t)(c - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
             Xv acc[NR];
 #pragma unroll
             for (int j = 0; j < NR; ++j) acc[j] = Xv{};
@@ -463,8 +620,84 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, 
     }
 }
 
+// Backward sweep of a small front by one CTA: for each pivot block, last
+// first, the contributions of the rows below the pivots (x gathered at
+// lowerStruct; tiles staged through shared memory for the transposed
+// product) and of the later block, then the transposed inverse.
 template <class T, bool C, bool CJ, int NR>
-__global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
+__device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq,
+                          V<T, C>* sL) {
+    using Xv = V<T, C>;
+    constexpr int ldl = kTile + 1;
+    const T* L = reinterpret_cast<const T*>(a.L);
+    const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
+    const T* SubT = reinterpret_cast<const T*>(a.subT);
+    T* X = reinterpret_cast<T*>(a.X);
+    Xv* st = sx;
+    Xv* xs = sx + kTile * NR;        // gathered x of one tile below the pivots
+    Xv* x1 = sq;                     // x_1 once solved
+    for (int c = nT - 1; c >= 0; --c) {
+        const int c0 = c * kTile, dc = min(kTile, f.n - c0);
+        Xv acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+        for (int R0 = f.n; R0 < f.m; R0 += kTile) {
+            const int nr = min(kTile, f.m - R0);
+            Xv pre[kE];
+#pragma unroll
+            for (int p = 0; p < kE; ++p) {
+                const int cc = q + kQ * p;
+                pre[p] = (r < nr && cc < dc) ? ldv<T, C>(L, f.L + R0 + r + (int64_t)(c0 + cc) * f.m) : Xv{};
+            }
+            __syncthreads();   // previous readers of sL / xs are done
+#pragma unroll
+            for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
+            for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
+                const int rr = idx % kTile, j = idx / kTile;
+                xs[rr * NR + j] = (rr < nr && j < a.nrhs)
+                                      ? ldv<T, C>(X, (int64_t)a.lower[f.lower + R0 - f.n + rr] + (int64_t)j * a.ldx) : Xv{};
+            }
+            __syncthreads();
+            Xv v[kE];
+#pragma unroll
+            for (int k = 0; k < kE; ++k) v[k] = sL[r * ldl + q * kE + k];
+            slice_mac<CJ, NR>(acc, v, xs, q);
+        }
+        if (c + 1 < nT) {
+            Xv lp[kE];
+            row_slice<T, C>(lp, SubT, f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);   // tile (c+1, c)
+            slice_mac<CJ, NR>(acc, lp, x1, q);
+        }
+        Xv u[NR / kQ];
+        reduce_slices<NR>(acc, red, u, r, q);
+        Xv tv[NR / kQ];
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            tv[b] = (r < dc && j < a.nrhs) ? ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx) - u[b] : Xv{};
+            st[r * NR + j] = tv[b];
+        }
+        __syncthreads();
+        Xv dv[kE];
+        row_slice<T, C>(dv, DinvT, f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+        slice_mac<CJ, NR>(acc, dv, st, q);
+        Xv xv[NR / kQ];
+        reduce_slices<NR>(acc, red, xv, r, q);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            const bool in = r < dc && j < a.nrhs;
+            if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xv[b]);
+            x1[r * NR + j] = in ? xv[b] : Xv{};
+        }
+        __syncthreads();
+    }
+}
+
+template <class T, bool C, bool CJ, int NR>
+__global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) bwd_sweep_kernel(SweepArgs a) {
     using Xv = V<T, C>;
     constexpr int ldl = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -482,6 +715,10 @@ __global__ void __launch_bounds__(kSolveThreads) bwd_sweep_kernel(SweepArgs a) {
     const int nT = (f.n + kTile - 1) / kTile;
     if (it.y == kItemChain) {
         bwd_chain<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sq);
+        return;
+    }
+    if (it.y == kItemWhole) {
+        bwd_whole<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sq, sL);
         return;
     }
     // column worker (kItemColumns) or helper (kItemLowerChunk, chunk it.w >= 1):
