@@ -59,7 +59,7 @@ struct Cfg {
 // pack: one CTA per (row tile, k step) block of one job; thread = row
 // ---------------------------------------------------------------------------
 template <bool C, bool CJ>
-__global__ void __launch_bounds__(256) pack_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+__global__ void __launch_bounds__(kTcBM) pack_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
                                                    const float* __restrict__ L, const double* __restrict__ D,
                                                    float* __restrict__ out) {
     using X = V<float, C>;
@@ -133,7 +133,7 @@ __device__ __forceinline__ float absmax(float v) { return fabsf(v); }
 __device__ __forceinline__ float absmax(cx<float> v) { return fmaxf(fabsf(v.r), fabsf(v.i)); }
 
 template <bool C, bool CJ>
-__global__ void __launch_bounds__(256) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+__global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
                                                        const float* __restrict__ L, const double* __restrict__ D,
                                                        const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
                                                        float* __restrict__ out) {
@@ -356,11 +356,12 @@ static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between) {
     float* pk = reinterpret_cast<float*>(P.pack);
     const PackJob* jobs = P.packjobs + ln.pack_items;
     const int64_t* jpre = P.prefix + ln.pack_prefix;
+    if (ln.pack_blocks <= 0) return;   // nothing to update
     if constexpr (F16)
-        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
+        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
                                                                                    pk);
     else
-        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, 256, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
     if (between) cudaEventRecord(between, P.stream);
     const size_t smem = tc2_smem(C);
     static bool attr = false;
