@@ -87,7 +87,7 @@ __device__ __forceinline__ float row_scale(float mx, float* inv) {
 }
 
 template <bool C>
-__global__ void __launch_bounds__(kPanelThreads, 1) panel_tc_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
+__global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
                                                                     int k, float* __restrict__ L, const double* __restrict__ D,
                                                                     const float* __restrict__ tinv, float* __restrict__ subT,
                                                                     float* __restrict__ subT2, uint32_t* __restrict__ eblk,
@@ -125,32 +125,23 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_tc_kernel(const FrontD
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x < kPanelRows) {
-        // ---- A: row i of A21, two passes over its 64 columns (the second hits L1 / L2) ----
+        // ---- A: row i of A21, all 64 columns loaded at once into registers ----
         const int i = threadIdx.x;
         const bool vr = i < rows;
         const int64_t a0 = f.L + r0 + i + (int64_t)k * f.m;
+        X v[nb];
+#pragma unroll
+        for (int t = 0; t < nb; ++t) v[t] = (vr && t < kb) ? ldv<float, C>(L, a0 + (int64_t)t * f.m) : X{};
         float mx = 0.f;
-#pragma unroll 1
-        for (int t0 = 0; t0 < nb; t0 += 16) {
-            X v[16];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = (vr && t0 + q < kb) ? ldv<float, C>(L, a0 + (int64_t)(t0 + q) * f.m) : X{};
-#pragma unroll
-            for (int q = 0; q < 16; ++q) mx = fmaxf(mx, cmax(v[q]));
-        }
+        for (int t = 0; t < nb; ++t) mx = fmaxf(mx, cmax(v[t]));
         float inv;
         const float s = row_scale(mx, &inv);
         inv_a[i] = inv;
-#pragma unroll 1
-        for (int ks = 0; ks < kPanelSteps; ++ks) {
-            X v[16];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const int t = ks * 16 + q;
-                v[q] = (vr && t < kb) ? ldv<float, C>(L, a0 + (int64_t)t * f.m) * s : X{};
-            }
-            put_row16<C>(sAop, i, ks, v, kPanelSteps * PC::kABlock, PC::kABlock);
-        }
+        for (int t = 0; t < nb; ++t) v[t] = v[t] * s;
+#pragma unroll
+        for (int ks = 0; ks < kPanelSteps; ++ks) put_row16<C>(sAop, i, ks, v + 16 * ks, kPanelSteps * PC::kABlock, PC::kABlock);
     } else {
         // ---- B: row c of W^T, B[c][t] = U[t][c] / d_c ----
         const int c = threadIdx.x - kPanelRows;
@@ -163,28 +154,22 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_tc_kernel(const FrontD
         } else {
             s_d[c] = X{};
         }
-        float mx = 0.f;
-#pragma unroll 1
-        for (int t0 = 0; t0 < nb; t0 += 16) {
+        X v[nb];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const int t = t0 + q;
-                mx = fmaxf(mx, cmax((t < kb && c < kb) ? U[t * nb + c] * rd : X{}));
-            }
+        for (int t = 0; t < nb; ++t) v[t] = (t < kb && c < kb) ? U[t * nb + c] : X{};
+        float mx = 0.f;
+#pragma unroll
+        for (int t = 0; t < nb; ++t) {
+            v[t] = v[t] * rd;
+            mx = fmaxf(mx, cmax(v[t]));
         }
         float inv;
         const float s = row_scale(mx, &inv);
         inv_b[c] = inv;
-#pragma unroll 1
-        for (int ks = 0; ks < kPanelSteps; ++ks) {
-            X v[16];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const int t = ks * 16 + q;
-                v[q] = (t < kb && c < kb) ? U[t * nb + c] * rd * s : X{};
-            }
-            put_row16<C>(sBop, c, ks, v, kPanelSteps * PC::kBBlock, PC::kBBlock);
-        }
+        for (int t = 0; t < nb; ++t) v[t] = v[t] * s;
+#pragma unroll
+        for (int ks = 0; ks < kPanelSteps; ++ks) put_row16<C>(sBop, c, ks, v + 16 * ks, kPanelSteps * PC::kBBlock, PC::kBBlock);
     }
     // operands written by the generic proxy, read by the tensor cores
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
