@@ -293,10 +293,10 @@ def run_ours(args):
                 "numerator": "Clique FactorizationWork counting (complex x4) of the update GEMMs over their CUDA-event "
                              "time (GEMM kernel only; operand packing is pack_ms); the three split products per real "
                              "product count against the fraction, not in the numerator (frac <= 1/3)",
-                "traffic": 575e6,
-                "traffic_note": "DRAM read+write bytes of one Schur-update launch (60^3, tree level 2, 855 CTAs; "
-                                "ncu --set full); its algorithmic bytes (packed operands read once, update read and "
-                                "written once) are 582 MB"}
+                "traffic": 580e6,
+                "traffic_note": "DRAM read+write bytes of one Schur-update launch (60^3, tree level 2, 1653 CTAs of "
+                                "128x128; ncu --set full); its algorithmic bytes (packed operands read once, update "
+                                "read and written once) are 582 MB"}
 
     # end-to-end through the C ABI with host buffers
     L32h = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
