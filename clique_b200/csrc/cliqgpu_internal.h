@@ -44,10 +44,10 @@ constexpr int kTcBM = 128;       // tensor-core update tile: rows
 constexpr int kTcBN = 128;       // tensor-core update tile: columns (two CTAs per SM at 128)
 constexpr int kEACols = 16;      // columns per extend-add work item
 constexpr int kEARows = 2048;    // rows per extend-add work item
-// Triangular sweeps: the chain CTA of a front adds the contributions of the
-// kSolveLag newest solved blocks itself; workers add the older ones.
-// The chain computes the newest block's contribution on its critical path and
-// the second newest right after publishing each block, off that path.
+// Triangular sweeps: the worker of pivot block s adds the contributions of
+// the solved blocks up to s - kSolveLag and applies the block's inverse; the
+// chain CTA of the front adds the newest block (s - 1) through the stored
+// product of that inverse with the coupling tile.
 constexpr int kSolveLag = 2;
 constexpr int kSolveRhsChunk = 16;   // right-hand sides per sweep (partial-sum stride)
 constexpr int kLowerChunkTiles = 16; // backward: 64-row tiles below the pivots per helper
@@ -167,8 +167,14 @@ struct Plan {
     void* tinv = nullptr;         // U = op(L11^{-1})^T of each front of one panel step (storage precision)
     void* dinv = nullptr;         // L11^{-1} of every 64-block of every front, kept for the solves
     void* dinvT = nullptr;        // the same blocks row-major (backward sweep)
-    void* subT = nullptr;         // per pivot block b: tile (b+1, b) of the front's L, row-major (backward sweep)
-    void* subT2 = nullptr;        // per pivot block b: tile (b+2, b), row-major
+    // chain tiles (64 x 64, column-major, at the front's dinv offset + 64*64*b):
+    //   m1 block b >= 1: L_bb^{-1} L_{b,b-1} (forward chain)
+    //   n1 block b <= nT-2: op(L_bb^{-1})^T op(L_{b+1,b})^T (backward chain)
+    void* m1 = nullptr;
+    void* n1 = nullptr;
+    int32_t* chain_items = nullptr;   // int4 {front, block b >= 1, 0, 0} of every chain front
+    int32_t nchain_items = 0;
+    unsigned long long* xprog = nullptr;   // per front: (epoch << 32) | blocks its chain has published
     void* hpart = nullptr;        // backward helpers' partial sums (kSolveRhsChunk x 64 per helper)
     int64_t helpers_total = 0;
     void* partial = nullptr;      // per pivot block: 64 x kSolveRhsChunk partial sums from the sweep workers
@@ -191,7 +197,7 @@ struct Plan {
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;
-    int32_t* flags = nullptr;     // solved-block flags, partial-sum flags (flags_total each), helper flags
+    int32_t* flags = nullptr;     // worker flags (flags_total), spare (flags_total), helper flags
     int32_t* tickets = nullptr;
     int32_t* status = nullptr;    // [0] first zero pivot + 1 (min), [1] timeout flag
     int64_t* rowptr = nullptr;    // FP64 matrix (keep_matrix)

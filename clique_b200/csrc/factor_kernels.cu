@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items, int k,
                                                          T* __restrict__ L, const double* __restrict__ D, const T* __restrict__ tinv,
-                                                         T* __restrict__ subT, T* __restrict__ subT2, uint32_t* __restrict__ eblk,
+                                                         uint32_t* __restrict__ eblk,
                                                          uint32_t* __restrict__ erow,
                                                          int64_t eblk_total, int64_t erow_total) {
     using X = V<T, C>;
@@ -426,21 +426,94 @@ __global__ void __launch_bounds__(kThreads) panel_kernel(const FrontDev* __restr
             }
         }
     }
-    // the first two row blocks under a full diagonal block are tiles (b+1, b)
-    // and (b+2, b) of the pivot rows: keep row-major copies (zero outside the
-    // pivot rows) for the backward sweep's chain
-    T* sub = rb == 0 ? subT : (rb == 1 ? subT2 : nullptr);
-    if (sub && kb == nb && r0 < f.n) {
-        X* S = reinterpret_cast<X*>(sub) + f.dinv + (int64_t)(k / nb) * nb * nb;
-        const int prow = min(rows, f.n - r0);
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const int r = ty + 16 * a, c = tx + 16 * b;
-                S[r * nb + c] = r < prow ? acc[a][b] * sR[c] : X{};
-            }
+}
+
+// ---------------------------------------------------------------------------
+// 2c. chain tiles for the triangular sweeps, formed once after the whole
+// factorization.  For pivot block b >= 1 of a front, with the coupling tile
+// S = L_{b,b-1} (rows of block b, columns of block b-1):
+//   m1_b     = L_bb^{-1} S                          (forward chain)
+//   n1_{b-1} = op(L_{b-1,b-1}^{-1})^T op(S)^T       (backward chain)
+// both 64 x 64 column-major, zero outside the rows (m1) / columns (n1) of
+// block b.  With them a chain step needs one 64 x 64 product with the newest
+// solved block instead of two dependent ones.  One CTA per (front, b); each
+// thread forms a 4 x 4 register tile of both products from shared memory.
+// ---------------------------------------------------------------------------
+template <class T, bool C>
+__host__ __device__ constexpr size_t chain_tiles_smem_bytes() {
+    return sizeof(V<T, C>) * 2 * kTile * (kTile + 1);
+}
+
+template <class T, bool C, bool CJ>
+__global__ void __launch_bounds__(kThreads) chain_tiles_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
+                                                               const T* __restrict__ L, const T* __restrict__ dinv,
+                                                               T* __restrict__ m1, T* __restrict__ n1) {
+    using X = V<T, C>;
+    constexpr int nb = kTile, ld = kTile + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    X* sS = reinterpret_cast<X*>(smem_raw);     // S(r, c) at sS[r + c * ld]
+    X* sD = sS + nb * ld;                         // inverse block (r, c) at sD[r + c * ld]
+    const int4 it = items[blockIdx.x];
+    const FrontDev f = F[it.x];
+    const int b = it.y;
+    const int db = min(nb, f.n - b * nb);         // rows of block b (block b - 1 is full)
+    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+    const X* Dv = reinterpret_cast<const X*>(dinv) + f.dinv;
+    for (int idx = tid; idx < nb * nb; idx += kThreads) {
+        const int r = idx % nb, c = idx / nb;
+        sS[r + c * ld] = r < db ? ldv<T, C>(L, f.L + (int64_t)(b * nb + r) + (int64_t)((b - 1) * nb + c) * f.m) : X{};
+        sD[r + c * ld] = Dv[(int64_t)b * nb * nb + r + c * nb];
     }
+    __syncthreads();
+    X acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = X{};
+    // m1_b(i, j) = sum_k Dinv_b(i, k) S(k, j)
+    for (int k = 0; k < db; ++k) {
+        X a[4], s[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = sD[ty + 16 * i + k * ld];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s[j] = sS[k + (tx + 16 * j) * ld];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) mac(acc[i][j], a[i], s[j]);
+    }
+    X* M = reinterpret_cast<X*>(m1) + f.dinv + (int64_t)b * nb * nb;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) M[(ty + 16 * i) + (tx + 16 * j) * nb] = acc[i][j];
+    __syncthreads();
+    for (int idx = tid; idx < nb * nb; idx += kThreads) {
+        const int r = idx % nb, c = idx / nb;
+        sD[r + c * ld] = Dv[(int64_t)(b - 1) * nb * nb + r + c * nb];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = X{};
+    // n1_{b-1}(i, j) = op(sum_k Dinv_{b-1}(k, i) S(j, k))
+    for (int k = 0; k < nb; ++k) {
+        X a[4], s[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = sD[k + (ty + 16 * i) * ld];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s[j] = sS[(tx + 16 * j) + k * ld];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) mac(acc[i][j], a[i], s[j]);
+    }
+    X* N = reinterpret_cast<X*>(n1) + f.dinv + (int64_t)(b - 1) * nb * nb;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) N[(ty + 16 * i) + (tx + 16 * j) * nb] = opc<CJ>(acc[i][j]);
 }
 
 // ---------------------------------------------------------------------------
@@ -585,8 +658,8 @@ static int run_factor_impl(Plan& P) {
                     break;
                 }
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
-                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), reinterpret_cast<T*>(P.subT),
-                    reinterpret_cast<T*>(P.subT2), P.eblk, P.erow, P.eblk_total, P.erow_total);
+                    P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), P.eblk, P.erow, P.eblk_total,
+                    P.erow_total);
                 break;
             case Launch::GEMM:
                 if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
@@ -597,6 +670,18 @@ static int run_factor_impl(Plan& P) {
                 break;
         }
         if (P.profile) cudaEventRecord(P.events[3 * li + 1], P.stream);
+        ++launches;
+    }
+    if (P.nchain_items > 0) {
+        static bool ct_attr = false;
+        if (!ct_attr) {
+            cudaFuncSetAttribute(chain_tiles_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)chain_tiles_smem_bytes<T, C>());
+            ct_attr = true;
+        }
+        chain_tiles_kernel<T, C, CJ><<<(unsigned)P.nchain_items, kThreads, chain_tiles_smem_bytes<T, C>(), P.stream>>>(
+            P.fronts, reinterpret_cast<const int4*>(P.chain_items), L, reinterpret_cast<const T*>(P.dinv),
+            reinterpret_cast<T*>(P.m1), reinterpret_cast<T*>(P.n1));
         ++launches;
     }
     P.prof_pending = P.profile != 0;
@@ -725,7 +810,7 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
         diag_ldl_kernel<T, C, CJ, T><<<1, kThreads, diag_smem_bytes<T, C>(), st>>>(F, items + s.diag_item, s.k, AL, D, tinv, dinv, nullptr, status);
         if (s.panel_blocks > 0)
             panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr,
-                                                                               nullptr, nullptr, nullptr, 0, 0);
+                                                                               nullptr, 0, 0);
         if (s.prob >= 0)
             gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, AL, ABR,
                                                                                ABR, D);

@@ -76,7 +76,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 }
 
 void free_plan(Plan& P) {
-    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.subT, P.subT2, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
+    void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
                     P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov};
@@ -435,6 +435,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     P.solve_levels.assign(P.max_depth + 1, SolveLevel{});
     P.helpers_total = 0;
     std::vector<int32_t> level_fronts;
+    std::vector<int32_t> chain_items;   // int4 {front, block, 0, 0}: chain tiles to form after the factorization
     int flag = 0;
     for (int d = 0; d <= P.max_depth; ++d) {
         SolveLevel& sl = P.solve_levels[d];
@@ -445,7 +446,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         sl.gather_chunks = 1;
         for (int s : P.level_list[d]) sl.gather_chunks = std::max(sl.gather_chunks, (P.hfronts[s].m + 1023) / 1024);
         // forward: each front's chain followed by its pivot-row workers in the
-        // order the chain consumes their partial sums, then the workers for the
+        // order the chain consumes their results, then the workers for the
         // rows below the pivots (they only wait on chains, all issued before)
         // Small fronts (whole()) get one CTA that solves the front alone, last.
         auto whole = [](const FrontDev& f) { return f.n <= 2 * kTile && f.m - f.n <= kWholeLowerRows; };
@@ -458,7 +459,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             flag += nT;
             if (whole(f)) continue;
             push_item(s, kItemChain, 0, 0);
-            for (int rb = kSolveLag + 1; rb < nT; ++rb) push_item(s, kItemPivotRows, rb, 0);
+            for (int rb = 0; rb < nT; ++rb) push_item(s, kItemPivotRows, rb, 0);
+            for (int b = 1; b < nT; ++b) {
+                chain_items.push_back(s); chain_items.push_back(b); chain_items.push_back(0); chain_items.push_back(0);
+            }
         }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
@@ -491,8 +495,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             if (f.n <= 0 || f.m <= 0 || whole(f)) continue;
             const int nT = (f.n + kTile - 1) / kTile;
             push_item(s, kItemChain, 0, 0);
-            for (int c = nT - 1; c >= 0; --c)
-                if (f.m > f.n || c + kSolveLag + 1 <= nT - 1) push_item(s, kItemColumns, c, 0);
+            for (int c = nT - 1; c >= 0; --c) push_item(s, kItemColumns, c, 0);
         }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
@@ -541,8 +544,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.tinv, (size_t)P.tinv_slots * nb * nb * eb));
     TRY(dev_alloc(P, &P.dinv, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.dinvT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
-    TRY(dev_alloc(P, &P.subT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
-    TRY(dev_alloc(P, &P.subT2, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.m1, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    TRY(dev_alloc(P, &P.n1, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.hpart, (size_t)std::max<int64_t>(P.helpers_total, 1) * kTile * kSolveRhsChunk * eb));
     TRY(dev_alloc(P, &P.partial, (size_t)P.flags_total * kTile * kSolveRhsChunk * eb));
     if (P.f16_scales()) {
@@ -563,6 +566,11 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.level_fronts, level_fronts));
     std::vector<int32_t> zeros_flags(2 * P.flags_total + P.helpers_total, 0);
     TRY(dev_upload(P, &P.flags, zeros_flags));
+    P.nchain_items = (int32_t)(chain_items.size() / 4);
+    if (chain_items.empty()) chain_items.assign(4, 0);
+    TRY(dev_upload(P, &P.chain_items, chain_items));
+    std::vector<unsigned long long> zprog(std::max(nn, 1), 0ull);
+    TRY(dev_upload(P, &P.xprog, zprog));
     std::vector<int32_t> zt(2 * (P.max_depth + 1) + 2, 0);
     TRY(dev_upload(P, &P.tickets, zt));
     std::vector<int32_t> st = {INT_MAX, 0, 0, 0};

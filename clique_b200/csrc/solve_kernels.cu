@@ -9,24 +9,25 @@
 //
 // Each tree level is one gather launch plus one sweep launch (forward), or
 // one sweep launch (backward).  Inside a sweep launch every front gets
-//   * one chain CTA, which walks the front's 64-wide pivot blocks in order.
-//     Step s needs the block's right-hand side minus the contributions of
-//     all solved blocks.  The newest block's contribution is the only
-//     product on the chain's critical path (x_{s-1} stays in its shared
-//     memory, the 64x64 tile was prefetched into registers during the
-//     previous step); the second newest, q_s, the chain formed right after
-//     publishing x_{s-2}; the older ones arrive from a worker as one
-//     finished 64 x nrhs partial sum, which the worker had two chain steps
-//     to produce.  Then the chain applies the stored inverse of the diagonal
-//     block and publishes x_s: two 64x64 products and one flag per step, with
-//     no global-memory round trip for x.
+//   * one chain CTA, which walks the front's 64-wide pivot blocks in order:
+//         forward   x_s = y_s - M_s x_{s-1},   M_s = L_ss^{-1} L_{s,s-1},
+//         backward  x_c = z_c - N_c x_{c+1},   N_c = op(L_cc^{-1})^T op(L_{c+1,c})^T,
+//     with y_s / z_c from the block's worker and M, N formed once per
+//     factorization.  One 64 x 64 product per step is the chain's whole
+//     critical path: x_{s-1} stays in its shared memory and the tile was
+//     loaded into registers two steps earlier.  After each block the chain
+//     publishes its progress, one word per front.
 //   * workers, which stream the rest of the front's L tiles as the chain
-//     publishes solved blocks: forward, one per 64-row block of pivot rows
-//     (its partial feeds the chain) and one per 64-row block below the
-//     pivots (subtracts into the update vector W_B); backward, one per
-//     pivot column block (the first 16 tiles of rows below the pivots, the
-//     sums of its helpers in chunk order, then the later pivot blocks), and
-//     helpers for the further 16-tile chunks of rows below the pivots.
+//     publishes solved blocks.  Forward: one per 64-row block of pivot rows,
+//         y_s = L_ss^{-1} (b_s - sum_{t <= s-2} L_st x_t),
+//     and one per 64-row block below the pivots (subtracts into the update
+//     vector W_B).  Backward: one per pivot column block c,
+//         z_c = op(L_cc^{-1})^T (y_c - sum_{r below the pivots} op(L_rc)^T x_r
+//                                    - sum_{r >= c+2} op(L_rc)^T x_r),
+//     taking the first 16 tiles of rows below the pivots itself and the sums
+//     of helpers for the further 16-tile chunks (issued first, no waits).
+//   Every worker keeps the next L tile and, once published, the next x tile
+//   in flight while it multiplies the current one.
 // Work items are taken from an atomic ticket counter in the order helpers
 // (which wait for nothing), then each chain followed by its workers in the
 // order the chain consumes them, so every CTA a resident CTA waits for was
@@ -43,7 +44,7 @@ namespace cliqgpu {
 constexpr int kSolveThreads = 256;
 constexpr int kQ = kSolveThreads / kTile;   // slices per tile row (4)
 constexpr int kE = kTile / kQ;              // tile elements per thread and slice (16)
-constexpr int kLag = kSolveLag;             // blocks the chain adds itself (the two newest)
+constexpr int kLag = kSolveLag;             // worker s adds the blocks t <= s - kLag
 constexpr int kMaxRhsChunk = kSolveRhsChunk;   // right-hand sides per sweep
 constexpr int kPartialStride = kTile * kMaxRhsChunk;   // elements per pivot block in the partial store
 constexpr int kGatherRows = 1024;           // front rows per gather CTA (grid y of the gather launch)
@@ -52,6 +53,12 @@ constexpr uint64_t kSpinNs = 500000000ull;  // 0.5 s bound on any single wait
 __device__ __forceinline__ int ld_acquire(const int32_t* p) {
     int v;
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -82,18 +89,58 @@ __device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_
     return s_ok != 0;
 }
 
-// thread 0 reads the flag once (no wait); the CTA learns whether it is set
-__device__ __forceinline__ bool test_flag(const int32_t* flag, int epoch) {
+// Publish after the CTA's stores: the barrier orders every thread's stores
+// before thread 0's fence, which makes them visible at device scope before
+// the flag.
+__device__ __forceinline__ void publish_flag(int32_t* flag, int epoch) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicExch(flag, epoch);
+    }
+}
+
+// Chain progress word of a front: (epoch << 32) | number of solved blocks
+// published in this launch.  A word from an older launch counts as zero.
+__device__ __forceinline__ int progress_count(unsigned long long w, int epoch) {
+    return (int)(w >> 32) == epoch ? (int)(w & 0xffffffffu) : 0;
+}
+
+// Chain: publish `count` solved blocks (thread 0) and meanwhile test the
+// flag of the next worker result (thread 32, null: none); returns whether
+// that flag is set, the same for the whole CTA.
+__device__ __forceinline__ bool publish_and_test(unsigned long long* word, int count, int epoch, const int32_t* next_flag) {
     __shared__ int s_set;
-    if (threadIdx.x == 0) s_set = ld_acquire(flag) == epoch;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicExch(word, ((unsigned long long)(unsigned)epoch << 32) | (unsigned)count);
+    } else if (threadIdx.x == 32) {
+        s_set = next_flag != nullptr && ld_acquire(next_flag) == epoch;
+    }
     __syncthreads();
     return s_set != 0;
 }
 
-__device__ __forceinline__ void publish_flag(int32_t* flag, int epoch) {
-    __threadfence();
+// thread 0 waits until the chain has published at least `need` blocks; the
+// CTA gets the count seen (every block below it is readable), or -1 after a
+// timeout (wait site 4) or another CTA's timeout
+__device__ __forceinline__ int wait_progress(const unsigned long long* word, int need, int epoch, int32_t* status) {
+    __shared__ int s_cnt;
+    if (threadIdx.x == 0) {
+        int cnt = progress_count(ld_acquire64(word), epoch);
+        if (cnt < need) {
+            const uint64_t t0 = global_ns();
+            while ((cnt = progress_count(ld_acquire64(word), epoch)) < need) {
+                if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) { cnt = -1; break; }
+                if (global_ns() - t0 > kSpinNs) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 4); cnt = -1; break; }
+                __nanosleep(64);
+            }
+        }
+        s_cnt = cnt;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) atomicExch(flag, epoch);
+    return s_cnt;
 }
 
 // v[k] = A(r, q*kE + k) of a column-major tile at element offset a0 with
@@ -140,15 +187,36 @@ __device__ __forceinline__ void reduce_slices(const Xv (&acc)[NR], Xv* red, Xv (
     }
 }
 
-// 64 x NR tile of right-hand sides from X (column-major, ldx) starting at
-// row x0, zero beyond nr rows or nrhs columns; L2-coherent loads for values
-// another CTA of this launch published
+// resident CTAs per SM the sweeps ask for: two when the L tiles of a thread
+// fit in half the register file (real or FP32 complex, up to 4 right-hand sides)
 template <class T, bool C, int NR>
-__device__ __forceinline__ void load_x_tile(V<T, C>* s, const T* X, int64_t x0, int64_t ldx, int nr, int nrhs) {
-    for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
-        const int rr = idx % kTile, j = idx / kTile;
-        s[rr * NR + j] = (rr < nr && j < nrhs) ? ldv_cg<T, C>(X, x0 + rr + (int64_t)j * ldx) : V<T, C>{};
+constexpr int sweep_min_blocks() { return (NR <= 4 && !(C && sizeof(T) == 8)) ? 2 : 1; }
+
+// Register staging of a 64 x NR tile of right-hand sides: element e of this
+// thread is (row (tid + 256 e) % 64, rhs (tid + 256 e) / 64).
+template <int NR>
+struct XStage {
+    static constexpr int kN = kTile * NR / kSolveThreads;
+    __device__ __forceinline__ static int row(int e) { return (threadIdx.x + kSolveThreads * e) % kTile; }
+    __device__ __forceinline__ static int rhs(int e) { return (threadIdx.x + kSolveThreads * e) / kTile; }
+};
+
+// x rows x0 .. x0 + nr - 1 of X (column-major, ldx) into registers, zero
+// beyond nr rows or nrhs columns; L2-coherent loads for values another CTA
+// of this launch published
+template <class T, bool C, int NR>
+__device__ __forceinline__ void stage_x(V<T, C> (&xr)[XStage<NR>::kN], const T* X, int64_t x0, int64_t ldx, int nr, int nrhs) {
+#pragma unroll
+    for (int e = 0; e < XStage<NR>::kN; ++e) {
+        const int rr = XStage<NR>::row(e), j = XStage<NR>::rhs(e);
+        xr[e] = (rr < nr && j < nrhs) ? ldv_cg<T, C>(X, x0 + rr + (int64_t)j * ldx) : V<T, C>{};
     }
+}
+
+template <int NR, class Xv>
+__device__ __forceinline__ void put_x(const Xv (&xr)[XStage<NR>::kN], Xv* s) {
+#pragma unroll
+    for (int e = 0; e < XStage<NR>::kN; ++e) s[XStage<NR>::row(e) * NR + XStage<NR>::rhs(e)] = xr[e];
 }
 
 // ---------------------------------------------------------------------------
@@ -203,22 +271,23 @@ __global__ void diag_scale_kernel(T* __restrict__ X, int64_t ldx, int64_t n, int
     }
 }
 
+
 // ---------------------------------------------------------------------------
 // sweep launches
 // ---------------------------------------------------------------------------
 struct SweepArgs {
     const FrontDev* F;
-    const int4* items;      // {front, kind, block, 0}
+    const int4* items;      // {front, kind, block, chunk}
     int32_t* ticket;
-    int32_t* xflags;        // per pivot block: x_b published (chain)
-    int32_t* pflags;        // per pivot block: partial sum published (worker)
+    unsigned long long* xprog;   // per front: the chain's progress word
+    int32_t* pflags;        // per pivot block: the worker's y / z published
     int epoch;
     const void* L;
     const void* dinv;       // L11^{-1} per 64-block, column-major
     const void* dinvT;      // the same, row-major
-    const void* subT;       // tile (b+1, b) of L per pivot block, row-major
-    const void* subT2;      // tile (b+2, b) of L per pivot block, row-major
-    void* partial;          // kPartialStride elements per pivot block
+    const void* m1;         // forward chain tiles L_ss^{-1} L_{s,s-1}
+    const void* n1;         // backward chain tiles op(L_cc^{-1})^T op(L_{c+1,c})^T
+    void* partial;          // kPartialStride elements per pivot block: y_s / z_c
     void* hpart;            // backward helpers' partial sums, kPartialStride each
     int32_t* hflags;        // backward helpers' flags
     void* X;                // n x nrhs, ND order, ld ldx
@@ -230,133 +299,72 @@ struct SweepArgs {
     int32_t* status;
 };
 
-// One L tile of a forward worker: wait for x_t, stage it, accumulate.
+// Forward chain of front fi: x_s = y_s - M_s x_{s-1}.  Step s multiplies the
+// tile M_s (in registers since step s-2) with x_{s-1} (in shared memory),
+// subtracts the product from y_s (the worker's result, loaded right after
+// publishing x_{s-1} when the worker had finished, else waited for now),
+// stores and publishes x_s.
 template <class T, bool C, int NR>
-__device__ __forceinline__ bool fwd_tile(const SweepArgs& a, const FrontDev& f, int t, const V<T, C>* lt, V<T, C> (&acc)[NR],
-                                         V<T, C>* sx, int q) {
-    V<T, C>* sb = sx + (t & 1) * kTile * NR;
-    if (!wait_flag(&a.xflags[f.flag_base + t], a.epoch, a.status)) return false;
-    load_x_tile<T, C, NR>(sb, reinterpret_cast<const T*>(a.X), f.off + (int64_t)t * kTile, a.ldx, min(kTile, f.n - t * kTile), a.nrhs);
-    __syncthreads();
-    slice_mac<false, NR>(acc, lt, sb, q);
-    return true;
-}
-
-// Forward chain of one front:
-//   x_s = L_ss^{-1} (b_s - partial_s - q_s - L_{s,s-1} x_{s-1}),
-// partial_s from the pivot-row worker (blocks < s - 2), q_s = L_{s,s-2} x_{s-2}
-// formed by the chain right after it published x_{s-2}.
-template <class T, bool C, int NR>
-__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq) {
+__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
     using Xv = V<T, C>;
-    static_assert(kLag == 2, "the chain adds the two newest blocks");
-    const T* L = reinterpret_cast<const T*>(a.L);
-    const T* Dinv = reinterpret_cast<const T*>(a.dinv);
+    const T* M1 = reinterpret_cast<const T*>(a.m1);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
-    Xv* sprev = sx;                 // x_{s-1}
-    Xv* st = sx + kTile * NR;       // right-hand side of the diagonal block
-    Xv lp[kE], dv[kE];
-    row_slice<T, C>(dv, Dinv, f.dinv, kTile, r, q, kTile, kTile);
-    // b_s - partial_s for the next step, gathered after each publish when the
-    // worker has already finished (then the step starts without a global
-    // round trip)
     Xv nxt[NR / kQ];
     bool have_next = false;
-    for (int s = 0; s < nT; ++s) {
+    auto load_y = [&](int s, Xv (&v)[NR / kQ]) {
+        const int ds = min(kTile, f.n - s * kTile);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            v[b] = (r < ds && j < a.nrhs) ? ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s) * kPartialStride + j * kTile + r) : Xv{};
+        }
+    };
+    // the product first: y_s, loaded at the end of the previous step (or
+    // waited for now), arrives meanwhile
+    auto step = [&](int s, Xv (&mt)[kE]) -> bool {
         const int r0 = s * kTile, ds = min(kTile, f.n - r0);
-        const bool fed = s > kLag;  // a worker holds the contributions of blocks < s - kLag
+        Xv u[NR / kQ];
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) u[b] = Xv{};
+        if (s > 0) {
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, mt, sx + ((s - 1) & 1) * kTile * NR, q);
+            reduce_slices<NR>(acc, red, u, r, q);
+        }
         Xv tv[NR / kQ];
         if (have_next) {
 #pragma unroll
             for (int b = 0; b < NR / kQ; ++b) tv[b] = nxt[b];
         } else {
-            if (fed && !wait_flag(&a.pflags[f.flag_base + s], a.epoch, a.status)) return;
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) {
-                const int j = q + kQ * b;
-                Xv v{};
-                if (r < ds && j < a.nrhs) {
-                    v = ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx);
-                    if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s) * kPartialStride + j * kTile + r);
-                }
-                tv[b] = v;
-            }
+            if (!wait_flag(&a.pflags[f.flag_base + s], a.epoch, a.status)) return false;
+            load_y(s, tv);
         }
+        Xv* xs = sx + (s & 1) * kTile * NR;
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            if (s >= 2 && r < ds && j < a.nrhs) tv[b] -= sq[(s & 1) * kTile * NR + r * NR + j];
+            const bool in = r < ds && j < a.nrhs;
+            const Xv x = tv[b] - u[b];
+            if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, x);
+            xs[r * NR + j] = in ? x : Xv{};
         }
-        if (s > 0) {
-            Xv acc[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<false, NR>(acc, lp, sprev, q);
-            Xv u[NR / kQ];
-            reduce_slices<NR>(acc, red, u, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) tv[b] -= u[b];
-        }
-#pragma unroll
-        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = tv[b];
-        __syncthreads();
-        {
-            Xv acc[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<false, NR>(acc, dv, st, q);
-            Xv xs[NR / kQ];
-            reduce_slices<NR>(acc, red, xs, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) {
-                const int j = q + kQ * b;
-                const bool in = r < ds && j < a.nrhs;
-                if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, xs[b]);
-                sprev[r * NR + j] = in ? xs[b] : Xv{};
-            }
-        }
-        if (s + 1 < nT) {
-            row_slice<T, C>(lp, L, f.L + (r0 + kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - kTile), kTile);
-            row_slice<T, C>(dv, Dinv, f.dinv + (int64_t)(s + 1) * kTile * kTile, kTile, r, q, kTile, kTile);
-        }
-        // tile of the off-path product, in flight during the publish
-        Xv lq[kE];
-        if (s + 2 < nT)
-            row_slice<T, C>(lq, L, f.L + (r0 + 2 * kTile) + (int64_t)r0 * f.m, f.m, r, q, min(kTile, f.n - r0 - 2 * kTile), kTile);
-        publish_flag(&a.xflags[f.flag_base + s], a.epoch);
-        have_next = false;
-        if (s + 1 < nT) {
-            const int s1 = s + 1, r1 = s1 * kTile, d1 = min(kTile, f.n - r1);
-            const bool fed1 = s1 > kLag;
-            if (!fed1 || test_flag(&a.pflags[f.flag_base + s1], a.epoch)) {
-#pragma unroll
-                for (int b = 0; b < NR / kQ; ++b) {
-                    const int j = q + kQ * b;
-                    Xv v{};
-                    if (r < d1 && j < a.nrhs) {
-                        v = ldv<T, C>(X, f.off + r1 + r + (int64_t)j * a.ldx);
-                        if (fed1) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + s1) * kPartialStride + j * kTile + r);
-                    }
-                    nxt[b] = v;
-                }
-                have_next = true;
-            }
-        }
-        // off the critical path: q_{s+2} = L_{s+2,s} x_s
-        if (s + 2 < nT) {
-            Xv acc[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<false, NR>(acc, lq, sprev, q);
-            Xv qv[NR / kQ];
-            reduce_slices<NR>(acc, red, qv, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) sq[(s & 1) * kTile * NR + r * NR + q + kQ * b] = qv[b];
-            __syncthreads();
-        }
+        have_next = publish_and_test(&a.xprog[fi], s + 1, a.epoch, s + 1 < nT ? &a.pflags[f.flag_base + s + 1] : nullptr);
+        if (have_next) load_y(s + 1, nxt);
+        // M_{s+2} for the step after next
+        if (s + 2 < nT) row_slice<T, C>(mt, M1, f.dinv + (int64_t)(s + 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+        return true;
+    };
+    Xv mA[kE], mB[kE];
+    if (nT > 1) row_slice<T, C>(mB, M1, f.dinv + (int64_t)kTile * kTile, kTile, r, q, kTile, kTile);
+    for (int s = 0; s < nT; s += 2) {
+        if (!step(s, mA)) return;
+        if (s + 1 < nT && !step(s + 1, mB)) return;
     }
 }
+
 
 // Forward sweep of a small front (at most two pivot blocks, kWholeLowerRows
 // rows below) by one CTA: both blocks, then every 64-row tile below the
@@ -437,60 +445,109 @@ __device__ void fwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, 
     }
 }
 
+
+// Forward worker: rows [R0, R0 + nr) of the front against the pivot blocks
+// t < t_end.  Pivot-row worker of block s (t_end = s - 1):
+//   y_s = L_ss^{-1} (b_s - sum_t L_st x_t)  -> partial store, flag;
+// lower-row worker (t_end = nT): W_B -= sum_t L_Bt x_t.
+// The L tile t + 1 is always in flight during tile t; the x tile t + 1 too
+// once the chain's progress word shows it published.
 template <class T, bool C, int NR>
-__global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) fwd_sweep_kernel(SweepArgs a) {
+__device__ void fwd_worker(const SweepArgs& a, const FrontDev& f, int fi, int nT, int kind, int blk, int r, int q, V<T, C>* sx,
+                           V<T, C>* red) {
     using Xv = V<T, C>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
-    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
-    Xv* sq = red + kQ * NR * kTile;               // 2 x [64][NR]: the chain's off-path products
-    __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
-    __syncthreads();
-    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
-    const int4 it = a.items[s_item];
-    const FrontDev f = a.F[it.x];
-    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
-    const int nT = (f.n + kTile - 1) / kTile;
-    if (it.y == kItemChain) {
-        fwd_chain<T, C, NR>(a, f, nT, r, q, sx, red, sq);
-        return;
-    }
-    if (it.y == kItemWhole) {
-        fwd_whole<T, C, NR>(a, f, nT, r, q, sx, red, sq);
-        return;
-    }
-    // worker: rows [R0, R0 + nr) against the pivot blocks t < t_end
+    using XS = XStage<NR>;
     const T* L = reinterpret_cast<const T*>(a.L);
-    int R0, nr, t_end;
-    if (it.y == kItemPivotRows) { R0 = kTile * it.z; nr = min(kTile, f.n - R0); t_end = it.z - kLag; }
-    else { R0 = f.n + kTile * it.z; nr = min(kTile, f.m - R0); t_end = nT; }
+    const T* X = reinterpret_cast<const T*>(a.X);
+    const bool piv = kind == kItemPivotRows;
+    const int R0 = piv ? kTile * blk : f.n + kTile * blk;
+    const int nr = min(kTile, (piv ? f.n : f.m) - R0);
+    const int t_end = piv ? blk - (kLag - 1) : nT;
+    // right-hand side rows of a pivot block, read before the chain overwrites them
+    Xv bv[NR / kQ];
+    if (piv) {
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            bv[b] = (r < nr && j < a.nrhs) ? ldv<T, C>(X, f.off + R0 + r + (int64_t)j * a.ldx) : Xv{};
+        }
+    }
     Xv acc[NR];
 #pragma unroll
     for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-    Xv la[kE], lb[kE];
-    row_slice<T, C>(la, L, f.L + R0, f.m, r, q, nr, min(kTile, f.n));
-    for (int t = 0; t < t_end; t += 2) {
-        // two tiles in flight: the next one loads while this one waits for its x block
-        if (t + 1 < t_end)
-            row_slice<T, C>(lb, L, f.L + R0 + (int64_t)(t + 1) * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - (t + 1) * kTile));
-        if (!fwd_tile<T, C, NR>(a, f, t, la, acc, sx, q)) return;
-        if (t + 1 >= t_end) break;
-        if (t + 2 < t_end)
-            row_slice<T, C>(la, L, f.L + R0 + (int64_t)(t + 2) * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - (t + 2) * kTile));
-        if (!fwd_tile<T, C, NR>(a, f, t + 1, lb, acc, sx, q)) return;
-    }
-    Xv out[NR / kQ];
-    reduce_slices<NR>(acc, red, out, r, q);
-    if (it.y == kItemPivotRows) {
+    int known = 0;            // blocks the chain is known to have published
+    Xv xr[XS::kN];
+    // tile t (L in cur, x_t staged in sx[t & 1]); loads tile t + 1 into oth,
+    // or the block inverse after the last tile of a pivot-row worker
+    auto tile = [&](int t, Xv (&cur)[kE], Xv (&oth)[kE]) -> bool {
+        const bool more = t + 1 < t_end;
+        if (more)
+            row_slice<T, C>(oth, L, f.L + R0 + (int64_t)(t + 1) * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - (t + 1) * kTile));
+        else if (piv)
+            row_slice<T, C>(oth, reinterpret_cast<const T*>(a.dinv), f.dinv + (int64_t)blk * kTile * kTile, kTile, r, q, kTile, kTile);
+        const bool pre = more && t + 1 < known;
+        if (pre) stage_x<T, C, NR>(xr, X, f.off + (int64_t)(t + 1) * kTile, a.ldx, min(kTile, f.n - (t + 1) * kTile), a.nrhs);
+        __syncthreads();   // x_t staged
+        slice_mac<false, NR>(acc, cur, sx + (t & 1) * kTile * NR, q);
+        if (more) {
+            if (!pre) {
+                const int c = wait_progress(&a.xprog[fi], t + 2, a.epoch, a.status);
+                if (c < 0) return false;
+                known = c;
+                stage_x<T, C, NR>(xr, X, f.off + (int64_t)(t + 1) * kTile, a.ldx, min(kTile, f.n - (t + 1) * kTile), a.nrhs);
+            }
+            put_x<NR>(xr, sx + ((t + 1) & 1) * kTile * NR);
+        }
+        return true;
+    };
+    // y_s = L_ss^{-1} (b_s - acc) with the inverse in dv
+    auto finish_pivot = [&](const Xv (&dv)[kE]) {
+        Xv out[NR / kQ];
+        reduce_slices<NR>(acc, red, out, r, q);
+        Xv* st = sx;   // every reader of sx passed the barrier in reduce_slices
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = bv[b] - out[b];
+        __syncthreads();
+        Xv acc2[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc2[j] = Xv{};
+        slice_mac<false, NR>(acc2, dv, st, q);
+        Xv y[NR / kQ];
+        reduce_slices<NR>(acc2, red, y, r, q);
         T* Part = reinterpret_cast<T*>(a.partial);
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + it.z) * kPartialStride + j * kTile + r, out[b]);
+            if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + blk) * kPartialStride + j * kTile + r, y[b]);
         }
-        publish_flag(&a.pflags[f.flag_base + it.z], a.epoch);
-    } else if (r < nr) {
+        publish_flag(&a.pflags[f.flag_base + blk], a.epoch);
+    };
+    Xv la[kE], lb[kE];
+    if (t_end <= 0) {   // pivot blocks 0 .. kLag-1: nothing to wait for
+        row_slice<T, C>(la, reinterpret_cast<const T*>(a.dinv), f.dinv + (int64_t)blk * kTile * kTile, kTile, r, q, kTile, kTile);
+        finish_pivot(la);
+        return;
+    }
+    row_slice<T, C>(la, L, f.L + R0, f.m, r, q, nr, min(kTile, f.n));
+    {
+        const int c = wait_progress(&a.xprog[fi], 1, a.epoch, a.status);
+        if (c < 0) return;
+        known = c;
+        stage_x<T, C, NR>(xr, X, f.off, a.ldx, min(kTile, f.n), a.nrhs);
+        put_x<NR>(xr, sx);
+    }
+    for (int t = 0; t < t_end; t += 2) {
+        if (!tile(t, la, lb)) return;
+        if (t + 1 < t_end && !tile(t + 1, lb, la)) return;
+    }
+    if (piv) {
+        if (t_end & 1) finish_pivot(lb);
+        else finish_pivot(la);
+        return;
+    }
+    Xv out[NR / kQ];
+    reduce_slices<NR>(acc, red, out, r, q);
+    if (r < nr) {
         T* wb = reinterpret_cast<T*>(f.pool == 0 ? a.w0 : a.w1);
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
@@ -503,159 +560,129 @@ __global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) fwd_sweep_kern
     }
 }
 
-// Backward chain of one front, last pivot block first:
-//   x_c = op(L_cc^{-1})^T (y_c - partial_c - q_c - op(L_{c+1,c})^T x_{c+1}),
-// partial_c from the column worker (rows below the pivots and pivot blocks
-// after c + 2), q_c = op(L_{c+2,c})^T x_{c+2} formed right after x_{c+2}.
-template <class T, bool C, bool CJ, int NR>
-__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq) {
+template <class T, bool C, int NR>
+__global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) fwd_sweep_kernel(SweepArgs a) {
     using Xv = V<T, C>;
-    static_assert(kLag == 2, "the chain adds the two newest blocks");
-    const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
-    const T* SubT = reinterpret_cast<const T*>(a.subT);
-    const T* SubT2 = reinterpret_cast<const T*>(a.subT2);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
+    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
+    Xv* sq = red + kQ * NR * kTile;               // 2 x [64][NR]: solved blocks of a small front
+    __shared__ int s_item;
+    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
+    __syncthreads();
+    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
+    const int4 it = a.items[s_item];
+    const FrontDev f = a.F[it.x];
+    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
+    const int nT = (f.n + kTile - 1) / kTile;
+    if (it.y == kItemChain) fwd_chain<T, C, NR>(a, f, it.x, nT, r, q, sx, red);
+    else if (it.y == kItemWhole) fwd_whole<T, C, NR>(a, f, nT, r, q, sx, red, sq);
+    else fwd_worker<T, C, NR>(a, f, it.x, nT, it.y, it.z, r, q, sx, red);
+}
+
+// Backward chain of front fi, last pivot block first: x_c = z_c - N_c x_{c+1}
+// with z_c from the column worker; after each block the progress word counts
+// the blocks solved from the end.
+template <class T, bool C, bool CJ, int NR>
+__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+    using Xv = V<T, C>;
+    const T* N1 = reinterpret_cast<const T*>(a.n1);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
-    Xv* sprev = sx;                 // x_{c+1}
-    Xv* st = sx + kTile * NR;
-    // thread (r, q) holds column r, rows q*kE .. q*kE+kE-1 of the row-major tiles
-    Xv lp[kE], dv[kE];
-    row_slice<T, C>(dv, DinvT, f.dinv + (int64_t)(nT - 1) * kTile * kTile, kTile, r, q, kTile, kTile);
-    // y_c - partial_c for the next step, gathered after each publish when the
-    // worker has already finished
     Xv nxt[NR / kQ];
     bool have_next = false;
-    for (int c = nT - 1; c >= 0; --c) {
-        const int c0 = c * kTile, dc = min(kTile, f.n - c0);
-        const bool fed = f.m > f.n || c + kLag + 1 <= nT - 1;
+    auto load_z = [&](int c, Xv (&v)[NR / kQ]) {
+        const int dc = min(kTile, f.n - c * kTile);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            v[b] = (r < dc && j < a.nrhs) ? ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r) : Xv{};
+        }
+    };
+    // i counts the chain's steps: block c = nT - 1 - i
+    auto step = [&](int i, Xv (&nt)[kE]) -> bool {
+        const int c = nT - 1 - i, c0 = c * kTile, dc = min(kTile, f.n - c0);
+        Xv u[NR / kQ];
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) u[b] = Xv{};
+        if (i > 0) {
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, nt, sx + ((i - 1) & 1) * kTile * NR, q);
+            reduce_slices<NR>(acc, red, u, r, q);
+        }
         Xv tv[NR / kQ];
         if (have_next) {
 #pragma unroll
             for (int b = 0; b < NR / kQ; ++b) tv[b] = nxt[b];
         } else {
-            if (fed && !wait_flag(&a.pflags[f.flag_base + c], a.epoch, a.status)) return;
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) {
-                const int j = q + kQ * b;
-                Xv v{};
-                if (r < dc && j < a.nrhs) {
-                    v = ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx);
-                    if (fed) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r);
-                }
-                tv[b] = v;
-            }
+            if (!wait_flag(&a.pflags[f.flag_base + c], a.epoch, a.status)) return false;
+            load_z(c, tv);
         }
+        Xv* xs = sx + (i & 1) * kTile * NR;
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            if (c + 2 < nT && r < dc && j < a.nrhs) tv[b] -= sq[(c & 1) * kTile * NR + r * NR + j];
+            const bool in = r < dc && j < a.nrhs;
+            const Xv x = tv[b] - u[b];
+            if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, x);
+            xs[r * NR + j] = in ? x : Xv{};
         }
-        if (c + 1 < nT) {
-            Xv acc[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<CJ, NR>(acc, lp, sprev, q);
-            Xv u[NR / kQ];
-            reduce_slices<NR>(acc, red, u, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) tv[b] -= u[b];
-        }
-#pragma unroll
-        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = tv[b];
-        __syncthreads();
-        {
-            Xv acc[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<CJ, NR>(acc, dv, st, q);
-            Xv xs[NR / kQ];
-            reduce_slices<NR>(acc, red, xs, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) {
-                const int j = q + kQ * b;
-                const bool in = r < dc && j < a.nrhs;
-                if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xs[b]);
-                sprev[r * NR + j] = in ? xs[b] : Xv{};
-            }
-        }
-        if (c > 0) {
-            const int64_t blk = f.dinv + (int64_t)(c - 1) * kTile * kTile;
-            row_slice<T, C>(lp, SubT, blk, kTile, r, q, kTile, kTile);
-            row_slice<T, C>(dv, DinvT, blk, kTile, r, q, kTile, kTile);
-        }
-        // tile of the off-path product, in flight during the publish
-        Xv lq[kE];
-        if (c >= 2) row_slice<T, C>(lq, SubT2, f.dinv + (int64_t)(c - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
-        publish_flag(&a.xflags[f.flag_base + c], a.epoch);
-        have_next = false;
-        if (c >= 1) {
-            const int c1 = c - 1, o1 = c1 * kTile;
-            const bool fed1 = f.m > f.n || c1 + kLag + 1 <= nT - 1;
-            if (!fed1 || test_flag(&a.pflags[f.flag_base + c1], a.epoch)) {
-#pragma unroll
-                for (int b = 0; b < NR / kQ; ++b) {
-                    const int j = q + kQ * b;
-                    Xv v{};
-                    if (j < a.nrhs) {   // blocks before the last are full
-                        v = ldv<T, C>(X, f.off + o1 + r + (int64_t)j * a.ldx);
-                        if (fed1) v -= ldv_cg<T, C>(Part, (int64_t)(f.flag_base + c1) * kPartialStride + j * kTile + r);
-                    }
-                    nxt[b] = v;
-                }
-                have_next = true;
-            }
-        }
-        // off the critical path: q_{c-2} = op(L_{c,c-2})^T x_c
-        if (c >= 2) {
-            Xv acc[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<CJ, NR>(acc, lq, sprev, q);
-            Xv qv[NR / kQ];
-            reduce_slices<NR>(acc, red, qv, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) sq[(c & 1) * kTile * NR + r * NR + q + kQ * b] = qv[b];
-            __syncthreads();
-        }
+        have_next = publish_and_test(&a.xprog[fi], i + 1, a.epoch, c >= 1 ? &a.pflags[f.flag_base + c - 1] : nullptr);
+        if (have_next) load_z(c - 1, nxt);
+        // N_{c-2} for the step after next
+        if (c >= 2) row_slice<T, C>(nt, N1, f.dinv + (int64_t)(c - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+        return true;
+    };
+    Xv nA[kE], nB[kE];
+    if (nT > 1) row_slice<T, C>(nB, N1, f.dinv + (int64_t)(nT - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+    for (int i = 0; i < nT; i += 2) {
+        if (!step(i, nA)) return;
+        if (i + 1 < nT && !step(i + 1, nB)) return;
     }
 }
 
 // Backward sweep of a small front by one CTA: for each pivot block, last
 // first, the contributions of the rows below the pivots (x gathered at
-// lowerStruct; tiles staged through shared memory for the transposed
-// product) and of the later block, then the transposed inverse.
+// lowerStruct) and of the later pivot block (x from this CTA's own stores),
+// tiles staged through shared memory for the transposed product, then the
+// transposed inverse.
 template <class T, bool C, bool CJ, int NR>
-__device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq,
-                          V<T, C>* sL) {
+__device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sL) {
     using Xv = V<T, C>;
     constexpr int ldl = kTile + 1;
     const T* L = reinterpret_cast<const T*>(a.L);
     const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
-    const T* SubT = reinterpret_cast<const T*>(a.subT);
     T* X = reinterpret_cast<T*>(a.X);
     Xv* st = sx;
-    Xv* xs = sx + kTile * NR;        // gathered x of one tile below the pivots
-    Xv* x1 = sq;                     // x_1 once solved
+    Xv* xs = sx + kTile * NR;        // x of one tile
     for (int c = nT - 1; c >= 0; --c) {
         const int c0 = c * kTile, dc = min(kTile, f.n - c0);
         Xv acc[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-        for (int R0 = f.n; R0 < f.m; R0 += kTile) {
-            const int nr = min(kTile, f.m - R0);
+        // row tiles: the later pivot block (c + 1 < nT), then the rows below the pivots
+        const int R1 = c + 1 < nT ? c0 + kTile : f.n;
+        for (int R0 = R1; R0 < f.m; R0 = R0 < f.n ? f.n : R0 + kTile) {
+            const bool pivrows = R0 < f.n;
+            const int nr = pivrows ? min(kTile, f.n - R0) : min(kTile, f.m - R0);
             Xv pre[kE];
 #pragma unroll
             for (int p = 0; p < kE; ++p) {
                 const int cc = q + kQ * p;
                 pre[p] = (r < nr && cc < dc) ? ldv<T, C>(L, f.L + R0 + r + (int64_t)(c0 + cc) * f.m) : Xv{};
             }
-            __syncthreads();   // previous readers of sL / xs are done
+            __syncthreads();   // previous readers of sL / xs are done; this CTA's x stores are visible
 #pragma unroll
             for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
             for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
                 const int rr = idx % kTile, j = idx / kTile;
-                xs[rr * NR + j] = (rr < nr && j < a.nrhs)
-                                      ? ldv<T, C>(X, (int64_t)a.lower[f.lower + R0 - f.n + rr] + (int64_t)j * a.ldx) : Xv{};
+                Xv v{};
+                if (rr < nr && j < a.nrhs)
+                    v = pivrows ? ldv<T, C>(X, f.off + R0 + rr + (int64_t)j * a.ldx)
+                                : ldv<T, C>(X, (int64_t)a.lower[f.lower + R0 - f.n + rr] + (int64_t)j * a.ldx);
+                xs[rr * NR + j] = v;
             }
             __syncthreads();
             Xv v[kE];
@@ -663,19 +690,12 @@ __device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, 
             for (int k = 0; k < kE; ++k) v[k] = sL[r * ldl + q * kE + k];
             slice_mac<CJ, NR>(acc, v, xs, q);
         }
-        if (c + 1 < nT) {
-            Xv lp[kE];
-            row_slice<T, C>(lp, SubT, f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);   // tile (c+1, c)
-            slice_mac<CJ, NR>(acc, lp, x1, q);
-        }
         Xv u[NR / kQ];
         reduce_slices<NR>(acc, red, u, r, q);
-        Xv tv[NR / kQ];
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            tv[b] = (r < dc && j < a.nrhs) ? ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx) - u[b] : Xv{};
-            st[r * NR + j] = tv[b];
+            st[r * NR + j] = (r < dc && j < a.nrhs) ? ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx) - u[b] : Xv{};
         }
         __syncthreads();
         Xv dv[kE];
@@ -688,59 +708,53 @@ __device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, 
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            const bool in = r < dc && j < a.nrhs;
-            if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xv[b]);
-            x1[r * NR + j] = in ? xv[b] : Xv{};
+            if (r < dc && j < a.nrhs) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xv[b]);
         }
         __syncthreads();
     }
 }
 
+// Backward column worker of pivot block c (kItemColumns) or helper
+// (kItemLowerChunk, chunk >= 1): op(L[R, c-block])^T x_R over its tiles of
+// rows R below the pivots (x gathered at lowerStruct, final since the
+// ancestors are solved).  The column worker then takes the pivot blocks
+// nT-1 .. c+2 as the chain publishes them, adds its helpers' sums in chunk
+// order and forms z_c = op(L_cc^{-1})^T (y_c - sum).  Tiles are staged
+// through shared memory for the transposed product; the next tile's L and,
+// when available, its x are in flight during the current one.
 template <class T, bool C, bool CJ, int NR>
-__global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) bwd_sweep_kernel(SweepArgs a) {
+__device__ void bwd_worker(const SweepArgs& a, const FrontDev& f, int fi, int nT, int kind, int c, int chunk, int r, int q,
+                           V<T, C>* sx, V<T, C>* red, V<T, C>* sL, int32_t* sidx) {
     using Xv = V<T, C>;
+    using XS = XStage<NR>;
     constexpr int ldl = kTile + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
-    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
-    Xv* sq = red + kQ * NR * kTile;               // 2 x [64][NR]: the chain's off-path products
-    Xv* sL = sq + 2 * kTile * NR;                 // [64 columns][65]
-    __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
-    __syncthreads();
-    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
-    const int4 it = a.items[s_item];
-    const FrontDev f = a.F[it.x];
-    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
-    const int nT = (f.n + kTile - 1) / kTile;
-    if (it.y == kItemChain) {
-        bwd_chain<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sq);
-        return;
-    }
-    if (it.y == kItemWhole) {
-        bwd_whole<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sq, sL);
-        return;
-    }
-    // column worker (kItemColumns) or helper (kItemLowerChunk, chunk it.w >= 1):
-    // op(L[R, c-block])^T x_R over rows R below the pivots (x gathered at
-    // lowerStruct, final since the ancestors are solved); the worker then adds
-    // the helpers' sums and the pivot blocks after c + kLag as the chain
-    // publishes them
-    const bool helper = it.y == kItemLowerChunk;
+    const bool helper = kind == kItemLowerChunk;
     const T* L = reinterpret_cast<const T*>(a.L);
     const T* X = reinterpret_cast<const T*>(a.X);
-    const int c = it.z, c0 = c * kTile, dc = min(kTile, f.n - c0);
+    const int c0 = c * kTile, dc = min(kTile, f.n - c0);
     const int nlow = (f.m - f.n + kTile - 1) / kTile;
-    const int low0 = helper ? it.w * kLowerChunkTiles : 0;
+    const int low0 = helper ? chunk * kLowerChunkTiles : 0;
     const int low1 = min(nlow, low0 + kLowerChunkTiles);
     const int nl = max(0, low1 - low0);
-    const int npiv = helper ? 0 : max(0, nT - 1 - (c + kLag));
+    const int npiv = helper ? 0 : max(0, nT - 1 - c - (kLag - 1));
     const int ntiles = nl + npiv;
-    // coalesced staging: element p of this thread is (row r, column q + kQ*p)
+    // right-hand side of the block, read before the chain overwrites it
+    Xv yv[NR / kQ];
+    if (!helper) {
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            yv[b] = (r < dc && j < a.nrhs) ? ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx) : Xv{};
+        }
+    }
+    // gather indices of this item's rows below the pivots
+    const int lrow0 = low0 * kTile, lrows = min(f.m - f.n - lrow0, nl * kTile);
+    for (int i = threadIdx.x; i < lrows; i += kSolveThreads) sidx[i] = a.lower[f.lower + lrow0 + i];
     auto tile_of = [&](int i, int& R0, int& nr) {
         if (i < nl) { R0 = f.n + kTile * (low0 + i); nr = min(kTile, f.m - R0); }
         else { R0 = kTile * (nT - 1 - (i - nl)); nr = min(kTile, f.n - R0); }
     };
+    // coalesced staging: element p of this thread is (row r, column q + kQ*p)
     Xv pre[kE];
     auto fetch = [&](int i) {
         int R0, nr;
@@ -751,38 +765,89 @@ __global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) bwd_sweep_kern
             pre[p] = (r < nr && cc < dc) ? ldv<T, C>(L, f.L + R0 + r + (int64_t)(c0 + cc) * f.m) : Xv{};
         }
     };
+    int known = 0;   // blocks the chain is known to have published (from the last)
+    Xv xr[XS::kN];
+    auto stage = [&](int i) {   // x of tile i into xr (pivot tiles: published)
+        int R0, nr;
+        tile_of(i, R0, nr);
+        if (i < nl) {
+            const int base = (i * kTile);
+#pragma unroll
+            for (int e = 0; e < XS::kN; ++e) {
+                const int rr = XS::row(e), j = XS::rhs(e);
+                xr[e] = (rr < nr && j < a.nrhs) ? ldv<T, C>(X, (int64_t)sidx[base + rr] + (int64_t)j * a.ldx) : Xv{};
+            }
+        } else {
+            stage_x<T, C, NR>(xr, X, f.off + R0, a.ldx, nr, a.nrhs);
+        }
+    };
+    auto ready = [&](int i) { int R0, nr; tile_of(i, R0, nr); return i < nl || nT - R0 / kTile <= known; };
     Xv acc[NR];
 #pragma unroll
     for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-    if (ntiles > 0) fetch(0);
+    if (ntiles > 0) {
+        fetch(0);
+        __syncthreads();   // gather indices in shared memory
+        if (!ready(0)) {
+            int R0, nr;
+            tile_of(0, R0, nr);
+            const int cnt = wait_progress(&a.xprog[fi], nT - R0 / kTile, a.epoch, a.status);
+            if (cnt < 0) return;
+            known = cnt;
+        }
+        stage(0);
+    }
+    // sums of the helpers of this column block (issued before this CTA), in
+    // chunk order; taken before the pivot tiles so that no wait on a helper
+    // follows the chain's last block
+    Xv hsum[NR / kQ];
+#pragma unroll
+    for (int b = 0; b < NR / kQ; ++b) hsum[b] = Xv{};
+    auto add_helpers = [&]() -> bool {
+        const T* HP = reinterpret_cast<const T*>(a.hpart);
+        for (int ch = 1; ch < f.nch; ++ch) {
+            const int64_t h = f.hbase + (int64_t)c * (f.nch - 1) + (ch - 1);
+            if (!wait_flag(&a.hflags[h], a.epoch, a.status)) return false;
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                if (j < a.nrhs) hsum[b] += ldv_cg<T, C>(HP, h * kPartialStride + j * kTile + r);
+            }
+        }
+        return true;
+    };
+    if (!helper && nl == 0 && !add_helpers()) return;
     for (int i = 0; i < ntiles; ++i) {
-        int R0, nr;
-        tile_of(i, R0, nr);
         __syncthreads();   // the previous tile's readers are done with sL and sx
 #pragma unroll
         for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
-        if (i + 1 < ntiles) fetch(i + 1);
-        if (i >= nl) {
-            if (!wait_flag(&a.xflags[f.flag_base + R0 / kTile], a.epoch, a.status)) return;
-            load_x_tile<T, C, NR>(sx, X, f.off + R0, a.ldx, nr, a.nrhs);
-        } else {
-            for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
-                const int rr = idx % kTile, j = idx / kTile;
-                sx[rr * NR + j] = (rr < nr && j < a.nrhs)
-                                      ? ldv<T, C>(X, (int64_t)a.lower[f.lower + R0 - f.n + rr] + (int64_t)j * a.ldx) : Xv{};
-            }
-        }
+        put_x<NR>(xr, sx);
+        const bool more = i + 1 < ntiles;
+        if (more) fetch(i + 1);
+        else if (!helper)   // pre is free: the block's transposed inverse, as a row slice
+            row_slice<T, C>(pre, reinterpret_cast<const T*>(a.dinvT), f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
+        const bool pre_x = more && ready(i + 1);
+        if (pre_x) stage(i + 1);
         __syncthreads();
         Xv v[kE];
 #pragma unroll
         for (int k = 0; k < kE; ++k) v[k] = sL[r * ldl + q * kE + k];
         slice_mac<CJ, NR>(acc, v, sx, q);
+        if (more && !pre_x) {
+            int R0, nr;
+            tile_of(i + 1, R0, nr);
+            const int cnt = wait_progress(&a.xprog[fi], nT - R0 / kTile, a.epoch, a.status);
+            if (cnt < 0) return;
+            known = cnt;
+            stage(i + 1);
+        }
+        if (!helper && i + 1 == nl && !add_helpers()) return;
     }
     Xv out[NR / kQ];
     reduce_slices<NR>(acc, red, out, r, q);
     if (helper) {
         T* HP = reinterpret_cast<T*>(a.hpart);
-        const int64_t h = f.hbase + (int64_t)c * (f.nch - 1) + (it.w - 1);
+        const int64_t h = f.hbase + (int64_t)c * (f.nch - 1) + (chunk - 1);
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
@@ -791,25 +856,51 @@ __global__ void __launch_bounds__(kSolveThreads, NR <= 4 ? 2 : 1) bwd_sweep_kern
         publish_flag(&a.hflags[h], a.epoch);
         return;
     }
-    // the helpers of this column block were issued before this CTA; add
-    // their sums in chunk order
-    const T* HP = reinterpret_cast<const T*>(a.hpart);
-    for (int ch = 1; ch < f.nch; ++ch) {
-        const int64_t h = f.hbase + (int64_t)c * (f.nch - 1) + (ch - 1);
-        if (!wait_flag(&a.hflags[h], a.epoch, a.status)) return;
+    if (ntiles == 0)
+        row_slice<T, C>(pre, reinterpret_cast<const T*>(a.dinvT), f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
 #pragma unroll
-        for (int b = 0; b < NR / kQ; ++b) {
-            const int j = q + kQ * b;
-            if (j < a.nrhs) out[b] += ldv_cg<T, C>(HP, h * kPartialStride + j * kTile + r);
-        }
-    }
+    for (int b = 0; b < NR / kQ; ++b) out[b] += hsum[b];
+    // z_c = op(L_cc^{-1})^T (y_c - sum); every reader of sx passed the
+    // barrier in reduce_slices
+    Xv* st = sx;
+#pragma unroll
+    for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = yv[b] - out[b];
+    __syncthreads();
+    Xv acc2[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) acc2[j] = Xv{};
+    slice_mac<CJ, NR>(acc2, pre, st, q);
+    Xv z[NR / kQ];
+    reduce_slices<NR>(acc2, red, z, r, q);
     T* Part = reinterpret_cast<T*>(a.partial);
 #pragma unroll
     for (int b = 0; b < NR / kQ; ++b) {
         const int j = q + kQ * b;
-        if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r, out[b]);
+        if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r, z[b]);
     }
     publish_flag(&a.pflags[f.flag_base + c], a.epoch);
+}
+
+template <class T, bool C, bool CJ, int NR>
+__global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) bwd_sweep_kernel(SweepArgs a) {
+    using Xv = V<T, C>;
+    constexpr int ldl = kTile + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
+    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
+    Xv* sL = red + kQ * NR * kTile;               // [64 columns][65]
+    int32_t* sidx = reinterpret_cast<int32_t*>(sL + kTile * ldl);   // gather indices, kLowerChunkTiles x 64
+    __shared__ int s_item;
+    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
+    __syncthreads();
+    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
+    const int4 it = a.items[s_item];
+    const FrontDev f = a.F[it.x];
+    const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
+    const int nT = (f.n + kTile - 1) / kTile;
+    if (it.y == kItemChain) bwd_chain<T, C, CJ, NR>(a, f, it.x, nT, r, q, sx, red);
+    else if (it.y == kItemWhole) bwd_whole<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sL);
+    else bwd_worker<T, C, CJ, NR>(a, f, it.x, nT, it.y, it.z, it.w, r, q, sx, red, sL, sidx);
 }
 
 // ---------------------------------------------------------------------------
@@ -819,7 +910,7 @@ template <class T, bool C, bool CJ, int NR>
 static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     using Xv = V<T, C>;
     const size_t smem_fwd = sizeof(Xv) * (4 + kQ) * kTile * NR;
-    const size_t smem_bwd = smem_fwd + sizeof(Xv) * kTile * (kTile + 1);
+    const size_t smem_bwd = sizeof(Xv) * ((2 + kQ) * kTile * NR + kTile * (kTile + 1)) + sizeof(int32_t) * kLowerChunkTiles * kTile;
     static bool attr_done = false;
     if (!attr_done) {
         cudaFuncSetAttribute(fwd_sweep_kernel<T, C, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fwd);
@@ -829,13 +920,13 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     const int4* items = reinterpret_cast<const int4*>(P.items);
     SweepArgs a{};
     a.F = P.fronts;
-    a.xflags = P.flags;
+    a.xprog = P.xprog;
     a.pflags = P.flags + P.flags_total;
     a.L = P.L;
     a.dinv = P.dinv;
     a.dinvT = P.dinvT;
-    a.subT = P.subT;
-    a.subT2 = P.subT2;
+    a.m1 = P.m1;
+    a.n1 = P.n1;
     a.partial = P.partial;
     a.hpart = P.hpart;
     a.hflags = P.flags + 2 * P.flags_total;

@@ -89,8 +89,7 @@ __device__ __forceinline__ float row_scale(float mx, float* inv) {
 template <bool C>
 __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
                                                                     int k, float* __restrict__ L, const double* __restrict__ D,
-                                                                    const float* __restrict__ tinv, float* __restrict__ subT,
-                                                                    float* __restrict__ subT2, uint32_t* __restrict__ eblk,
+                                                                    const float* __restrict__ tinv, uint32_t* __restrict__ eblk,
                                                                     uint32_t* __restrict__ erow, int64_t eblk_total,
                                                                     int64_t erow_total, int32_t* __restrict__ status) {
     using X = V<float, C>;
@@ -215,14 +214,6 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
             const float ia = inv_a[i];
             const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
             const int nT = (f.n + nb - 1) / nb;
-            // tile 0 of a full block covers the pivot rows of the tiles
-            // (b+1, b) (rows 0-63) and (b+2, b) (rows 64-127): their row-major
-            // copies, zero outside the pivot rows
-            const int prow = r0 + i;
-            const bool pin = prow < f.n && vr;
-            X* S = nullptr;
-            if (tile == 0 && kb == nb)
-                S = reinterpret_cast<X*>(i < nb ? subT : subT2) + f.dinv + (int64_t)(k / nb) * nb * nb + (int64_t)(i % nb) * nb;
             float ml = 0.f, ms = 0.f;
 #pragma unroll 1
             for (int c0 = 0; c0 < nb; c0 += 16) {
@@ -241,7 +232,6 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
                         ml = fmaxf(ml, cmax(v));
                         ms = fmaxf(ms, cmax(v * s_d[c]));
                     }
-                    if (S) S[c] = pin ? v : X{};
                 }
             }
             if (eblk && vr) {
@@ -273,14 +263,12 @@ int launch_panel_tc(Plan& P, const Launch& ln) {
         const size_t smem = tc2::panel_tc_smem<true>();
         if (!attr[1]) { cudaFuncSetAttribute(tc2::panel_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[1] = true; }
         tc2::panel_tc_kernel<true><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, P.stream>>>(
-            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), reinterpret_cast<float*>(P.subT),
-            reinterpret_cast<float*>(P.subT2), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
+            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
     } else {
         const size_t smem = tc2::panel_tc_smem<false>();
         if (!attr[0]) { cudaFuncSetAttribute(tc2::panel_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[0] = true; }
         tc2::panel_tc_kernel<false><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, P.stream>>>(
-            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), reinterpret_cast<float*>(P.subT),
-            reinterpret_cast<float*>(P.subT2), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
+            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
     }
     return CLIQ_OK;
 }
