@@ -368,7 +368,10 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
 
 // Forward sweep of a small front (at most two pivot blocks, kWholeLowerRows
 // rows below) by one CTA: both blocks, then every 64-row tile below the
-// pivots, with the solved blocks kept in shared memory (no flags).
+// pivots, with the solved blocks kept in shared memory (no flags).  The
+// right-hand sides, the first inverse and the coupling tile are loaded up
+// front; below the pivots the (tile, block) products stream with the next
+// L tile and the tile's W_B entries in flight.
 template <class T, bool C, int NR>
 __device__ void fwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sq) {
     using Xv = V<T, C>;
@@ -377,30 +380,24 @@ __device__ void fwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, 
     T* X = reinterpret_cast<T*>(a.X);
     Xv* st = sx;                     // right-hand side of the diagonal block
     Xv* xb = sq;                     // x_0, x_1
-    for (int s = 0; s < nT; ++s) {
-        const int r0 = s * kTile, ds = min(kTile, f.n - r0);
-        Xv tv[NR / kQ];
+    Xv bv[2][NR / kQ];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const int ds = min(kTile, f.n - s * kTile);
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            tv[b] = (r < ds && j < a.nrhs) ? ldv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx) : Xv{};
+            bv[s][b] = (s < nT && r < ds && j < a.nrhs) ? ldv<T, C>(X, f.off + s * kTile + r + (int64_t)j * a.ldx) : Xv{};
         }
-        Xv dv[kE];
-        row_slice<T, C>(dv, Dinv, f.dinv + (int64_t)s * kTile * kTile, kTile, r, q, kTile, kTile);
-        if (s == 1) {
-            Xv lp[kE];
-            row_slice<T, C>(lp, L, f.L + kTile, f.m, r, q, ds, kTile);   // L_{1,0}
-            Xv acc[NR];
+    }
+    Xv la[kE], lb[kE];
+    row_slice<T, C>(la, Dinv, f.dinv, kTile, r, q, kTile, kTile);
+    if (nT > 1) row_slice<T, C>(lb, L, f.L + kTile, f.m, r, q, f.n - kTile, kTile);   // L_{1,0}
+    // x_s = L_ss^{-1} t, t in st; result to X and xb[s]
+    auto solve_block = [&](int s, const Xv (&dv)[kE], const Xv (&t)[NR / kQ]) {
+        const int ds = min(kTile, f.n - s * kTile);
 #pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<false, NR>(acc, lp, xb, q);
-            Xv u[NR / kQ];
-            reduce_slices<NR>(acc, red, u, r, q);
-#pragma unroll
-            for (int b = 0; b < NR / kQ; ++b) tv[b] -= u[b];
-        }
-#pragma unroll
-        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = tv[b];
+        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = t[b];
         __syncthreads();
         Xv acc[NR];
 #pragma unroll
@@ -412,39 +409,71 @@ __device__ void fwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, 
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
             const bool in = r < ds && j < a.nrhs;
-            if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, xs[b]);
+            if (in) stv<T, C>(X, f.off + s * kTile + r + (int64_t)j * a.ldx, xs[b]);
             xb[s * kTile * NR + r * NR + j] = in ? xs[b] : Xv{};
         }
         __syncthreads();
-    }
-    // rows below the pivots: W_B -= L_B x_T
-    T* wb = reinterpret_cast<T*>(f.pool == 0 ? a.w0 : a.w1);
-    for (int R0 = f.n; R0 < f.m; R0 += kTile) {
-        const int nr = min(kTile, f.m - R0);
+    };
+    solve_block(0, la, bv[0]);
+    if (nT > 1) {
+        row_slice<T, C>(la, Dinv, f.dinv + (int64_t)kTile * kTile, kTile, r, q, kTile, kTile);
         Xv acc[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-        for (int t = 0; t < nT; ++t) {
-            Xv lt[kE];
-            row_slice<T, C>(lt, L, f.L + R0 + (int64_t)t * kTile * f.m, f.m, r, q, nr, min(kTile, f.n - t * kTile));
-            slice_mac<false, NR>(acc, lt, xb + t * kTile * NR, q);
+        slice_mac<false, NR>(acc, lb, xb, q);
+        Xv u[NR / kQ];
+        reduce_slices<NR>(acc, red, u, r, q);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) bv[1][b] -= u[b];
+        solve_block(1, la, bv[1]);
+    }
+    // rows below the pivots: W_B -= L_B x_T, unit u = (tile u / nT, block u % nT)
+    const int ntl = (f.m - f.n + kTile - 1) / kTile;
+    const int units = ntl * nT;
+    if (units == 0) return;
+    T* wb = reinterpret_cast<T*>(f.pool == 0 ? a.w0 : a.w1);
+    auto load_unit = [&](int u, Xv (&dst)[kE]) {
+        const int i = u / nT, t = u % nT, R0 = f.n + kTile * i;
+        row_slice<T, C>(dst, L, f.L + R0 + (int64_t)t * kTile * f.m, f.m, r, q, min(kTile, f.m - R0), min(kTile, f.n - t * kTile));
+    };
+    Xv acc[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+    Xv wv[NR / kQ];
+    auto load_w = [&](int i) {
+        const int R0 = f.n + kTile * i, nr = min(kTile, f.m - R0);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            wv[b] = (r < nr && j < a.nrhs) ? ldv<T, C>(wb, f.W * a.nrhs + (R0 - f.n + r) + (int64_t)j * f.u) : Xv{};
         }
-        Xv out[NR / kQ];
-        reduce_slices<NR>(acc, red, out, r, q);
-        if (r < nr) {
+    };
+    auto unit = [&](int u, const Xv (&cur)[kE], Xv (&oth)[kE]) {
+        const int i = u / nT, t = u % nT;
+        if (u + 1 < units) load_unit(u + 1, oth);
+        slice_mac<false, NR>(acc, cur, xb + t * kTile * NR, q);
+        if (t == nT - 1) {
+            Xv out[NR / kQ];
+            reduce_slices<NR>(acc, red, out, r, q);
+            const int R0 = f.n + kTile * i, nr = min(kTile, f.m - R0);
 #pragma unroll
             for (int b = 0; b < NR / kQ; ++b) {
                 const int j = q + kQ * b;
-                if (j < a.nrhs) {
-                    const int64_t e = f.W * a.nrhs + (R0 - f.n + r) + (int64_t)j * f.u;
-                    stv<T, C>(wb, e, ldv<T, C>(wb, e) - out[b]);
-                }
+                if (r < nr && j < a.nrhs) stv<T, C>(wb, f.W * a.nrhs + (R0 - f.n + r) + (int64_t)j * f.u, wv[b] - out[b]);
             }
+            if (i + 1 < ntl) load_w(i + 1);
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            __syncthreads();   // red is read before the next tile's reduction writes it
         }
-        __syncthreads();
+    };
+    load_w(0);
+    load_unit(0, la);
+    for (int u = 0; u < units; u += 2) {
+        unit(u, la, lb);
+        if (u + 1 < units) unit(u + 1, lb, la);
     }
 }
-
 
 // Forward worker: rows [R0, R0 + nr) of the front against the pivot blocks
 // t < t_end.  Pivot-row worker of block s (t_end = s - 1):
@@ -644,62 +673,79 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
 }
 
 // Backward sweep of a small front by one CTA: for each pivot block, last
-// first, the contributions of the rows below the pivots (x gathered at
-// lowerStruct) and of the later pivot block (x from this CTA's own stores),
-// tiles staged through shared memory for the transposed product, then the
-// transposed inverse.
+// first, the transposed products with the later pivot block (x kept in
+// shared memory) and with the rows below the pivots (x gathered at
+// lowerStruct), then the transposed inverse.  The tiles of both blocks form
+// one stream: the next tile's L and gathered x are in flight during the
+// current one, staged through shared memory for the transposed product.
+static_assert(kWholeLowerRows <= kLowerChunkTiles * kTile, "gather indices of a small front fit the index buffer");
+
 template <class T, bool C, bool CJ, int NR>
-__device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sL) {
+__device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, int q, V<T, C>* sx, V<T, C>* red, V<T, C>* sL,
+                          int32_t* sidx) {
     using Xv = V<T, C>;
+    using XS = XStage<NR>;
     constexpr int ldl = kTile + 1;
     const T* L = reinterpret_cast<const T*>(a.L);
     const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
     T* X = reinterpret_cast<T*>(a.X);
-    Xv* st = sx;
-    Xv* xs = sx + kTile * NR;        // x of one tile
-    for (int c = nT - 1; c >= 0; --c) {
-        const int c0 = c * kTile, dc = min(kTile, f.n - c0);
-        Xv acc[NR];
+    Xv* st = sx;                     // right-hand side of the diagonal block
+    Xv* xg = sx + kTile * NR;        // gathered x of one tile below the pivots
+    Xv* xk = sx + 2 * kTile * NR;    // x of the later pivot block
+    const int nlr = f.m - f.n, nl = (nlr + kTile - 1) / kTile;
+    for (int i = threadIdx.x; i < nlr; i += kSolveThreads) sidx[i] = a.lower[f.lower + i];
+    // y of both blocks, read before this CTA overwrites them
+    Xv yv[2][NR / kQ];
 #pragma unroll
-        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-        // row tiles: the later pivot block (c + 1 < nT), then the rows below the pivots
-        const int R1 = c + 1 < nT ? c0 + kTile : f.n;
-        for (int R0 = R1; R0 < f.m; R0 = R0 < f.n ? f.n : R0 + kTile) {
-            const bool pivrows = R0 < f.n;
-            const int nr = pivrows ? min(kTile, f.n - R0) : min(kTile, f.m - R0);
-            Xv pre[kE];
-#pragma unroll
-            for (int p = 0; p < kE; ++p) {
-                const int cc = q + kQ * p;
-                pre[p] = (r < nr && cc < dc) ? ldv<T, C>(L, f.L + R0 + r + (int64_t)(c0 + cc) * f.m) : Xv{};
-            }
-            __syncthreads();   // previous readers of sL / xs are done; this CTA's x stores are visible
-#pragma unroll
-            for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
-            for (int idx = threadIdx.x; idx < kTile * NR; idx += kSolveThreads) {
-                const int rr = idx % kTile, j = idx / kTile;
-                Xv v{};
-                if (rr < nr && j < a.nrhs)
-                    v = pivrows ? ldv<T, C>(X, f.off + R0 + rr + (int64_t)j * a.ldx)
-                                : ldv<T, C>(X, (int64_t)a.lower[f.lower + R0 - f.n + rr] + (int64_t)j * a.ldx);
-                xs[rr * NR + j] = v;
-            }
-            __syncthreads();
-            Xv v[kE];
-#pragma unroll
-            for (int k = 0; k < kE; ++k) v[k] = sL[r * ldl + q * kE + k];
-            slice_mac<CJ, NR>(acc, v, xs, q);
-        }
-        Xv u[NR / kQ];
-        reduce_slices<NR>(acc, red, u, r, q);
+    for (int s = 0; s < 2; ++s) {
+        const int ds = min(kTile, f.n - s * kTile);
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            st[r * NR + j] = (r < dc && j < a.nrhs) ? ldv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx) - u[b] : Xv{};
+            yv[s][b] = (s < nT && r < ds && j < a.nrhs) ? ldv<T, C>(X, f.off + s * kTile + r + (int64_t)j * a.ldx) : Xv{};
         }
-        __syncthreads();
+    }
+    // units: block nT-1 has its nl lower tiles; block nT-2 (if any) the
+    // pivot tile of block nT-1, then its nl lower tiles
+    const int total = nl + (nT > 1 ? 1 + nl : 0);
+    auto unit = [&](int u, int& c, int& R0, int& nr, bool& piv) {
+        if (u < nl) { c = nT - 1; piv = false; R0 = f.n + kTile * u; }
+        else { c = nT - 2; const int k = u - nl; piv = k == 0; R0 = piv ? (c + 1) * kTile : f.n + kTile * (k - 1); }
+        nr = min(kTile, (piv ? f.n : f.m) - R0);
+    };
+    Xv pre[kE];
+    Xv xr[XS::kN];
+    auto fetch = [&](int u) {
+        int c, R0, nr;
+        bool piv;
+        unit(u, c, R0, nr, piv);
+        const int c0 = c * kTile, dc = min(kTile, f.n - c0);
+#pragma unroll
+        for (int p = 0; p < kE; ++p) {
+            const int cc = q + kQ * p;
+            pre[p] = (r < nr && cc < dc) ? ldv<T, C>(L, f.L + R0 + r + (int64_t)(c0 + cc) * f.m) : Xv{};
+        }
+        if (!piv) {
+#pragma unroll
+            for (int e = 0; e < XS::kN; ++e) {
+                const int rr = XS::row(e), j = XS::rhs(e);
+                xr[e] = (rr < nr && j < a.nrhs) ? ldv<T, C>(X, (int64_t)sidx[R0 - f.n + rr] + (int64_t)j * a.ldx) : Xv{};
+            }
+        }
+    };
+    Xv acc[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+    // x_c = op(L_cc^{-1})^T (y_c - acc): to X and xk
+    auto finish = [&](int c) {
+        const int dc = min(kTile, f.n - c * kTile);
         Xv dv[kE];
         row_slice<T, C>(dv, DinvT, f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
+        Xv u[NR / kQ];
+        reduce_slices<NR>(acc, red, u, r, q);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = (c == 1 ? yv[1][b] : yv[0][b]) - u[b];
+        __syncthreads();
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = Xv{};
         slice_mac<CJ, NR>(acc, dv, st, q);
@@ -708,9 +754,35 @@ __device__ void bwd_whole(const SweepArgs& a, const FrontDev& f, int nT, int r, 
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
-            if (r < dc && j < a.nrhs) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xv[b]);
+            const bool in = r < dc && j < a.nrhs;
+            if (in) stv<T, C>(X, f.off + c * kTile + r + (int64_t)j * a.ldx, xv[b]);
+            xk[r * NR + j] = in ? xv[b] : Xv{};
         }
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
         __syncthreads();
+    };
+    __syncthreads();   // gather indices
+    if (total > 0) fetch(0);
+    if (nl == 0) finish(nT - 1);
+    for (int u = 0; u < total; ++u) {
+        int c, R0, nr;
+        bool piv;
+        unit(u, c, R0, nr, piv);
+        __syncthreads();   // the previous tile's readers are done with sL and xg
+#pragma unroll
+        for (int p = 0; p < kE; ++p) sL[(q + kQ * p) * ldl + r] = pre[p];
+        if (!piv) put_x<NR>(xr, xg);
+        if (u + 1 < total) fetch(u + 1);
+        __syncthreads();
+        Xv v[kE];
+#pragma unroll
+        for (int k = 0; k < kE; ++k) v[k] = sL[r * ldl + q * kE + k];
+        slice_mac<CJ, NR>(acc, v, piv ? xk : xg, q);
+        int cn = -1, R0n, nrn;
+        bool pn;
+        if (u + 1 < total) unit(u + 1, cn, R0n, nrn, pn);
+        if (cn != c) finish(c);
     }
 }
 
@@ -886,8 +958,8 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) b
     using Xv = V<T, C>;
     constexpr int ldl = kTile + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
-    Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
+    Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 3 x [64][NR]
+    Xv* red = sx + 3 * kTile * NR;                // [kQ][NR][64]
     Xv* sL = red + kQ * NR * kTile;               // [64 columns][65]
     int32_t* sidx = reinterpret_cast<int32_t*>(sL + kTile * ldl);   // gather indices, kLowerChunkTiles x 64
     __shared__ int s_item;
@@ -899,7 +971,7 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) b
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
     const int nT = (f.n + kTile - 1) / kTile;
     if (it.y == kItemChain) bwd_chain<T, C, CJ, NR>(a, f, it.x, nT, r, q, sx, red);
-    else if (it.y == kItemWhole) bwd_whole<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sL);
+    else if (it.y == kItemWhole) bwd_whole<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sL, sidx);
     else bwd_worker<T, C, CJ, NR>(a, f, it.x, nT, it.y, it.z, it.w, r, q, sx, red, sL, sidx);
 }
 
@@ -910,7 +982,7 @@ template <class T, bool C, bool CJ, int NR>
 static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     using Xv = V<T, C>;
     const size_t smem_fwd = sizeof(Xv) * (4 + kQ) * kTile * NR;
-    const size_t smem_bwd = sizeof(Xv) * ((2 + kQ) * kTile * NR + kTile * (kTile + 1)) + sizeof(int32_t) * kLowerChunkTiles * kTile;
+    const size_t smem_bwd = sizeof(Xv) * ((3 + kQ) * kTile * NR + kTile * (kTile + 1)) + sizeof(int32_t) * kLowerChunkTiles * kTile;
     static bool attr_done = false;
     if (!attr_done) {
         cudaFuncSetAttribute(fwd_sweep_kernel<T, C, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fwd);
