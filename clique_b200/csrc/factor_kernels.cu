@@ -45,9 +45,13 @@ __device__ __forceinline__ float cabsmax(cx<double> v) { return (float)fmax(fabs
 // 1. extend-add (gather form)
 //
 // Work item (front, j0, i0): columns j0 .. j0+15, rows i0 .. i0+kEARows-1 on
-// or below the diagonal; the CTA sweeps each column down a contiguous run of
-// rows (consecutive threads, consecutive rows).
+// or below the diagonal; the CTA sweeps one column at a time down a
+// contiguous run of rows (consecutive threads, consecutive rows: few DRAM
+// pages open per CTA), each thread taking kEAUnroll rows per pass with all
+// their loads issued before any store.
 // ---------------------------------------------------------------------------
+constexpr int kEAUnroll = 4;
+
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
                                                               T* __restrict__ L, T* __restrict__ pool0, T* __restrict__ pool1,
@@ -66,21 +70,30 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
         if (j >= f.m) break;
         const int lj = lm ? lm[j] : -1, rj = rm ? rm[j] : -1;
         if (j < f.n && lj < 0 && rj < 0) continue;
-        for (int i = max(j, it.z) + threadIdx.x; i < i_end; i += blockDim.x) {
-            X v = X{};
-            if (lj >= 0) {
-                const int li = lm[i];
-                if (li >= 0) v += ldv<T, C>(cp, f.CU[0] + li + (int64_t)lj * f.cu[0]);
+        for (int ib = max(j, it.z) + threadIdx.x; ib < i_end; ib += kEAUnroll * blockDim.x) {
+            int li[kEAUnroll], ri[kEAUnroll];
+#pragma unroll
+            for (int u = 0; u < kEAUnroll; ++u) {
+                const int i = ib + u * blockDim.x;
+                li[u] = (lj >= 0 && i < i_end) ? lm[i] : -1;
+                ri[u] = (rj >= 0 && i < i_end) ? rm[i] : -1;
             }
-            if (rj >= 0) {
-                const int ri = rm[i];
-                if (ri >= 0) v += ldv<T, C>(cp, f.CU[1] + ri + (int64_t)rj * f.cu[1]);
+            X v[kEAUnroll], o[kEAUnroll];
+#pragma unroll
+            for (int u = 0; u < kEAUnroll; ++u) {
+                const int i = ib + u * blockDim.x;
+                X t = X{};
+                if (li[u] >= 0) t += ldv<T, C>(cp, f.CU[0] + li[u] + (int64_t)lj * f.cu[0]);
+                if (ri[u] >= 0) t += ldv<T, C>(cp, f.CU[1] + ri[u] + (int64_t)rj * f.cu[1]);
+                v[u] = t;
+                o[u] = (j < f.n && i < i_end) ? ldv<T, C>(L, f.L + i + (int64_t)j * f.m) : X{};
             }
-            if (j < f.n) {
-                const int64_t e = f.L + i + (int64_t)j * f.m;
-                stv<T, C>(L, e, ldv<T, C>(L, e) + v);
-            } else {
-                stv<T, C>(up, f.U + (i - f.n) + (int64_t)(j - f.n) * f.u, v);
+#pragma unroll
+            for (int u = 0; u < kEAUnroll; ++u) {
+                const int i = ib + u * blockDim.x;
+                if (i >= i_end) break;
+                if (j < f.n) stv<T, C>(L, f.L + i + (int64_t)j * f.m, o[u] + v[u]);
+                else stv<T, C>(up, f.U + (i - f.n) + (int64_t)(j - f.n) * f.u, v[u]);
             }
         }
     }
