@@ -110,6 +110,9 @@ struct Launch {
     double work;          // GEMM: algorithmic flops; EXTEND_ADD: algorithmic bytes
     int32_t schur;        // GEMM: 1 for the Schur-complement update, 0 for an in-panel update
     int32_t simt = 0;     // GEMM: CUDA-core kernel (64 x 64 tiles) even on the tensor path
+    // GEMM: lookahead part of an outer-block update (columns two outer blocks
+    // and more to the right), run on the second stream; k = the outer block
+    int32_t bulk = 0;
     // tensor-core path: operand packing for this GEMM
     int64_t pack_items = 0, pack_prefix = 0, pack_blocks = 0;
     int32_t pack_njobs = 0;
@@ -192,7 +195,15 @@ struct Plan {
     GemmProb* probs = nullptr;
     PackJob* packjobs = nullptr;
     void* pack = nullptr;         // packed tensor-core operands of one GEMM launch
+    void* pack2 = nullptr;        // the same for the lookahead launches (second stream)
     int64_t pack_floats = 0;
+    // lookahead (CLIQGPU_LOOKAHEAD=0: off): the outer-block updates of the
+    // columns two outer blocks and more to the right run on stream2 while
+    // the next outer block is factored on stream
+    int lookahead = 1;
+    cudaStream_t stream1 = nullptr;   // internal, highest priority: the factorization's critical path
+    cudaStream_t stream2 = nullptr;   // internal, lowest priority: lookahead updates
+    std::vector<cudaEvent_t> sync_events;   // fork / lookahead-done events, one pair per lookahead launch
     int64_t* prefix = nullptr;
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
@@ -260,10 +271,11 @@ int launch_multi_axpy(Plan& P, const double* V, int64_t vstride, int nv, const d
 int launch_col_scale(Plan& P, const double* w, double* v, int nrhs, const double* s);
 
 int check_cuda(const char* where);
-// packs the launch's operands, records `between` (if given), runs the GEMM
-int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between);
+// packs the launch's operands into `pack`, records `between` (if given),
+// runs the GEMM, all on stream st
+int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack);
 size_t tc2_smem(bool cplx);
-int launch_panel_tc(Plan& P, const Launch& ln);
+int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);
 void free_plan(Plan& P);

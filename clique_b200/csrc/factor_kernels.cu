@@ -622,8 +622,8 @@ __global__ void __launch_bounds__(kThreads) gemm_update_kernel(const GemmProb* _
 // FP32 storage FP32 unless the plan asks for FP64 (CLIQGPU_DIAG_FP64=1).
 // The pivots are stored in FP64 either way.
 template <class T, bool C, bool CJ, class WT>
-static void launch_diag(const Plan& P, const Launch& ln, T* L, const int4* items) {
-    diag_ldl_kernel<T, C, CJ, WT><<<(unsigned)ln.nblocks, kThreads, diag_smem_bytes<WT, C>(), P.stream>>>(
+static void launch_diag(const Plan& P, const Launch& ln, T* L, const int4* items, cudaStream_t st) {
+    diag_ldl_kernel<T, C, CJ, WT><<<(unsigned)ln.nblocks, kThreads, diag_smem_bytes<WT, C>(), st>>>(
         P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<T*>(P.tinv), reinterpret_cast<T*>(P.dinv),
         reinterpret_cast<T*>(P.dinvT), P.status);
 }
@@ -652,39 +652,84 @@ static int run_factor_impl(Plan& P) {
         P.events.resize(3 * P.launches.size());
         for (size_t i = old; i < P.events.size(); ++i) cudaEventCreate(&P.events[i]);
     }
-    if (P.erow) cudaMemsetAsync(P.erow, 0, sizeof(uint32_t) * 2 * (size_t)P.erow_total, P.stream);
+    // Lookahead: the critical path (extend-add, diagonal blocks, panels,
+    // in-panel and next-outer-block updates) on the high-priority stream1,
+    // the updates of the columns two outer blocks and more to the right on
+    // stream2.  Before the first diagonal block of outer block K the main
+    // stream waits for the lookahead update of outer block K - 2 nbo (the
+    // last one that writes columns of K); it joins stream2 completely before
+    // each extend-add, each Schur update and the chain tiles.
+    const bool la = P.stream2 != nullptr;
+    cudaStream_t s1 = la ? P.stream1 : P.stream;
+    const int nbo = std::max(P.nb, P.outer_nb / P.nb * P.nb);
+    size_t next_ev = 0;
+    cudaEvent_t last_done = nullptr;
+    struct Pending { int depth, k0; cudaEvent_t done; };
+    std::vector<Pending> pending;
+    if (la) {
+        cudaEvent_t fork = P.sync_events[next_ev++];
+        cudaEventRecord(fork, P.stream);
+        cudaStreamWaitEvent(s1, fork, 0);
+        cudaStreamWaitEvent(P.stream2, fork, 0);
+    }
+    auto join = [&]() {
+        if (last_done) cudaStreamWaitEvent(s1, last_done, 0);
+        last_done = nullptr;
+        pending.clear();
+    };
+    if (P.erow) cudaMemsetAsync(P.erow, 0, sizeof(uint32_t) * 2 * (size_t)P.erow_total, s1);
     for (size_t li = 0; li < P.launches.size(); ++li) {
         const Launch& ln = P.launches[li];
         if (ln.nblocks <= 0) continue;
-        if (P.profile) cudaEventRecord(P.events[3 * li], P.stream);
+        if (la) {
+            if (ln.kind == Launch::EXTEND_ADD || (ln.kind == Launch::GEMM && ln.schur)) join();
+            if (ln.kind == Launch::DIAG && ln.k % nbo == 0 && ln.k >= 2 * nbo)
+                for (const Pending& pd : pending)
+                    if (pd.depth == ln.depth && pd.k0 == ln.k - 2 * nbo) cudaStreamWaitEvent(s1, pd.done, 0);
+        }
+        const bool on2 = la && ln.bulk;
+        cudaStream_t st = on2 ? P.stream2 : s1;
+        if (on2) {   // the lookahead update reads panels produced on stream1 so far
+            cudaEvent_t fork = P.sync_events[next_ev++];
+            cudaEventRecord(fork, s1);
+            cudaStreamWaitEvent(P.stream2, fork, 0);
+        }
+        if (P.profile) cudaEventRecord(P.events[3 * li], st);
         switch (ln.kind) {
             case Launch::EXTEND_ADD:
-                extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
+                extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
                 break;
             case Launch::DIAG:
-                if (std::is_same<T, float>::value && !P.diag_fp64) launch_diag<T, C, CJ, T>(P, ln, L, items);
-                else launch_diag<T, C, CJ, double>(P, ln, L, items);
+                if (std::is_same<T, float>::value && !P.diag_fp64) launch_diag<T, C, CJ, T>(P, ln, L, items, st);
+                else launch_diag<T, C, CJ, double>(P, ln, L, items, st);
                 break;
             case Launch::PANEL:
                 if (std::is_same<T, float>::value && P.f16_scales()) {
-                    launch_panel_tc(P, ln);
+                    launch_panel_tc(P, ln, st);
                     break;
                 }
-                panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, P.stream>>>(
+                panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, st>>>(
                     P.fronts, items + ln.items, ln.k, L, P.D, reinterpret_cast<const T*>(P.tinv), P.eblk, P.erow, P.eblk_total,
                     P.erow_total);
                 break;
             case Launch::GEMM:
                 if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
-                    launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr);
+                    launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr, st, on2 ? P.pack2 : P.pack);
                 else
-                    gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, P.stream>>>(
+                    gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(
                         P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
                 break;
         }
-        if (P.profile) cudaEventRecord(P.events[3 * li + 1], P.stream);
+        if (P.profile) cudaEventRecord(P.events[3 * li + 1], st);
+        if (on2) {
+            cudaEvent_t done = P.sync_events[next_ev++];
+            cudaEventRecord(done, P.stream2);
+            pending.push_back({ln.depth, ln.k, done});
+            last_done = done;
+        }
         ++launches;
     }
+    if (la) join();
     if (P.nchain_items > 0) {
         static bool ct_attr = false;
         if (!ct_attr) {
@@ -692,10 +737,15 @@ static int run_factor_impl(Plan& P) {
                                  (int)chain_tiles_smem_bytes<T, C>());
             ct_attr = true;
         }
-        chain_tiles_kernel<T, C, CJ><<<(unsigned)P.nchain_items, kThreads, chain_tiles_smem_bytes<T, C>(), P.stream>>>(
+        chain_tiles_kernel<T, C, CJ><<<(unsigned)P.nchain_items, kThreads, chain_tiles_smem_bytes<T, C>(), s1>>>(
             P.fronts, reinterpret_cast<const int4*>(P.chain_items), L, reinterpret_cast<const T*>(P.dinv),
             reinterpret_cast<T*>(P.m1), reinterpret_cast<T*>(P.n1));
         ++launches;
+    }
+    if (la) {   // the caller's stream continues after the whole factorization
+        cudaEvent_t end = P.sync_events[next_ev++];
+        cudaEventRecord(end, s1);
+        cudaStreamWaitEvent(P.stream, end, 0);
     }
     P.prof_pending = P.profile != 0;
     P.last_launches = launches;

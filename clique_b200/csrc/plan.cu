@@ -78,12 +78,16 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
-                    P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0],
+                    P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
                     P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : P.events) cudaEventDestroy(e);
     P.events.clear();
+    for (cudaEvent_t e : P.sync_events) cudaEventDestroy(e);
+    P.sync_events.clear();
+    if (P.stream1) cudaStreamDestroy(P.stream1);
+    if (P.stream2) cudaStreamDestroy(P.stream2);
     if (P.own_stream && P.stream) cudaStreamDestroy(P.stream);
 }
 
@@ -227,6 +231,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     const int planes = P.cplx() ? 4 : 2;
     const int64_t blkA = (int64_t)planes * kTcBM * 8, blkB = (int64_t)planes * kTcBN * 8;   // floats per packed block
     int64_t pack_max = 1;
+    int nbulk = 0;   // lookahead launches
     auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur, bool inpanel) {
         if (lst.empty()) return;
         Launch ln{};
@@ -381,29 +386,47 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 if (pn.nitems) P.launches.push_back(pn);
                 add_gemm(trail, d, 0, true);
             }
-            std::vector<GemmProb> outer;
+            // the outer block's update of the columns to its right: with
+            // lookahead, the next outer block's columns [c1, c2) on the main
+            // stream and the columns from c2 on the second stream (tensor
+            // path: the GEMM epilogue adds atomically, so both may overlap
+            // other updates of the same columns)
+            const bool la = tcp && P.lookahead;
+            std::vector<GemmProb> outer, bulk;
             for (int s : lv) {
                 const FrontDev& f = P.hfronts[s];
                 const int c1 = K0 + nbo;
                 if (f.n <= c1) continue;
-                GemmProb pr{};
-                pr.front = s;
-                pr.row0 = c1;
-                pr.kb0 = K0 / kTile;
-                pr.nkb = nbo / kTile;
-                pr.A = f.L + c1 + (int64_t)K0 * f.m;
-                pr.B = pr.A;
-                pr.C = f.L + c1 + (int64_t)c1 * f.m;
-                pr.d = f.off + K0;
-                pr.lda = f.m;
-                pr.ldc = f.m;
-                pr.M = f.m - c1;
-                pr.N = f.n - c1;
-                pr.K = nbo;
-                pr.cpool = -1;
-                outer.push_back(pr);
+                const int c2 = la ? std::min(f.n, c1 + nbo) : f.n;
+                for (int part = 0; part < 2; ++part) {
+                    const int r0 = part == 0 ? c1 : c2;
+                    const int N = part == 0 ? c2 - c1 : f.n - c2;
+                    if (N <= 0) continue;
+                    GemmProb pr{};
+                    pr.front = s;
+                    pr.row0 = r0;
+                    pr.kb0 = K0 / kTile;
+                    pr.nkb = nbo / kTile;
+                    pr.A = f.L + r0 + (int64_t)K0 * f.m;
+                    pr.B = pr.A;
+                    pr.C = f.L + r0 + (int64_t)r0 * f.m;
+                    pr.d = f.off + K0;
+                    pr.lda = f.m;
+                    pr.ldc = f.m;
+                    pr.M = f.m - r0;
+                    pr.N = N;
+                    pr.K = nbo;
+                    pr.cpool = -1;
+                    (part == 0 ? outer : bulk).push_back(pr);
+                }
             }
             add_gemm(outer, d, 0, false);
+            if (!bulk.empty()) {
+                add_gemm(bulk, d, 0, false);
+                P.launches.back().bulk = 1;
+                P.launches.back().k = K0;
+                ++nbulk;
+            }
         }
         std::vector<GemmProb> schur;
         for (int s : lv) {
@@ -560,6 +583,17 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.probs, probs));
     TRY(dev_upload(P, &P.packjobs, packjobs));
     if (P.pack_floats > 0) TRY(dev_alloc(P, &P.pack, (size_t)P.pack_floats * sizeof(float)));
+    if (nbulk > 0) {
+        TRY(dev_alloc(P, &P.pack2, (size_t)P.pack_floats * sizeof(float)));
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (cudaStreamCreateWithPriority(&P.stream1, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&P.stream2, cudaStreamNonBlocking, least) != cudaSuccess)
+            return check_cuda("lookahead streams");
+        P.sync_events.resize(2 * (size_t)nbulk + 4, nullptr);
+        for (cudaEvent_t& e : P.sync_events)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return check_cuda("lookahead events");
+    }
     TRY(dev_upload(P, &P.prefix, prefix));
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));
@@ -657,6 +691,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_SPLIT")) P.split_f16 = strcmp(e, "tf32") != 0;
     if (const char* e = getenv("CLIQGPU_INPANEL_TC")) P.inpanel_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_REFINE")) P.refine_gmres = strcmp(e, "ir") != 0;
+    if (const char* e = getenv("CLIQGPU_LOOKAHEAD")) P.lookahead = atoi(e) != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }

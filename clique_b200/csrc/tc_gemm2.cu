@@ -349,37 +349,40 @@ size_t tc2_smem(bool cplx) {
 
 // pack the launch's operands, then run the tensor-core GEMM
 template <bool C, bool CJ, bool F16>
-static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between) {
+static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack) {
     float* L = reinterpret_cast<float*>(P.L);
     float* p0 = reinterpret_cast<float*>(P.pool[0]);
     float* p1 = reinterpret_cast<float*>(P.pool[1]);
-    float* pk = reinterpret_cast<float*>(P.pack);
+    float* pk = reinterpret_cast<float*>(pack);
     const PackJob* jobs = P.packjobs + ln.pack_items;
     const int64_t* jpre = P.prefix + ln.pack_prefix;
     if (ln.pack_blocks <= 0) return;   // nothing to update
     if constexpr (F16)
-        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
+        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
                                                                                    pk);
     else
-        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, P.stream>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
-    if (between) cudaEventRecord(between, P.stream);
+        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+    if (between) cudaEventRecord(between, st);
     const size_t smem = tc2_smem(C);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(tc2::tc_gemm_kernel<C, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    tc2::tc_gemm_kernel<C, F16><<<(unsigned)ln.nblocks, tc2::kThreads, smem, P.stream>>>(
+    tc2::tc_gemm_kernel<C, F16><<<(unsigned)ln.nblocks, tc2::kThreads, smem, st>>>(
         P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
 }
 
-int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between) {
+int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack) {
     const bool f16 = P.split_f16 != 0;
     if (P.cplx()) {
-        if (P.conjugate) { if (f16) launch_pair<true, true, true>(P, ln, between); else launch_pair<true, true, false>(P, ln, between); }
-        else { if (f16) launch_pair<true, false, true>(P, ln, between); else launch_pair<true, false, false>(P, ln, between); }
+        if (P.conjugate) {
+            if (f16) launch_pair<true, true, true>(P, ln, between, st, pack); else launch_pair<true, true, false>(P, ln, between, st, pack);
+        } else {
+            if (f16) launch_pair<true, false, true>(P, ln, between, st, pack); else launch_pair<true, false, false>(P, ln, between, st, pack);
+        }
     } else {
-        if (f16) launch_pair<false, false, true>(P, ln, between); else launch_pair<false, false, false>(P, ln, between);
+        if (f16) launch_pair<false, false, true>(P, ln, between, st, pack); else launch_pair<false, false, false>(P, ln, between, st, pack);
     }
     P.total_launches += 1;   // the pack kernel (the caller counts the GEMM)
     return CLIQ_OK;

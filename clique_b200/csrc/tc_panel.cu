@@ -255,19 +255,19 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
 }  // namespace tc2
 
 // launch the tensor-core panel for one PANEL step of the schedule
-int launch_panel_tc(Plan& P, const Launch& ln) {
+int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st) {
     float* L = reinterpret_cast<float*>(P.L);
     const int4* items = reinterpret_cast<const int4*>(P.items) + ln.items;
     static bool attr[2] = {false, false};
     if (P.cplx()) {
         const size_t smem = tc2::panel_tc_smem<true>();
         if (!attr[1]) { cudaFuncSetAttribute(tc2::panel_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[1] = true; }
-        tc2::panel_tc_kernel<true><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, P.stream>>>(
+        tc2::panel_tc_kernel<true><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, st>>>(
             P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
     } else {
         const size_t smem = tc2::panel_tc_smem<false>();
         if (!attr[0]) { cudaFuncSetAttribute(tc2::panel_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[0] = true; }
-        tc2::panel_tc_kernel<false><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, P.stream>>>(
+        tc2::panel_tc_kernel<false><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, st>>>(
             P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
     }
     return CLIQ_OK;
