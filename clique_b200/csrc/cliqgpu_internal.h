@@ -97,6 +97,11 @@ struct PackJob {
     int64_t dst_scale;    // FP16 split: float offset of the R (padded to tiles) inverse row scales
     int64_t emax;         // FP16 split: row maxima of the job's first row (block kb0), in the eblk / erow arrays
     int32_t enT, nkb;     // row stride of eblk (blocks per row); blocks in K (0: use erow)
+    // FP16 split: the same job also writes S = D[dS + k] op(rows) for its
+    // first RS rows (the B operand, a prefix of the A rows) at dstS with
+    // inverse row scales at dst_scaleS, row maxima at emaxS (RS = 0: A only)
+    int64_t dstS, dst_scaleS, emaxS, dS;
+    int32_t RS;
 };
 
 struct Launch {

@@ -260,7 +260,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 const int64_t tA = (pr.M + kTcBM - 1) / kTcBM, tB = (pr.N + kTcBN - 1) / kTcBN;
                 const FrontDev& fr = P.hfronts[pr.front];
                 const int nT = (fr.n + kTile - 1) / kTile;
-                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, kTcBM, 0, 0, nT, pr.nkb};
+                PackJob a{pr.A, off, -1, pr.M, pr.K, pr.lda, kTcBM, 0, 0, nT, pr.nkb, 0, 0, 0, -1, 0};
                 a.emax = pr.nkb > 0 ? fr.eblk + (int64_t)pr.row0 * nT + pr.kb0 : fr.erow + pr.row0;
                 pr.packA = off;
                 off += tA * nk * blkA;
@@ -277,10 +277,22 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 off += tB * nk * blkB;
                 b.dst_scale = pr.scaleB = off;
                 if (f16) off += tB * kTcBN;
-                for (const PackJob& j : {a, b}) {
+                if (f16 && pr.B == pr.A && pr.N <= pr.M && kTcBN == kTcBM) {
+                    // one job: the B rows are the first N rows of A, read once
+                    a.dS = pr.d;
+                    a.dstS = b.dst;
+                    a.dst_scaleS = b.dst_scale;
+                    a.emaxS = b.emax;
+                    a.RS = pr.N;
                     prefix.push_back(blocks);
-                    blocks += (int64_t)((j.R + j.tile_rows - 1) / j.tile_rows) * nk;
-                    packjobs.push_back(j);
+                    blocks += (int64_t)((a.R + a.tile_rows - 1) / a.tile_rows) * nk;
+                    packjobs.push_back(a);
+                } else {
+                    for (const PackJob& j : {a, b}) {
+                        prefix.push_back(blocks);
+                        blocks += (int64_t)((j.R + j.tile_rows - 1) / j.tile_rows) * nk;
+                        packjobs.push_back(j);
+                    }
                 }
             }
             ln.pack_njobs = (int32_t)(packjobs.size() - ln.pack_items);

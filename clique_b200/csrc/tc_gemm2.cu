@@ -132,45 +132,31 @@ __device__ __forceinline__ V<float, C> pack_load(const PackJob& jb, const float*
 __device__ __forceinline__ float absmax(float v) { return fabsf(v); }
 __device__ __forceinline__ float absmax(cx<float> v) { return fmaxf(fabsf(v.r), fabsf(v.i)); }
 
-template <bool C, bool CJ>
-__global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
-                                                       const float* __restrict__ L, const double* __restrict__ D,
-                                                       const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
-                                                       float* __restrict__ out) {
-    using X = V<float, C>;
-    const int64_t bid = blockIdx.x;
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
-    }
-    const PackJob jb = jobs[lo];
-    const int64_t blk = bid - prefix[lo];
-    const int nks = (jb.K + kKS16 - 1) / kKS16;
-    const int tile = (int)(blk / nks), ks = (int)(blk % nks);
-    const int row = threadIdx.x;
-    if (row >= jb.tile_rows) return;
-    const int r = tile * jb.tile_rows + row;
-    X v[kKS16];
-#pragma unroll
-    for (int q = 0; q < kKS16; ++q) v[q] = pack_load<C, CJ>(jb, L, D, r, ks * kKS16 + q);
+// scale and split one row's 16 values of block blk into the FP16 planes at
+// float offset dst (inverse row scale at dst_scale + r when ks == 0); the
+// row maxima come from eblk (nkb blocks from emax) or erow
+template <bool C>
+__device__ __forceinline__ void pack_f16_planes(const PackJob& jb, const V<float, C> (&v)[kKS16], int64_t dst, int64_t dst_scale,
+                                                int64_t emax, int R, int64_t blk, int ks, int row, int r,
+                                                const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
+                                                float* __restrict__ out) {
     float mx = 0.f;
-    if (r < jb.R) {
+    if (r < R) {
         if (jb.nkb > 0) {
-            for (int b = 0; b < jb.nkb; ++b) mx = fmaxf(mx, __uint_as_float(eblk[jb.emax + (int64_t)r * jb.enT + b]));
+            for (int b = 0; b < jb.nkb; ++b) mx = fmaxf(mx, __uint_as_float(eblk[emax + (int64_t)r * jb.enT + b]));
         } else {
-            mx = __uint_as_float(erow[jb.emax + r]);
+            mx = __uint_as_float(erow[emax + r]);
         }
     }
     // s = 2^(14 - e) for mx in [2^e, 2^(e+1)): s * mx in [2^14, 2^15)
     int e = mx > 0.f ? ((__float_as_int(mx) >> 23) & 0xff) - 127 : 0;
     e = max(-100, min(100, e));
     const float s = __int_as_float((127 + 14 - e) << 23);
-    if (ks == 0) out[jb.dst_scale + r] = __int_as_float((127 - 14 + e) << 23);
+    if (ks == 0) out[dst_scale + r] = __int_as_float((127 - 14 + e) << 23);
     // planes (re_hi, re_lo, im_hi, im_lo) of this k step
     constexpr int planes = C ? 4 : 2;
     const int64_t plane_bytes = (int64_t)jb.tile_rows * kKS16 * 2;
-    uint8_t* base = reinterpret_cast<uint8_t*>(out + jb.dst) + blk * plane_bytes * planes;
+    uint8_t* base = reinterpret_cast<uint8_t*>(out + dst) + blk * plane_bytes * planes;
     float y[kKS16];
     uint4 h, l;
 #pragma unroll
@@ -192,6 +178,41 @@ __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restri
             *reinterpret_cast<uint4*>(base + 2 * plane_bytes + core_off(row, c)) = h;
             *reinterpret_cast<uint4*>(base + 3 * plane_bytes + core_off(row, c)) = l;
         }
+    }
+}
+
+template <bool C, bool CJ>
+__global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+                                                       const float* __restrict__ L, const double* __restrict__ D,
+                                                       const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
+                                                       float* __restrict__ out) {
+    using X = V<float, C>;
+    using W = DV<C>;
+    const int64_t bid = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const PackJob jb = jobs[lo];
+    const int64_t blk = bid - prefix[lo];
+    const int nks = (jb.K + kKS16 - 1) / kKS16;
+    const int tile = (int)(blk / nks), ks = (int)(blk % nks);
+    const int row = threadIdx.x;
+    if (row >= jb.tile_rows) return;
+    const int r = tile * jb.tile_rows + row;
+    X v[kKS16];
+#pragma unroll
+    for (int q = 0; q < kKS16; ++q) v[q] = pack_load<C, CJ>(jb, L, D, r, ks * kKS16 + q);
+    pack_f16_planes<C>(jb, v, jb.dst, jb.dst_scale, jb.emax, jb.R, blk, ks, row, r, eblk, erow, out);
+    // the S operand from the same rows (a prefix of this job's rows)
+    if (jb.RS > 0 && tile * jb.tile_rows < jb.RS) {
+#pragma unroll
+        for (int q = 0; q < kKS16; ++q) {
+            const int k = ks * kKS16 + q;
+            v[q] = (r < jb.RS && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.dS + k]) * opc<CJ>(v[q]) : X{};
+        }
+        pack_f16_planes<C>(jb, v, jb.dstS, jb.dst_scaleS, jb.emaxS, jb.RS, blk, ks, row, r, eblk, erow, out);
     }
 }
 
