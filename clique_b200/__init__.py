@@ -375,9 +375,11 @@ def Solve(info, L: DistSymmFrontTree, X):
     return _solve_array(L, X, nodal=False)
 
 
-def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20):
+def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20, X=None):
     """X = A^{-1} B by iterative refinement over the stored factors (FP64
-    residuals and updates).  Returns (X, iterations, relative residual)."""
+    residuals and updates).  Returns (X, iterations, relative residual).
+    For host right-hand sides an output array X (Fortran-ordered, B's shape
+    and dtype, e.g. a view of pinned memory) may be passed and is filled."""
     lib = _capi.load()
     it = C.c_int32()
     rr = C.c_double()
@@ -390,10 +392,15 @@ def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20):
                                 tol, max_iter, C.byref(it), C.byref(rr))
     else:
         B2 = np.asfortranarray(np.asarray(B).reshape(B.shape[0], -1), np.complex128 if L.is_complex else np.float64)
-        X = np.zeros_like(B2, order="F")
-        st = lib.cliqgpu_refine(L._h, B2.ctypes.data_as(C.c_void_p), X.ctypes.data_as(C.c_void_p), B2.shape[0],
+        if X is None:
+            Xo = np.zeros_like(B2, order="F")
+        else:
+            Xo = X.reshape(B2.shape[0], -1, order="A")
+            if Xo.dtype != B2.dtype or Xo.shape != B2.shape or not Xo.flags.f_contiguous or not Xo.flags.writeable:
+                raise LogicError(_capi.CLIQ_ERR_ARG, "X must be a writable Fortran-ordered array of B's shape and dtype")
+        st = lib.cliqgpu_refine(L._h, B2.ctypes.data_as(C.c_void_p), Xo.ctypes.data_as(C.c_void_p), B2.shape[0],
                                 B2.shape[1], 0, tol, max_iter, C.byref(it), C.byref(rr))
-        X = X.reshape(np.asarray(B).shape)
+        X = X if X is not None else Xo.reshape(np.asarray(B).shape)
     if st not in (_capi.CLIQ_OK, _capi.CLIQ_ERR_NOCONV):
         check(st, "RefinedSolve")
     return X, it.value, rr.value

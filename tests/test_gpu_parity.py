@@ -147,6 +147,27 @@ def test_refinement_fgmres_vs_classical(complex_, monkeypatch):
     assert rel(Xg, Xi) <= 1e-8
 
 
+def test_refined_solve_into_pinned_host_buffer():
+    """RefinedSolve with host buffers writes into a caller-provided
+    Fortran-ordered X (pinned memory, as the end-to-end benchmark passes it)
+    the same solution it returns in a fresh array."""
+    import torch
+    n = 20
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=5)
+    B = np.asfortranarray(ops.random_rhs(A.n, 3, seed=2, complex_=True))
+    map_, info, L = build(A, (n, n, n), 64, precision="single")
+    X0, it0, rr0 = cliq.RefinedSolve(L, B, tol=1e-11, max_iter=30)
+    Xp = torch.empty((3, A.n), dtype=torch.complex128, pin_memory=True).numpy().T
+    Bp = torch.empty((3, A.n), dtype=torch.complex128, pin_memory=True).numpy().T
+    Bp[...] = B
+    X1, it1, rr1 = cliq.RefinedSolve(L, Bp, tol=1e-11, max_iter=30, X=Xp)
+    assert X1 is Xp
+    assert rr1 <= 1e-11 and residual(A, X1, B) <= 1e-11
+    assert rel(X1, X0) <= 1e-9
+    with pytest.raises(Exception):
+        cliq.RefinedSolve(L, Bp, tol=1e-11, max_iter=30, X=np.zeros((A.n, 3), np.complex128))   # C-ordered: rejected
+
+
 def _magnetic(dims, shift=6.5, theta=0.3):
     A = ops.laplacian_3d(*dims, shift)
     vals = A.values.astype(np.complex128)
