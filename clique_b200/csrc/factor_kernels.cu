@@ -628,8 +628,10 @@ static void launch_diag(const Plan& P, const Launch& ln, T* L, const int4* items
         reinterpret_cast<T*>(P.dinvT), P.status);
 }
 
+// captured: issue for a graph captured from stream1 (no dependency on the
+// caller's stream inside; the replay wrapper forks and joins it)
 template <class T, bool C, bool CJ>
-static int run_factor_impl(Plan& P) {
+static int64_t issue_factor(Plan& P, bool captured = false) {
     using X = V<T, C>;
     using W = DV<C>;
     const size_t smem_diag = diag_smem_bytes<double, C>();
@@ -668,8 +670,8 @@ static int run_factor_impl(Plan& P) {
     std::vector<Pending> pending;
     if (la) {
         cudaEvent_t fork = P.sync_events[next_ev++];
-        cudaEventRecord(fork, P.stream);
-        cudaStreamWaitEvent(s1, fork, 0);
+        cudaEventRecord(fork, captured ? s1 : P.stream);
+        if (!captured) cudaStreamWaitEvent(s1, fork, 0);
         cudaStreamWaitEvent(P.stream2, fork, 0);
     }
     auto join = [&]() {
@@ -742,12 +744,54 @@ static int run_factor_impl(Plan& P) {
             reinterpret_cast<T*>(P.m1), reinterpret_cast<T*>(P.n1));
         ++launches;
     }
-    if (la) {   // the caller's stream continues after the whole factorization
+    if (la && !captured) {   // the caller's stream continues after the whole factorization
         cudaEvent_t end = P.sync_events[next_ev++];
         cudaEventRecord(end, s1);
         cudaStreamWaitEvent(P.stream, end, 0);
     }
-    P.prof_pending = P.profile != 0;
+    return launches;
+}
+
+// Direct launches for the first factorization of a plan and for profiled
+// ones; otherwise the launch sequence (static for a plan: same grids, items
+// and buffers every time) is captured once from the plan's stream, across
+// both internal streams, and replayed as one graph.
+template <class T, bool C, bool CJ>
+static int run_factor_impl(Plan& P) {
+    int64_t launches = 0;
+    const bool graphs = P.use_graph && P.stream1 && P.stream2 && P.sync_events.size() >= 2;
+    if (graphs && !P.profile && P.factor_runs > 0 && !P.factor_exec) {
+        if (cudaStreamBeginCapture(P.stream1, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            // the launchers count their side launches (operand packing) in
+            // total_launches: nothing ran yet, so keep that count for the replays
+            const int64_t before = P.total_launches;
+            const int64_t n = issue_factor<T, C, CJ>(P, true);
+            const int64_t side = P.total_launches - before;
+            P.total_launches = before;
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(P.stream1, &g);
+            if (e == cudaSuccess && g && cudaGraphInstantiate(&P.factor_exec, g, 0) == cudaSuccess) P.graph_launches = n + side;
+            else P.factor_exec = nullptr;
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        if (!P.factor_exec) P.use_graph = 0;   // capture refused: direct launches from now on
+    }
+    if (graphs && !P.profile && P.factor_exec) {
+        // the last two sync events are not used inside the graph
+        cudaEvent_t fork = P.sync_events[P.sync_events.size() - 2], end = P.sync_events.back();
+        cudaEventRecord(fork, P.stream);
+        cudaStreamWaitEvent(P.stream1, fork, 0);
+        if (cudaGraphLaunch(P.factor_exec, P.stream1) != cudaSuccess) return check_cuda("factor graph launch");
+        cudaEventRecord(end, P.stream1);
+        cudaStreamWaitEvent(P.stream, end, 0);
+        launches = P.graph_launches;
+        P.prof_pending = false;
+    } else {
+        launches = issue_factor<T, C, CJ>(P);
+        P.prof_pending = P.profile != 0;
+    }
+    ++P.factor_runs;
     P.last_launches = launches;
     P.total_launches += launches;
     return check_cuda("factor launch");

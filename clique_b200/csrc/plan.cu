@@ -86,6 +86,7 @@ void free_plan(Plan& P) {
     P.events.clear();
     for (cudaEvent_t e : P.sync_events) cudaEventDestroy(e);
     P.sync_events.clear();
+    if (P.factor_exec) cudaGraphExecDestroy(P.factor_exec);
     if (P.stream1) cudaStreamDestroy(P.stream1);
     if (P.stream2) cudaStreamDestroy(P.stream2);
     if (P.own_stream && P.stream) cudaStreamDestroy(P.stream);
@@ -704,6 +705,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_INPANEL_TC")) P.inpanel_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_REFINE")) P.refine_gmres = strcmp(e, "ir") != 0;
     if (const char* e = getenv("CLIQGPU_LOOKAHEAD")) P.lookahead = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_GRAPH")) P.use_graph = atoi(e) != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
