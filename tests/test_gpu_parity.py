@@ -168,6 +168,28 @@ def test_refined_solve_into_pinned_host_buffer():
         cliq.RefinedSolve(L, Bp, tol=1e-11, max_iter=30, X=np.zeros((A.n, 3), np.complex128))   # C-ordered: rejected
 
 
+def test_factor_graph_replay_matches_direct(monkeypatch):
+    """CLIQGPU_GRAPH=1: the second and later factorizations replay a captured
+    graph of the launch sequence; the factors and the refined solution match
+    the direct launches."""
+    n = 24
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=11)
+    B = ops.random_rhs(A.n, 2, seed=4, complex_=True)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("CLIQGPU_GRAPH", mode)
+        map_, info, L = build(A, (n, n, n), 64, precision="single")
+        for _ in range(3):   # the first run launches directly, the second captures, the third replays
+            L.Initialize(A.values)
+            cliq.LDL(info, L)
+        out[mode] = cliq.RefinedSolve(L, B, tol=1e-11, max_iter=30)
+        del L
+    (X0, it0, rr0), (X1, it1, rr1) = out["0"], out["1"]
+    assert rr0 <= 1e-11 and rr1 <= 1e-11
+    assert residual(A, X1, B) <= 1e-11
+    assert rel(X1, X0) <= 1e-8
+
+
 def _magnetic(dims, shift=6.5, theta=0.3):
     A = ops.laplacian_3d(*dims, shift)
     vals = A.values.astype(np.complex128)
