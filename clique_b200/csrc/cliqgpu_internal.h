@@ -120,6 +120,11 @@ struct Launch {
     // GEMM: lookahead part of an outer-block update (columns two outer blocks
     // and more to the right), run on the second stream; k = the outer block
     int32_t bulk = 0;
+    // GEMM: operands written by the preceding tensor-core panel (no packing);
+    // PANEL: offset of that GEMM's problems in the problem array (-1: none),
+    // the panel item's w field is the front's problem index there (-1: none)
+    int32_t prepacked = 0;
+    int64_t pk_probs = -1;
     // tensor-core path: operand packing for this GEMM
     int64_t pack_items = 0, pack_prefix = 0, pack_blocks = 0;
     int32_t pack_njobs = 0;
@@ -290,7 +295,7 @@ int check_cuda(const char* where);
 // runs the GEMM, all on stream st
 int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack);
 size_t tc2_smem(bool cplx);
-int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st);
+int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st, void* pack);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);
 void free_plan(Plan& P);

@@ -707,7 +707,7 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
                 break;
             case Launch::PANEL:
                 if (std::is_same<T, float>::value && P.f16_scales()) {
-                    launch_panel_tc(P, ln, st);
+                    launch_panel_tc(P, ln, st, P.pack);
                     break;
                 }
                 panel_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, smem_panel, st>>>(

@@ -233,6 +233,9 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     const int64_t blkA = (int64_t)planes * kTcBM * 8, blkB = (int64_t)planes * kTcBN * 8;   // floats per packed block
     int64_t pack_max = 1;
     int nbulk = 0;   // lookahead launches
+    // in-panel updates on the tensor path with the 2xFP16 split: the panel
+    // writes their packed operands itself
+    const bool prepack = tcp && P.split_f16 && P.inpanel_tc;
     auto add_gemm = [&](std::vector<GemmProb>& lst, int depth, int schur, bool inpanel) {
         if (lst.empty()) return;
         Launch ln{};
@@ -278,7 +281,9 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 off += tB * nk * blkB;
                 b.dst_scale = pr.scaleB = off;
                 if (f16) off += tB * kTcBN;
-                if (f16 && pr.B == pr.A && pr.N <= pr.M && kTcBN == kTcBM) {
+                if (inpanel && prepack) {
+                    // written by the panel kernel at the same offsets
+                } else if (f16 && pr.B == pr.A && pr.N <= pr.M && kTcBN == kTcBM) {
                     // one job: the B rows are the first N rows of A, read once
                     a.dS = pr.d;
                     a.dstS = b.dst;
@@ -298,6 +303,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             }
             ln.pack_njobs = (int32_t)(packjobs.size() - ln.pack_items);
             ln.pack_blocks = blocks;
+            ln.prepacked = inpanel && prepack ? 1 : 0;
             pack_max = std::max(pack_max, off);
         }
         ln.prefix = (int64_t)prefix.size();
@@ -373,8 +379,9 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                     const int kb = std::min(nb, f.n - k);
                     const int rows = f.m - k - kb;
                     const int prows = P.f16_scales() ? 128 : kTile;   // tensor-core panel: 128-row tiles
-                    for (int rb = 0; rb * prows < rows; ++rb) push_item(a.first, a.second, rb, 0);
                     const int N = std::min(K0 + nbo, f.n) - k - kb;
+                    const int w = N > 0 ? (int)trail.size() : -1;   // this front's in-panel problem
+                    for (int rb = 0; rb * prows < rows; ++rb) push_item(a.first, a.second, rb, w);
                     if (N > 0) {
                         GemmProb pr{};
                         pr.front = a.first;
@@ -396,6 +403,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 }
                 pn.nitems = (int32_t)(items.size() / 4 - pn.items);
                 pn.nblocks = pn.nitems;
+                pn.pk_probs = prepack && !trail.empty() ? (int64_t)probs.size() : -1;
                 if (pn.nitems) P.launches.push_back(pn);
                 add_gemm(trail, d, 0, true);
             }

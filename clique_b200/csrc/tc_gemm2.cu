@@ -377,8 +377,10 @@ static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between, cudaStre
     float* pk = reinterpret_cast<float*>(pack);
     const PackJob* jobs = P.packjobs + ln.pack_items;
     const int64_t* jpre = P.prefix + ln.pack_prefix;
-    if (ln.pack_blocks <= 0) return;   // nothing to update
-    if constexpr (F16)
+    if (ln.pack_blocks <= 0 && !ln.prepacked) return;   // nothing to update
+    if (ln.pack_blocks <= 0) {
+        // operands written by the panel kernel
+    } else if constexpr (F16)
         tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
                                                                                    pk);
     else
@@ -405,7 +407,7 @@ int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, 
     } else {
         if (f16) launch_pair<false, false, true>(P, ln, between, st, pack); else launch_pair<false, false, false>(P, ln, between, st, pack);
     }
-    P.total_launches += 1;   // the pack kernel (the caller counts the GEMM)
+    if (ln.pack_blocks > 0) P.total_launches += 1;   // the pack kernel (the caller counts the GEMM)
     return CLIQ_OK;
 }
 

@@ -91,7 +91,9 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
                                                                     int k, float* __restrict__ L, const double* __restrict__ D,
                                                                     const float* __restrict__ tinv, uint32_t* __restrict__ eblk,
                                                                     uint32_t* __restrict__ erow, int64_t eblk_total,
-                                                                    int64_t erow_total, int32_t* __restrict__ status) {
+                                                                    int64_t erow_total, int32_t* __restrict__ status,
+                                                                    const GemmProb* __restrict__ probs, float* __restrict__ pack,
+                                                                    int conj) {
     using X = V<float, C>;
     using W = DV<C>;
     using PC = PanelCfg<C>;
@@ -242,6 +244,96 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
                 atomicMax(&erow[f.erow + row], __float_as_uint(ml));
                 atomicMax(&erow[erow_total + f.erow + row], __float_as_uint(ms));
             }
+            // packed operands of the following in-panel update (rows of this
+            // tile are rows tile*128 + i of its problem, K = kb): the A planes
+            // scaled by the row maximum ml, and for the first N problem rows
+            // the S = D op(L21) planes scaled by ms, in the layout and with
+            // the scales the operand packing would produce
+            if (probs && it.w >= 0) {
+                const GemmProb pr = probs[it.w];
+                const int rp = tile * kPanelRows + i;   // row in the problem
+                const int nks = (pr.K + 15) / 16;
+                const bool srow = tile * kPanelRows < pr.N;
+                constexpr int planes = C ? 4 : 2;
+                constexpr int64_t plane_bytes = (int64_t)kPanelRows * 16 * 2;
+                auto scale_of = [](float mx, float* inv) {
+                    int e = mx > 0.f ? ((__float_as_int(mx) >> 23) & 0xff) - 127 : 0;
+                    e = max(-100, min(100, e));
+                    *inv = __int_as_float((127 - 14 + e) << 23);
+                    return __int_as_float((127 + 14 - e) << 23);
+                };
+                float inv_sa, inv_ss;
+                const float sa = scale_of(vr ? ml : 0.f, &inv_sa), ss = scale_of(vr && rp < pr.N ? ms : 0.f, &inv_ss);
+                pack[pr.scaleA + rp] = inv_sa;
+                if (srow) pack[pr.scaleB + rp] = inv_ss;
+#pragma unroll 1
+                for (int ks = 0; ks < nks; ++ks) {
+                    float re[16], im[16];
+                    tmem_ld16(lane_base + 16 * ks, re);
+                    if constexpr (C) tmem_ld16(lane_base + nb + 16 * ks, im);
+                    X v[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int c = 16 * ks + q;
+                        const float sc = ia * inv_b[c];
+                        if constexpr (C) v[q] = X{re[q] * sc, im[q] * sc}; else v[q] = re[q] * sc;
+                        if (c >= kb || !vr) v[q] = X{};
+                    }
+                    const int64_t blk = (int64_t)tile * nks + ks;
+                    uint8_t* base = reinterpret_cast<uint8_t*>(pack + pr.packA) + blk * plane_bytes * planes;
+                    float y[16];
+                    uint4 h, l;
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        if constexpr (C) y[q] = v[q].r * sa; else y[q] = v[q] * sa;
+                    }
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        split8(y + 8 * cc, h, l);
+                        *reinterpret_cast<uint4*>(base + 0 * plane_bytes + core_off(i, cc)) = h;
+                        *reinterpret_cast<uint4*>(base + 1 * plane_bytes + core_off(i, cc)) = l;
+                    }
+                    if constexpr (C) {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) y[q] = v[q].i * sa;
+#pragma unroll
+                        for (int cc = 0; cc < 2; ++cc) {
+                            split8(y + 8 * cc, h, l);
+                            *reinterpret_cast<uint4*>(base + 2 * plane_bytes + core_off(i, cc)) = h;
+                            *reinterpret_cast<uint4*>(base + 3 * plane_bytes + core_off(i, cc)) = l;
+                        }
+                    }
+                    if (srow) {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            X sv = v[q];
+                            if constexpr (C) { if (conj) sv.i = -sv.i; }
+                            v[q] = rp < pr.N ? s_d[16 * ks + q] * sv : X{};
+                        }
+                        uint8_t* bs = reinterpret_cast<uint8_t*>(pack + pr.packB) + blk * plane_bytes * planes;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            if constexpr (C) y[q] = v[q].r * ss; else y[q] = v[q] * ss;
+                        }
+#pragma unroll
+                        for (int cc = 0; cc < 2; ++cc) {
+                            split8(y + 8 * cc, h, l);
+                            *reinterpret_cast<uint4*>(bs + 0 * plane_bytes + core_off(i, cc)) = h;
+                            *reinterpret_cast<uint4*>(bs + 1 * plane_bytes + core_off(i, cc)) = l;
+                        }
+                        if constexpr (C) {
+#pragma unroll
+                            for (int q = 0; q < 16; ++q) y[q] = v[q].i * ss;
+#pragma unroll
+                            for (int cc = 0; cc < 2; ++cc) {
+                                split8(y + 8 * cc, h, l);
+                                *reinterpret_cast<uint4*>(bs + 2 * plane_bytes + core_off(i, cc)) = h;
+                                *reinterpret_cast<uint4*>(bs + 3 * plane_bytes + core_off(i, cc)) = l;
+                            }
+                        }
+                    }
+                }
+            }
         }
     }
     tc_fence_before();
@@ -255,7 +347,8 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
 }  // namespace tc2
 
 // launch the tensor-core panel for one PANEL step of the schedule
-int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st) {
+int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st, void* pack) {
+    const GemmProb* probs = ln.pk_probs >= 0 ? P.probs + ln.pk_probs : nullptr;
     float* L = reinterpret_cast<float*>(P.L);
     const int4* items = reinterpret_cast<const int4*>(P.items) + ln.items;
     static bool attr[2] = {false, false};
@@ -263,12 +356,14 @@ int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st) {
         const size_t smem = tc2::panel_tc_smem<true>();
         if (!attr[1]) { cudaFuncSetAttribute(tc2::panel_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[1] = true; }
         tc2::panel_tc_kernel<true><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, st>>>(
-            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
+            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status, probs,
+            reinterpret_cast<float*>(pack), P.conjugate);
     } else {
         const size_t smem = tc2::panel_tc_smem<false>();
         if (!attr[0]) { cudaFuncSetAttribute(tc2::panel_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); attr[0] = true; }
         tc2::panel_tc_kernel<false><<<(unsigned)ln.nblocks, tc2::kPanelThreads, smem, st>>>(
-            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status);
+            P.fronts, items, ln.k, L, P.D, reinterpret_cast<const float*>(P.tinv), P.eblk, P.erow, P.eblk_total, P.erow_total, P.status, probs,
+            reinterpret_cast<float*>(pack), P.conjugate);
     }
     return CLIQ_OK;
 }
