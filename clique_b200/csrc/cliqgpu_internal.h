@@ -117,8 +117,9 @@ struct Launch {
     double work;          // GEMM: algorithmic flops; EXTEND_ADD: algorithmic bytes
     int32_t schur;        // GEMM: 1 for the Schur-complement update, 0 for an in-panel update
     int32_t simt = 0;     // GEMM: CUDA-core kernel (64 x 64 tiles) even on the tensor path
-    // GEMM: lookahead part of an outer-block update (columns two outer blocks
-    // and more to the right), run on the second stream; k = the outer block
+    // GEMM: 1 = lookahead part of an outer-block update (columns two outer
+    // blocks and more to the right), run on stream2, k = the outer block;
+    // 2 = one K chunk of the Schur-complement update, run on stream3
     int32_t bulk = 0;
     // GEMM: operands written by the preceding tensor-core panel (no packing);
     // PANEL: offset of that GEMM's problems in the problem array (-1: none),
@@ -215,6 +216,14 @@ struct Plan {
     int lookahead = 1;
     cudaStream_t stream1 = nullptr;   // internal, highest priority: the factorization's critical path
     cudaStream_t stream2 = nullptr;   // internal, lowest priority: lookahead updates
+    cudaStream_t stream3 = nullptr;   // internal, lowest priority: Schur-complement chunks
+    void* pack3 = nullptr;            // packed operands of the Schur chunks
+    // CLIQGPU_SCHUR_CHUNK=c > 0: the Schur complement is applied in chunks of
+    // c pivot columns on stream3 as soon as their panels are final (per-chunk
+    // row scales); needs the lookahead streams.  0 (default): one update with
+    // K = n at the end of the level (at 100^3 the chunks overlap the next
+    // panels but cost as much in extra update traffic: 128.9 vs 128.7 ms)
+    int schur_chunk = 0;
     std::vector<cudaEvent_t> sync_events;   // fork / lookahead-done events, one pair per lookahead launch
     // CLIQGPU_GRAPH=1: the factorization's launches replayed as one CUDA
     // graph from the second unprofiled factorization on (off by default: at

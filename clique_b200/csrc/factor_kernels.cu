@@ -665,7 +665,7 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
     cudaStream_t s1 = la ? P.stream1 : P.stream;
     const int nbo = std::max(P.nb, P.outer_nb / P.nb * P.nb);
     size_t next_ev = 0;
-    cudaEvent_t last_done = nullptr;
+    cudaEvent_t last_done = nullptr, last_done3 = nullptr;
     struct Pending { int depth, k0; cudaEvent_t done; };
     std::vector<Pending> pending;
     if (la) {
@@ -673,10 +673,12 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
         cudaEventRecord(fork, captured ? s1 : P.stream);
         if (!captured) cudaStreamWaitEvent(s1, fork, 0);
         cudaStreamWaitEvent(P.stream2, fork, 0);
+        cudaStreamWaitEvent(P.stream3, fork, 0);
     }
     auto join = [&]() {
         if (last_done) cudaStreamWaitEvent(s1, last_done, 0);
-        last_done = nullptr;
+        if (last_done3) cudaStreamWaitEvent(s1, last_done3, 0);
+        last_done = last_done3 = nullptr;
         pending.clear();
     };
     if (P.erow) cudaMemsetAsync(P.erow, 0, sizeof(uint32_t) * 2 * (size_t)P.erow_total, s1);
@@ -684,17 +686,18 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
         const Launch& ln = P.launches[li];
         if (ln.nblocks <= 0) continue;
         if (la) {
-            if (ln.kind == Launch::EXTEND_ADD || (ln.kind == Launch::GEMM && ln.schur)) join();
+            if (ln.kind == Launch::EXTEND_ADD || (ln.kind == Launch::GEMM && ln.schur && !ln.bulk)) join();
             if (ln.kind == Launch::DIAG && ln.k % nbo == 0 && ln.k >= 2 * nbo)
                 for (const Pending& pd : pending)
                     if (pd.depth == ln.depth && pd.k0 == ln.k - 2 * nbo) cudaStreamWaitEvent(s1, pd.done, 0);
         }
         const bool on2 = la && ln.bulk;
-        cudaStream_t st = on2 ? P.stream2 : s1;
+        cudaStream_t sb = ln.bulk == 2 ? P.stream3 : P.stream2;
+        cudaStream_t st = on2 ? sb : s1;
         if (on2) {   // the lookahead update reads panels produced on stream1 so far
             cudaEvent_t fork = P.sync_events[next_ev++];
             cudaEventRecord(fork, s1);
-            cudaStreamWaitEvent(P.stream2, fork, 0);
+            cudaStreamWaitEvent(sb, fork, 0);
         }
         if (P.profile) cudaEventRecord(P.events[3 * li], st);
         switch (ln.kind) {
@@ -716,7 +719,8 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
                 break;
             case Launch::GEMM:
                 if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
-                    launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr, st, on2 ? P.pack2 : P.pack);
+                    launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr, st,
+                               on2 ? (ln.bulk == 2 ? P.pack3 : P.pack2) : P.pack);
                 else
                     gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(
                         P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
@@ -725,9 +729,13 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
         if (P.profile) cudaEventRecord(P.events[3 * li + 1], st);
         if (on2) {
             cudaEvent_t done = P.sync_events[next_ev++];
-            cudaEventRecord(done, P.stream2);
-            pending.push_back({ln.depth, ln.k, done});
-            last_done = done;
+            cudaEventRecord(done, sb);
+            if (ln.bulk == 2) {
+                last_done3 = done;
+            } else {
+                pending.push_back({ln.depth, ln.k, done});
+                last_done = done;
+            }
         }
         ++launches;
     }

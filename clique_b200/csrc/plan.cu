@@ -79,7 +79,7 @@ void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
-                    P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov};
+                    P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov, P.pack3};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : P.events) cudaEventDestroy(e);
@@ -89,6 +89,7 @@ void free_plan(Plan& P) {
     if (P.factor_exec) cudaGraphExecDestroy(P.factor_exec);
     if (P.stream1) cudaStreamDestroy(P.stream1);
     if (P.stream2) cudaStreamDestroy(P.stream2);
+    if (P.stream3) cudaStreamDestroy(P.stream3);
     if (P.own_stream && P.stream) cudaStreamDestroy(P.stream);
 }
 
@@ -232,7 +233,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     const int planes = P.cplx() ? 4 : 2;
     const int64_t blkA = (int64_t)planes * kTcBM * 8, blkB = (int64_t)planes * kTcBN * 8;   // floats per packed block
     int64_t pack_max = 1;
-    int nbulk = 0;   // lookahead launches
+    int nbulk = 0;   // lookahead launches (both kinds)
+    int nschur_chunks = 0;
+    const bool chunked = tcp && P.lookahead && P.schur_chunk > 0;
+    const int schur_chunk = std::max(kTile, P.schur_chunk / kTile * kTile);
     // in-panel updates on the tensor path with the 2xFP16 split: the panel
     // writes their packed operands itself
     const bool prepack = tcp && P.split_f16 && P.inpanel_tc;
@@ -351,6 +355,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         // at once (K = nbo), which the reference spreads over nbo/nb Gemm
         // calls (ldl/local_front.hpp:67).
         const int nbo = std::max(nb, P.outer_nb / nb * nb);
+        int schur_done = 0;   // pivot columns whose Schur-complement update is issued
         for (int K0 = 0; K0 < maxn; K0 += nbo) {
             for (int k = K0; k < std::min(K0 + nbo, maxn); k += nb) {
                 Launch dg{};
@@ -448,11 +453,47 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 P.launches.back().k = K0;
                 ++nbulk;
             }
+            // the Schur-complement update of the chunk of pivot columns that
+            // just became final (all panels of the chunk done), on stream3
+            const int kc1 = K0 + nbo;
+            if (chunked && (kc1 - schur_done >= schur_chunk || kc1 >= maxn)) {
+                const int kc0 = schur_done;
+                schur_done = kc1;
+                std::vector<GemmProb> sc;
+                for (int s : lv) {
+                    const FrontDev& f = P.hfronts[s];
+                    if (f.u <= 0 || f.n <= kc0) continue;
+                    const int ke = std::min(kc1, f.n);
+                    GemmProb pr{};
+                    pr.front = s;
+                    pr.row0 = f.n;
+                    pr.kb0 = kc0 / kTile;
+                    pr.nkb = (ke - kc0 + kTile - 1) / kTile;
+                    pr.A = f.L + f.n + (int64_t)kc0 * f.m;
+                    pr.B = pr.A;
+                    pr.C = f.U;
+                    pr.d = f.off + kc0;
+                    pr.lda = f.m;
+                    pr.ldc = f.u;
+                    pr.M = f.u;
+                    pr.N = f.u;
+                    pr.K = ke - kc0;
+                    pr.cpool = f.pool;
+                    sc.push_back(pr);
+                }
+                if (!sc.empty()) {
+                    add_gemm(sc, d, 1, false);
+                    P.launches.back().bulk = 2;
+                    P.launches.back().k = -1;
+                    ++nbulk;
+                    ++nschur_chunks;
+                }
+            }
         }
         std::vector<GemmProb> schur;
         for (int s : lv) {
             const FrontDev& f = P.hfronts[s];
-            if (f.u <= 0 || f.n <= 0) continue;
+            if (f.u <= 0 || f.n <= 0 || chunked) continue;
             GemmProb pr{};
             pr.front = s;
             pr.row0 = f.n;
@@ -609,8 +650,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
         if (cudaStreamCreateWithPriority(&P.stream1, cudaStreamNonBlocking, greatest) != cudaSuccess ||
-            cudaStreamCreateWithPriority(&P.stream2, cudaStreamNonBlocking, least) != cudaSuccess)
+            cudaStreamCreateWithPriority(&P.stream2, cudaStreamNonBlocking, least) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&P.stream3, cudaStreamNonBlocking, least) != cudaSuccess)
             return check_cuda("lookahead streams");
+        if (nschur_chunks > 0) TRY(dev_alloc(P, &P.pack3, (size_t)P.pack_floats * sizeof(float)));
         P.sync_events.resize(2 * (size_t)nbulk + 4, nullptr);
         for (cudaEvent_t& e : P.sync_events)
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return check_cuda("lookahead events");
@@ -714,6 +757,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_REFINE")) P.refine_gmres = strcmp(e, "ir") != 0;
     if (const char* e = getenv("CLIQGPU_LOOKAHEAD")) P.lookahead = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_GRAPH")) P.use_graph = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_SCHUR_CHUNK")) P.schur_chunk = std::max(0, atoi(e));
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }

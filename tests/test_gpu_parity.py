@@ -190,6 +190,27 @@ def test_factor_graph_replay_matches_direct(monkeypatch):
     assert rel(X1, X0) <= 1e-8
 
 
+def test_schur_chunks_match_single_update(monkeypatch):
+    """CLIQGPU_SCHUR_CHUNK: the Schur complement applied in K chunks on the
+    third stream gives the same refined solution as the single update."""
+    n = 28
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=13)
+    B = ops.random_rhs(A.n, 2, seed=6, complex_=True)
+    out = {}
+    for chunk in ("0", "128"):
+        monkeypatch.setenv("CLIQGPU_SCHUR_CHUNK", chunk)
+        monkeypatch.setenv("CLIQGPU_OUTER_BLOCK", "64")
+        map_, info, L = build(A, (n, n, n), 64, precision="single")
+        L.Initialize(A.values)
+        cliq.LDL(info, L)
+        out[chunk] = cliq.RefinedSolve(L, B, tol=1e-11, max_iter=30)
+        del L
+    (X0, it0, rr0), (X1, it1, rr1) = out["0"], out["128"]
+    assert rr0 <= 1e-11 and rr1 <= 1e-11
+    assert residual(A, X1, B) <= 1e-11
+    assert rel(X1, X0) <= 1e-8
+
+
 def _magnetic(dims, shift=6.5, theta=0.3):
     A = ops.laplacian_3d(*dims, shift)
     vals = A.values.astype(np.complex128)
