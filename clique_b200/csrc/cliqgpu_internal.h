@@ -73,7 +73,7 @@ struct FrontDev {
     int32_t m, n, off, u;
     int32_t cu[2];      // children's update sizes
     int32_t pool;       // parity of the depth
-    int32_t flag_base;  // first chain-solve flag of this front
+    int32_t flag_base;  // first pivot-block slot of this front (worker flag, worker result)
     int64_t dinv;       // inverse diagonal blocks (ceil(n/64) blocks of 64 x 64) in the dinv store
     int32_t hbase;      // backward sweep: first helper slot ((nch - 1) per pivot block)
     int32_t nch;        // backward sweep: 16-tile chunks of the rows below the pivots
@@ -237,7 +237,7 @@ struct Plan {
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;
-    int32_t* flags = nullptr;     // worker flags (flags_total), spare (flags_total), helper flags
+    int32_t* flags = nullptr;     // worker flags (flags_total, one per pivot block), then helper flags
     int32_t* tickets = nullptr;
     int32_t* status = nullptr;    // [0] first zero pivot + 1 (min), [1] timeout flag
     int64_t* rowptr = nullptr;    // FP64 matrix (keep_matrix)

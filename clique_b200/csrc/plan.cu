@@ -662,7 +662,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));
     TRY(dev_upload(P, &P.level_fronts, level_fronts));
-    std::vector<int32_t> zeros_flags(2 * P.flags_total + P.helpers_total, 0);
+    std::vector<int32_t> zeros_flags(P.flags_total + P.helpers_total, 0);
     TRY(dev_upload(P, &P.flags, zeros_flags));
     P.nchain_items = (int32_t)(chain_items.size() / 4);
     if (chain_items.empty()) chain_items.assign(4, 0);

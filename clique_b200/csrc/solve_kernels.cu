@@ -993,7 +993,7 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     SweepArgs a{};
     a.F = P.fronts;
     a.xprog = P.xprog;
-    a.pflags = P.flags + P.flags_total;
+    a.pflags = P.flags;
     a.L = P.L;
     a.dinv = P.dinv;
     a.dinvT = P.dinvT;
@@ -1001,7 +1001,7 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     a.n1 = P.n1;
     a.partial = P.partial;
     a.hpart = P.hpart;
-    a.hflags = P.flags + 2 * P.flags_total;
+    a.hflags = P.flags + P.flags_total;
     a.X = X;
     a.ldx = P.n;
     a.w0 = P.wpool[0];
