@@ -128,6 +128,9 @@ struct Launch {
     int64_t pk_probs = -1;
     // tensor-core path: operand packing for this GEMM
     int64_t pack_items = 0, pack_prefix = 0, pack_blocks = 0;
+    // offsets into the block map: the job of every pack block, the problem of
+    // every GEMM tile (one load instead of a binary search over the prefix)
+    int64_t pack_map = 0, gemm_map = 0;
     int32_t pack_njobs = 0;
 };
 
@@ -234,6 +237,7 @@ struct Plan {
     cudaGraphExec_t factor_exec = nullptr;
     int64_t graph_launches = 0;
     int64_t* prefix = nullptr;
+    int32_t* bmap = nullptr;      // block -> job / problem index of every pack and GEMM launch
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;

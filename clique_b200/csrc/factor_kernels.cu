@@ -534,18 +534,23 @@ __global__ void __launch_bounds__(kThreads) chain_tiles_kernel(const FrontDev* _
 // ---------------------------------------------------------------------------
 template <class T, bool C, bool CJ>
 __global__ void __launch_bounds__(kThreads) gemm_update_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
-                                                               int nprobs, T* __restrict__ L, T* __restrict__ pool0,
-                                                               T* __restrict__ pool1, const double* __restrict__ D) {
+                                                               int nprobs, const int32_t* __restrict__ bmap, T* __restrict__ L,
+                                                               T* __restrict__ pool0, T* __restrict__ pool1, const double* __restrict__ D) {
     using X = V<T, C>;
     using W = DV<C>;
     constexpr int BM = 64, BK = C ? 8 : 16, PAD = 1;
     __shared__ X sA[BK][BM + PAD];
     __shared__ X sB[BK][BM + PAD];
     const int64_t bid = blockIdx.x;
-    int lo = 0, hi = nprobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+    int lo = 0;
+    if (bmap) {
+        lo = bmap[bid];   // this tile's problem
+    } else {
+        int hi = nprobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
+        }
     }
     const GemmProb pr = probs[lo];
     int64_t t = bid - prefix[lo];
@@ -723,7 +728,7 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
                                on2 ? (ln.bulk == 2 ? P.pack3 : P.pack2) : P.pack);
                 else
                     gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(
-                        P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, L, p0, p1, P.D);
+                        P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, P.bmap + ln.gemm_map, L, p0, p1, P.D);
                 break;
         }
         if (P.profile) cudaEventRecord(P.events[3 * li + 1], st);
@@ -927,11 +932,11 @@ static void launch_all(unsigned char* base, int m, int n, T* AL, T* ABR, const s
             panel_kernel<T, C><<<s.panel_blocks, kThreads, smem_panel, st>>>(F, items + s.panel_item, s.k, AL, D, tinv, nullptr,
                                                                                nullptr, 0, 0);
         if (s.prob >= 0)
-            gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, AL, ABR,
+            gemm_update_kernel<T, C, CJ><<<(unsigned)s.tiles, kThreads, 0, st>>>(probs + s.prob, prefix + s.prob, 1, nullptr, AL, ABR,
                                                                                ABR, D);
     }
     if (schur_prob >= 0)
-        gemm_update_kernel<T, C, CJ><<<(unsigned)schur_tiles, kThreads, 0, st>>>(probs + schur_prob, prefix + schur_prob, 1, AL,
+        gemm_update_kernel<T, C, CJ><<<(unsigned)schur_tiles, kThreads, 0, st>>>(probs + schur_prob, prefix + schur_prob, 1, nullptr, AL,
                                                                                ABR, ABR, D);
     put_diag<T, C><<<(n + 255) / 256, 256, 0, st>>>(AL, (int64_t)m, n, D);
 }

@@ -77,7 +77,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 
 void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
-                    P.prefix, P.dest,
+                    P.prefix, P.bmap, P.dest,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
                     P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov, P.pack3};
     for (void* p : ptrs)
@@ -213,6 +213,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     std::vector<int32_t> items;   // int4 quads
     std::vector<GemmProb> probs;
     std::vector<int64_t> prefix;
+    std::vector<int32_t> bmap;   // block -> job / problem, per launch
     auto push_item = [&](int a, int b, int c, int d) { items.push_back(a); items.push_back(b); items.push_back(c); items.push_back(d); };
     P.launches.clear();
     int64_t max_slots = 1;
@@ -307,12 +308,25 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             }
             ln.pack_njobs = (int32_t)(packjobs.size() - ln.pack_items);
             ln.pack_blocks = blocks;
+            ln.pack_map = (int64_t)bmap.size();
+            for (int32_t j = 0; j < ln.pack_njobs; ++j) {
+                const int64_t b0 = prefix[ln.pack_prefix + j];
+                const int64_t b1 = j + 1 < ln.pack_njobs ? prefix[ln.pack_prefix + j + 1] : blocks;
+                for (int64_t b = b0; b < b1; ++b) bmap.push_back(j);
+            }
             ln.prepacked = inpanel && prepack ? 1 : 0;
             pack_max = std::max(pack_max, off);
         }
         ln.prefix = (int64_t)prefix.size();
+        ln.gemm_map = (int64_t)bmap.size();
         int64_t tot = 0;
-        for (auto& pr : lst) { prefix.push_back(tot); tot += tiles_of(tc, pr.M, pr.N); probs.push_back(pr); }
+        for (auto& pr : lst) {
+            prefix.push_back(tot);
+            const int64_t nt = tiles_of(tc, pr.M, pr.N);
+            for (int64_t t = 0; t < nt; ++t) bmap.push_back((int32_t)probs.size() - (int32_t)ln.items);
+            tot += nt;
+            probs.push_back(pr);
+        }
         ln.nblocks = tot;
         ln.depth = depth;
         P.launches.push_back(ln);
@@ -659,6 +673,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return check_cuda("lookahead events");
     }
     TRY(dev_upload(P, &P.prefix, prefix));
+    TRY(dev_upload(P, &P.bmap, bmap));
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));
     TRY(dev_upload(P, &P.level_fronts, level_fronts));

@@ -59,17 +59,14 @@ struct Cfg {
 // pack: one CTA per (row tile, k step) block of one job; thread = row
 // ---------------------------------------------------------------------------
 template <bool C, bool CJ>
-__global__ void __launch_bounds__(kTcBM) pack_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+__global__ void __launch_bounds__(kTcBM) pack_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix,
+                                                   const int32_t* __restrict__ bmap,
                                                    const float* __restrict__ L, const double* __restrict__ D,
                                                    float* __restrict__ out) {
     using X = V<float, C>;
     using W = DV<C>;
     const int64_t bid = blockIdx.x;
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
-    }
+    const int lo = bmap[bid];
     const PackJob jb = jobs[lo];
     const int64_t blk = bid - prefix[lo];
     const int nks = (jb.K + kKS - 1) / kKS;
@@ -182,18 +179,15 @@ __device__ __forceinline__ void pack_f16_planes(const PackJob& jb, const V<float
 }
 
 template <bool C, bool CJ>
-__global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix, int njobs,
+__global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix,
+                                                       const int32_t* __restrict__ bmap,
                                                        const float* __restrict__ L, const double* __restrict__ D,
                                                        const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
                                                        float* __restrict__ out) {
     using X = V<float, C>;
     using W = DV<C>;
     const int64_t bid = blockIdx.x;
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
-    }
+    const int lo = bmap[bid];
     const PackJob jb = jobs[lo];
     const int64_t blk = bid - prefix[lo];
     const int nks = (jb.K + kKS16 - 1) / kKS16;
@@ -221,7 +215,8 @@ __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restri
 // ---------------------------------------------------------------------------
 template <bool C, bool F16>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
-                                                              int nprobs, const float* __restrict__ pack, float* __restrict__ L,
+                                                              const int32_t* __restrict__ bmap, const float* __restrict__ pack,
+                                                              float* __restrict__ L,
                                                               float* __restrict__ pool0, float* __restrict__ pool1,
                                                               int32_t* __restrict__ status) {
     using CF = Cfg<C>;
@@ -235,11 +230,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const Gem
 
     // tile of this CTA: kBM-row tiles ti, kBN-column tiles tj, needed when ti >= kRatio tj
     const int64_t bid = blockIdx.x;
-    int lo = 0, hi = nprobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= bid) lo = mid; else hi = mid - 1;
-    }
+    const int lo = bmap[bid];   // this tile's problem
     const GemmProb pr = probs[lo];
     int64_t t = bid - prefix[lo];
     const int Mt = (pr.M + kBM - 1) / kBM, Nt = (pr.N + kBN - 1) / kBN;
@@ -381,10 +372,10 @@ static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between, cudaStre
     if (ln.pack_blocks <= 0) {
         // operands written by the panel kernel
     } else if constexpr (F16)
-        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, ln.pack_njobs, L, P.D, P.eblk, P.erow,
+        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, P.eblk, P.erow,
                                                                                    pk);
     else
-        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, ln.pack_njobs, L, P.D, pk);
+        tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, pk);
     if (between) cudaEventRecord(between, st);
     const size_t smem = tc2_smem(C);
     static bool attr = false;
@@ -393,7 +384,7 @@ static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between, cudaStre
         attr = true;
     }
     tc2::tc_gemm_kernel<C, F16><<<(unsigned)ln.nblocks, tc2::kThreads, smem, st>>>(
-        P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, pk, L, p0, p1, P.status);
+        P.probs + ln.items, P.prefix + ln.prefix, P.bmap + ln.gemm_map, pk, L, p0, p1, P.status);
 }
 
 int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack) {
