@@ -54,6 +54,7 @@ _SIGS = {
     "cliqgpu_get_front": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cliqgpu_plan_query": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "cliqgpu_synchronize": (C.c_int, [C.c_void_p]),
+    "cliqgpu_wait_selftest": (C.c_int, [C.c_void_p, C.c_int64]),
     "cliqgpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "cliqgpu_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "cliqgpu_plan_destroy": (None, [C.c_void_p]),

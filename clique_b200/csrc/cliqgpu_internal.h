@@ -304,6 +304,8 @@ int launch_multi_axpy(Plan& P, const double* V, int64_t vstride, int nv, const d
 int launch_col_scale(Plan& P, const double* w, double* v, int nrhs, const double* s);
 
 int check_cuda(const char* where);
+// bounded-wait check: one CTA waits on a flag nothing sets (solve_kernels.cu)
+int launch_wait_selftest(Plan& P, uint64_t limit_ns);
 // packs the launch's operands into `pack`, records `between` (if given),
 // runs the GEMM, all on stream st
 int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack);

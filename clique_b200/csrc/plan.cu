@@ -1186,6 +1186,23 @@ int cliqgpu_profile_read(cliqgpu_plan h, double* out, int32_t nout) {
     return CLIQ_OK;
 }
 
+int cliqgpu_wait_selftest(cliqgpu_plan h, int64_t limit_ns) {
+    if (!h || limit_ns <= 0 || limit_ns > 2000000000ll) {
+        set_last_error("wait_selftest: limit_ns must be in (0, 2e9]");
+        return CLIQ_ERR_ARG;
+    }
+    Plan& P = h->p;
+    if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("wait_selftest sync");
+    int st = launch_wait_selftest(P, (uint64_t)limit_ns);
+    if (st == CLIQ_OK) st = read_status(P, nullptr);
+    // clear the recorded timeout: the plan stays usable
+    const int32_t st0[4] = {INT_MAX, 0, 0, 0};
+    if (cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream) != cudaSuccess ||
+        cudaStreamSynchronize(P.stream) != cudaSuccess)
+        return check_cuda("wait_selftest reset");
+    return st;
+}
+
 int cliqgpu_synchronize(cliqgpu_plan h) {
     if (!h) return CLIQ_ERR_ARG;
     if (cudaStreamSynchronize(h->p.stream) != cudaSuccess) return check_cuda("sync");

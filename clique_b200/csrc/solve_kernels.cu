@@ -36,6 +36,8 @@
 // Waits are bounded: on expiry a CTA records a timeout in the status word
 // and returns, and every other wait gives up as soon as it sees that word
 // set.
+#include <climits>
+
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
 
@@ -71,7 +73,7 @@ __device__ __forceinline__ uint64_t global_ns() {
 // thread 0 waits for flag == epoch; returns false (and records a timeout,
 // wait site 4) once the wall-clock bound expires, or at once when another
 // CTA has recorded one
-__device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_t* status) {
+__device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_t* status, uint64_t limit_ns = kSpinNs) {
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
         int ok = 1;
@@ -79,7 +81,7 @@ __device__ __forceinline__ bool wait_flag(const int32_t* flag, int epoch, int32_
             const uint64_t t0 = global_ns();
             while (ld_acquire(flag) != epoch) {
                 if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) { ok = 0; break; }
-                if (global_ns() - t0 > kSpinNs) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 4); ok = 0; break; }
+                if (global_ns() - t0 > limit_ns) { atomicExch(&status[1], 1); atomicCAS(&status[2], 0, 4); ok = 0; break; }
                 __nanosleep(100);
             }
         }
@@ -1059,6 +1061,18 @@ static int run_solve_impl(Plan& P, T* xn, int nrhs_total) {
     P.last_launches += launches;
     P.total_launches += launches;
     return check_cuda("solve launch");
+}
+
+// Failure-detection check: one CTA waits on a flag for an epoch that is
+// never published, through the same bounded wait as the sweeps, so the wait
+// gives up after limit_ns and records a timeout (wait site 4).
+__global__ void wait_selftest_kernel(const int32_t* __restrict__ flag, int32_t* __restrict__ status, uint64_t limit_ns) {
+    wait_flag(flag, INT_MAX, status, limit_ns);
+}
+
+int launch_wait_selftest(Plan& P, uint64_t limit_ns) {
+    wait_selftest_kernel<<<1, kSolveThreads, 0, P.stream>>>(P.flags, P.status, limit_ns);
+    return check_cuda("wait self-test launch");
 }
 
 template <class T, bool C>

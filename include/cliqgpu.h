@@ -184,6 +184,14 @@ int cliqgpu_profile_read(cliqgpu_plan plan, double* out, int32_t nout);
 /* Wait for all work queued on the plan's stream. */
 int cliqgpu_synchronize(cliqgpu_plan plan);
 
+/* Failure-detection check (no counterpart in the reference): one CTA waits,
+ * through the same bounded wait as the solve sweeps, on a flag that nothing
+ * sets.  The wait gives up after limit_ns (0 < limit_ns <= 2e9) and the call
+ * returns CLIQ_ERR_TIMEOUT with the wait site in cliqgpu_last_error(); the
+ * plan's status word is cleared afterwards, so the plan and the CUDA context
+ * stay usable. */
+int cliqgpu_wait_selftest(cliqgpu_plan plan, int64_t limit_ns);
+
 void cliqgpu_plan_destroy(cliqgpu_plan plan);
 
 /* Human-readable text for a status code, and the last error detail. */

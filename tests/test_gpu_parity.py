@@ -211,6 +211,32 @@ def test_schur_chunks_match_single_update(monkeypatch):
     assert rel(X1, X0) <= 1e-8
 
 
+def test_bounded_wait_times_out_and_plan_stays_usable():
+    """A device-side wait on a flag that nothing sets gives up after its
+    limit: the call reports CLIQ_ERR_TIMEOUT with the wait site, and the same
+    plan then refactors and solves correctly (no GPU fault, no hang)."""
+    import time
+    from clique_b200 import _capi
+    n = 16
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=9)
+    B = ops.random_rhs(A.n, 1, seed=1, complex_=True)
+    map_, info, L = build(A, (n, n, n), 64, precision="single")
+    X0, _, rr0 = cliq.RefinedSolve(L, B, tol=1e-11, max_iter=30)
+    lib = _capi.load()
+    t0 = time.perf_counter()
+    st = lib.cliqgpu_wait_selftest(L._h, 50_000_000)   # 50 ms
+    dt = time.perf_counter() - t0
+    assert st == _capi.CLIQ_ERR_TIMEOUT
+    assert "solve: block flag" in lib.cliqgpu_last_error().decode()
+    assert 0.04 <= dt < 5.0
+    assert lib.cliqgpu_wait_selftest(L._h, 0) == _capi.CLIQ_ERR_ARG
+    L.Initialize(A.values)
+    cliq.LDL(info, L)
+    X1, _, rr1 = cliq.RefinedSolve(L, B, tol=1e-11, max_iter=30)
+    assert rr1 <= 1e-11 and residual(A, X1, B) <= 1e-11
+    assert rel(X1, X0) <= 1e-8
+
+
 def _magnetic(dims, shift=6.5, theta=0.3):
     A = ops.laplacian_3d(*dims, shift)
     vals = A.values.astype(np.complex128)
