@@ -316,21 +316,50 @@ class DistNodalMultiVec:
         if X is not None:
             self.Pull(inverseMap, info, X)
 
+    @staticmethod
+    def _device_map(inverseMap, device):
+        import torch
+        cached = getattr(inverseMap, "_dev", None)
+        if cached is None or cached.device != device:
+            cached = torch.as_tensor(inverseMap.array, dtype=torch.int32).to(device)
+            inverseMap._dev = cached
+        return cached
+
+    @staticmethod
+    def _nodal_call(fn, inverseMap, src, dst):
+        """One pull / push kernel on the current stream (FP64 or complex128
+        device tensors, column-major n x nrhs)."""
+        import torch
+        if src.dtype not in (torch.float64, torch.complex128) or dst.dtype != src.dtype:
+            raise LogicError(_capi.CLIQ_ERR_ARG, "device multivectors must be float64 or complex128")
+        s2 = src if src.dim() == 2 else src.reshape(-1, 1)
+        d2 = dst if dst.dim() == 2 else dst.reshape(-1, 1)
+        if s2.stride(0) != 1 or d2.stride(0) != 1:
+            raise LogicError(_capi.CLIQ_ERR_ARG, "device multivectors must be column-major")
+        n, k = s2.shape
+        lds = s2.stride(1) if k > 1 else n
+        ldd = d2.stride(1) if k > 1 else n
+        perm = DistNodalMultiVec._device_map(inverseMap, src.device)
+        field = _capi.CLIQ_COMPLEX if src.is_complex() else _capi.CLIQ_REAL
+        stream = torch.cuda.current_stream(src.device).cuda_stream
+        check(fn(field, n, C.c_void_p(perm.data_ptr()), C.c_void_p(s2.data_ptr()), lds, C.c_void_p(d2.data_ptr()), ldd, k,
+                 C.c_void_p(stream)), "DistNodalMultiVec")
+
     def Pull(self, inverseMap, info, X):
         self._info = info
         if _is_torch_cuda(X):
             import torch
-            perm = torch.as_tensor(inverseMap.array, device=X.device, dtype=torch.long)
-            self.X = X[perm].clone()
+            Xn = torch.empty_like(X if X.dim() == 2 else X.reshape(-1, 1)).t().contiguous().t() if X.dim() == 2 \
+                else torch.empty_like(X)
+            self._nodal_call(_capi.load().cliqgpu_nodal_pull, inverseMap, X, Xn)
+            self.X = Xn
         else:
             X = np.asarray(X)
             self.X = np.asfortranarray(X[inverseMap.array])
 
     def Push(self, inverseMap, info, X):
         if _is_torch_cuda(X):
-            import torch
-            perm = torch.as_tensor(inverseMap.array, device=X.device, dtype=torch.long)
-            X[perm] = self.X
+            self._nodal_call(_capi.load().cliqgpu_nodal_push, inverseMap, self.X, X)
         else:
             X[inverseMap.array] = self.X
         return X

@@ -49,6 +49,13 @@ _SIGS = {
     "cliqgpu_factor": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "cliqgpu_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32]),
     "cliqgpu_multiply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
+    "cliqgpu_sparse_multiply": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                                          C.c_void_p]),
+    "cliqgpu_nodal_pull": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                     C.c_int32, C.c_void_p]),
+    "cliqgpu_nodal_push": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                     C.c_int32, C.c_void_p]),
     "cliqgpu_refine": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_double,
                                  C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "cliqgpu_get_front": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),

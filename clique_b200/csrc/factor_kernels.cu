@@ -843,7 +843,8 @@ template int run_factor<double, true>(Plan&);
 // is held by every GPU that loads the library until the process exits.  The
 // first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture.  All calls share the array and it
+// first call before any stream capture.  Every call waits for its stream and
+// reads the status word back before it returns.  All calls share the array and it
 // keeps the previous call's contents, so calls that overlap on the GPU (other
 // streams, other host threads) race: serialise them.
 // ===========================================================================
@@ -962,6 +963,10 @@ extern "C" int cliqgpu_front_ldl_noalloc(int32_t field, int32_t precision, int32
         set_last_error("front_ldl_noalloc: AL must be stored with leading dimension m");
         return CLIQ_ERR_ARG;
     }
+    if (ldabr > INT_MAX) {   // the update problem stores ABR's leading dimension as int32
+        set_last_error("front_ldl_noalloc: ldabr must not exceed INT_MAX");
+        return CLIQ_ERR_ARG;
+    }
     if (n == 0) return CLIQ_OK;
     void* scratch = nullptr;
     int st = scratch_address(&scratch);
@@ -1049,5 +1054,9 @@ extern "C" int cliqgpu_front_ldl_noalloc(int32_t field, int32_t precision, int32
         set_last_error("front_ldl_noalloc: a device-side wait timed out");
         return CLIQ_ERR_TIMEOUT;
     }
-    return out[0] == INT_MAX ? CLIQ_OK : CLIQ_ERR_ZERO_PIVOT;
+    if (out[0] != INT_MAX) {
+        set_last_error("front_ldl_noalloc: zero pivot at column " + std::to_string(out[0] - 1));
+        return CLIQ_ERR_ZERO_PIVOT;
+    }
+    return CLIQ_OK;
 }

@@ -1,5 +1,7 @@
 // Bandwidth-bound helpers: front assembly, nodal pull/push with precision
 // conversion, FP64 CSR multiply and column norms for refinement.
+#include <algorithm>
+
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
 
@@ -290,4 +292,113 @@ int launch_col_scale(Plan& P, const double* w, double* v, int nrhs, const double
     return check_cuda("col_scale");
 }
 
+// Nodal pull / push of FP64 multivectors between natural and ND order
+// (DistNodalMultiVec::Pull / Push, dist_nodal_multi_vec/impl.hpp:67-219 at P=1):
+// dir 0: Y[p, j] = X[perm[p], j]; dir 1: Y[perm[p], j] = X[p, j]
+template <bool C>
+__global__ void permute_rows_kernel(const double* __restrict__ X, int64_t ldx, double* __restrict__ Y, int64_t ldy, int64_t n,
+                                    int nrhs, const int32_t* __restrict__ perm, int dir) {
+    using W = DV<C>;
+    const int64_t total = n * nrhs;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = idx % n, j = idx / n;
+        const int64_t q = perm[p];
+        if (dir == 0) reinterpret_cast<W*>(Y)[p + j * ldy] = reinterpret_cast<const W*>(X)[q + j * ldx];
+        else reinterpret_cast<W*>(Y)[q + j * ldy] = reinterpret_cast<const W*>(X)[p + j * ldx];
+    }
+}
+
 }  // namespace cliqgpu
+
+using namespace cliqgpu;
+
+// ===========================================================================
+// cliqgpu_nodal_pull / cliqgpu_nodal_push: FP64 device multivectors between
+// natural and nested-dissection order through a device copy of the inverse
+// map (ND index -> natural index).
+// ===========================================================================
+static int permute_rows(int32_t field, int64_t n, const int32_t* inverse_map, const void* X, int64_t ldx, void* Y, int64_t ldy,
+                        int32_t nrhs, int dir, void* stream) {
+    if (n < 0 || nrhs < 0 || ldx < n || ldy < n || (n > 0 && nrhs > 0 && (!inverse_map || !X || !Y))) {
+        set_last_error("nodal pull/push: invalid sizes or pointers");
+        return CLIQ_ERR_ARG;
+    }
+    if (n == 0 || nrhs == 0) return CLIQ_OK;
+    const unsigned g = grid_for(n * nrhs, 256);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (field == CLIQ_COMPLEX)
+        permute_rows_kernel<true><<<g, 256, 0, st>>>((const double*)X, ldx, (double*)Y, ldy, n, nrhs, inverse_map, dir);
+    else
+        permute_rows_kernel<false><<<g, 256, 0, st>>>((const double*)X, ldx, (double*)Y, ldy, n, nrhs, inverse_map, dir);
+    return check_cuda(dir == 0 ? "nodal pull" : "nodal push");
+}
+
+extern "C" int cliqgpu_nodal_pull(int32_t field, int64_t n, const int32_t* inverse_map, const void* X, int64_t ldx, void* Xn,
+                                  int64_t ldn, int32_t nrhs, void* stream) {
+    return permute_rows(field, n, inverse_map, X, ldx, Xn, ldn, nrhs, 0, stream);
+}
+
+extern "C" int cliqgpu_nodal_push(int32_t field, int64_t n, const int32_t* inverse_map, const void* Xn, int64_t ldn, void* X,
+                                  int64_t ldx, int32_t nrhs, void* stream) {
+    return permute_rows(field, n, inverse_map, Xn, ldn, X, ldx, nrhs, 1, stream);
+}
+
+// ===========================================================================
+// cliqgpu_sparse_multiply: Y := alpha A X + beta Y for a CSR matrix that is not
+// held by a plan (the free function cliq::Multiply, multiply.hpp:18-21,28-166).
+// Host buffers are staged through stream-ordered device allocations.
+// ===========================================================================
+extern "C" int cliqgpu_sparse_multiply(int32_t field, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                                       const double* values, const double* alpha, const void* X, const double* beta,
+                                       void* Y, int64_t ld, int32_t nrhs, int32_t on_device, void* stream) {
+    if (n < 0 || nrhs < 0 || !alpha || !beta || (n > 0 && nrhs > 0 && (!rowptr || !colind || !values || !X || !Y)) ||
+        ld < n) {
+        set_last_error("sparse_multiply: invalid sizes or pointers");
+        return CLIQ_ERR_ARG;
+    }
+    if (n == 0 || nrhs == 0) return CLIQ_OK;
+    const bool c = field == CLIQ_COMPLEX;
+    const int w = c ? 2 : 1;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t *rp = rowptr;
+    const int32_t* ci = colind;
+    const double *va = values, *xd = (const double*)X;
+    double* yd = (double*)Y;
+    void* tmp[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int64_t nnz = 0;
+    const size_t vec = sizeof(double) * w * (size_t)ld * nrhs;
+    if (!on_device) {
+        nnz = rowptr[n];
+        const size_t sz[5] = {sizeof(int64_t) * (size_t)(n + 1), sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1),
+                              sizeof(double) * w * (size_t)std::max<int64_t>(nnz, 1), vec, vec};
+        const void* src[5] = {rowptr, colind, values, X, Y};
+        for (int i = 0; i < 5; ++i) {
+            if (cudaMallocAsync(&tmp[i], sz[i], st) != cudaSuccess) {
+                for (int k = 0; k < i; ++k) cudaFreeAsync(tmp[k], st);
+                return check_cuda("sparse_multiply: staging");
+            }
+            const size_t b = (i == 1 || i == 2) && nnz == 0 ? 0 : sz[i];
+            if (b && cudaMemcpyAsync(tmp[i], src[i], b, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                for (int k = 0; k <= i; ++k) cudaFreeAsync(tmp[k], st);
+                return check_cuda("sparse_multiply: copy in");
+            }
+        }
+        rp = (const int64_t*)tmp[0];
+        ci = (const int32_t*)tmp[1];
+        va = (const double*)tmp[2];
+        xd = (const double*)tmp[3];
+        yd = (double*)tmp[4];
+    }
+    const unsigned g = grid_for(n, 256);
+    if (c)
+        spmv_kernel<true><<<g, 256, 0, st>>>(rp, ci, va, n, cx<double>{alpha[0], alpha[1]}, xd, cx<double>{beta[0], beta[1]}, yd, ld, nrhs);
+    else
+        spmv_kernel<false><<<g, 256, 0, st>>>(rp, ci, va, n, alpha[0], xd, beta[0], yd, ld, nrhs);
+    int rc = check_cuda("sparse_multiply");
+    if (!on_device) {
+        if (rc == CLIQ_OK && cudaMemcpyAsync(Y, yd, vec, cudaMemcpyDeviceToHost, st) != cudaSuccess) rc = check_cuda("copy Y");
+        for (void* p : tmp) cudaFreeAsync(p, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess && rc == CLIQ_OK) rc = check_cuda("sparse_multiply sync");
+    }
+    return rc;
+}

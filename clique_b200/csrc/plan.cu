@@ -733,7 +733,9 @@ int read_status(Plan& P, int64_t* zero_pivot) {
         set_last_error(std::string("a device-side wait timed out at ") + sites[(st[2] >= 0 && st[2] <= 6) ? st[2] : 0]);
         return CLIQ_ERR_TIMEOUT;
     }
-    return st[0] == INT_MAX ? CLIQ_OK : CLIQ_ERR_ZERO_PIVOT;
+    if (st[0] == INT_MAX) return CLIQ_OK;
+    set_last_error("zero pivot at ND index " + std::to_string((int64_t)st[0] - 1));
+    return CLIQ_ERR_ZERO_PIVOT;
 }
 
 }  // namespace cliqgpu
@@ -1193,10 +1195,20 @@ int cliqgpu_wait_selftest(cliqgpu_plan h, int64_t limit_ns) {
     }
     Plan& P = h->p;
     if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("wait_selftest sync");
+    // the zero-pivot record of an earlier factorization survives the test
+    int32_t saved[4];
+    if (cudaMemcpy(saved, P.status, sizeof(saved), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return check_cuda("wait_selftest save");
+    const int32_t clean[4] = {INT_MAX, 0, 0, 0};
+    if (cudaMemcpy(P.status, clean, sizeof(clean), cudaMemcpyHostToDevice) != cudaSuccess)
+        return check_cuda("wait_selftest clear");
     int st = launch_wait_selftest(P, (uint64_t)limit_ns);
-    if (st == CLIQ_OK) st = read_status(P, nullptr);
-    // clear the recorded timeout: the plan stays usable
-    const int32_t st0[4] = {INT_MAX, 0, 0, 0};
+    if (st == CLIQ_OK) {
+        st = read_status(P, nullptr);
+        if (st == CLIQ_ERR_ZERO_PIVOT) st = CLIQ_OK;   // not possible here: the word was clean
+    }
+    // clear the recorded timeout (status[1..3]) and put back status[0]: the plan stays usable
+    const int32_t st0[4] = {saved[0], 0, 0, 0};
     if (cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream) != cudaSuccess ||
         cudaStreamSynchronize(P.stream) != cudaSuccess)
         return check_cuda("wait_selftest reset");

@@ -142,6 +142,27 @@ int cliqgpu_solve(cliqgpu_plan plan, void* X, int64_t ldx, int32_t nrhs,
 int cliqgpu_multiply(cliqgpu_plan plan, const double* alpha, const void* X, const double* beta,
                      void* Y, int64_t ld, int32_t nrhs);
 
+/* The same product for a CSR matrix held by no plan: the free function
+ * cliq::Multiply(alpha, A, X, beta, Y), include/clique/numeric/multiply.hpp:18-21,28-166.
+ * rowptr [n+1], colind, values (FP64, real or interleaved complex as field),
+ * X, Y: n x nrhs, leading dimension ld; all on the device (on_device = 1) or
+ * all on the host (on_device = 0: staged through stream-ordered device
+ * buffers, the call returns when Y is back on the host). */
+int cliqgpu_sparse_multiply(int32_t field, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                            const double* values, const double* alpha, const void* X, const double* beta,
+                            void* Y, int64_t ld, int32_t nrhs, int32_t on_device, void* stream);
+
+/* Natural -> ND (pull: Xn[p, j] = X[inverse_map[p], j]) and ND -> natural
+ * (push: X[inverse_map[p], j] = Xn[p, j]) reordering of FP64 device
+ * multivectors (n x nrhs, real or interleaved complex as field) through a
+ * device copy of the inverse map (ND index -> natural index), on stream.
+ * Replace cliq::DistNodalMultiVec<F>::Pull / Push at P=1,
+ * include/clique/numeric/dist_nodal_multi_vec/impl.hpp:67-219,221-... */
+int cliqgpu_nodal_pull(int32_t field, int64_t n, const int32_t* inverse_map, const void* X, int64_t ldx,
+                       void* Xn, int64_t ldn, int32_t nrhs, void* stream);
+int cliqgpu_nodal_push(int32_t field, int64_t n, const int32_t* inverse_map, const void* Xn, int64_t ldn,
+                       void* X, int64_t ldx, int32_t nrhs, void* stream);
+
 /* Mixed-precision solve: X := A^{-1} B by iterative refinement with the
  * stored factors (any precision), FP64 residuals r = B - A X and FP64
  * updates, until max_j ||r_j|| / ||b_j|| <= tol or max_iter refinement steps.
@@ -218,10 +239,13 @@ int cliqgpu_front_ldl(int32_t field, int32_t precision, int32_t conjugate, int32
  * another library's allocation lock.  All scratch lives in one fixed device
  * array inside the library (about 1.2 MB, held on every GPU that loads the
  * library until exit); nothing is allocated or freed.  Limits: n <= 1024,
- * m <= 16384, lda == m, ldabr >= m - n; larger fronts return CLIQ_ERR_ARG.
- * The first call on a device looks up the array's address (do it before any
- * stream capture).  Calls share the array, so calls that overlap on the GPU
- * race; serialise them.  Uses the CUDA-core update kernel in every precision.
+ * m <= 16384, lda == m, m - n <= ldabr <= INT_MAX; other sizes return
+ * CLIQ_ERR_ARG.  The first call on a device looks up the array's address
+ * (make it before any stream capture).  Every call waits for its stream and
+ * reads a status word back before it returns; a zero pivot returns
+ * CLIQ_ERR_ZERO_PIVOT with its column in cliqgpu_last_error().  Calls share
+ * the array, so calls that overlap on the GPU race; serialise them.  Uses
+ * the CUDA-core update kernel in every precision.
  * No counterpart in the reference (Clique allocates freely in FrontLDL). */
 int cliqgpu_front_ldl_noalloc(int32_t field, int32_t precision, int32_t conjugate, int32_t m, int32_t n,
                               void* AL, int64_t lda, void* ABR, int64_t ldabr, void* stream);

@@ -18,8 +18,7 @@
 //
 // Scalar types: double and Complex<double> factor in FP64; float and
 // Complex<float> factor in FP32 (values pass through the ABI as FP64).
-// Multiply is the reference's host-side CSR product; LDL and Solve run on
-// the device only.
+// Multiply, LDL and Solve run on the device only.
 #pragma once
 
 #include <algorithm>
@@ -193,16 +192,24 @@ void Norms(const DistMultiVec<F>& X, std::vector<double>& norms) {
     }
 }
 
-// Y := alpha A X + beta Y (host CSR product, multiply.hpp:28-166 at P=1)
+// Y := alpha A X + beta Y (multiply.hpp:28-166 at P=1), computed on the
+// device by cliqgpu_sparse_multiply (host buffers staged through device
+// memory; FP64 arithmetic for every scalar type)
 template <class F>
 void Multiply(F alpha, const DistSparseMatrix<F>& A, const DistMultiVec<F>& X, F beta, DistMultiVec<F>& Y) {
+    using D = typename std::conditional<Traits<F>::complex, Complex<double>, double>::type;
     const auto& g = A.LockedDistGraph();
-    const auto& v = A.Values();
-    for (int j = 0; j < Y.Width(); ++j)
-        for (int i = 0; i < Y.Height(); ++i) Y.SetLocal(i, j, beta * Y.GetLocal(i, j));
-    for (int i = 0; i < g.n_; ++i)
-        for (int64_t e = g.rowptr_[i]; e < g.rowptr_[i + 1]; ++e)
-            for (int j = 0; j < X.Width(); ++j) Y.UpdateLocal(i, j, alpha * v[e] * X.GetLocal(g.colind_[e], j));
+    const int n = g.n_, k = Y.Width();
+    if (X.Height() != n || Y.Height() != n || X.Width() != k) throw LogicError("Multiply: nonconformal");
+    std::vector<D> v(A.Values().begin(), A.Values().end());
+    std::vector<D> x(X.LockedBuffer(), X.LockedBuffer() + (size_t)n * k), y(Y.LockedBuffer(), Y.LockedBuffer() + (size_t)n * k);
+    const D a = D(alpha), b = D(beta);
+    Check(cliqgpu_sparse_multiply(Traits<F>::complex ? CLIQ_COMPLEX : CLIQ_REAL, n, g.rowptr_.data(), g.colind_.data(),
+                                  reinterpret_cast<const double*>(v.data()), reinterpret_cast<const double*>(&a),
+                                  x.data(), reinterpret_cast<const double*>(&b), y.data(), n, k, 0, nullptr),
+          "Multiply");
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < n; ++i) Y.SetLocal(i, j, F(y[i + (size_t)j * n]));
 }
 
 // ---- symbolic --------------------------------------------------------------

@@ -509,6 +509,11 @@ void orc_front_dims(const orc_fronts* f, int s, int* m, int* n) {
 void orc_front_set(orc_fronts* f, int s, const double* L_in) {
     if (f->is_complex) front_set_z(f->impl, s, (const zd*)L_in); else front_set_d(f->impl, s, L_in);
 }
+/* install frontL and D of node s factored elsewhere (then orc_solve uses them) */
+void orc_front_set_factored(orc_fronts* f, int s, const double* L_in, const double* d_in) {
+    if (f->is_complex) front_set_factored_z(f->impl, s, (const zd*)L_in, (const zd*)d_in);
+    else front_set_factored_d(f->impl, s, L_in, d_in);
+}
 /* Solve on a nodal multivector in ND order (N x nrhs, column-major, ld = N). */
 i64 orc_solve(orc_fronts* f, double* X, int nrhs) {
     return f->is_complex ? solve_z(f->impl, (zd*)X, nrhs) : solve_d(f->impl, X, nrhs);

@@ -50,6 +50,7 @@ def lib():
     L.orc_front_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_front_dims.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.orc_front_set.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.orc_front_set_factored.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_solve.restype = C.c_int64
     L.orc_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     L.orc_front_ldl.restype = C.c_int64
@@ -153,6 +154,14 @@ class Fronts:
         d = np.zeros(n, dt)
         lib().orc_front_get(self.h, s, _ptr(L), _ptr(d))
         return L, d
+
+    def set_factored(self, s, L, d):
+        """Install a front factored elsewhere (unit-lower L, m x n, and D)."""
+        dt = np.complex128 if self.is_complex else np.float64
+        Lf = np.asfortranarray(L, dt)
+        df = np.ascontiguousarray(d, dt)
+        assert Lf.shape == self.dims(s) and df.shape == (Lf.shape[1],)
+        lib().orc_front_set_factored(self.h, s, _ptr(Lf), _ptr(df))
 
     def solve_nodal(self, Xn):
         """In-place solve on an ND-ordered (N x nrhs) multivector; returns status."""

@@ -406,3 +406,94 @@ def test_fp32_tensor_core_fronts(oracle, complex_, split, monkeypatch):
     print(f"worst front error: tensor cores {worst_tc:.2e}, CUDA cores {worst_cc:.2e}")
     assert worst_tc <= 4 * worst_cc + 1e-6, (worst_tc, worst_cc)
     assert worst_tc <= 1e-3
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_gpu_multiply_matches_oracle(oracle, complex_):
+    """Y := alpha A X + beta Y on the device (the plan's copy of A, and the
+    plan-free cliqgpu_sparse_multiply with device and host buffers) against
+    the oracle's Multiply (multiply.hpp:28-166)."""
+    import ctypes as C
+    import torch
+    from clique_b200 import _capi
+    n = 11
+    if complex_:
+        A, _, _ = ops.helmholtz_workload_3d(n, seed=2)
+    else:
+        A = ops.laplacian_3d(n, n, n, 6.1)
+    rng = np.random.default_rng(4)
+    dt = np.complex128 if complex_ else np.float64
+    X = np.asfortranarray(ops.random_rhs(A.n, 3, seed=5, complex_=complex_))
+    Y0 = np.asfortranarray(ops.random_rhs(A.n, 3, seed=6, complex_=complex_))
+    alpha, beta = (dt(1.5 - 0.5j), dt(-0.25 + 2j)) if complex_ else (1.5, -0.25)
+    Yo = oracle.multiply(A.rowptr, A.colind, A.values, alpha, X, beta, Y0.copy(order="F"))
+    # plan-held matrix
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, 32)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+    Xt = torch.from_numpy(X).cuda().t().contiguous().t()
+    Yt = torch.from_numpy(Y0).cuda().t().contiguous().t()
+    cliq.Multiply(alpha, L, Xt, beta, Yt)
+    assert rel(Yt.cpu().numpy(), Yo) <= 1e-14
+    # plan-free product, device buffers
+    lib = _capi.load()
+    a = np.array([alpha], dt).view(np.float64)
+    b = np.array([beta], dt).view(np.float64)
+    rp = torch.from_numpy(A.rowptr).cuda()
+    ci = torch.from_numpy(A.colind).cuda()
+    va = torch.from_numpy(A.values).cuda()
+    Yt = torch.from_numpy(Y0).cuda().t().contiguous().t()
+    st = lib.cliqgpu_sparse_multiply(int(complex_), A.n, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+                                     C.c_void_p(va.data_ptr()), a.ctypes.data_as(C.c_void_p), C.c_void_p(Xt.data_ptr()),
+                                     b.ctypes.data_as(C.c_void_p), C.c_void_p(Yt.data_ptr()), A.n, 3, 1, None)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert rel(Yt.cpu().numpy(), Yo) <= 1e-14
+    # plan-free product, host buffers (the C++ drop-in's Multiply)
+    Yh = Y0.copy(order="F")
+    st = lib.cliqgpu_sparse_multiply(int(complex_), A.n, A.rowptr.ctypes.data_as(C.c_void_p),
+                                     A.colind.ctypes.data_as(C.c_void_p), A.values.ctypes.data_as(C.c_void_p),
+                                     a.ctypes.data_as(C.c_void_p), X.ctypes.data_as(C.c_void_p),
+                                     b.ctypes.data_as(C.c_void_p), Yh.ctypes.data_as(C.c_void_p), A.n, 3, 0, None)
+    assert st == 0
+    assert rel(Yh, Yo) <= 1e-14
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_nodal_pull_push_on_device(complex_):
+    """DistNodalMultiVec.Pull / Push on device tensors run the pull / push
+    kernels and match the host permutation exactly."""
+    import torch
+    n = 9
+    A = ops.laplacian_3d(n, n, n, 6.1)
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, 16)
+    inv = map_.FormInverse()
+    X = ops.random_rhs(A.n, 2, seed=3, complex_=complex_)
+    Xt = torch.from_numpy(X).cuda().t().contiguous().t()
+    nod = cliq.DistNodalMultiVec(inv, info, Xt)
+    assert np.array_equal(nod.X.cpu().numpy(), X[inv.array])
+    Yt = torch.zeros_like(Xt)
+    nod.Push(inv, info, Yt)
+    assert np.array_equal(Yt.cpu().numpy(), X)
+
+
+def test_helmholtz48_fp64_vs_oracle(oracle):
+    """The largest complex FP64 case the oracle factors in seconds: 48^3
+    Helmholtz-PML workload, cutoff 128, 4 right-hand sides."""
+    n = 48
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=0)
+    B = ops.random_rhs(A.n, 4, seed=1, complex_=True)
+    map_, info, L = build(A, (n, n, n), 128)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    oracle.enable_blas(0)
+    try:
+        S = oracle.Symbolic(n, n, n, A.rowptr, A.colind, cutoff=128)
+        F = oracle.Fronts(S, A.values, is_complex=True)
+        assert F.ldl(96) == 0
+        Xo = F.solve(B.copy(order="F"))
+    finally:
+        oracle.disable_blas()
+    err = rel(X, Xo)
+    res = residual(A, X, B)
+    print(f"48^3 FP64: vs oracle {err:.2e}, residual {res:.2e} (oracle {residual(A, Xo, B):.2e})")
+    assert err <= 1e-10
+    assert res <= 1e-12
