@@ -264,6 +264,13 @@ struct Plan {
     int64_t total_launches = 0;   // every kernel this plan has launched
     // FP32 updates on the tensor cores (tcgen05 3xTF32); CLIQGPU_TENSOR_CORES=0 selects the CUDA-core kernel
     int use_tc = 1;
+    // triangular sweeps: substitution form of the chain steps (default for
+    // FP64 storage) or the product form through the stored chain tiles M, N
+    // (default for FP32 storage); CLIQGPU_SOLVE_FORM=exact|tiles overrides
+    int solve_exact = 0;
+    // FP64 storage: updates on the FP64 tensor cores (DMMA, default) or on the
+    // CUDA cores (CLIQGPU_FP64_DMMA=0)
+    int fp64_dmma = 1;
     // FP32 storage: diagonal-block LDL in FP64 arithmetic (CLIQGPU_DIAG_FP64=1) instead of FP32
     int diag_fp64 = 0;
     bool tensor_path() const { return use_tc && precision == CLIQ_FP32; }
@@ -298,6 +305,8 @@ int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t
 int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double beta_r, double beta_i,
                 double* Y, int64_t ld, int nrhs);
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
+// out[e] = -sum_j Xbar[row(e), j] op(X[col(e), j]) over the kept matrix's pattern
+int launch_grad_pattern(Plan& P, const double* Xbar, const double* X, int64_t ld, int nrhs, int conj_x, double* out);
 // Krylov refinement: out[i][j] = <V_i[:, j], w[:, j]> (pairs), w += sign * sum_i h[i][j] V_i, v = s_j w
 int launch_multi_dot(Plan& P, const double* V, int64_t vstride, int nv, const double* w, int nrhs, double* part, double* out);
 int launch_multi_axpy(Plan& P, const double* V, int64_t vstride, int nv, const double* h, double* w, int nrhs, double sign);
@@ -310,6 +319,8 @@ int launch_wait_selftest(Plan& P, uint64_t limit_ns);
 // runs the GEMM, all on stream st
 int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack);
 size_t tc2_smem(bool cplx);
+// FP64 update C -= A D op(B)^T on the FP64 tensor cores (dmma_update.cu); same tiles as gemm_update_kernel
+int launch_dmma_update(Plan& P, const Launch& ln, cudaStream_t st);
 int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st, void* pack);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);

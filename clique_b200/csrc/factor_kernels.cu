@@ -726,6 +726,8 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
                 if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
                     launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr, st,
                                on2 ? (ln.bulk == 2 ? P.pack3 : P.pack2) : P.pack);
+                else if (std::is_same<T, double>::value && P.fp64_dmma)
+                    launch_dmma_update(P, ln, st);
                 else
                     gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(
                         P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, P.bmap + ln.gemm_map, L, p0, p1, P.D);
@@ -745,7 +747,7 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
         ++launches;
     }
     if (la) join();
-    if (P.nchain_items > 0) {
+    if (P.nchain_items > 0 && !P.solve_exact) {
         static bool ct_attr = false;
         if (!ct_attr) {
             cudaFuncSetAttribute(chain_tiles_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,

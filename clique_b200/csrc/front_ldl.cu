@@ -35,6 +35,7 @@ extern "C" int cliqgpu_front_ldl(int32_t field, int32_t precision, int32_t conju
     P.conjugate = conjugate ? 1 : 0;
     P.nb = kTile;
     if (const char* e = getenv("CLIQGPU_TENSOR_CORES")) P.use_tc = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_FP64_DMMA")) P.fp64_dmma = atoi(e) != 0;
     P.stream = (cudaStream_t)stream;
     // one node: pivots 0..n-1, update rows n..m-1
     std::vector<int32_t> size{n}, off{0}, parent{-1}, children{-1, -1}, lower(m - n), map(n);

@@ -308,6 +308,43 @@ __global__ void permute_rows_kernel(const double* __restrict__ X, int64_t ldx, d
     }
 }
 
+// Pattern-restricted gradient of a linear solve X = A^{-1} B with respect to
+// the stored entries of A: out[e] = -sum_j Xbar[row(e), j] op(X[col(e), j])
+// (op = conjugation for the conjugate-linear convention of complex autograd),
+// one warp per row, the row's entries split over the lanes.
+template <bool C, bool CJ>
+__global__ void grad_pattern_kernel(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ colind, int64_t n,
+                                    const double* __restrict__ Xbar, const double* __restrict__ X, int64_t ld, int nrhs,
+                                    double* __restrict__ out) {
+    using W = DV<C>;
+    const W* gb = reinterpret_cast<const W*>(Xbar);
+    const W* x = reinterpret_cast<const W*>(X);
+    W* o = reinterpret_cast<W*>(out);
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+        const int64_t e0 = rowptr[i], e1 = rowptr[i + 1];
+        for (int64_t e = e0 + lane; e < e1; e += 32) {
+            const int64_t c = colind[e];
+            W s{};
+            for (int j = 0; j < nrhs; ++j) mac(s, gb[i + j * ld], opc<CJ>(x[c + j * ld]));
+            o[e] = W{} - s;
+        }
+    }
+}
+
+int launch_grad_pattern(Plan& P, const double* Xbar, const double* X, int64_t ld, int nrhs, int conj_x, double* out) {
+    const unsigned g = grid_for(P.n * 32, 256);
+    if (P.cplx()) {
+        if (conj_x) grad_pattern_kernel<true, true><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.n, Xbar, X, ld, nrhs, out);
+        else grad_pattern_kernel<true, false><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.n, Xbar, X, ld, nrhs, out);
+    } else {
+        grad_pattern_kernel<false, false><<<g, 256, 0, P.stream>>>(P.rowptr, P.colind, P.n, Xbar, X, ld, nrhs, out);
+    }
+    P.total_launches += 1;
+    return check_cuda("grad_A_pattern");
+}
+
 }  // namespace cliqgpu
 
 using namespace cliqgpu;

@@ -643,8 +643,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.tinv, (size_t)P.tinv_slots * nb * nb * eb));
     TRY(dev_alloc(P, &P.dinv, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.dinvT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
-    TRY(dev_alloc(P, &P.m1, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
-    TRY(dev_alloc(P, &P.n1, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
+    // chain tiles only for the product form of the sweeps
+    const int64_t chain_elems = P.solve_exact ? 1 : std::max<int64_t>(P.dinv_elems, 1);
+    TRY(dev_alloc(P, &P.m1, (size_t)chain_elems * eb));
+    TRY(dev_alloc(P, &P.n1, (size_t)chain_elems * eb));
     TRY(dev_alloc(P, &P.hpart, (size_t)std::max<int64_t>(P.helpers_total, 1) * kTile * kSolveRhsChunk * eb));
     TRY(dev_alloc(P, &P.partial, (size_t)P.flags_total * kTile * kSolveRhsChunk * eb));
     if (P.f16_scales()) {
@@ -769,6 +771,9 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_TENSOR_CORES")) P.use_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_OUTER_BLOCK")) P.outer_nb = std::max(kTile, atoi(e));
     if (const char* e = getenv("CLIQGPU_DIAG_FP64")) P.diag_fp64 = atoi(e) != 0;
+    if (const char* e = getenv("CLIQGPU_FP64_DMMA")) P.fp64_dmma = atoi(e) != 0;
+    P.solve_exact = P.precision == CLIQ_FP64 ? 1 : 0;
+    if (const char* e = getenv("CLIQGPU_SOLVE_FORM")) P.solve_exact = strcmp(e, "tiles") != 0;
     if (const char* e = getenv("CLIQGPU_SPLIT")) P.split_f16 = strcmp(e, "tf32") != 0;
     if (const char* e = getenv("CLIQGPU_INPANEL_TC")) P.inpanel_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_REFINE")) P.refine_gmres = strcmp(e, "ir") != 0;
@@ -877,6 +882,15 @@ int cliqgpu_multiply(cliqgpu_plan h, const double* alpha, const void* X, const d
     if (!P.keep_matrix || !P.assembled) { set_last_error("multiply: plan holds no FP64 matrix"); return CLIQ_ERR_STATE; }
     const bool c = P.cplx();
     return launch_spmv(P, alpha[0], c ? alpha[1] : 0.0, (const double*)X, beta[0], c ? beta[1] : 0.0, (double*)Y, ld, nrhs);
+}
+
+int cliqgpu_grad_A_pattern(cliqgpu_plan h, const void* Xbar, const void* X, int64_t ld, int32_t nrhs, int32_t conj_x,
+                           void* out) {
+    if (!h || !Xbar || !X || !out || nrhs <= 0) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (ld < P.n) return CLIQ_ERR_ARG;
+    if (!P.keep_matrix) { set_last_error("grad_A_pattern: the plan holds no matrix pattern (keep_matrix = 0)"); return CLIQ_ERR_STATE; }
+    return launch_grad_pattern(P, (const double*)Xbar, (const double*)X, ld, nrhs, conj_x ? 1 : 0, (double*)out);
 }
 
 // ---------------------------------------------------------------------------

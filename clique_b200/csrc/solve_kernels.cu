@@ -37,6 +37,7 @@
 // and returns, and every other wait gives up as soon as it sees that word
 // set.
 #include <climits>
+#include <type_traits>
 
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
@@ -299,6 +300,10 @@ struct SweepArgs {
     const int32_t* lower;
     int nrhs;
     int32_t* status;
+    // 1: substitution form of the chain steps, x_s = L_ss^{-1} (t_s - L_{s,s-1} x_{s-1})
+    // (and its backward counterpart) with the workers publishing t_s; 0: the
+    // product form x_s = y_s - M_s x_{s-1} through the stored chain tiles
+    int exact;
 };
 
 // Forward chain of front fi: x_s = y_s - M_s x_{s-1}.  Step s multiplies the
@@ -306,14 +311,32 @@ struct SweepArgs {
 // subtracts the product from y_s (the worker's result, loaded right after
 // publishing x_{s-1} when the worker had finished, else waited for now),
 // stores and publishes x_s.
+// Substitution form (a.exact): the tile is L_{s,s-1} itself and the worker
+// publishes t_s = b_s - sum_{t <= s-2} L_st x_t; the step forms
+// v = t_s - L_{s,s-1} x_{s-1} in shared memory (sv) and x_s = L_ss^{-1} v,
+// with L_ss^{-1} loaded one step ahead.  Two dependent products per step
+// instead of one, but the rounding of the inverse enters after the
+// cancellation between t_s and L_{s,s-1} x_{s-1}, as in a triangular solve.
 template <class T, bool C, int NR>
-__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+__device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT, int r, int q, V<T, C>* sx, V<T, C>* red,
+                          V<T, C>* sv) {
     using Xv = V<T, C>;
     const T* M1 = reinterpret_cast<const T*>(a.m1);
+    const T* L = reinterpret_cast<const T*>(a.L);
+    const T* Dinv = reinterpret_cast<const T*>(a.dinv);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
+    const bool exact = std::is_same<T, double>::value && a.exact != 0;   // FP32 sweeps keep the product form
     Xv nxt[NR / kQ];
     bool have_next = false;
+    Xv dt[kE];   // exact form: L_ss^{-1} of the current step
+    auto load_m = [&](int s, Xv (&dst)[kE]) {   // the coupling tile of step s >= 1
+        if (exact)
+            row_slice<T, C>(dst, L, f.L + (int64_t)s * kTile + (int64_t)(s - 1) * kTile * f.m, f.m, r, q,
+                            min(kTile, f.n - s * kTile), kTile);
+        else
+            row_slice<T, C>(dst, M1, f.dinv + (int64_t)s * kTile * kTile, kTile, r, q, kTile, kTile);
+    };
     auto load_y = [&](int s, Xv (&v)[NR / kQ]) {
         const int ds = min(kTile, f.n - s * kTile);
 #pragma unroll
@@ -344,23 +367,38 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
             if (!wait_flag(&a.pflags[f.flag_base + s], a.epoch, a.status)) return false;
             load_y(s, tv);
         }
+        Xv xv[NR / kQ];
+        if (exact) {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) sv[r * NR + q + kQ * b] = tv[b] - u[b];
+            __syncthreads();
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<false, NR>(acc, dt, sv, q);
+            reduce_slices<NR>(acc, red, xv, r, q);
+            if (s + 1 < nT) row_slice<T, C>(dt, Dinv, f.dinv + (int64_t)(s + 1) * kTile * kTile, kTile, r, q, kTile, kTile);
+        } else {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) xv[b] = tv[b] - u[b];
+        }
         Xv* xs = sx + (s & 1) * kTile * NR;
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
             const bool in = r < ds && j < a.nrhs;
-            const Xv x = tv[b] - u[b];
-            if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, x);
-            xs[r * NR + j] = in ? x : Xv{};
+            if (in) stv<T, C>(X, f.off + r0 + r + (int64_t)j * a.ldx, xv[b]);
+            xs[r * NR + j] = in ? xv[b] : Xv{};
         }
         have_next = publish_and_test(&a.xprog[fi], s + 1, a.epoch, s + 1 < nT ? &a.pflags[f.flag_base + s + 1] : nullptr);
         if (have_next) load_y(s + 1, nxt);
-        // M_{s+2} for the step after next
-        if (s + 2 < nT) row_slice<T, C>(mt, M1, f.dinv + (int64_t)(s + 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+        // the coupling tile for the step after next
+        if (s + 2 < nT) load_m(s + 2, mt);
         return true;
     };
     Xv mA[kE], mB[kE];
-    if (nT > 1) row_slice<T, C>(mB, M1, f.dinv + (int64_t)kTile * kTile, kTile, r, q, kTile, kTile);
+    if (exact) row_slice<T, C>(dt, Dinv, f.dinv, kTile, r, q, kTile, kTile);
+    if (nT > 1) load_m(1, mB);
     for (int s = 0; s < nT; s += 2) {
         if (!step(s, mA)) return;
         if (s + 1 < nT && !step(s + 1, mB)) return;
@@ -531,10 +569,21 @@ __device__ void fwd_worker(const SweepArgs& a, const FrontDev& f, int fi, int nT
         }
         return true;
     };
-    // y_s = L_ss^{-1} (b_s - acc) with the inverse in dv
+    // y_s = L_ss^{-1} (b_s - acc) with the inverse in dv (substitution form:
+    // t_s = b_s - acc, the chain applies the inverse)
     auto finish_pivot = [&](const Xv (&dv)[kE]) {
         Xv out[NR / kQ];
         reduce_slices<NR>(acc, red, out, r, q);
+        if (std::is_same<T, double>::value && a.exact) {
+            T* Part = reinterpret_cast<T*>(a.partial);
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) {
+                const int j = q + kQ * b;
+                if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + blk) * kPartialStride + j * kTile + r, bv[b] - out[b]);
+            }
+            publish_flag(&a.pflags[f.flag_base + blk], a.epoch);
+            return;
+        }
         Xv* st = sx;   // every reader of sx passed the barrier in reduce_slices
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) st[r * NR + q + kQ * b] = bv[b] - out[b];
@@ -606,7 +655,7 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) f
     const FrontDev f = a.F[it.x];
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
     const int nT = (f.n + kTile - 1) / kTile;
-    if (it.y == kItemChain) fwd_chain<T, C, NR>(a, f, it.x, nT, r, q, sx, red);
+    if (it.y == kItemChain) fwd_chain<T, C, NR>(a, f, it.x, nT, r, q, sx, red, sq);
     else if (it.y == kItemWhole) fwd_whole<T, C, NR>(a, f, nT, r, q, sx, red, sq);
     else fwd_worker<T, C, NR>(a, f, it.x, nT, it.y, it.z, r, q, sx, red);
 }
@@ -614,14 +663,38 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) f
 // Backward chain of front fi, last pivot block first: x_c = z_c - N_c x_{c+1}
 // with z_c from the column worker; after each block the progress word counts
 // the blocks solved from the end.
+// Substitution form (a.exact): the worker publishes w_c (z_c before its
+// inverse) and the step forms v = w_c - op(L_{c+1,c})^T x_{c+1} in shared
+// memory (sv), then x_c = op(L_cc^{-1})^T v; the coupling tile is read
+// transposed from the arena (each thread a contiguous run of one column).
 template <class T, bool C, bool CJ, int NR>
-__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT, int r, int q, V<T, C>* sx, V<T, C>* red) {
+__device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT, int r, int q, V<T, C>* sx, V<T, C>* red,
+                          V<T, C>* sv) {
     using Xv = V<T, C>;
     const T* N1 = reinterpret_cast<const T*>(a.n1);
+    const T* L = reinterpret_cast<const T*>(a.L);
+    const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
+    const bool exact = std::is_same<T, double>::value && a.exact != 0;   // FP32 sweeps keep the product form
     Xv nxt[NR / kQ];
     bool have_next = false;
+    Xv dt[kE];   // exact form: op(L_cc^{-1})^T of the current step, as a row slice of the row-major inverse
+    // coupling tile of block c <= nT - 2: N_c, or (exact) element (r, k) = L[(c+1)*64 + k, c*64 + r]
+    // (op is applied in the product)
+    auto load_n = [&](int c, Xv (&dst)[kE]) {
+        if (exact) {
+            const int dc = min(kTile, f.n - c * kTile), dn = min(kTile, f.n - (c + 1) * kTile);
+            const int64_t a0 = f.L + (int64_t)(c + 1) * kTile + (int64_t)(c * kTile + r) * f.m;
+#pragma unroll
+            for (int k = 0; k < kE; ++k) {
+                const int kk = q * kE + k;
+                dst[k] = (r < dc && kk < dn) ? ldv<T, C>(L, a0 + kk) : Xv{};
+            }
+        } else {
+            row_slice<T, C>(dst, N1, f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
+        }
+    };
     auto load_z = [&](int c, Xv (&v)[NR / kQ]) {
         const int dc = min(kTile, f.n - c * kTile);
 #pragma unroll
@@ -640,7 +713,8 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
             Xv acc[NR];
 #pragma unroll
             for (int j = 0; j < NR; ++j) acc[j] = Xv{};
-            slice_mac<false, NR>(acc, nt, sx + ((i - 1) & 1) * kTile * NR, q);
+            if (exact) slice_mac<CJ, NR>(acc, nt, sx + ((i - 1) & 1) * kTile * NR, q);
+            else slice_mac<false, NR>(acc, nt, sx + ((i - 1) & 1) * kTile * NR, q);
             reduce_slices<NR>(acc, red, u, r, q);
         }
         Xv tv[NR / kQ];
@@ -651,23 +725,38 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
             if (!wait_flag(&a.pflags[f.flag_base + c], a.epoch, a.status)) return false;
             load_z(c, tv);
         }
+        Xv xv[NR / kQ];
+        if (exact) {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) sv[r * NR + q + kQ * b] = tv[b] - u[b];
+            __syncthreads();
+            Xv acc[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+            slice_mac<CJ, NR>(acc, dt, sv, q);
+            reduce_slices<NR>(acc, red, xv, r, q);
+            if (c >= 1) row_slice<T, C>(dt, DinvT, f.dinv + (int64_t)(c - 1) * kTile * kTile, kTile, r, q, kTile, kTile);
+        } else {
+#pragma unroll
+            for (int b = 0; b < NR / kQ; ++b) xv[b] = tv[b] - u[b];
+        }
         Xv* xs = sx + (i & 1) * kTile * NR;
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {
             const int j = q + kQ * b;
             const bool in = r < dc && j < a.nrhs;
-            const Xv x = tv[b] - u[b];
-            if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, x);
-            xs[r * NR + j] = in ? x : Xv{};
+            if (in) stv<T, C>(X, f.off + c0 + r + (int64_t)j * a.ldx, xv[b]);
+            xs[r * NR + j] = in ? xv[b] : Xv{};
         }
         have_next = publish_and_test(&a.xprog[fi], i + 1, a.epoch, c >= 1 ? &a.pflags[f.flag_base + c - 1] : nullptr);
         if (have_next) load_z(c - 1, nxt);
-        // N_{c-2} for the step after next
-        if (c >= 2) row_slice<T, C>(nt, N1, f.dinv + (int64_t)(c - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+        // the coupling tile for the step after next
+        if (c >= 2) load_n(c - 2, nt);
         return true;
     };
     Xv nA[kE], nB[kE];
-    if (nT > 1) row_slice<T, C>(nB, N1, f.dinv + (int64_t)(nT - 2) * kTile * kTile, kTile, r, q, kTile, kTile);
+    if (exact) row_slice<T, C>(dt, DinvT, f.dinv + (int64_t)(nT - 1) * kTile * kTile, kTile, r, q, kTile, kTile);
+    if (nT > 1) load_n(nT - 2, nB);
     for (int i = 0; i < nT; i += 2) {
         if (!step(i, nA)) return;
         if (i + 1 < nT && !step(i + 1, nB)) return;
@@ -934,6 +1023,16 @@ __device__ void bwd_worker(const SweepArgs& a, const FrontDev& f, int fi, int nT
         row_slice<T, C>(pre, reinterpret_cast<const T*>(a.dinvT), f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
 #pragma unroll
     for (int b = 0; b < NR / kQ; ++b) out[b] += hsum[b];
+    if (std::is_same<T, double>::value && a.exact) {   // substitution form: w_c = y_c - sum, the chain applies the inverse
+        T* Part = reinterpret_cast<T*>(a.partial);
+#pragma unroll
+        for (int b = 0; b < NR / kQ; ++b) {
+            const int j = q + kQ * b;
+            if (j < a.nrhs) stv<T, C>(Part, (int64_t)(f.flag_base + c) * kPartialStride + j * kTile + r, yv[b] - out[b]);
+        }
+        publish_flag(&a.pflags[f.flag_base + c], a.epoch);
+        return;
+    }
     // z_c = op(L_cc^{-1})^T (y_c - sum); every reader of sx passed the
     // barrier in reduce_slices
     Xv* st = sx;
@@ -972,7 +1071,7 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) b
     const FrontDev f = a.F[it.x];
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
     const int nT = (f.n + kTile - 1) / kTile;
-    if (it.y == kItemChain) bwd_chain<T, C, CJ, NR>(a, f, it.x, nT, r, q, sx, red);
+    if (it.y == kItemChain) bwd_chain<T, C, CJ, NR>(a, f, it.x, nT, r, q, sx, red, sx + 2 * kTile * NR);
     else if (it.y == kItemWhole) bwd_whole<T, C, CJ, NR>(a, f, nT, r, q, sx, red, sL, sidx);
     else bwd_worker<T, C, CJ, NR>(a, f, it.x, nT, it.y, it.z, it.w, r, q, sx, red, sL, sidx);
 }
@@ -1011,6 +1110,7 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     a.lower = P.lower;
     a.nrhs = nrhs;
     a.status = P.status;
+    a.exact = P.solve_exact;
     T* w0 = reinterpret_cast<T*>(P.wpool[0]);
     T* w1 = reinterpret_cast<T*>(P.wpool[1]);
     const int nlev = P.max_depth + 1;

@@ -203,6 +203,22 @@ def helmholtz_workload_2d(n, seed=0, ppw=10.0, b=5, sigma=1.5, p=2.0):
     return helmholtz_pml_2d(n, n, omega, c, b=b, sigma=sigma, p=p), omega, c
 
 
+def helmholtz_slowness_parts(n1, n2, n3, omega, b=5, sigma=1.5, p=2.0):
+    """The 3D Helmholtz-PML operator as an affine function of the per-cell
+    squared slowness m = 1 / c^2: A(m).values = base + (diag_pos -> coef * m),
+    with coef = -omega^2 s1 s2 s3 (the PML-stretched mass term of
+    examples/HelmholtzPML3D.cpp).  Returns (pattern CSR holding the base
+    values, diag_pos: CSR index of each diagonal entry, coef)."""
+    n = n1 * n2 * n3
+    base = helmholtz_pml_3d(n1, n2, n3, omega, np.full(n, np.inf), b=b, sigma=sigma, p=p)
+    unit = helmholtz_pml_3d(n1, n2, n3, omega, np.ones(n), b=b, sigma=sigma, p=p)
+    rows = np.repeat(np.arange(n), np.diff(base.rowptr))
+    diag_pos = np.nonzero(base.colind == rows)[0]
+    assert len(diag_pos) == n
+    coef = unit.values[diag_pos] - base.values[diag_pos]
+    return base, diag_pos, coef
+
+
 def random_rhs(n, nrhs, seed=0, complex_=False):
     rng = np.random.default_rng(seed)
     if complex_:

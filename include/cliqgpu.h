@@ -175,6 +175,21 @@ int cliqgpu_nodal_push(int32_t field, int64_t n, const int32_t* inverse_map, con
 int cliqgpu_refine(cliqgpu_plan plan, const void* B, void* X, int64_t ld, int32_t nrhs,
                    int32_t on_device, double tol, int32_t max_iter, int32_t* iters, double* relres);
 
+/* Gradient of X = A^{-1} B with respect to the stored entries of A, given the
+ * adjoint solution Xbar = A^{-H} (dL/dX) (A^{-T} for real data): for every
+ * entry e = (i, j) of A's pattern (the CSR given to plan_create, which must
+ * have been created with keep_matrix = 1),
+ *     out[e] = - sum_k Xbar[i, k] * op(X[j, k]),   op = conj if conj_x else identity,
+ * i.e. dL/dA = -Xbar X^H restricted to the pattern.  Xbar, X: n x nrhs, natural
+ * order, leading dimension ld, FP64 (interleaved complex as the plan's field),
+ * on the device; out: nnz entries on the device.  The adjoint solve itself is
+ * cliqgpu_solve / cliqgpu_refine with the stored factors (A = A^T for the
+ * complex-symmetric and real cases, A = A^H for the Hermitian case).
+ * No reference counterpart (Clique has no differentiation); used by the
+ * torch.autograd.Function in clique_b200/autograd.py. */
+int cliqgpu_grad_A_pattern(cliqgpu_plan plan, const void* Xbar, const void* X, int64_t ld, int32_t nrhs,
+                           int32_t conj_x, void* out);
+
 /* Copy front s back to the host: L (m x n, column-major, in the plan's
  * storage precision widened to FP64) and D (n entries, FP64).
  * Either pointer may be NULL.  dims[0..1] receives m, n.

@@ -12,7 +12,7 @@ HDR = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "cliqg
 def declared_symbols():
     src = open(HDR).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b((?:cliq|cliqgpu)_[a-z_0-9]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b((?:cliq|cliqgpu)_[A-Za-z_0-9]+)\s*\(", src)))
 
 
 def test_header_declares_entry_points():

@@ -497,3 +497,30 @@ def test_helmholtz48_fp64_vs_oracle(oracle):
     print(f"48^3 FP64: vs oracle {err:.2e}, residual {res:.2e} (oracle {residual(A, Xo, B):.2e})")
     assert err <= 1e-10
     assert res <= 1e-12
+
+
+@pytest.mark.parametrize("complex_,conjugate", [(False, False), (True, False), (True, True)])
+def test_fp64_dmma_updates_match_cuda_cores(oracle, complex_, conjugate, monkeypatch):
+    """The FP64 updates on the FP64 tensor cores (DMMA, the default) and on the
+    CUDA cores give the same fronts to FP64 rounding, and both match the oracle."""
+    dims, cutoff = (17, 15, 14), 48
+    if complex_:
+        A = _magnetic(dims) if conjugate else \
+            ops.helmholtz_pml_3d(*dims, omega=22.0, velocity=ops.smooth_velocity(dims, 2), b=3)
+    else:
+        A = ops.laplacian_3d(*dims, 6.1)
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=complex_, conjugate=conjugate)
+    assert F.ldl(96) == 0
+    fronts = {}
+    for v in ("1", "0"):
+        monkeypatch.setenv("CLIQGPU_FP64_DMMA", v)
+        map_, info, L = build(A, dims, cutoff, conjugate=conjugate)
+        fronts[v] = [L.front(s) for s in range(S.num_nodes)]
+    for s in range(S.num_nodes):
+        Lo, do = F.front(s)
+        for v in ("1", "0"):
+            Lg, dg = fronts[v][s]
+            assert rel(Lg, Lo) <= 1e-11, (v, s)
+            assert rel(dg, do) <= 1e-11, (v, s)
+        assert rel(fronts["1"][s][0], fronts["0"][s][0]) <= 1e-12
