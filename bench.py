@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass (a second FP32 plan)")
+    p.add_argument("--operator", default="helmholtz", choices=["helmholtz", "laplacian"])
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline sample")
     p.add_argument("--ref-steps", type=int, default=1, help="full-size steps of the reference arm")
     return p.parse_args()
@@ -143,11 +145,16 @@ def measured_peaks():
         return None
 
 
-def workload(n, nrhs, seed):
+def workload(n, nrhs, seed, operator="helmholtz"):
+    """(A, B, description): the seeded synthetic operator and right-hand sides."""
     from clique_b200 import operators as ops
+    if operator == "laplacian":
+        A = ops.laplacian_3d(n, n, n, 6.1)
+        B = ops.random_rhs(A.n, nrhs, seed=seed + 1, complex_=False)
+        return A, B, f"{n}^3 real 7-point Laplacian + shift (diagonal 6.1)"
     A, omega, c = ops.helmholtz_workload_3d(n, seed=seed)
     B = ops.random_rhs(A.n, nrhs, seed=seed + 1, complex_=True)
-    return A, B, omega
+    return A, B, f"{n}^3 complex-symmetric Helmholtz PML (omega={omega:.2f}, 10 ppw)"
 
 
 # ---------------------------------------------------------------------------
@@ -327,7 +334,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dist = dist_init("nccl")
 
-    A, B, omega = workload(args.n, args.nrhs, args.seed)
+    A, B, wdesc = workload(args.n, args.nrhs, args.seed, args.operator)
+    cplx = np.iscomplexobj(A.values)
     n = args.n
     stream = torch.cuda.current_stream()
     map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, args.cutoff)
@@ -335,6 +343,8 @@ def run_ours(args):
     B_d = torch.from_numpy(B).cuda().t().contiguous().t()
 
     L32 = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single", stream=stream.cuda_stream)
+    free0, total_hbm = torch.cuda.mem_get_info()
+    memory = {"fp32_plan_bytes": L32.query(3), "hbm_total_bytes": total_hbm, "hbm_used_max_bytes": total_hbm - free0}
     phase_ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
 
     def step32():
@@ -399,32 +409,47 @@ def run_ours(args):
 
     # end-to-end through the C ABI with host buffers (pinned): matrix values
     # and right-hand sides copied in, the solution copied out, every step
-    L32h = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
-    vals_h = torch.from_numpy(A.values).pin_memory().numpy()
-    nrhs_h = B.shape[1]
-    B_h = torch.empty((nrhs_h, B.shape[0]), dtype=torch.complex128, pin_memory=True).numpy().T
-    B_h[...] = B
-    X_h = torch.empty((nrhs_h, B.shape[0]), dtype=torch.complex128, pin_memory=True).numpy().T
-
-    def step_host():
-        L32h.Initialize(vals_h)
-        cliq.LDL(info, L32h)
-        return cliq.RefinedSolve(L32h, B_h, args.tol, 30, X=X_h)
-    step_host()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        Xh, ith, rrh = step_host()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    e2e_s = max_over_ranks(e2e_s, dist, "cuda")
-    del L32h
-    # the returned solution checked on the host (scipy FP64 product)
     As = A.to_scipy()
-    host_check = {"fp32ir": host_residuals(As, np.asarray(Xh), B)}
+    e2e = None
+    if args.no_e2e:
+        # the solution of the last device step, checked on the host
+        Xd, _, _ = cliq.RefinedSolve(L32, B_d, args.tol, 30)
+        host_check = {"fp32ir": host_residuals(As, Xd.cpu().numpy(), B)}
+    else:
+        L32h = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
+        vals_h = torch.from_numpy(A.values).pin_memory().numpy()
+        nrhs_h = B.shape[1]
+        hdt = torch.complex128 if cplx else torch.float64
+        B_h = torch.empty((nrhs_h, B.shape[0]), dtype=hdt, pin_memory=True).numpy().T
+        B_h[...] = B
+        X_h = torch.empty((nrhs_h, B.shape[0]), dtype=hdt, pin_memory=True).numpy().T
+
+        def step_host():
+            L32h.Initialize(vals_h)
+            cliq.LDL(info, L32h)
+            return cliq.RefinedSolve(L32h, B_h, args.tol, 30, X=X_h)
+        step_host()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            Xh, ith, rrh = step_host()
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        e2e_s = max_over_ranks(e2e_s, dist, "cuda")
+        memory["hbm_used_max_bytes"] = max(memory["hbm_used_max_bytes"], total_hbm - torch.cuda.mem_get_info()[0])
+        del L32h
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(A.values.nbytes + B.nbytes),
+               "d2h_bytes_per_step": int(B.nbytes)}
+        # the returned solution checked on the host (scipy FP64 product)
+        host_check = {"fp32ir": host_residuals(As, np.asarray(Xh), B)}
 
     fp64 = None
     if not args.no_fp64:
+        # the FP32 plan's numbers are taken: free it before the FP64 plan (at
+        # 160^3 the two do not fit in HBM together)
+        del L32
+        torch.cuda.synchronize()
         L64 = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double", stream=stream.cuda_stream)
         X64 = torch.zeros_like(B_d)
+        memory["fp64_plan_bytes"] = L64.query(3)
 
         def step64():
             L64.Initialize(vals_d)
@@ -440,6 +465,7 @@ def run_ours(args):
             step64()
         ev1.record()
         torch.cuda.synchronize()
+        memory["hbm_used_max_bytes"] = max(memory["hbm_used_max_bytes"], total_hbm - torch.cuda.mem_get_info()[0])
         fp64_ms = ev0.elapsed_time(ev1) / args.steps
         fp64_ms = max_over_ranks(fp64_ms, dist, "cuda")
         Xc = X64.cpu().numpy()
@@ -455,10 +481,10 @@ def run_ours(args):
 
     line = {"metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c64+c128-IR", "data": "synthetic",
-            "config": {"workload": f"{n}^3 complex-symmetric Helmholtz PML (omega={omega:.2f}, 10 ppw), "
-                                   f"{args.nrhs} RHS, natural ND cutoff {args.cutoff}",
-                       "precision": "CFP32 fronts, FP64 pivots, FP64 refinement", "tol": args.tol,
+            "vs_baseline": None, "dtype": "c64+c128-IR" if cplx else "f32+f64-IR", "data": "synthetic",
+            "config": {"workload": f"{wdesc}, {args.nrhs} RHS, natural ND cutoff {args.cutoff}",
+                       "precision": ("CFP32" if cplx else "FP32") + " fronts, FP64 pivots, FP64 refinement",
+                       "tol": args.tol,
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (factor arena >> 126 MB)"},
             "refine_iters": its, "relres": max(rrs), "factor_gflop": factor_flops / 1e9,
             "factor_tflops_effective": factor_flops / (ms / 1e3) / 1e12,
@@ -466,10 +492,10 @@ def run_ours(args):
             "phases_ms": {"assemble+factor": factor_phase_ms, "refined_solve": solve_phase_ms},
             "factor_profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")},
             "roofline": roofline,
-            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(A.values.nbytes + B.nbytes),
-                    "d2h_bytes_per_step": int(B.nbytes)},
+            "e2e": e2e,
             "clocks": clk.summary()}
     line["host_check"] = host_check
+    line["memory"] = memory
     line["backward_error"] = host_check["fp32ir"]["backward_error"]
     if fp64:
         line.update(fp64)

@@ -26,7 +26,8 @@ receives the sum of both entries from autograd.
 Precision: ``"double"`` factors and solves in FP64; ``"single"`` factors in
 FP32 and solves (forward and adjoint) by FP64 iterative refinement to
 ``tol``.  If another forward ran on the same solver before a backward, the
-backward refactors from the values it saved.
+backward refactors from the values it saved.  The solver's kernels run on the
+torch stream that was current when it was constructed.
 """
 from __future__ import annotations
 
@@ -51,7 +52,12 @@ class SparseLDLSolver:
         self.precision = precision
         self.tol, self.max_iter = tol, max_iter
         self.map, self.sep, self.info = NaturalNestedDissection(*dims, csr, cutoff)
-        self.L = DistSymmFrontTree(csr, self.map, self.sep, self.info, conjugate, precision=precision, keep_matrix=True)
+        # the plan runs on the torch stream current at construction, so that
+        # its kernels are ordered with the torch ops that produce and consume
+        # values, right-hand sides and gradients
+        self.stream = torch.cuda.current_stream()
+        self.L = DistSymmFrontTree(csr, self.map, self.sep, self.info, conjugate, precision=precision, keep_matrix=True,
+                                   stream=self.stream.cuda_stream)
         self.nnz = csr.nnz
         self.epoch = 0            # bumped by every factorization
         self.last_iters = []      # refinement steps of the last solves (single precision)

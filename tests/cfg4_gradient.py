@@ -87,7 +87,7 @@ def main():
                 fd = (loss_of(m0 + h * dm) - loss_of(m0 - h * dm)) / (2 * h)
                 ad = torch.dot(gm, dm)
                 rel_err.append(abs(float(fd - ad)) / abs(float(ad)))
-        out[prec] = {"loss": float(L), "forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2),
+        out[prec] = {"loss": float(L.detach()), "forward_ms": e0.elapsed_time(e1), "backward_ms": e1.elapsed_time(e2),
                      "fd_max_rel_err": max(rel_err), "fd_median_rel_err": float(np.median(rel_err)),
                      "grad_b_norm": float(bb.grad.norm()), "grad_m_norm": float(gm.norm()),
                      "refine_solves": solver.last_iters[-4:] if solver.last_iters else None}
