@@ -223,6 +223,11 @@ class DistSymmFrontTree:
         lib = _capi.load()
         h = C.c_void_p()
         self._map = np.ascontiguousarray(map.array, np.int32)
+        # None: a private stream; 0 (torch's default stream): the legacy
+        # default stream, passed as its CUDA handle 0x1 (a null handle would
+        # ask for a private stream)
+        if stream is not None and int(stream) == 0:
+            stream = 1
         check(lib.cliqgpu_plan_create(C.byref(info._view), csr.n, self._map.ctypes.data_as(C.c_void_p),
                                       csr.rowptr.ctypes.data_as(C.c_void_p), csr.colind.ctypes.data_as(C.c_void_p),
                                       C.byref(opt), C.c_void_p(stream), C.byref(h)), "DistSymmFrontTree")

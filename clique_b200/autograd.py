@@ -57,7 +57,7 @@ class SparseLDLSolver:
         # values, right-hand sides and gradients
         self.stream = torch.cuda.current_stream()
         self.L = DistSymmFrontTree(csr, self.map, self.sep, self.info, conjugate, precision=precision, keep_matrix=True,
-                                   stream=self.stream.cuda_stream)
+                                   stream=int(self.stream.cuda_stream))
         self.nnz = csr.nnz
         self.epoch = 0            # bumped by every factorization
         self.last_iters = []      # refinement steps of the last solves (single precision)

@@ -31,6 +31,26 @@ int cliq_natural_nested_dissection(int32_t nx, int32_t ny, int32_t nz, int64_t n
     return CLIQ_OK;
 }
 
+int cliq_batch_nested_dissection(int32_t count, const int32_t* dims, int64_t n, const int64_t* rowptr,
+                                 const int32_t* colind, int32_t cutoff, cliq_symbolic* out) {
+    if (!out) return CLIQ_ERR_ARG;
+    *out = nullptr;
+    cliq_symbolic h = new (std::nothrow) cliq_symbolic_s;
+    if (!h) return CLIQ_ERR_OOM;
+    int st;
+    try {
+        st = cliqgpu::batch_nested_dissection(count, dims, n, rowptr, colind, cutoff, h->s);
+    } catch (const std::bad_alloc&) {
+        st = CLIQ_ERR_OOM;
+    }
+    if (st != CLIQ_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CLIQ_OK;
+}
+
 int cliq_symbolic_info(cliq_symbolic h, cliq_symm_info* out) {
     if (!h || !out) return CLIQ_ERR_ARG;
     Symbolic& S = h->s;

@@ -36,6 +36,9 @@ struct Symbolic {
 int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* rowptr, const int32_t* colind,
                               int cutoff, Symbolic& S);
 
+int batch_nested_dissection(int count, const int32_t* dims, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                            int cutoff, Symbolic& S);
+
 void set_last_error(const std::string& msg);
 
 // ---------------------------------------------------------------------------
@@ -132,6 +135,16 @@ struct Launch {
     // every GEMM tile (one load instead of a binary search over the prefix)
     int64_t pack_map = 0, gemm_map = 0;
     int32_t pack_njobs = 0;
+    // GEMM: the launch may run either on the tensor cores (tcgen05 on the
+    // FP32 path, DMMA on the FP64 path) or on the CUDA cores; simt selects
+    // the CUDA-core kernel.  The FP32 tensor-core tiling is 128 x 128, so
+    // those launches also carry the 64 x 64 tiling of the CUDA-core kernel
+    // (alt_*); FP64 launches use 64 x 64 tiles for both kernels.
+    int32_t switchable = 0;
+    int64_t alt_prefix = -1, alt_gemm_map = 0, alt_nblocks = 0;
+    // largest M, N, K over the launch's problems and their number (the
+    // autotuner's size bucket)
+    int32_t maxM = 0, maxN = 0, maxK = 0;
 };
 
 // per-kernel-kind device time of the last profiled factorization (ms) and
@@ -290,6 +303,19 @@ struct Plan {
 
     // host-side staging for host-resident inputs/outputs
     std::vector<int32_t> hitems;
+
+    // batch runs (cliqgpu_batch_run): row segments of the independent
+    // problems, their residual norms, and the captured run
+    int64_t* seg = nullptr;           // device, nseg + 1 natural-row offsets
+    std::vector<int64_t> hseg;
+    double* segnorm = nullptr;        // device: nseg * nrhs squared norms of r, then of b
+    double* hsegnorm = nullptr;       // pinned host copy
+    int64_t segnorm_cap = 0;          // doubles
+    cudaGraphExec_t batch_exec = nullptr;
+    std::vector<int64_t> batch_key;   // arguments the captured run was recorded with
+    int64_t batch_runs = 0, batch_graph_launches = 0;
+    int batch_graph = 1;              // CLIQGPU_BATCH_GRAPH=0: direct launches only
+    int nseg_run() const { return (int)hseg.size() - 1; }
 };
 
 // launchers (factor_kernels.cu)
@@ -305,6 +331,9 @@ int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t
 int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double beta_r, double beta_i,
                 double* Y, int64_t ld, int nrhs);
 int launch_col_norms(Plan& P, const double* X, int64_t ld, int nrhs, double* out);
+// squared 2-norms per (segment of rows seg[s] .. seg[s+1]-1, column): out[j * nseg + s]
+int launch_seg_norms(Plan& P, const double* X, int64_t ld, int nrhs, int nseg, const int64_t* seg, double* out);
+int launch_reset_status(Plan& P);
 // out[e] = -sum_j Xbar[row(e), j] op(X[col(e), j]) over the kept matrix's pattern
 int launch_grad_pattern(Plan& P, const double* Xbar, const double* X, int64_t ld, int nrhs, int conj_x, double* out);
 // Krylov refinement: out[i][j] = <V_i[:, j], w[:, j]> (pairs), w += sign * sum_i h[i][j] V_i, v = s_j w
@@ -324,7 +353,18 @@ int launch_dmma_update(Plan& P, const Launch& ln, cudaStream_t st);
 int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st, void* pack);
 int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* map, const int64_t* rowptr,
                const int32_t* colind);
+int ensure_workspace(Plan& P, int nrhs);
+int solve_nodal_dispatch(Plan& P, void* xn, int nrhs);
+int run_factor_dispatch(Plan& P);
+// autotuner (batch.cu): sets Launch::simt of switchable GEMM launches from
+// the process-wide table of measured choices
+void apply_tuned_choices(Plan& P);
 void free_plan(Plan& P);
 int read_status(Plan& P, int64_t* zero_pivot);
 
 }  // namespace cliqgpu
+
+// the opaque handle of the C ABI
+struct cliqgpu_plan_s {
+    cliqgpu::Plan p;
+};

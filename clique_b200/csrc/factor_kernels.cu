@@ -678,7 +678,7 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
         cudaEventRecord(fork, captured ? s1 : P.stream);
         if (!captured) cudaStreamWaitEvent(s1, fork, 0);
         cudaStreamWaitEvent(P.stream2, fork, 0);
-        cudaStreamWaitEvent(P.stream3, fork, 0);
+        if (P.pack3) cudaStreamWaitEvent(P.stream3, fork, 0);   // stream3 only carries Schur chunks
     }
     auto join = [&]() {
         if (last_done) cudaStreamWaitEvent(s1, last_done, 0);
@@ -726,11 +726,14 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
                 if (std::is_same<T, float>::value && P.tensor_path() && !ln.simt)
                     launch_tc2(P, ln, P.profile ? P.events[3 * li + 2] : nullptr, st,
                                on2 ? (ln.bulk == 2 ? P.pack3 : P.pack2) : P.pack);
-                else if (std::is_same<T, double>::value && P.fp64_dmma)
+                else if (std::is_same<T, double>::value && P.fp64_dmma && !ln.simt)
                     launch_dmma_update(P, ln, st);
-                else
-                    gemm_update_kernel<T, C, CJ><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(
-                        P.probs + ln.items, P.prefix + ln.prefix, ln.nitems, P.bmap + ln.gemm_map, L, p0, p1, P.D);
+                else {   // CUDA cores, on the launch's 64 x 64 tiling
+                    const bool alt = ln.alt_prefix >= 0;
+                    gemm_update_kernel<T, C, CJ><<<(unsigned)(alt ? ln.alt_nblocks : ln.nblocks), kThreads, 0, st>>>(
+                        P.probs + ln.items, P.prefix + (alt ? ln.alt_prefix : ln.prefix), ln.nitems,
+                        P.bmap + (alt ? ln.alt_gemm_map : ln.gemm_map), L, p0, p1, P.D);
+                }
                 break;
         }
         if (P.profile) cudaEventRecord(P.events[3 * li + 1], st);

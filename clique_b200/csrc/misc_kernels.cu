@@ -1,6 +1,7 @@
 // Bandwidth-bound helpers: front assembly, nodal pull/push with precision
 // conversion, FP64 CSR multiply and column norms for refinement.
 #include <algorithm>
+#include <climits>
 
 #include "cliqgpu_internal.h"
 #include "device_common.cuh"
@@ -306,6 +307,49 @@ __global__ void permute_rows_kernel(const double* __restrict__ X, int64_t ldx, d
         if (dir == 0) reinterpret_cast<W*>(Y)[p + j * ldy] = reinterpret_cast<const W*>(X)[q + j * ldx];
         else reinterpret_cast<W*>(Y)[q + j * ldy] = reinterpret_cast<const W*>(X)[p + j * ldx];
     }
+}
+
+// Squared 2-norms per (segment, column): out[j * nseg + s] = sum over rows
+// seg[s] .. seg[s+1]-1 of |X[row, j]|^2 (complex: |re|^2 + |im|^2), one CTA
+// per (segment, column), fixed reduction order.
+template <bool C>
+__global__ void seg_norms_kernel(const double* __restrict__ X, int64_t ld, const int64_t* __restrict__ seg, int nseg,
+                                 double* __restrict__ out) {
+    const int sgi = blockIdx.x, j = blockIdx.y;
+    const int w = C ? 2 : 1;
+    const int64_t b = seg[sgi] * w, e = seg[sgi + 1] * w;
+    const double* x = X + (int64_t)w * j * ld;
+    double acc = 0;
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) acc = fma(x[i], x[i], acc);
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+        out[(int64_t)j * nseg + sgi] = t;
+    }
+}
+
+int launch_seg_norms(Plan& P, const double* X, int64_t ld, int nrhs, int nseg, const int64_t* seg, double* out) {
+    const dim3 grid(nseg, nrhs);
+    if (P.cplx()) seg_norms_kernel<true><<<grid, 256, 0, P.stream>>>(X, ld, seg, nseg, out);
+    else seg_norms_kernel<false><<<grid, 256, 0, P.stream>>>(X, ld, seg, nseg, out);
+    P.total_launches += 1;
+    return check_cuda("segment norms");
+}
+
+// status word := {no zero pivot, no timeout, no site, 0}, written on the
+// device so that the reset can be part of a captured graph
+__global__ void reset_status_kernel(int32_t* status) {
+    if (threadIdx.x == 0) { status[0] = INT_MAX; status[1] = 0; status[2] = 0; status[3] = 0; }
+}
+
+int launch_reset_status(Plan& P) {
+    reset_status_kernel<<<1, 32, 0, P.stream>>>(P.status);
+    P.total_launches += 1;
+    return check_cuda("status reset");
 }
 
 // Pattern-restricted gradient of a linear solve X = A^{-1} B with respect to

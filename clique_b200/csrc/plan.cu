@@ -24,9 +24,6 @@
 
 #include "cliqgpu_internal.h"
 
-struct cliqgpu_plan_s {
-    cliqgpu::Plan p;
-};
 
 namespace cliqgpu {
 
@@ -87,6 +84,10 @@ void free_plan(Plan& P) {
     for (cudaEvent_t e : P.sync_events) cudaEventDestroy(e);
     P.sync_events.clear();
     if (P.factor_exec) cudaGraphExecDestroy(P.factor_exec);
+    if (P.batch_exec) cudaGraphExecDestroy(P.batch_exec);
+    if (P.seg) cudaFree(P.seg);
+    if (P.segnorm) cudaFree(P.segnorm);
+    if (P.hsegnorm) cudaFreeHost(P.hsegnorm);
     if (P.stream1) cudaStreamDestroy(P.stream1);
     if (P.stream2) cudaStreamDestroy(P.stream2);
     if (P.stream3) cudaStreamDestroy(P.stream3);
@@ -320,14 +321,31 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         ln.prefix = (int64_t)prefix.size();
         ln.gemm_map = (int64_t)bmap.size();
         int64_t tot = 0;
-        for (auto& pr : lst) {
+        for (size_t q = 0; q < lst.size(); ++q) {
+            const GemmProb& pr = lst[q];
             prefix.push_back(tot);
             const int64_t nt = tiles_of(tc, pr.M, pr.N);
-            for (int64_t t = 0; t < nt; ++t) bmap.push_back((int32_t)probs.size() - (int32_t)ln.items);
+            for (int64_t t = 0; t < nt; ++t) bmap.push_back((int32_t)q);
             tot += nt;
-            probs.push_back(pr);
+            ln.maxM = std::max(ln.maxM, pr.M);
+            ln.maxN = std::max(ln.maxN, pr.N);
+            ln.maxK = std::max(ln.maxK, pr.K);
         }
         ln.nblocks = tot;
+        if (tc) {   // the CUDA-core kernel's 64 x 64 tiling of the same problems
+            ln.alt_prefix = (int64_t)prefix.size();
+            ln.alt_gemm_map = (int64_t)bmap.size();
+            int64_t alt = 0;
+            for (size_t q = 0; q < lst.size(); ++q) {
+                prefix.push_back(alt);
+                const int64_t nt = tiles_of(false, lst[q].M, lst[q].N);
+                for (int64_t t = 0; t < nt; ++t) bmap.push_back((int32_t)q);
+                alt += nt;
+            }
+            ln.alt_nblocks = alt;
+        }
+        ln.switchable = tc || !tcp ? 1 : 0;
+        for (auto& pr : lst) probs.push_back(pr);
         ln.depth = depth;
         P.launches.push_back(ln);
     };
@@ -527,6 +545,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
         add_gemm(schur, d, 1, false);
     }
+    apply_tuned_choices(P);   // kernel choices an earlier autotuning made for launches of the same size bucket
     P.tinv_slots = max_slots;
     P.pack_floats = tcp ? pack_max : 0;
 
@@ -700,7 +719,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     return CLIQ_OK;
 }
 
-static int ensure_workspace(Plan& P, int nrhs) {
+int ensure_workspace(Plan& P, int nrhs) {
     if (nrhs <= P.ws_nrhs) return CLIQ_OK;
     void* old[] = {P.wpool[0], P.wpool[1], P.xnodal, P.xwork, P.norms};
     for (void* p : old)
@@ -718,7 +737,7 @@ static int ensure_workspace(Plan& P, int nrhs) {
     return CLIQ_OK;
 }
 
-static int solve_nodal_dispatch(Plan& P, void* xn, int nrhs) {
+int solve_nodal_dispatch(Plan& P, void* xn, int nrhs) {
     if (P.precision == CLIQ_FP64)
         return P.cplx() ? run_solve_nodal<double, true>(P, xn, nrhs) : run_solve_nodal<double, false>(P, xn, nrhs);
     return P.cplx() ? run_solve_nodal<float, true>(P, xn, nrhs) : run_solve_nodal<float, false>(P, xn, nrhs);
@@ -780,6 +799,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_LOOKAHEAD")) P.lookahead = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_GRAPH")) P.use_graph = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_SCHUR_CHUNK")) P.schur_chunk = std::max(0, atoi(e));
+    if (const char* e = getenv("CLIQGPU_BATCH_GRAPH")) P.batch_graph = atoi(e) != 0;
     if (stream) P.stream = (cudaStream_t)stream;
     else {
         if (cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return check_cuda("stream"); }
@@ -822,6 +842,17 @@ int cliqgpu_assemble(cliqgpu_plan h, const void* values, int32_t values_on_devic
     return CLIQ_OK;
 }
 
+}  // extern "C"
+
+namespace cliqgpu {
+int run_factor_dispatch(Plan& P) {
+    if (P.precision == CLIQ_FP64) return P.cplx() ? run_factor<double, true>(P) : run_factor<double, false>(P);
+    return P.cplx() ? run_factor<float, true>(P) : run_factor<float, false>(P);
+}
+}  // namespace cliqgpu
+
+extern "C" {
+
 int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
     if (!h) return CLIQ_ERR_ARG;
     Plan& P = h->p;
@@ -829,9 +860,7 @@ int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
     if (P.factored) { set_last_error("Matrix is already factored"); return CLIQ_ERR_STATE; }
     int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
-    int st;
-    if (P.precision == CLIQ_FP64) st = P.cplx() ? run_factor<double, true>(P) : run_factor<double, false>(P);
-    else st = P.cplx() ? run_factor<float, true>(P) : run_factor<float, false>(P);
+    const int st = run_factor_dispatch(P);
     if (st != CLIQ_OK) return st;
     P.factored = true;
     return read_status(P, zero_pivot);

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "cliqgpu_internal.h"
@@ -192,6 +193,80 @@ int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* 
             for (size_t i = 0; i < S.orig_rel[s].size(); ++i) S.orig_rel[s][i] = (int)i + S.size[s];
         }
         my_off += S.size[s];
+    }
+    S.finalize_views();
+    return CLIQ_OK;
+}
+
+// Forest of independent grid problems: the block-diagonal matrix whose
+// diagonal block p is problem p (rows rowoff_p .. rowoff_p + n_p - 1, natural
+// order within the block).  Each block gets its own natural nested
+// dissection; the union numbers problem p's nodes after those of problems
+// 0 .. p-1 and its ND indices after theirs (ND block p = natural block p), so
+// the forest is in post-order with every root's parent -1.  No reference
+// counterpart (Clique factors one matrix per tree).
+int batch_nested_dissection(int count, const int32_t* dims, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                            int cutoff, Symbolic& S) {
+    if (count <= 0 || !dims || !rowptr || !colind || n <= 0 || n > INT32_MAX / 2) return CLIQ_ERR_ARG;
+    S = Symbolic{};
+    S.n = n;
+    S.map.assign(n, 0);
+    S.inv_map.assign(n, 0);
+    int64_t r0 = 0;
+    for (int p = 0; p < count; ++p) {
+        const int nx = dims[3 * p], ny = dims[3 * p + 1], nz = dims[3 * p + 2];
+        const int64_t np = (int64_t)nx * ny * nz;
+        if (nx <= 0 || ny <= 0 || nz <= 0 || r0 + np > n) {
+            set_last_error("batch_nested_dissection: problem sizes do not match the matrix");
+            return CLIQ_ERR_ARG;
+        }
+        // the diagonal block of problem p, with block-local column indices
+        std::vector<int64_t> rp(np + 1);
+        std::vector<int32_t> ci(rowptr[r0 + np] - rowptr[r0]);
+        for (int64_t i = 0; i <= np; ++i) rp[i] = rowptr[r0 + i] - rowptr[r0];
+        for (size_t e = 0; e < ci.size(); ++e) {
+            const int64_t c = colind[rowptr[r0] + (int64_t)e] - r0;
+            if (c < 0 || c >= np) {
+                set_last_error("batch_nested_dissection: the matrix is not block diagonal in the problems' rows");
+                return CLIQ_ERR_ARG;
+            }
+            ci[e] = (int32_t)c;
+        }
+        Symbolic Q;
+        const int st = natural_nested_dissection(nx, ny, nz, np, rp.data(), ci.data(), cutoff, Q);
+        if (st != CLIQ_OK) return st;
+        const int n0 = S.num_nodes, nq = Q.num_nodes, off = (int)r0;
+        auto node = [&](int t) { return (t >= 0 && t < nq) ? t + n0 : -1; };   // parents outside the problem: none
+        auto shift = [&](std::vector<int>& v) { for (int& x : v) x += off; };
+        for (int t = 0; t < nq; ++t) {
+            S.size.push_back(Q.size[t]);
+            S.off.push_back(Q.off[t] + off);
+            S.my_off.push_back(Q.my_off[t] + off);
+            S.parent.push_back(node(Q.parent[t]));
+            S.sep_parent.push_back(node(Q.sep_parent[t]));
+            S.children.push_back(node(Q.children[2 * t]));
+            S.children.push_back(node(Q.children[2 * t + 1]));
+            S.on_left.push_back(Q.on_left[t]);
+            shift(Q.lower[t]);
+            shift(Q.orig_lower[t]);
+            shift(Q.inds[t]);
+            S.lower.push_back(std::move(Q.lower[t]));
+            S.orig_lower.push_back(std::move(Q.orig_lower[t]));
+            S.orig_rel.push_back(std::move(Q.orig_rel[t]));
+            S.left_rel.push_back(std::move(Q.left_rel[t]));
+            S.right_rel.push_back(std::move(Q.right_rel[t]));
+            S.inds.push_back(std::move(Q.inds[t]));
+        }
+        for (int64_t i = 0; i < np; ++i) {
+            S.map[r0 + i] = Q.map[i] + off;
+            S.inv_map[r0 + i] = Q.inv_map[i] + off;
+        }
+        S.num_nodes += nq;
+        r0 += np;
+    }
+    if (r0 != n) {
+        set_last_error("batch_nested_dissection: the problems do not cover the matrix");
+        return CLIQ_ERR_ARG;
     }
     S.finalize_views();
     return CLIQ_OK;

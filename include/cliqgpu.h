@@ -103,7 +103,8 @@ typedef struct {
 /* Build the device front tree: front sizes and relative indices from the
  * analysis, the assembly map from A's pattern, and all HBM buffers (factor
  * arena, update stacks, workspaces).  map is natural -> ND (length n).
- * stream: cudaStream_t to run on, or NULL for a private stream.
+ * stream: cudaStream_t to run on (cudaStreamLegacy, i.e. (void*)1, for the
+ * legacy default stream), or NULL for a private non-blocking stream.
  * Replaces the structural part of cliq::DistSymmFrontTree<F>::DistSymmFrontTree
  * / Initialize, include/clique/numeric/dist_symm_front_tree/impl.hpp:24-385,
  * plus SymmetricAnalysis's relative indices (LocalSymmetricAnalysis.cpp:84-92). */
@@ -189,6 +190,47 @@ int cliqgpu_refine(cliqgpu_plan plan, const void* B, void* X, int64_t ld, int32_
  * torch.autograd.Function in clique_b200/autograd.py. */
 int cliqgpu_grad_A_pattern(cliqgpu_plan plan, const void* Xbar, const void* X, int64_t ld, int32_t nrhs,
                            int32_t conj_x, void* out);
+
+/* ======================= many problems, tuning ============================ */
+
+/* Forest of independent grid problems: natural nested dissection of each
+ * diagonal block of a block-diagonal matrix (problem p: an nx*ny*nz grid,
+ * dims[3p..3p+2], rows rowoff_p .. rowoff_p + n_p - 1 in order, no entries
+ * outside its block) and the symbolic analysis of all of them as one forest,
+ * problem by problem in post-order.  The result feeds cliqgpu_plan_create like
+ * a single analysis: every factor and solve launch then covers the fronts of
+ * all problems at one tree depth.  No reference counterpart (Clique analyses
+ * one matrix, natural_nested_dissection.hpp:17-26,447-488 per problem). */
+int cliq_batch_nested_dissection(int32_t count, const int32_t* dims, int64_t n, const int64_t* rowptr,
+                                 const int32_t* colind, int32_t cutoff, cliq_symbolic* out);
+
+/* One run over a batch plan (created from cliq_batch_nested_dissection, with
+ * keep_matrix = 1): assemble A from values (device, FP64), factor, then
+ * `steps` classical refinement steps x += A_f^{-1} r, r = b - A x (FP64) for
+ * B (device, n x nrhs, ld), writing X (device).  Problem s owns rows
+ * seg_rows[s] .. seg_rows[s+1]-1 (host array of nseg + 1 offsets, 0 .. n);
+ * relres (host, may be NULL) receives ||r_s,j|| / ||b_s,j|| for every
+ * (problem s, column j) at relres[j * nseg + s] (0 for a zero column).
+ * The first call launches the sequence directly, the second call with the
+ * same arguments records it as one CUDA graph and replays it, later calls
+ * replay it (CLIQGPU_BATCH_GRAPH=0: direct launches only).  Problems still
+ * above tol get up to max_extra further steps; *steps_taken receives the
+ * steps done.  Returns CLIQ_ERR_NOCONV if a problem stays above tol.
+ * No reference counterpart. */
+int cliqgpu_batch_run(cliqgpu_plan plan, int32_t nseg, const int64_t* seg_rows, const void* values, const void* B,
+                      void* X, int64_t ld, int32_t nrhs, int32_t steps, double tol, int32_t max_extra,
+                      double* relres, int32_t* steps_taken);
+
+/* Autotuner: times the factorization with every update launch on the tensor
+ * cores and with every one on the CUDA cores (best of reps, CUDA events around
+ * each launch), keeps the faster kernel per launch, and records the choice in
+ * a process-wide table keyed by size bucket (field, precision, update kind,
+ * log2 of the largest M, N, K and of the problem count) that later plans
+ * apply when they are built.  Needs assembled fronts and keep_matrix = 1; the
+ * plan is left factored.  report (may be NULL) receives 5 values: GEMM ms on
+ * the tensor cores, on the CUDA cores, with the choices made, launches moved
+ * to the CUDA cores, launches that could move.  No reference counterpart. */
+int cliqgpu_autotune(cliqgpu_plan plan, int32_t reps, double* report);
 
 /* Copy front s back to the host: L (m x n, column-major, in the plan's
  * storage precision widened to FP64) and D (n entries, FP64).

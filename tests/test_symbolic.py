@@ -71,3 +71,48 @@ def test_symbolic_100cubed_shape():
     assert nodes[-1].size == 100 * 100
     assert sum(n.size for n in nodes) == A.n
     assert sorted(map_.array.tolist()) == list(range(A.n))
+
+
+def test_batch_forest_is_the_union_of_the_problems():
+    """cliq_batch_nested_dissection on a block-diagonal matrix equals the
+    per-problem analyses shifted by each problem's node and row offsets."""
+    import ctypes as C
+    import clique_b200 as cliq
+    from clique_b200 import _capi, operators as ops
+    from clique_b200.batch import block_diagonal
+    rng = np.random.default_rng(1)
+    mats, dims = [], []
+    for i in range(7):
+        s = int(rng.integers(1, 24))
+        mats.append(ops.helmholtz_workload_2d(s, seed=i)[0] if s > 1 else ops.laplacian_2d(1, 1))
+        dims.append((s, s, 1))
+    mats.append(ops.laplacian_3d(5, 4, 3, 6.1))
+    dims.append((5, 4, 3))
+    A = block_diagonal([ops.CSR(M.n, M.rowptr, M.colind, M.values.astype(np.complex128)) for M in mats])
+    d = np.array([list(t) for t in dims], np.int32).reshape(-1)
+    lib = _capi.load()
+    h = C.c_void_p()
+    assert lib.cliq_batch_nested_dissection(len(mats), d.ctypes.data_as(C.c_void_p), A.n,
+                                            A.rowptr.ctypes.data_as(C.c_void_p), A.colind.ctypes.data_as(C.c_void_p),
+                                            16, C.byref(h)) == 0
+    info = cliq.DistSymmInfo(h.value, A.n)
+    m = np.zeros(A.n, np.int32)
+    lib.cliq_symbolic_map(h.value, m.ctypes.data_as(C.c_void_p), None)
+    r0 = n0 = 0
+    for B, dd in zip(mats, dims):
+        m1, _, i1 = cliq.NaturalNestedDissection(*dd, B, 16)
+        assert np.array_equal(m[r0:r0 + B.n], m1.array + r0)
+        for t in range(i1.num_nodes):
+            a, b = i1.localNodes[t], info.localNodes[n0 + t]
+            assert (a.size, a.off + r0) == (b.size, b.off)
+            assert (a.parent + n0 if 0 <= a.parent < i1.num_nodes else -1) == b.parent
+            assert np.array_equal(a.lowerStruct + r0, b.lowerStruct)
+            assert np.array_equal(a.leftRelInds, b.leftRelInds) and np.array_equal(a.rightRelInds, b.rightRelInds)
+        r0 += B.n
+        n0 += i1.num_nodes
+    assert info.num_nodes == n0
+    # a matrix that is not block diagonal in the given problems is rejected
+    bad = np.array([3, 3, 1, 3, 3, 1], np.int32)
+    Ab = ops.laplacian_2d(3, 6)
+    assert lib.cliq_batch_nested_dissection(2, bad.ctypes.data_as(C.c_void_p), Ab.n, Ab.rowptr.ctypes.data_as(C.c_void_p),
+                                            Ab.colind.ctypes.data_as(C.c_void_p), 16, C.byref(h)) == _capi.CLIQ_ERR_ARG
