@@ -239,6 +239,7 @@ class DistSymmFrontTree:
         """(Re)assemble the fronts from A's values (same pattern)."""
         lib = _capi.load()
         if _is_torch_cuda(values):
+            values = values.resolve_conj().contiguous()
             check(lib.cliqgpu_assemble(self._h, C.c_void_p(values.data_ptr()), 1), "assemble")
         else:
             v = np.ascontiguousarray(values, np.complex128 if self.is_complex else np.float64)
@@ -337,6 +338,9 @@ class DistNodalMultiVec:
         import torch
         if src.dtype not in (torch.float64, torch.complex128) or dst.dtype != src.dtype:
             raise LogicError(_capi.CLIQ_ERR_ARG, "device multivectors must be float64 or complex128")
+        if dst.is_conj():
+            raise LogicError(_capi.CLIQ_ERR_ARG, "the destination must not be a lazily conjugated view")
+        src = src.resolve_conj()
         s2 = src if src.dim() == 2 else src.reshape(-1, 1)
         d2 = dst if dst.dim() == 2 else dst.reshape(-1, 1)
         if s2.stride(0) != 1 or d2.stride(0) != 1:
@@ -383,6 +387,8 @@ class DistNodalMultiVec:
 def _solve_array(L, X, nodal):
     lib = _capi.load()
     if _is_torch_cuda(X):
+        if X.is_conj():
+            raise LogicError(_capi.CLIQ_ERR_ARG, "device right-hand sides must not be lazily conjugated views")
         assert X.is_contiguous() or X.t().is_contiguous()
         Xc = X if X.dim() == 2 else X.reshape(-1, 1)
         # column-major expected: a (n, k) tensor stored with stride (1, n)
@@ -419,6 +425,7 @@ def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20, X=None):
     rr = C.c_double()
     if _is_torch_cuda(B):
         import torch
+        B = B.resolve_conj()
         Bc = B if B.dim() == 2 else B.reshape(-1, 1)
         X = torch.zeros_like(Bc).t().contiguous().t()
         Bc = Bc.t().contiguous().t()
@@ -447,6 +454,9 @@ def Multiply(alpha, L: DistSymmFrontTree, X, beta, Y):
     dt = np.complex128 if L.is_complex else np.float64
     a = np.array([alpha], dt).view(np.float64)
     b = np.array([beta], dt).view(np.float64)
+    if Y.is_conj():
+        raise LogicError(_capi.CLIQ_ERR_ARG, "Y must not be a lazily conjugated view")
+    X = X.resolve_conj()
     Xc = X if X.dim() == 2 else X.reshape(-1, 1)
     Yc = Y if Y.dim() == 2 else Y.reshape(-1, 1)
     check(lib.cliqgpu_multiply(L._h, a.ctypes.data_as(C.c_void_p), C.c_void_p(Xc.data_ptr()), b.ctypes.data_as(C.c_void_p),

@@ -71,14 +71,14 @@ class SparseLDLSolver:
         v = values.detach()
         if not v.is_cuda or v.dtype != self.dtype or v.numel() != self.nnz:
             raise LogicError(_capi.CLIQ_ERR_ARG, f"values must be a CUDA {self.dtype} vector of {self.nnz} entries")
-        self.L.Initialize(v.contiguous())
+        self.L.Initialize(v.resolve_conj().contiguous())
         LDL(self.info, self.L)
         self.epoch += 1
 
     def solve(self, B):
         """A^{-1} B with the stored factors (B: n or n x k CUDA tensor)."""
         from . import RefinedSolve, Solve
-        B2 = B.detach().reshape(self.n, -1).to(self.dtype)
+        B2 = B.detach().resolve_conj().reshape(self.n, -1).to(self.dtype)
         if self.precision == "double":
             X = B2.t().contiguous().t().clone() if B2.shape[1] > 1 else B2.clone()
             Solve(self.info, self.L, X)
@@ -95,8 +95,9 @@ class SparseLDLSolver:
 
     def grad_pattern(self, Gb, X):
         """dL/dA on the pattern: out[e] = -sum_k Gb[i, k] conj(X[j, k])."""
-        G2 = Gb.detach().reshape(self.n, -1).to(self.dtype).t().contiguous().t()
-        X2 = X.detach().reshape(self.n, -1).to(self.dtype).t().contiguous().t()
+        # data pointers go to the C ABI: conjugate views must be materialised
+        G2 = Gb.detach().resolve_conj().reshape(self.n, -1).to(self.dtype).t().contiguous().t()
+        X2 = X.detach().resolve_conj().reshape(self.n, -1).to(self.dtype).t().contiguous().t()
         out = torch.empty(self.nnz, dtype=self.dtype, device=G2.device)
         k = G2.shape[1]
         ld = G2.stride(1) if k > 1 else self.n

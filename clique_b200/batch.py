@@ -39,6 +39,7 @@ class BatchSolver:
     """One plan over a forest of independent problems (see module docstring)."""
 
     def __init__(self, mats, dims, cutoff=64, precision="single", stream=None):
+        """stream: a torch.cuda.Stream for the plan (default: a new side stream)."""
         import torch
         from . import DistMap, DistSeparatorTree, DistSymmFrontTree, DistSymmInfo
         self.count = len(mats)
@@ -56,10 +57,11 @@ class BatchSolver:
         m = np.zeros(self.A.n, np.int32)
         check(lib.cliq_symbolic_map(h.value, m.ctypes.data_as(C.c_void_p), None))
         self.map = DistMap(m)
-        if stream is None:
-            stream = torch.cuda.current_stream().cuda_stream
+        # a torch side stream of its own: the run is captured as a CUDA graph,
+        # which the legacy default stream does not allow
+        self.stream = torch.cuda.Stream() if stream is None else stream
         self.L = DistSymmFrontTree(self.A, self.map, DistSeparatorTree(self.info), self.info, precision=precision,
-                                   keep_matrix=True, stream=int(stream))
+                                   keep_matrix=True, stream=int(self.stream.cuda_stream))
         self.is_complex = np.iscomplexobj(self.A.values)
 
     @property
@@ -86,12 +88,16 @@ class BatchSolver:
             X = torch.empty((nrhs, self.n), dtype=Bc.dtype, device=Bc.device).t()
         elif X.stride(0) != 1 or (nrhs > 1 and X.stride(1) != self.n):
             raise ValueError("X must be column-major with leading dimension n")
+        values = values.resolve_conj().contiguous()
+        Bc = Bc.resolve_conj()
         rel = np.zeros(self.count * nrhs)
         taken = C.c_int32()
+        self.stream.wait_stream(torch.cuda.current_stream())   # inputs produced on the caller's stream
         st = _capi.load().cliqgpu_batch_run(self.L._h, self.count, self.seg.ctypes.data_as(C.c_void_p),
                                             C.c_void_p(values.data_ptr()), C.c_void_p(Bc.data_ptr()),
                                             C.c_void_p(X.data_ptr()), ld, nrhs, steps, tol, max_extra,
                                             rel.ctypes.data_as(C.c_void_p), C.byref(taken))
+        torch.cuda.current_stream().wait_stream(self.stream)
         if st not in (_capi.CLIQ_OK, _capi.CLIQ_ERR_NOCONV):
             check(st, "BatchSolver.run")
         return X, rel.reshape(nrhs, self.count).T, taken.value

@@ -268,7 +268,8 @@ int cliqgpu_batch_run(cliqgpu_plan h, int32_t nseg, const int64_t* seg_rows, con
         if (cudaGraphLaunch(P.batch_exec, P.stream) != cudaSuccess) return check_cuda("batch graph launch");
         P.total_launches += P.batch_graph_launches;
         P.last_launches = P.batch_graph_launches;
-    } else if (P.batch_graph && P.batch_runs > 0) {
+    } else if (P.batch_graph && P.batch_runs > 0 && P.stream != cudaStreamLegacy && P.stream != nullptr) {
+        // (the legacy default stream cannot be captured: such plans keep direct launches)
         const int64_t before = P.total_launches;
         if (cudaStreamBeginCapture(P.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return check_cuda("batch capture");
         st = batch_issue(P, (const double*)values, (const double*)B, (double*)X, ld, nrhs, steps);

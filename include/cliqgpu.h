@@ -213,7 +213,8 @@ int cliq_batch_nested_dissection(int32_t count, const int32_t* dims, int64_t n, 
  * (problem s, column j) at relres[j * nseg + s] (0 for a zero column).
  * The first call launches the sequence directly, the second call with the
  * same arguments records it as one CUDA graph and replays it, later calls
- * replay it (CLIQGPU_BATCH_GRAPH=0: direct launches only).  Problems still
+ * replay it (CLIQGPU_BATCH_GRAPH=0, or a plan on the legacy default stream,
+ * which cannot be captured: direct launches only).  Problems still
  * above tol get up to max_extra further steps; *steps_taken receives the
  * steps done.  Returns CLIQ_ERR_NOCONV if a problem stays above tol.
  * No reference counterpart. */
