@@ -38,6 +38,9 @@ def main():
     ap.add_argument("--cutoff", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--precision", default="single", choices=["single", "double"])
+    ap.add_argument("--check-worst", type=int, default=0,
+                    help="re-solve this many of the worst problems alone (FP64 and FP32 plans) and report them")
     args = ap.parse_args()
     import torch
     from clique_b200 import operators as ops
@@ -48,7 +51,7 @@ def main():
     t0 = time.perf_counter()
     mats = [ops.helmholtz_workload_2d(int(s), seed=args.seed * 100003 + i)[0] for i, s in enumerate(sides)]
     dims = [(int(s), int(s), 1) for s in sides]
-    bs = BatchSolver(mats, dims, cutoff=args.cutoff, precision="single")
+    bs = BatchSolver(mats, dims, cutoff=args.cutoff, precision=args.precision)
     k = int(nrhs.max())
     n = bs.n
     B = np.zeros((n, k), np.complex128, order="F")
@@ -83,6 +86,25 @@ def main():
     out["launches_per_run"] = bs.last_launches()
     out["steps_taken"] = taken
     out["worst_relres_device"] = worst
+    # phases of one run, through the plan's own factor and solve entry points
+    import clique_b200 as cliq
+    torch.cuda.synchronize()
+    with torch.cuda.stream(bs.stream):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        bs.L.set_profiling(True)
+        ev[0].record()
+        bs.L.Initialize(vals)
+        cliq.LDL(bs.info, bs.L)
+        ev[1].record()
+        Xs = Bt.clone()
+        Xs = Xs.t().contiguous().t()
+        cliq.Solve(bs.info, bs.L, Xs)
+        ev[2].record()
+        torch.cuda.synchronize()
+        prof = bs.L.profile()
+        bs.L.set_profiling(False)
+    out["phases_ms"] = {"assemble+factor": ev[0].elapsed_time(ev[1]), "one_solve": ev[1].elapsed_time(ev[2]),
+                        "factor_breakdown": {k: v for k, v in prof.items() if k.endswith("_ms")}}
     # host check of every problem and column
     Xh = X.cpu().numpy()
     hw = 0.0
@@ -92,6 +114,29 @@ def main():
         R = As @ Xh[r0:r1, :nrhs[p]] - B[r0:r1, :nrhs[p]]
         hw = max(hw, float((np.linalg.norm(R, axis=0) / np.linalg.norm(B[r0:r1, :nrhs[p]], axis=0)).max()))
     out["worst_relres_host"] = hw
+    prob = rel.max(axis=1)
+    out["problems_above_tol"] = int((prob > 1e-10).sum())
+    if args.check_worst:
+        import clique_b200 as cliq
+        worst_p = np.argsort(-prob)[:args.check_worst]
+        rows = []
+        for p in worst_p:
+            A = mats[p]
+            s = int(sides[p])
+            r0, r1 = bs.seg[p], bs.seg[p + 1]
+            Bp = B[r0:r1, :nrhs[p]].copy(order="F")
+            m1, s1, i1 = cliq.NaturalNestedDissection(s, s, 1, A, args.cutoff)
+            L64 = cliq.DistSymmFrontTree(A, m1, s1, i1, precision="double")
+            cliq.LDL(i1, L64)
+            X64 = cliq.Solve(i1, L64, Bp.copy(order="F"))
+            L32 = cliq.DistSymmFrontTree(A, m1, s1, i1, precision="single")
+            cliq.LDL(i1, L32)
+            X32, it, rr = cliq.RefinedSolve(L32, Bp, 1e-10, 30)
+            As = A.to_scipy()
+            rows.append({"problem": int(p), "side": s, "nrhs": int(nrhs[p]), "batch_relres": float(prob[p]),
+                         "alone_fp64_relres": float(np.linalg.norm(As @ X64 - Bp) / np.linalg.norm(Bp)),
+                         "alone_fp32ir_relres": float(rr), "alone_fp32ir_solves": int(it)})
+        out["worst_problems"] = rows
     out["problems_per_s"] = args.count / (min(times[1:]) / 1e3) if len(times) > 1 else None
     print(json.dumps(out), flush=True)
 
