@@ -30,7 +30,6 @@
 // the epilogue multiplies by 1 / (s_i s_j).
 // Complex: Re C -= Ar Sr^T - Ai Si^T (negate-A bit), Im C -= Ar Si^T + Ai Sr^T.
 // All waits are bounded by wall-clock time and report a wait site.
-#include <algorithm>
 #include <cuda_fp16.h>
 
 #include "cliqgpu_internal.h"
@@ -179,76 +178,35 @@ __device__ __forceinline__ void pack_f16_planes(const PackJob& jb, const V<float
     }
 }
 
-// Persistent form: a fixed grid walks the launch's blocks (block b, then
-// b + gridDim.x, ...).  A thread issues the 16 loads of its row of the next
-// block before it scales, splits and stores the current one, so every
-// thread keeps a block's loads in flight while it writes (one block per CTA
-// left the launch latency-bound: a CTA's few loads and stores could not
-// cover its start-up).
 template <bool C, bool CJ>
 __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix,
                                                        const int32_t* __restrict__ bmap,
                                                        const float* __restrict__ L, const double* __restrict__ D,
                                                        const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
-                                                       float* __restrict__ out, int64_t nblocks) {
+                                                       float* __restrict__ out) {
     using X = V<float, C>;
     using W = DV<C>;
+    const int64_t bid = blockIdx.x;
+    const int lo = bmap[bid];
+    const PackJob jb = jobs[lo];
+    const int64_t blk = bid - prefix[lo];
+    const int nks = (jb.K + kKS16 - 1) / kKS16;
+    const int tile = (int)(blk / nks), ks = (int)(blk % nks);
     const int row = threadIdx.x;
-    int64_t bid = blockIdx.x;
-    if (bid >= nblocks) return;
-    // where block b sits: its job, the block within the job, tile and k step
-    auto locate = [&](int64_t b, int& lo, int64_t& blk, int& tile, int& ks) {
-        lo = bmap[b];
-        blk = b - prefix[lo];
-        const int nks = (jobs[lo].K + kKS16 - 1) / kKS16;
-        tile = (int)(blk / nks);
-        ks = (int)(blk % nks);
-    };
-    int lo, tile, ks;
-    int64_t blk;
-    locate(bid, lo, blk, tile, ks);
+    if (row >= jb.tile_rows) return;
+    const int r = tile * jb.tile_rows + row;
     X v[kKS16];
-    {
-        const PackJob& jb = jobs[lo];
-        const int r = tile * jb.tile_rows + row;
 #pragma unroll
-        for (int q = 0; q < kKS16; ++q) v[q] = row < jb.tile_rows ? pack_load<C, CJ>(jb, L, D, r, ks * kKS16 + q) : X{};
-    }
-    for (;;) {
-        const int64_t nb = bid + gridDim.x;
-        const bool more = nb < nblocks;
-        int lo2 = 0, tile2 = 0, ks2 = 0;
-        int64_t blk2 = 0;
-        X w[kKS16];
-        if (more) {   // the next block's loads, in flight while this block is written
-            locate(nb, lo2, blk2, tile2, ks2);
-            const PackJob& jn = jobs[lo2];
-            const int r2 = tile2 * jn.tile_rows + row;
+    for (int q = 0; q < kKS16; ++q) v[q] = pack_load<C, CJ>(jb, L, D, r, ks * kKS16 + q);
+    pack_f16_planes<C>(jb, v, jb.dst, jb.dst_scale, jb.emax, jb.R, blk, ks, row, r, eblk, erow, out);
+    // the S operand from the same rows (a prefix of this job's rows)
+    if (jb.RS > 0 && tile * jb.tile_rows < jb.RS) {
 #pragma unroll
-            for (int q = 0; q < kKS16; ++q) w[q] = row < jn.tile_rows ? pack_load<C, CJ>(jn, L, D, r2, ks2 * kKS16 + q) : X{};
+        for (int q = 0; q < kKS16; ++q) {
+            const int k = ks * kKS16 + q;
+            v[q] = (r < jb.RS && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.dS + k]) * opc<CJ>(v[q]) : X{};
         }
-        const PackJob jb = jobs[lo];
-        if (row < jb.tile_rows) {
-            const int r = tile * jb.tile_rows + row;
-            pack_f16_planes<C>(jb, v, jb.dst, jb.dst_scale, jb.emax, jb.R, blk, ks, row, r, eblk, erow, out);
-            // the S operand from the same rows (a prefix of this job's rows)
-            if (jb.RS > 0 && tile * jb.tile_rows < jb.RS) {
-#pragma unroll
-                for (int q = 0; q < kKS16; ++q) {
-                    const int k = ks * kKS16 + q;
-                    v[q] = (r < jb.RS && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.dS + k]) * opc<CJ>(v[q]) : X{};
-                }
-                pack_f16_planes<C>(jb, v, jb.dstS, jb.dst_scaleS, jb.emaxS, jb.RS, blk, ks, row, r, eblk, erow, out);
-            }
-        }
-        if (!more) break;
-        bid = nb;
-        lo = lo2;
-        blk = blk2;
-        tile = tile2;
-        ks = ks2;
-#pragma unroll
-        for (int q = 0; q < kKS16; ++q) v[q] = w[q];
+        pack_f16_planes<C>(jb, v, jb.dstS, jb.dst_scaleS, jb.emaxS, jb.RS, blk, ks, row, r, eblk, erow, out);
     }
 }
 
@@ -414,19 +372,8 @@ static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between, cudaStre
     if (ln.pack_blocks <= 0) {
         // operands written by the panel kernel
     } else if constexpr (F16)
-    {
-        // persistent grid: as many CTAs as fit on the GPU at once
-        static int64_t grid = 0;
-        if (!grid) {
-            int per_sm = 0, sms = 0, dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc2::pack_f16_kernel<C, CJ>, kTcBM, 0);
-            grid = (int64_t)std::max(1, sms) * std::max(1, per_sm);
-        }
-        tc2::pack_f16_kernel<C, CJ><<<(unsigned)std::min<int64_t>(ln.pack_blocks, grid), kTcBM, 0, st>>>(
-            jobs, jpre, P.bmap + ln.pack_map, L, P.D, P.eblk, P.erow, pk, ln.pack_blocks);
-    }
+        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, P.eblk, P.erow,
+                                                                                   pk);
     else
         tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, pk);
     if (between) cudaEventRecord(between, st);

@@ -96,14 +96,13 @@ def main():
         bs.L.Initialize(vals)
         cliq.LDL(bs.info, bs.L)
         ev[1].record()
-        Xs = Bt.clone()
-        Xs = Xs.t().contiguous().t()
+        Xs = Bt[:, :16].t().contiguous().t()        # one 16-column sweep chunk
         cliq.Solve(bs.info, bs.L, Xs)
         ev[2].record()
         torch.cuda.synchronize()
         prof = bs.L.profile()
         bs.L.set_profiling(False)
-    out["phases_ms"] = {"assemble+factor": ev[0].elapsed_time(ev[1]), "one_solve": ev[1].elapsed_time(ev[2]),
+    out["phases_ms"] = {"assemble+factor": ev[0].elapsed_time(ev[1]), "one_solve_16_columns": ev[1].elapsed_time(ev[2]),
                         "factor_breakdown": {k: v for k, v in prof.items() if k.endswith("_ms")}}
     # host check of every problem and column
     Xh = X.cpu().numpy()
