@@ -8,7 +8,10 @@ plan over it, so that every factor and sweep launch covers the fronts of all
 problems at one tree depth.  ``run(values, B)`` assembles, factors and
 refines all problems with ``cliqgpu_batch_run`` (captured as one CUDA graph
 from the second call on) and returns the solutions and every problem's
-relative residuals.  ``autotune()`` picks, launch by launch, the faster of
+relative residuals; a problem still above the tolerance (an unpivoted FP32
+factorization spoilt by pivot growth, or slow classical refinement) is
+solved again on its own plans with FGMRES refinement and, if needed, FP64
+fronts.  ``autotune()`` picks, launch by launch, the faster of
 the tensor-core and CUDA-core update kernels (``cliqgpu_autotune``).
 """
 from __future__ import annotations
@@ -43,6 +46,11 @@ class BatchSolver:
         import torch
         from . import DistMap, DistSeparatorTree, DistSymmFrontTree, DistSymmInfo
         self.count = len(mats)
+        self.mats = list(mats)
+        self.dims = [tuple(t) for t in dims]
+        self.cutoff = cutoff
+        self.precision = precision
+        self._alone = {}          # problem -> its own plans (fallback), built on first use
         self.A = block_diagonal(mats)
         self.sizes = np.array([A.n for A in mats], np.int64)
         self.seg = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
@@ -75,9 +83,48 @@ class BatchSolver:
         return {"tensor_ms": out[0], "cuda_core_ms": out[1], "chosen_ms": out[2], "moved_to_cuda_cores": int(out[3]),
                 "switchable": int(out[4])}
 
-    def run(self, values, B, X=None, steps=4, tol=1e-10, max_extra=8):
+    def _solve_alone(self, p, values, Bc, X, tol):
+        """Problem p on its own plans: FP32 fronts + FGMRES refinement, then, if
+        that stalls (an unpivoted FP32 factorization spoilt by pivot growth),
+        FP64 fronts + FP64 refinement.  Writes X's rows of p; returns
+        (relative residual, precision used)."""
+        import torch
+        from . import LDL, DistSymmFrontTree, NaturalNestedDissection, RefinedSolve
+        r0, r1 = int(self.seg[p]), int(self.seg[p + 1])
+        e0, e1 = int(self.A.rowptr[r0]), int(self.A.rowptr[r1])
+        vals = values[e0:e1].contiguous()
+        Bp = Bc[r0:r1]
+        nz = Bp.abs().amax(dim=0) > 0
+        if not bool(nz.any()):
+            X[r0:r1] = 0
+            return 0.0, "none"
+        if p not in self._alone:
+            A = self.mats[p]
+            m, sp, info = NaturalNestedDissection(*self.dims[p], A, self.cutoff)
+            self._alone[p] = {"A": A, "map": m, "sep": sp, "info": info, "plans": {}}
+        ent = self._alone[p]
+        best = (np.inf, None, None)
+        for prec in (["single", "double"] if self.precision == "single" else ["double"]):
+            if prec not in ent["plans"]:
+                ent["plans"][prec] = DistSymmFrontTree(ent["A"], ent["map"], ent["sep"], ent["info"], precision=prec,
+                                                       keep_matrix=True, stream=int(self.stream.cuda_stream))
+            L = ent["plans"][prec]
+            L.Initialize(vals)
+            LDL(ent["info"], L)
+            Xp, it, rr = RefinedSolve(L, Bp.t().contiguous().t(), tol, 30)
+            if rr < best[0]:
+                best = (rr, prec, Xp)
+            if rr <= tol:
+                break
+        X[r0:r1] = best[2]
+        return float(best[0]), best[1]
+
+    def run(self, values, B, X=None, steps=4, tol=1e-10, max_extra=8, fallback=True):
         """Assemble values (device, the block-diagonal CSR order), factor, refine
-        B (device, n x nrhs column-major).  Returns (X, relres[count, nrhs], steps)."""
+        B (device, n x nrhs column-major).  Returns (X, relres[count, nrhs], steps).
+        Problems still above tol after the batch run are solved again on their
+        own plans (fallback=True; see _solve_alone): self.last_fallback lists
+        them with the residual and precision they reached."""
         import torch
         Bc = B if B.dim() == 2 else B.reshape(-1, 1)
         nrhs = Bc.shape[1]
@@ -100,7 +147,16 @@ class BatchSolver:
         torch.cuda.current_stream().wait_stream(self.stream)
         if st not in (_capi.CLIQ_OK, _capi.CLIQ_ERR_NOCONV):
             check(st, "BatchSolver.run")
-        return X, rel.reshape(nrhs, self.count).T, taken.value
+        rel = rel.reshape(nrhs, self.count).T.copy()
+        self.last_fallback = []
+        if fallback and st == _capi.CLIQ_ERR_NOCONV:
+            with torch.cuda.stream(self.stream):
+                for p in np.nonzero(rel.max(axis=1) > tol)[0]:
+                    rr, prec = self._solve_alone(int(p), values, Bc, X, tol)
+                    rel[p, :] = np.minimum(rel[p, :], rr) if prec == "none" else rr
+                    self.last_fallback.append({"problem": int(p), "relres": rr, "precision": prec})
+            torch.cuda.current_stream().wait_stream(self.stream)
+        return X, rel, taken.value
 
     def last_launches(self):
         return self.L.last_launches()

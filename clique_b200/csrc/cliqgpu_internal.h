@@ -78,6 +78,8 @@ struct FrontDev {
     int32_t pool;       // parity of the depth
     int32_t flag_base;  // first pivot-block slot of this front (worker flag, worker result)
     int64_t dinv;       // inverse diagonal blocks (ceil(n/64) blocks of 64 x 64) in the dinv store
+    int64_t chain;      // chain tiles (ceil(n/64) blocks of 64 x 64) in the m1 / n1 stores; -1: the front has
+                        // none (solved by one CTA, or the sweeps use the substitution form)
     int32_t hbase;      // backward sweep: first helper slot ((nch - 1) per pivot block)
     int32_t nch;        // backward sweep: 16-tile chunks of the rows below the pivots
     int64_t eblk;       // 2xFP16 split: per (row, 64-column block) largest |component| of L and of D op(L), m x nT
@@ -206,6 +208,7 @@ struct Plan {
     void* n1 = nullptr;
     int32_t* chain_items = nullptr;   // int4 {front, block b >= 1, 0, 0} of every chain front
     int32_t nchain_items = 0;
+    int64_t chain_elems = 0;          // elements of m1 / n1 (chain fronts only)
     unsigned long long* xprog = nullptr;   // per front: (epoch << 32) | blocks its chain has published
     void* hpart = nullptr;        // backward helpers' partial sums (kSolveRhsChunk x 64 per helper)
     int64_t helpers_total = 0;

@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(kThreads) chain_tiles_kernel(const FrontDev* _
 #pragma unroll
             for (int j = 0; j < 4; ++j) mac(acc[i][j], a[i], s[j]);
     }
-    X* M = reinterpret_cast<X*>(m1) + f.dinv + (int64_t)b * nb * nb;
+    X* M = reinterpret_cast<X*>(m1) + f.chain + (int64_t)b * nb * nb;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(kThreads) chain_tiles_kernel(const FrontDev* _
 #pragma unroll
             for (int j = 0; j < 4; ++j) mac(acc[i][j], a[i], s[j]);
     }
-    X* N = reinterpret_cast<X*>(n1) + f.dinv + (int64_t)(b - 1) * nb * nb;
+    X* N = reinterpret_cast<X*>(n1) + f.chain + (int64_t)(b - 1) * nb * nb;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -985,7 +985,7 @@ extern "C" int cliqgpu_front_ldl_noalloc(int32_t field, int32_t precision, int32
     // host-side schedule for the single front (the whole tree has one node)
     FrontDev f{};
     f.L = 0; f.U = 0; f.CU[0] = f.CU[1] = -1; f.cmap = -1; f.lower = 0; f.W = 0;
-    f.m = m; f.n = n; f.off = 0; f.u = u; f.pool = 0; f.flag_base = 0; f.dinv = 0;
+    f.m = m; f.n = n; f.off = 0; f.u = u; f.pool = 0; f.flag_base = 0; f.dinv = 0; f.chain = -1;
     std::vector<int4> items;
     std::vector<GemmProb> probs;
     std::vector<int64_t> prefix;

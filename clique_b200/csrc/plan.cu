@@ -135,6 +135,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     std::vector<int64_t> level_pool(P.max_depth + 1, 0), level_w(P.max_depth + 1, 0);
     P.factor_flops = P.solve_flops = P.factor_entries = 0;
     P.dinv_elems = 0;
+    P.chain_elems = 0;
     P.eblk_total = P.erow_total = 0;
     for (int s = 0; s < nn; ++s) {
         FrontDev& f = P.hfronts[s];
@@ -159,6 +160,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         f.erow = P.erow_total;
         P.erow_total += f.m;
         f.cmap = -1;
+        f.chain = -1;
         f.CU[0] = f.CU[1] = -1;
         f.CW[0] = f.CW[1] = 0;
         f.cu[0] = f.cu[1] = 0;
@@ -576,6 +578,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             f.flag_base = flag;
             flag += nT;
             if (whole(f)) continue;
+            if (!P.solve_exact) {   // chain tiles: only fronts whose sweeps run a chain in the product form
+                f.chain = P.chain_elems;
+                P.chain_elems += (int64_t)nT * kTile * kTile;
+            }
             push_item(s, kItemChain, 0, 0);
             for (int rb = 0; rb < nT; ++rb) push_item(s, kItemPivotRows, rb, 0);
             for (int b = 1; b < nT; ++b) {
@@ -663,7 +669,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_alloc(P, &P.dinv, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     TRY(dev_alloc(P, &P.dinvT, (size_t)std::max<int64_t>(P.dinv_elems, 1) * eb));
     // chain tiles only for the product form of the sweeps
-    const int64_t chain_elems = P.solve_exact ? 1 : std::max<int64_t>(P.dinv_elems, 1);
+    const int64_t chain_elems = std::max<int64_t>(P.chain_elems, 1);
     TRY(dev_alloc(P, &P.m1, (size_t)chain_elems * eb));
     TRY(dev_alloc(P, &P.n1, (size_t)chain_elems * eb));
     TRY(dev_alloc(P, &P.hpart, (size_t)std::max<int64_t>(P.helpers_total, 1) * kTile * kSolveRhsChunk * eb));

@@ -335,7 +335,7 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
             row_slice<T, C>(dst, L, f.L + (int64_t)s * kTile + (int64_t)(s - 1) * kTile * f.m, f.m, r, q,
                             min(kTile, f.n - s * kTile), kTile);
         else
-            row_slice<T, C>(dst, M1, f.dinv + (int64_t)s * kTile * kTile, kTile, r, q, kTile, kTile);
+            row_slice<T, C>(dst, M1, f.chain + (int64_t)s * kTile * kTile, kTile, r, q, kTile, kTile);
     };
     auto load_y = [&](int s, Xv (&v)[NR / kQ]) {
         const int ds = min(kTile, f.n - s * kTile);
@@ -692,7 +692,7 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
                 dst[k] = (r < dc && kk < dn) ? ldv<T, C>(L, a0 + kk) : Xv{};
             }
         } else {
-            row_slice<T, C>(dst, N1, f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
+            row_slice<T, C>(dst, N1, f.chain + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
         }
     };
     auto load_z = [&](int c, Xv (&v)[NR / kQ]) {

@@ -81,6 +81,7 @@ def main():
         times.append(e0.elapsed_time(e1))
         worst.append(float(rel.max()))
         taken.append(st)
+    out["fallback"] = bs.last_fallback
     out["run_ms"] = times
     out["run_kinds"] = ["direct", "recorded+replayed"] + ["replay"] * max(0, args.runs - 2)
     out["launches_per_run"] = bs.last_launches()

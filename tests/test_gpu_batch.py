@@ -125,3 +125,33 @@ def test_autotune_keeps_results_and_reports():
     bs2 = BatchSolver(mats, dims, cutoff=32, precision="single")
     X2, rel2, _ = bs2.run(vals, Bt, steps=4, tol=1e-10)
     _check(mats, X2.cpu().numpy(), B, 1e-10)
+
+
+def test_batch_fallback_rescues_a_problem_fp32_cannot_factor():
+    """One problem whose first pivot (ND order) is 1e-8 of its neighbours:
+    the unpivoted FP32 factorization grows by ~1e8 and its refinement stalls,
+    so the batch run leaves it above the tolerance; the fallback re-solves it
+    on its own plans (FP64 fronts if FP32 + FGMRES does not reach tol).  The
+    other problems keep the batch solution."""
+    import torch
+    mats, dims, nrhs = _problems(5, 6, lo=16, hi=32)
+    s = 20
+    bad = ops.laplacian_2d(s, s, 4.0)
+    m1, _, _ = cliq.NaturalNestedDissection(s, s, 1, bad, 32)
+    first = int(np.nonzero(m1.array == 0)[0][0])          # natural index of ND index 0
+    rows = np.repeat(np.arange(bad.n), np.diff(bad.rowptr))
+    e = np.nonzero((rows == first) & (bad.colind == first))[0][0]
+    vals = bad.values.astype(np.complex128)
+    vals[e] = 4e-8
+    bad = ops.CSR(bad.n, bad.rowptr, bad.colind, vals)
+    mats = mats + [bad]
+    dims = dims + [(s, s, 1)]
+    nrhs = np.concatenate([nrhs, [2]])
+    bs = BatchSolver(mats, dims, cutoff=32, precision="single")
+    B = _rhs(mats, nrhs, 17)
+    v = torch.from_numpy(bs.A.values).cuda()
+    Bt = torch.from_numpy(B).cuda().t().contiguous().t()
+    X, rel, _ = bs.run(v, Bt, steps=4, tol=1e-10, max_extra=2)
+    assert [f["problem"] for f in bs.last_fallback] == [len(mats) - 1], bs.last_fallback
+    assert rel.max() <= 1e-10
+    _check(mats, X.cpu().numpy(), B, 1e-10)
