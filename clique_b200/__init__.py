@@ -40,10 +40,15 @@ __all__ = [
 
 
 class SymmFrontType:
-    """Subset of the reference's SymmFrontType enum (dist_symm_front_tree/decl.hpp:17-26)."""
+    """The reference's SymmFrontType enum (dist_symm_front_tree/decl.hpp:17-26), same values."""
     SYMM_1D, SYMM_2D, LDL_1D, LDL_2D = 0, 1, 2, 3
     LDL_SELINV_1D, LDL_SELINV_2D, LDL_INTRAPIV_1D, LDL_INTRAPIV_2D = 4, 5, 6, 7
-    SUPPORTED = (LDL_1D, LDL_2D)
+    LDL_INTRAPIV_SELINV_1D, LDL_INTRAPIV_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D = 8, 9, 10, 11
+    BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D = 12, 13
+    # unpivoted LDL and its selective-inversion forms: at one process the
+    # reference inverts no local front for the latter (change_front_type.hpp:
+    # 86-98 inverts distributed nodes 1 ..), so they factor and solve as LDL
+    SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D)
 
 
 # ---------------------------------------------------------------------------
@@ -302,8 +307,9 @@ class DistSymmFrontTree:
 def LDL(info, L: DistSymmFrontTree, frontType=SymmFrontType.LDL_2D):
     """Multifrontal LDL^T in place (ldl.hpp:57-75).  Returns None; raises on a zero pivot."""
     if frontType not in SymmFrontType.SUPPORTED:
-        raise LogicError(_capi.CLIQ_ERR_ARG, "only the unpivoted LDL_1D / LDL_2D front types are provided")
-    if L.frontType in (SymmFrontType.LDL_1D, SymmFrontType.LDL_2D):
+        raise LogicError(_capi.CLIQ_ERR_ARG, "only the unpivoted LDL_1D / LDL_2D (and LDL_SELINV_1D / LDL_SELINV_2D) "
+                                             "front types are provided")
+    if L.frontType not in (SymmFrontType.SYMM_1D, SymmFrontType.SYMM_2D):
         raise LogicError(_capi.CLIQ_ERR_STATE, "Matrix is already factored")
     zp = C.c_int64(-1)
     st = _capi.load().cliqgpu_factor(L._h, C.byref(zp))
@@ -407,7 +413,7 @@ def _solve_array(L, X, nodal):
 def Solve(info, L: DistSymmFrontTree, X):
     """Forward, diagonal and backward solves (solve.hpp:41-65), in place.
     X: a DistNodalMultiVec (ND order), or a natural-order array (Pull/Push done on the device)."""
-    if L.frontType not in (SymmFrontType.LDL_1D, SymmFrontType.LDL_2D):
+    if L.frontType not in SymmFrontType.SUPPORTED:
         raise LogicError(_capi.CLIQ_ERR_STATE, "Invalid front type for solve (factor with LDL first)")
     if isinstance(X, DistNodalMultiVec):
         _solve_array(L, X.X, nodal=True)

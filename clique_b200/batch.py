@@ -119,7 +119,7 @@ class BatchSolver:
         X[r0:r1] = best[2]
         return float(best[0]), best[1]
 
-    def run(self, values, B, X=None, steps=4, tol=1e-10, max_extra=8, fallback=True):
+    def run(self, values, B, X=None, steps=6, tol=1e-10, max_extra=2, fallback=True):
         """Assemble values (device, the block-diagonal CSR order), factor, refine
         B (device, n x nrhs column-major).  Returns (X, relres[count, nrhs], steps).
         Problems still above tol after the batch run are solved again on their

@@ -274,7 +274,16 @@ inline void NaturalNestedDissection(int nx, int ny, int nz, const DistGraph& gra
 }
 
 // ---- numeric ---------------------------------------------------------------
-enum SymmFrontType { SYMM_1D, SYMM_2D, LDL_1D, LDL_2D };
+// the reference's enum (dist_symm_front_tree/decl.hpp:17-26), same order
+enum SymmFrontType {
+    SYMM_1D, SYMM_2D, LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D, LDL_INTRAPIV_1D, LDL_INTRAPIV_2D,
+    LDL_INTRAPIV_SELINV_1D, LDL_INTRAPIV_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D, BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D
+};
+inline bool Unfactored(SymmFrontType t) { return t == SYMM_1D || t == SYMM_2D; }
+// front types this library factors: unpivoted LDL, and its selective-inversion
+// forms, which at one process invert no local front (change_front_type.hpp:86-98
+// inverts distributed nodes 1 .. only), so they factor and solve as LDL
+inline bool Provided(SymmFrontType t) { return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D; }
 
 template <class F>
 class DistSymmFrontTree {
@@ -325,8 +334,9 @@ private:
 
 template <class F>
 void LDL(DistSymmInfo&, DistSymmFrontTree<F>& L, SymmFrontType newFrontType = LDL_2D) {
-    if (L.frontType == LDL_1D || L.frontType == LDL_2D) throw LogicError("Matrix is already factored");
-    if (newFrontType != LDL_1D && newFrontType != LDL_2D) throw LogicError("Only unpivoted LDL_1D / LDL_2D are provided");
+    if (!Unfactored(L.frontType)) throw LogicError("Matrix is already factored");
+    if (!Provided(newFrontType))
+        throw LogicError("Only the unpivoted LDL_1D / LDL_2D (and LDL_SELINV_1D / LDL_SELINV_2D) front types are provided");
     int64_t zp = -1;
     Check(cliqgpu_factor(L.Plan(), &zp), "LDL");
     L.frontType = newFrontType;
@@ -358,7 +368,7 @@ private:
 
 template <class F>
 void Solve(const DistSymmInfo&, const DistSymmFrontTree<F>& L, DistNodalMultiVec<F>& X) {
-    if (L.frontType != LDL_1D && L.frontType != LDL_2D) throw LogicError("Invalid front type for solve");
+    if (!Provided(L.frontType)) throw LogicError("Invalid front type for solve");
     const int n = X.Height(), w = X.Width();
     if constexpr (std::is_same<F, double>::value || std::is_same<F, Complex<double>>::value) {
         Check(cliqgpu_solve(L.Plan(), X.data.data(), n, w, 0, 1), "Solve");

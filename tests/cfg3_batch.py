@@ -34,7 +34,8 @@ def main():
     ap.add_argument("--hi", type=int, default=256)
     ap.add_argument("--rhs-hi", type=int, default=64)
     ap.add_argument("--runs", type=int, default=5)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--max-extra", type=int, default=2)
     ap.add_argument("--cutoff", type=int, default=64)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true")
@@ -75,7 +76,7 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record()
-        X, rel, st = bs.run(vals, Bt, X=X, steps=args.steps, tol=1e-10)
+        X, rel, st = bs.run(vals, Bt, X=X, steps=args.steps, tol=1e-10, max_extra=args.max_extra)
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))

@@ -524,3 +524,25 @@ def test_fp64_dmma_updates_match_cuda_cores(oracle, complex_, conjugate, monkeyp
             assert rel(Lg, Lo) <= 1e-11, (v, s)
             assert rel(dg, do) <= 1e-11, (v, s)
         assert rel(fronts["1"][s][0], fronts["0"][s][0]) <= 1e-12
+
+
+def test_selinv_front_types_factor_and_solve_as_ldl():
+    """LDL_SELINV_1D / LDL_SELINV_2D at one process: the reference inverts only
+    distributed fronts (change_front_type.hpp:86-98), so the factorization and
+    the solve are the LDL_2D ones; pivoted and block types are refused."""
+    n = 12
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=4)
+    B = ops.random_rhs(A.n, 2, seed=5, complex_=True)
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, 64)
+    X = {}
+    for ft in (cliq.SymmFrontType.LDL_2D, cliq.SymmFrontType.LDL_SELINV_2D, cliq.SymmFrontType.LDL_SELINV_1D):
+        L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+        cliq.LDL(info, L, ft)
+        assert L.frontType == ft
+        X[ft] = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(X[cliq.SymmFrontType.LDL_SELINV_2D], X[cliq.SymmFrontType.LDL_2D]) <= 1e-14
+    assert residual(A, X[cliq.SymmFrontType.LDL_SELINV_1D], B) <= 1e-12
+    for ft in (cliq.SymmFrontType.LDL_INTRAPIV_2D, cliq.SymmFrontType.BLOCK_LDL_2D):
+        L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+        with pytest.raises(cliq.LogicError):
+            cliq.LDL(info, L, ft)
