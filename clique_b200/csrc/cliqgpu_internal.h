@@ -255,6 +255,13 @@ struct Plan {
     int64_t* prefix = nullptr;
     int32_t* bmap = nullptr;      // block -> job / problem index of every pack and GEMM launch
     int64_t* dest = nullptr;      // assembly destination per CSR entry (-1: upper, skipped)
+    // assembly inside the factorization: the kept entries grouped by the tree
+    // depth of their front (CSR entry, destination), level d at
+    // [asm_level[d], asm_level[d + 1]); added to the fronts right after the
+    // level's extend-add, which writes every lower entry of those fronts
+    int64_t* asm_src = nullptr;
+    int64_t* asm_dst = nullptr;
+    std::vector<int64_t> asm_level;
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;
     int32_t* flags = nullptr;     // worker flags (flags_total, one per pivot block), then helper flags
@@ -328,7 +335,14 @@ int run_factor(Plan& P);
 template <class T, bool C>
 int run_solve_nodal(Plan& P, void* xn, int nrhs);   // xn: n x nrhs in storage precision, ND order
 // misc (misc_kernels.cu)
+// A's values (FP64, device, CSR order) into the plan's copy P.aval; the
+// fronts receive them during the factorization (level by level)
 int launch_assemble(Plan& P, const double* dvals);
+// the fronts as Initialize leaves them (arena cleared, every kept entry
+// scattered), for reading an assembled but unfactored tree
+int launch_materialize_assembly(Plan& P);
+// adds the kept entries of tree depth d to the fronts (after the level's extend-add)
+int launch_assemble_level(Plan& P, int d, cudaStream_t st);
 int launch_pull(Plan& P, const int32_t* perm, const double* X, int64_t ldx, int nrhs, void* xn, double scale);
 int launch_push(Plan& P, const int32_t* perm, const void* xn, double* X, int64_t ldx, int nrhs, double scale, int accumulate);
 int launch_spmv(Plan& P, double alpha_r, double alpha_i, const double* X, double beta_r, double beta_i,

@@ -10,8 +10,11 @@
 //
 // Here every tree level (all fronts at one depth) is processed at once:
 //   1. extend_add_kernel  -- gather form of the extend-add: each entry of the
-//      parent's lower triangle is written exactly once (frontL += children,
-//      ABR := children), using per-front inverse maps of the relative indices.
+//      parent's lower triangle is written exactly once (frontL := children,
+//      ABR := children, zero where no child contributes), using per-front
+//      inverse maps of the relative indices; then A's entries of the level's
+//      fronts are added (assemble_add_kernel), so the fronts are never
+//      cleared or read before this point.
 //   2. for k in steps of nb over the level's widest front:
 //        diag_ldl_kernel  -- LDL of the kb x kb diagonal block in shared memory
 //                            (FP64 arithmetic for FP64 storage, FP32 for FP32
@@ -69,7 +72,6 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
         const int j = j0 + jj;
         if (j >= f.m) break;
         const int lj = lm ? lm[j] : -1, rj = rm ? rm[j] : -1;
-        if (j < f.n && lj < 0 && rj < 0) continue;
         for (int ib = max(j, it.z) + threadIdx.x; ib < i_end; ib += kEAUnroll * blockDim.x) {
             int li[kEAUnroll], ri[kEAUnroll];
 #pragma unroll
@@ -78,21 +80,19 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
                 li[u] = (lj >= 0 && i < i_end) ? lm[i] : -1;
                 ri[u] = (rj >= 0 && i < i_end) ? rm[i] : -1;
             }
-            X v[kEAUnroll], o[kEAUnroll];
+            X v[kEAUnroll];
 #pragma unroll
             for (int u = 0; u < kEAUnroll; ++u) {
-                const int i = ib + u * blockDim.x;
                 X t = X{};
                 if (li[u] >= 0) t += ldv<T, C>(cp, f.CU[0] + li[u] + (int64_t)lj * f.cu[0]);
                 if (ri[u] >= 0) t += ldv<T, C>(cp, f.CU[1] + ri[u] + (int64_t)rj * f.cu[1]);
                 v[u] = t;
-                o[u] = (j < f.n && i < i_end) ? ldv<T, C>(L, f.L + i + (int64_t)j * f.m) : X{};
             }
 #pragma unroll
             for (int u = 0; u < kEAUnroll; ++u) {
                 const int i = ib + u * blockDim.x;
                 if (i >= i_end) break;
-                if (j < f.n) stv<T, C>(L, f.L + i + (int64_t)j * f.m, o[u] + v[u]);
+                if (j < f.n) stv<T, C>(L, f.L + i + (int64_t)j * f.m, v[u]);
                 else stv<T, C>(up, f.U + (i - f.n) + (int64_t)(j - f.n) * f.u, v[u]);
             }
         }
@@ -218,6 +218,9 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
     }
     __syncthreads();
     const int sr = tid % kSub, sc = tid / kSub;    // this thread's sub-block entry
+    // unrolled: the rows below each sub-block (R = 48, 32, 16) become
+    // compile-time constants in the index arithmetic of the panel and update loops
+#pragma unroll
     for (int p = 0; p < nb / kSub; ++p) {
         const int b0 = kSub * p;
         // ---- 16 x 16 sub-block: LDL and inverse ----
@@ -708,6 +711,7 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
         switch (ln.kind) {
             case Launch::EXTEND_ADD:
                 extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps);
+                launch_assemble_level(P, ln.depth, st);   // A's entries of this level's fronts
                 break;
             case Launch::DIAG:
                 if (std::is_same<T, float>::value && !P.diag_fp64) launch_diag<T, C, CJ, T>(P, ln, L, items, st);

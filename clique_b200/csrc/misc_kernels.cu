@@ -31,19 +31,63 @@ __global__ void assemble_kernel(const int64_t* __restrict__ dest, const double* 
 }
 
 template <class T, bool C>
-static int assemble_t(Plan& P, const double* dvals) {
+static int materialize_t(Plan& P) {
     cudaMemsetAsync(P.L, 0, (size_t)P.arena_elems * P.elem_bytes(), P.stream);
     if (P.conjugate && C)
-        assemble_kernel<T, C, true><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, dvals, P.nnz, reinterpret_cast<T*>(P.L));
+        assemble_kernel<T, C, true><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, P.aval, P.nnz, reinterpret_cast<T*>(P.L));
     else
-        assemble_kernel<T, C, false><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, dvals, P.nnz, reinterpret_cast<T*>(P.L));
+        assemble_kernel<T, C, false><<<grid_for(P.nnz, 256), 256, 0, P.stream>>>(P.dest, P.aval, P.nnz, reinterpret_cast<T*>(P.L));
     P.total_launches += 1;
     return check_cuda("assemble");
 }
 
+int launch_materialize_assembly(Plan& P) {
+    if (P.precision == CLIQ_FP64) return P.cplx() ? materialize_t<double, true>(P) : materialize_t<double, false>(P);
+    return P.cplx() ? materialize_t<float, true>(P) : materialize_t<float, false>(P);
+}
+
 int launch_assemble(Plan& P, const double* dvals) {
-    if (P.precision == CLIQ_FP64) return P.cplx() ? assemble_t<double, true>(P, dvals) : assemble_t<double, false>(P, dvals);
-    return P.cplx() ? assemble_t<float, true>(P, dvals) : assemble_t<float, false>(P, dvals);
+    if (dvals != P.aval &&
+        cudaMemcpyAsync(P.aval, dvals, sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)P.nnz, cudaMemcpyDeviceToDevice,
+                        P.stream) != cudaSuccess)
+        return check_cuda("assemble");
+    return CLIQ_OK;
+}
+
+// DistSymmFrontTree::Initialize's scatter for the fronts of one tree depth,
+// as an addition: the level's extend-add has just written every lower entry
+// of these fronts (children's contributions, or zero), and each kept entry of
+// A has its own destination (dist_symm_front_tree/impl.hpp:275-294)
+template <class T, bool C, bool CJ>
+__global__ void assemble_add_kernel(const int64_t* __restrict__ src, const int64_t* __restrict__ dst, int64_t cnt,
+                                    const double* __restrict__ vals, T* __restrict__ L) {
+    using Xv = V<T, C>;
+    using W = DV<C>;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = dst[i];
+        const W v = opc<CJ>(reinterpret_cast<const W*>(vals)[src[i]]);
+        stv<T, C>(L, d, ldv<T, C>(L, d) + conv<Xv>(v));
+    }
+}
+
+template <class T, bool C>
+static int assemble_level_t(Plan& P, int d, cudaStream_t st) {
+    const int64_t b = P.asm_level[d], cnt = P.asm_level[d + 1] - b;
+    if (cnt <= 0) return CLIQ_OK;
+    if (P.conjugate && C)
+        assemble_add_kernel<T, C, true><<<grid_for(cnt, 256), 256, 0, st>>>(P.asm_src + b, P.asm_dst + b, cnt, P.aval,
+                                                                               reinterpret_cast<T*>(P.L));
+    else
+        assemble_add_kernel<T, C, false><<<grid_for(cnt, 256), 256, 0, st>>>(P.asm_src + b, P.asm_dst + b, cnt, P.aval,
+                                                                                reinterpret_cast<T*>(P.L));
+    P.total_launches += 1;
+    return CLIQ_OK;
+}
+
+int launch_assemble_level(Plan& P, int d, cudaStream_t st) {
+    if (d < 0 || d + 1 >= (int)P.asm_level.size()) return CLIQ_OK;
+    if (P.precision == CLIQ_FP64) return P.cplx() ? assemble_level_t<double, true>(P, d, st) : assemble_level_t<double, false>(P, d, st);
+    return P.cplx() ? assemble_level_t<float, true>(P, d, st) : assemble_level_t<float, false>(P, d, st);
 }
 
 // Pull (dist_nodal_multi_vec/impl.hpp:67-219 at P=1): xn[p, j] = scale * X[inv[p], j]

@@ -74,7 +74,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 
 void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
-                    P.prefix, P.bmap, P.dest,
+                    P.prefix, P.bmap, P.dest, P.asm_src, P.asm_dst,
                     P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
                     P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov, P.pack3};
     for (void* p : ptrs)
@@ -360,11 +360,10 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
             ln.items = (int64_t)items.size() / 4;
             for (int s : lv) {
                 const FrontDev& f = P.hfronts[s];
-                const bool leaf = f.cmap < 0;
-                for (int j0 = 0; j0 < f.m; j0 += kEACols) {
-                    if (leaf && j0 + kEACols <= f.n) continue;
+                // every front, leaves included: the extend-add writes each lower
+                // entry (the fronts are not cleared beforehand)
+                for (int j0 = 0; j0 < f.m; j0 += kEACols)
                     for (int i0 = j0 / kEARows * kEARows; i0 < f.m; i0 += kEARows) push_item(s, j0, i0, 0);
-                }
             }
             ln.nitems = (int32_t)(items.size() / 4 - ln.items);
             ln.nblocks = ln.nitems;
@@ -373,10 +372,9 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
                 const FrontDev& f = P.hfronts[s];
                 const double m = f.m, nn2 = f.n, u = f.u, eb = P.elem_bytes();
                 double b = u * (u + 1) / 2 * eb;                                  // ABR written
-                if (f.cmap >= 0) {
-                    b += 2 * (m * nn2 - nn2 * (nn2 - 1) / 2) * eb;                // frontL read + written
+                b += (m * nn2 - nn2 * (nn2 - 1) / 2) * eb;                        // frontL written (lower part)
+                if (f.cmap >= 0)
                     for (int c = 0; c < 2; ++c) b += (double)f.cu[c] * (f.cu[c] + 1) / 2 * eb;   // children read
-                }
                 ln.work += b;
             }
             if (ln.nitems) P.launches.push_back(ln);
@@ -659,6 +657,27 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
     }
 
+    // ---- assembly by level (kept entries grouped by their front's depth) ----
+    {
+        std::vector<int64_t> cnt(P.max_depth + 2, 0);
+        for (int64_t i = 0; i < n; ++i) {
+            const int d = P.depth[node_of[map[i]]];
+            for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e)
+                if (dest[e] >= 0) ++cnt[d + 1];
+        }
+        P.asm_level.assign(P.max_depth + 2, 0);
+        for (int d = 0; d <= P.max_depth; ++d) P.asm_level[d + 1] = P.asm_level[d] + cnt[d + 1];
+        std::vector<int64_t> src(std::max<int64_t>(P.asm_level.back(), 1)), dst(src.size());
+        std::vector<int64_t> pos(P.asm_level.begin(), P.asm_level.end() - 1);
+        for (int64_t i = 0; i < n; ++i) {
+            const int d = P.depth[node_of[map[i]]];
+            for (int64_t e = rowptr[i]; e < rowptr[i + 1]; ++e)
+                if (dest[e] >= 0) { src[pos[d]] = e; dst[pos[d]] = dest[e]; ++pos[d]; }
+        }
+        TRY(dev_upload(P, &P.asm_src, src));
+        TRY(dev_upload(P, &P.asm_dst, dst));
+    }
+
     // ---- device allocations ----
     const int eb = P.elem_bytes();
     TRY(dev_alloc(P, &P.L, (size_t)P.arena_elems * eb));
@@ -715,12 +734,13 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.tickets, zt));
     std::vector<int32_t> st = {INT_MAX, 0, 0, 0};
     TRY(dev_upload(P, &P.status, st));
+    // A's values stay on the device (the factorization assembles from them)
+    TRY(dev_alloc(P, (void**)&P.aval, sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)std::max<int64_t>(P.nnz, 1)));
     if (P.keep_matrix) {
         std::vector<int64_t> rp(rowptr, rowptr + n + 1);
         std::vector<int32_t> ci(colind, colind + P.nnz);
         TRY(dev_upload(P, &P.rowptr, rp));
         TRY(dev_upload(P, &P.colind, ci));
-        TRY(dev_alloc(P, (void**)&P.aval, sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)std::max<int64_t>(P.nnz, 1)));
     }
     return CLIQ_OK;
 }
@@ -825,22 +845,12 @@ int cliqgpu_assemble(cliqgpu_plan h, const void* values, int32_t values_on_devic
     if (!h || !values) return CLIQ_ERR_ARG;
     Plan& P = h->p;
     const size_t bytes = sizeof(double) * (P.cplx() ? 2 : 1) * (size_t)P.nnz;
-    const double* dvals = (const double*)values;
-    void* tmp = nullptr;
-    if (!values_on_device) {
-        if (P.keep_matrix) {
-            if (cudaMemcpyAsync(P.aval, values, bytes, cudaMemcpyHostToDevice, P.stream) != cudaSuccess) return check_cuda("copy A");
-            dvals = P.aval;
-        } else {
-            if (cudaMallocAsync(&tmp, std::max<size_t>(bytes, 16), P.stream) != cudaSuccess) return check_cuda("alloc A");
-            if (cudaMemcpyAsync(tmp, values, bytes, cudaMemcpyHostToDevice, P.stream) != cudaSuccess) return check_cuda("copy A");
-            dvals = (const double*)tmp;
-        }
-    } else if (P.keep_matrix) {
-        if (cudaMemcpyAsync(P.aval, values, bytes, cudaMemcpyDeviceToDevice, P.stream) != cudaSuccess) return check_cuda("copy A");
-    }
-    int st = launch_assemble(P, dvals);
-    if (tmp) cudaFreeAsync(tmp, P.stream);
+    // the values go to the plan's device copy; the factorization adds them to
+    // the fronts level by level, right after each level's extend-add
+    if (cudaMemcpyAsync(P.aval, values, bytes, values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        P.stream) != cudaSuccess)
+        return check_cuda("copy A");
+    int st = launch_assemble(P, P.aval);
     if (st != CLIQ_OK) return st;
     if (!values_on_device && cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("assemble sync");
     P.assembled = true;
@@ -1150,6 +1160,8 @@ int cliqgpu_get_front(cliqgpu_plan h, int32_t s, double* Lout, double* Dout, int
     if (s < 0 || s >= P.num_fronts) return CLIQ_ERR_ARG;
     const FrontDev& f = P.hfronts[s];
     if (dims) { dims[0] = f.m; dims[1] = f.n; }
+    if (!Lout && !Dout) return CLIQ_OK;
+    if (P.assembled && !P.factored) TRY(launch_materialize_assembly(P));   // the fronts as Initialize leaves them
     if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("sync");
     const int w = P.cplx() ? 2 : 1;
     if (Lout) {
@@ -1163,6 +1175,10 @@ int cliqgpu_get_front(cliqgpu_plan h, int32_t s, double* Lout, double* Dout, int
                 return check_cuda("get front");
             for (size_t i = 0; i < cnt; ++i) Lout[i] = tmp[i];
         }
+        // strictly upper part of the pivot block: zero (the kernels never write it)
+        for (int j = 0; j < f.n; ++j)
+            for (int i = 0; i < j && i < f.m; ++i)
+                for (int c = 0; c < w; ++c) Lout[(size_t)w * (i + (size_t)j * f.m) + c] = 0.0;
     }
     if (Dout && f.n > 0) {
         if (cudaMemcpy(Dout, P.D + (size_t)w * f.off, sizeof(double) * w * f.n, cudaMemcpyDeviceToHost) != cudaSuccess)
