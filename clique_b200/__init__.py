@@ -47,8 +47,11 @@ class SymmFrontType:
     BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D = 12, 13
     # unpivoted LDL and its selective-inversion forms: at one process the
     # reference inverts no local front for the latter (change_front_type.hpp:
-    # 86-98 inverts distributed nodes 1 ..), so they factor and solve as LDL
-    SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D)
+    # 86-98 inverts distributed nodes 1 ..), so they factor and solve as LDL;
+    # the unpivoted block-LDL forms keep inv(A11) and A21 in every front
+    # (ldl/local.hpp:30-33, ldl/local_front_block.hpp:27-71)
+    SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D)
+    BLOCK = (BLOCK_LDL_1D, BLOCK_LDL_2D)
 
 
 # ---------------------------------------------------------------------------
@@ -307,8 +310,8 @@ class DistSymmFrontTree:
 def LDL(info, L: DistSymmFrontTree, frontType=SymmFrontType.LDL_2D):
     """Multifrontal LDL^T in place (ldl.hpp:57-75).  Returns None; raises on a zero pivot."""
     if frontType not in SymmFrontType.SUPPORTED:
-        raise LogicError(_capi.CLIQ_ERR_ARG, "only the unpivoted LDL_1D / LDL_2D (and LDL_SELINV_1D / LDL_SELINV_2D) "
-                                             "front types are provided")
+        raise LogicError(_capi.CLIQ_ERR_ARG, "only the unpivoted LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D and "
+                                             "BLOCK_LDL_1D / BLOCK_LDL_2D front types are provided")
     if L.frontType not in (SymmFrontType.SYMM_1D, SymmFrontType.SYMM_2D):
         raise LogicError(_capi.CLIQ_ERR_STATE, "Matrix is already factored")
     zp = C.c_int64(-1)
@@ -316,6 +319,8 @@ def LDL(info, L: DistSymmFrontTree, frontType=SymmFrontType.LDL_2D):
     L.zero_pivot = zp.value
     L.frontType = frontType
     check(st, "LDL")
+    if frontType in SymmFrontType.BLOCK:
+        check(_capi.load().cliqgpu_block_ldl(L._h), "LDL (block form)")
 
 
 class DistNodalMultiVec:

@@ -229,6 +229,7 @@ int cliqgpu_batch_run(cliqgpu_plan h, int32_t nseg, const int64_t* seg_rows, con
         set_last_error("batch_run: segments must cover rows 0 .. n");
         return CLIQ_ERR_ARG;
     }
+    P.block = false;   // every run refactors in the LDL form
     for (int s = 0; s < nseg; ++s)
         if (seg_rows[s + 1] < seg_rows[s]) { set_last_error("batch_run: segments must be ordered"); return CLIQ_ERR_ARG; }
     int st = ensure_workspace(P, nrhs);

@@ -283,6 +283,8 @@ struct Plan {
 
     int32_t epoch = 0;
     bool assembled = false, factored = false;
+    bool block = false;           // fronts hold the block-LDL form (inv(A11), A21)
+    void* block_state = nullptr;  // block sweeps: schedules per right-hand-side count and scratch
     int64_t last_launches = 0;
     int64_t total_launches = 0;   // every kernel this plan has launched
     // FP32 updates on the tensor cores (tcgen05 3xTF32); CLIQGPU_TENSOR_CORES=0 selects the CUDA-core kernel
@@ -377,6 +379,12 @@ int run_factor_dispatch(Plan& P);
 // the process-wide table of measured choices
 void apply_tuned_choices(Plan& P);
 void free_plan(Plan& P);
+// block-LDL front type (block_ldl.cu)
+int convert_to_block(Plan& P);
+int run_block_solve(Plan& P, void* xn, int nrhs);
+void free_block_state(Plan& P);
+template <class T, bool C>
+void launch_fwd_gather(Plan& P, const SolveLevel& lv, T* X, T* w0, T* w1, int nrhs);
 int read_status(Plan& P, int64_t* zero_pivot);
 
 }  // namespace cliqgpu

@@ -92,6 +92,7 @@ void free_plan(Plan& P) {
     if (P.stream2) cudaStreamDestroy(P.stream2);
     if (P.stream3) cudaStreamDestroy(P.stream3);
     if (P.own_stream && P.stream) cudaStreamDestroy(P.stream);
+    free_block_state(P);
 }
 
 #define TRY(x)                      \
@@ -764,6 +765,7 @@ int ensure_workspace(Plan& P, int nrhs) {
 }
 
 int solve_nodal_dispatch(Plan& P, void* xn, int nrhs) {
+    if (P.block) return run_block_solve(P, xn, nrhs);
     if (P.precision == CLIQ_FP64)
         return P.cplx() ? run_solve_nodal<double, true>(P, xn, nrhs) : run_solve_nodal<double, false>(P, xn, nrhs);
     return P.cplx() ? run_solve_nodal<float, true>(P, xn, nrhs) : run_solve_nodal<float, false>(P, xn, nrhs);
@@ -876,10 +878,22 @@ int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
     if (P.factored) { set_last_error("Matrix is already factored"); return CLIQ_ERR_STATE; }
     int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
+    P.block = false;
     const int st = run_factor_dispatch(P);
     if (st != CLIQ_OK) return st;
     P.factored = true;
     return read_status(P, zero_pivot);
+}
+
+int cliqgpu_block_ldl(cliqgpu_plan h) {
+    if (!h) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (!P.factored) { set_last_error("block LDL: the front tree is not factored"); return CLIQ_ERR_STATE; }
+    if (P.block) return CLIQ_OK;
+    const int st = convert_to_block(P);
+    if (st != CLIQ_OK) return st;
+    P.block = true;
+    return CLIQ_OK;
 }
 
 int cliqgpu_solve(cliqgpu_plan h, void* X, int64_t ldx, int32_t nrhs, int32_t x_on_device, int32_t nodal) {
@@ -1175,8 +1189,9 @@ int cliqgpu_get_front(cliqgpu_plan h, int32_t s, double* Lout, double* Dout, int
                 return check_cuda("get front");
             for (size_t i = 0; i < cnt; ++i) Lout[i] = tmp[i];
         }
-        // strictly upper part of the pivot block: zero (the kernels never write it)
-        for (int j = 0; j < f.n; ++j)
+        // strictly upper part of the pivot block: zero (the kernels never write it);
+        // the block-LDL form keeps the full inv(A11) there
+        for (int j = 0; j < (P.block ? 0 : f.n); ++j)
             for (int i = 0; i < j && i < f.m; ++i)
                 for (int c = 0; c < w; ++c) Lout[(size_t)w * (i + (size_t)j * f.m) + c] = 0.0;
     }

@@ -1181,6 +1181,17 @@ int run_solve_nodal(Plan& P, void* xn, int nrhs) {
     return run_solve_impl<T, C, false>(P, reinterpret_cast<T*>(xn), nrhs);
 }
 
+template <class T, bool C>
+void launch_fwd_gather(Plan& P, const SolveLevel& lv, T* X, T* w0, T* w1, int nrhs) {
+    fwd_gather_kernel<T, C><<<dim3(lv.nfronts, lv.gather_chunks), kSolveThreads, 0, P.stream>>>(
+        P.fronts, P.level_fronts + lv.fronts, X, P.n, w0, w1, P.cmaps, nrhs);
+}
+
+template void launch_fwd_gather<float, false>(Plan&, const SolveLevel&, float*, float*, float*, int);
+template void launch_fwd_gather<float, true>(Plan&, const SolveLevel&, float*, float*, float*, int);
+template void launch_fwd_gather<double, false>(Plan&, const SolveLevel&, double*, double*, double*, int);
+template void launch_fwd_gather<double, true>(Plan&, const SolveLevel&, double*, double*, double*, int);
+
 template int run_solve_nodal<float, false>(Plan&, void*, int);
 template int run_solve_nodal<float, true>(Plan&, void*, int);
 template int run_solve_nodal<double, false>(Plan&, void*, int);

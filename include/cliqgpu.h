@@ -126,6 +126,18 @@ int cliqgpu_assemble(cliqgpu_plan plan, const void* values, int32_t values_on_de
  * (LocalLDL ldl/local.hpp:25-122, FrontLDL ldl/local_front.hpp:30-71). */
 int cliqgpu_factor(cliqgpu_plan plan, int64_t* zero_pivot);
 
+/* After cliqgpu_factor: turn every front into the block-LDL form -- the top
+ * n x n block holds inv(A11) (full, symmetric or Hermitian), the rows below
+ * it the original A21 -- so that the solves are products only (no
+ * triangular or diagonal solves).  cliqgpu_solve, cliqgpu_refined_solve and
+ * cliqgpu_get_front then use / return that form until the next
+ * cliqgpu_factor.  Runs on the plan's stream and returns when done.
+ * Replaces the blockLDL branch of LocalLDL, include/clique/numeric/ldl/
+ * local.hpp:30-33 with FrontBlockLDL (ldl/local_front_block.hpp:27-71,
+ * unpivoted), i.e. cliq::LDL(info, L, BLOCK_LDL_1D/BLOCK_LDL_2D), and its
+ * solves lower_solve/local_front_block.hpp:29-70, solve.hpp:48-53. */
+int cliqgpu_block_ldl(cliqgpu_plan plan);
+
 /* Solve A X = B in place using the stored factors: forward sweep, diagonal
  * solve, backward sweep.  X is n x nrhs column-major with leading dimension
  * ldx, FP64 (real or interleaved complex), on the host or the device.

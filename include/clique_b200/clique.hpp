@@ -283,7 +283,9 @@ inline bool Unfactored(SymmFrontType t) { return t == SYMM_1D || t == SYMM_2D; }
 // front types this library factors: unpivoted LDL, and its selective-inversion
 // forms, which at one process invert no local front (change_front_type.hpp:86-98
 // inverts distributed nodes 1 .. only), so they factor and solve as LDL
-inline bool Provided(SymmFrontType t) { return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D; }
+inline bool Provided(SymmFrontType t) {
+    return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D || t == BLOCK_LDL_1D || t == BLOCK_LDL_2D;
+}
 
 template <class F>
 class DistSymmFrontTree {
@@ -336,10 +338,11 @@ template <class F>
 void LDL(DistSymmInfo&, DistSymmFrontTree<F>& L, SymmFrontType newFrontType = LDL_2D) {
     if (!Unfactored(L.frontType)) throw LogicError("Matrix is already factored");
     if (!Provided(newFrontType))
-        throw LogicError("Only the unpivoted LDL_1D / LDL_2D (and LDL_SELINV_1D / LDL_SELINV_2D) front types are provided");
+        throw LogicError("Only the unpivoted LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D and BLOCK_LDL_1D / BLOCK_LDL_2D front types are provided");
     int64_t zp = -1;
     Check(cliqgpu_factor(L.Plan(), &zp), "LDL");
     L.frontType = newFrontType;
+    if (newFrontType == BLOCK_LDL_1D || newFrontType == BLOCK_LDL_2D) Check(cliqgpu_block_ldl(L.Plan()), "LDL (block form)");
 }
 
 template <class F>

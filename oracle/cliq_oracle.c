@@ -498,6 +498,11 @@ void orc_fronts_free(orc_fronts* f) {
 }
 /* LocalLDL with blocksize nb; returns 0, or 1 + (ND index) of the first zero pivot. */
 i64 orc_ldl(orc_fronts* f, int nb) { return f->is_complex ? local_ldl_z(f->impl, nb) : local_ldl_d(f->impl, nb); }
+/* LocalLDL with the front type chosen: block = 1 for BLOCK_LDL_2D (FrontBlockLDL, block solves) */
+i64 orc_ldl_ex(orc_fronts* f, int nb, int block) {
+    if (f->is_complex) set_block_z(f->impl, block); else set_block_d(f->impl, block);
+    return orc_ldl(f, nb);
+}
 /* copy frontL (m x n, column-major) or diag (n) of node s */
 void orc_front_get(const orc_fronts* f, int s, double* L_out, double* d_out) {
     if (f->is_complex) front_get_z(f->impl, s, (zd*)L_out, (zd*)d_out); else front_get_d(f->impl, s, L_out, d_out);

@@ -47,6 +47,8 @@ def lib():
     L.orc_fronts_free.argtypes = [C.c_void_p]
     L.orc_ldl.restype = C.c_int64
     L.orc_ldl.argtypes = [C.c_void_p, C.c_int]
+    L.orc_ldl_ex.restype = C.c_int64
+    L.orc_ldl_ex.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.orc_front_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_front_dims.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.orc_front_set.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -139,8 +141,9 @@ class Fronts:
         self.h = lib().orc_fronts_create(symb.h, symb._rowptr, symb._colind, _ptr(self._vals),
                                          int(self.is_complex), int(conjugate))
 
-    def ldl(self, nb=96):
-        return int(lib().orc_ldl(self.h, nb))
+    def ldl(self, nb=96, block=False):
+        """LocalLDL; block=True for the BLOCK_LDL_2D front type (FrontBlockLDL)."""
+        return int(lib().orc_ldl_ex(self.h, nb, int(bool(block))))
 
     def dims(self, s):
         m, n = C.c_int(), C.c_int()

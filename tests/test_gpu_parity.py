@@ -529,7 +529,7 @@ def test_fp64_dmma_updates_match_cuda_cores(oracle, complex_, conjugate, monkeyp
 def test_selinv_front_types_factor_and_solve_as_ldl():
     """LDL_SELINV_1D / LDL_SELINV_2D at one process: the reference inverts only
     distributed fronts (change_front_type.hpp:86-98), so the factorization and
-    the solve are the LDL_2D ones; pivoted and block types are refused."""
+    the solve are the LDL_2D ones; the pivoted types are refused."""
     n = 12
     A, _, _ = ops.helmholtz_workload_3d(n, seed=4)
     B = ops.random_rhs(A.n, 2, seed=5, complex_=True)
@@ -542,7 +542,52 @@ def test_selinv_front_types_factor_and_solve_as_ldl():
         X[ft] = cliq.Solve(info, L, B.copy(order="F"))
     assert rel(X[cliq.SymmFrontType.LDL_SELINV_2D], X[cliq.SymmFrontType.LDL_2D]) <= 1e-14
     assert residual(A, X[cliq.SymmFrontType.LDL_SELINV_1D], B) <= 1e-12
-    for ft in (cliq.SymmFrontType.LDL_INTRAPIV_2D, cliq.SymmFrontType.BLOCK_LDL_2D):
+    for ft in (cliq.SymmFrontType.LDL_INTRAPIV_2D, cliq.SymmFrontType.BLOCK_LDL_INTRAPIV_2D):
         L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
         with pytest.raises(cliq.LogicError):
             cliq.LDL(info, L, ft)
+
+
+@pytest.mark.parametrize("kind,precision", [("real", "double"), ("complex", "double"), ("hermitian", "double"),
+                                            ("complex", "single")])
+def test_block_ldl_matches_oracle(oracle, kind, precision):
+    """BLOCK_LDL_2D (FrontBlockLDL, ldl/local_front_block.hpp:27-71): every
+    front holds inv(A11) over A21 as in the oracle, the product-only block
+    sweeps (20 right-hand sides: a 16-column chunk and a 4-column one) give
+    the oracle's solution, and a refactorization in the LDL_2D form goes back
+    to the triangular sweeps."""
+    dims, cutoff = (17, 15, 14), 48
+    conj = kind == "hermitian"
+    if kind == "real":
+        A = ops.laplacian_3d(*dims, 6.1)
+    elif kind == "complex":
+        A = ops.helmholtz_pml_3d(*dims, omega=22.0, velocity=ops.smooth_velocity(dims, 2), b=3)
+    else:
+        A = _magnetic(dims)
+    cplx = kind != "real"
+    map_, sep, info = cliq.NaturalNestedDissection(*dims, A, cutoff)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, conj, precision=precision)
+    cliq.LDL(info, L, cliq.SymmFrontType.BLOCK_LDL_2D)
+    assert L.frontType == cliq.SymmFrontType.BLOCK_LDL_2D
+    B = ops.random_rhs(A.n, 20, seed=11, complex_=cplx)
+    if precision == "double":
+        S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+        F = oracle.Fronts(S, A.values, is_complex=cplx, conjugate=conj)
+        assert F.ldl(96, block=True) == 0
+        for s in range(S.num_nodes):
+            Lg, _ = L.front(s)
+            Lo, _ = F.front(s)
+            assert rel(Lg, Lo) <= 1e-10, s
+        X = cliq.Solve(info, L, B.copy(order="F"))
+        assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+        assert residual(A, X, B) <= 1e-11
+    else:
+        X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 40)
+        assert rr <= 1e-10, (it, rr)
+        assert residual(A, X, B) <= 1e-10
+    L.Initialize(A.values)
+    cliq.LDL(info, L, cliq.SymmFrontType.LDL_2D)
+    if precision == "double":
+        X2 = cliq.Solve(info, L, B.copy(order="F"))
+        assert residual(A, X2, B) <= 1e-12
+        assert rel(X2, X) <= 1e-10
