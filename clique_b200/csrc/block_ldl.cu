@@ -44,7 +44,7 @@ struct Prob {
     int8_t maskB;   // 1: B is op of a unit lower triangle (stored element (j, k): j > k kept, j == k one, else zero)
 };
 
-constexpr int kBufs = 6;   // 0 arena, 1 X (nodal), 2 scratch Y, 3 scratch G, 4 / 5 solve W pools
+constexpr int kBufs = 7;   // 0 arena, 1 X (nodal), 2 scratch Y, 3 scratch G, 4 / 5 solve W pools, 6 partial sums
 struct Bufs {
     void* p[kBufs];
 };
@@ -128,6 +128,199 @@ __global__ void __launch_bounds__(kThreads) bgemm_kernel(const Prob* __restrict_
             Cm[e] = pr.beta1 ? Cm[e] + v : v;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// skinny products of the block sweeps: C (M x N, N <= 16) (+)= (-) op(A) B.
+// A (inv(A11) or A21) is streamed once from HBM; K is split over CTAs and the
+// partial sums (buffer 6) are added in a fixed order by a second launch, so
+// the result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+struct SProb {
+    int64_t A, B, C, part;           // part: partial sums of split s at part + s * M * N (when ks > 1)
+    int32_t M, N, K, lda, ldb, ldc;
+    int32_t kc, ks, rows;            // K per split, splits, rows per CTA
+    int8_t opA, ba, bb, bc, beta1, neg, pad0, pad1;
+};
+
+constexpr int kSkRows = 64;        // opA 0: rows per CTA (one per thread of each k-group)
+constexpr int kSkGroups = 4;       // opA 0: k-groups per CTA, reduced in shared memory at the end
+constexpr int kSkK = 128;          // opA 0: rows of B staged per step (32 per k-group)
+constexpr int kSkWarps = 8;        // opA 1 / 2: warps per CTA, two rows per warp
+constexpr int kSkTRows = 2 * kSkWarps;
+constexpr int kSkThreads = 256;
+
+template <class X, int NR>
+__device__ __forceinline__ void sk_store(const SProb& pr, X* Cm, X* part, int sp, int i, const X* acc) {
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        if (j >= pr.N) break;
+        if (pr.ks > 1) {
+            part[pr.part + (int64_t)sp * pr.M * pr.N + i + (int64_t)j * pr.M] = acc[j];
+        } else {
+            const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
+            const X v = pr.neg ? X{} - acc[j] : acc[j];
+            Cm[e] = pr.beta1 ? Cm[e] + v : v;
+        }
+    }
+}
+
+// opA 0: A column-major M x K.  64 rows x 4 k-groups per CTA: a warp reads
+// 32 consecutive rows of one column (coalesced), each thread keeps 8 loads
+// in flight, and the k-groups' sums are added in a fixed order at the end.
+template <class T, bool C, int NR>
+__global__ void __launch_bounds__(kSkThreads) skinny_kernel(const SProb* __restrict__ probs, const int64_t* __restrict__ prefix,
+                                                            const int32_t* __restrict__ bmap, Bufs bufs) {
+    using X = V<T, C>;
+    constexpr int U = 8;
+    __shared__ X sbuf[kSkK * NR];   // staged B rows [k][j]; at the end the k-groups' sums [slot][j][row]
+    const int lo = bmap[blockIdx.x];
+    const SProb pr = probs[lo];
+    const int64_t t = blockIdx.x - prefix[lo];
+    const int rt = (int)(t / pr.ks), sp = (int)(t % pr.ks);
+    const int k0 = sp * pr.kc, k1 = min(pr.K, k0 + pr.kc);
+    const X* A = reinterpret_cast<const X*>(bufs.p[pr.ba]) + pr.A;
+    const X* B = reinterpret_cast<const X*>(bufs.p[pr.bb]) + pr.B;
+    const int r = threadIdx.x % kSkRows, g = threadIdx.x / kSkRows;
+    const int i = rt * kSkRows + r;
+    const bool row = i < pr.M;
+    X acc[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) acc[j] = X{};
+    for (int kb = k0; kb < k1; kb += kSkK) {
+        const int kn = min(kSkK, k1 - kb);
+        for (int e = threadIdx.x; e < kSkK * NR; e += kSkThreads) {
+            const int kk = e % kSkK, j = e / kSkK;
+            sbuf[kk * NR + j] = (kk < kn && j < pr.N) ? B[kb + kk + (int64_t)j * pr.ldb] : X{};
+        }
+        __syncthreads();
+        if (row) {
+            const X* a = A + i + (int64_t)kb * pr.lda;
+#pragma unroll
+            for (int h = 0; h < kSkK / kSkGroups; h += U) {
+                const int kq = g * (kSkK / kSkGroups) + h;
+                X av[U];
+#pragma unroll
+                for (int q = 0; q < U; ++q) av[q] = kq + q < kn ? a[(int64_t)(kq + q) * pr.lda] : X{};
+#pragma unroll
+                for (int q = 0; q < U; ++q)
+#pragma unroll
+                    for (int j = 0; j < NR; ++j) mac(acc[j], av[q], sbuf[(kq + q) * NR + j]);
+            }
+        }
+        __syncthreads();
+    }
+    // k-groups 2, 3 -> shared; 0, 1 add them; 1 -> shared; 0 adds and stores
+    X* red = sbuf;
+    if (g >= 2)
+#pragma unroll
+        for (int j = 0; j < NR; ++j) red[((g - 2) * NR + j) * kSkRows + r] = acc[j];
+    __syncthreads();
+    if (g < 2)
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] += red[(g * NR + j) * kSkRows + r];
+    __syncthreads();
+    if (g == 1)
+#pragma unroll
+        for (int j = 0; j < NR; ++j) red[j * kSkRows + r] = acc[j];
+    __syncthreads();
+    if (g == 0 && row) {
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] += red[j * kSkRows + r];
+        sk_store<X, NR>(pr, reinterpret_cast<X*>(bufs.p[pr.bc]), reinterpret_cast<X*>(bufs.p[6]), sp, i, acc);
+    }
+}
+
+// opA 1 / 2: C row i is column i of A (conjugated for 2).  Two rows per warp,
+// lanes coalesced down the columns with 4-8 loads each in flight; B staged
+// transposed so that lanes hit consecutive words.
+template <class T, bool C, int NR, bool CJ>
+__global__ void __launch_bounds__(kSkThreads) skinny_t_kernel(const SProb* __restrict__ probs, const int64_t* __restrict__ prefix,
+                                                              const int32_t* __restrict__ bmap, Bufs bufs) {
+    using X = V<T, C>;
+    constexpr int U = sizeof(X) >= 16 ? 4 : 8;
+    constexpr int KT = 32 * U;
+    __shared__ X sB[NR][KT + 1];
+    const int lo = bmap[blockIdx.x];
+    const SProb pr = probs[lo];
+    const int64_t t = blockIdx.x - prefix[lo];
+    const int rt = (int)(t / pr.ks), sp = (int)(t % pr.ks);
+    const int k0 = sp * pr.kc, k1 = min(pr.K, k0 + pr.kc);
+    const X* A = reinterpret_cast<const X*>(bufs.p[pr.ba]) + pr.A;
+    const X* B = reinterpret_cast<const X*>(bufs.p[pr.bb]) + pr.B;
+    const int lane = threadIdx.x % 32, w = threadIdx.x / 32;
+    const int i0 = rt * kSkTRows + 2 * w;
+    const bool row0 = i0 < pr.M, row1 = i0 + 1 < pr.M;
+    X acc0[NR], acc1[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) acc0[j] = acc1[j] = X{};
+    for (int kb = k0; kb < k1; kb += KT) {
+        const int kn = min(KT, k1 - kb);
+        for (int e = threadIdx.x; e < KT * NR; e += kSkThreads) {
+            const int kk = e % KT, j = e / KT;
+            sB[j][kk] = (kk < kn && j < pr.N) ? B[kb + kk + (int64_t)j * pr.ldb] : X{};
+        }
+        __syncthreads();
+        if (row0) {
+            const X* a0 = A + kb + (int64_t)i0 * pr.lda;
+            const X* a1 = row1 ? a0 + pr.lda : a0;
+            X v0[U], v1[U];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                const int k = lane + 32 * q;
+                v0[q] = k < kn ? opc<CJ>(a0[k]) : X{};
+                v1[q] = (k < kn && row1) ? opc<CJ>(a1[k]) : X{};
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q)
+#pragma unroll
+                for (int j = 0; j < NR; ++j) {
+                    const X b = sB[j][lane + 32 * q];
+                    mac(acc0[j], v0[q], b);
+                    mac(acc1[j], v1[q], b);
+                }
+        }
+        __syncthreads();
+    }
+    if (!row0) return;
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+#pragma unroll
+        for (int o = 16; o > 0; o /= 2) {
+            if constexpr (C) {
+                acc0[j].r += __shfl_xor_sync(0xffffffffu, acc0[j].r, o);
+                acc0[j].i += __shfl_xor_sync(0xffffffffu, acc0[j].i, o);
+                acc1[j].r += __shfl_xor_sync(0xffffffffu, acc1[j].r, o);
+                acc1[j].i += __shfl_xor_sync(0xffffffffu, acc1[j].i, o);
+            } else {
+                acc0[j] += __shfl_xor_sync(0xffffffffu, acc0[j], o);
+                acc1[j] += __shfl_xor_sync(0xffffffffu, acc1[j], o);
+            }
+        }
+    }
+    X* Cm = reinterpret_cast<X*>(bufs.p[pr.bc]);
+    X* part = reinterpret_cast<X*>(bufs.p[6]);
+    if (lane == 0) sk_store<X, NR>(pr, Cm, part, sp, i0, acc0);
+    if (lane == 1 && row1) sk_store<X, NR>(pr, Cm, part, sp, i0 + 1, acc1);
+}
+
+// C (+)= (-) sum over the splits of the partial sums, in split order
+template <class T, bool C>
+__global__ void skinny_reduce_kernel(const SProb* __restrict__ probs, const int64_t* __restrict__ prefix,
+                                     const int32_t* __restrict__ bmap, Bufs bufs) {
+    using X = V<T, C>;
+    const int lo = bmap[blockIdx.x];
+    const SProb pr = probs[lo];
+    const int64_t e = (int64_t)(blockIdx.x - prefix[lo]) * 256 + threadIdx.x;
+    const int64_t mn = (int64_t)pr.M * pr.N;
+    if (e >= mn) return;
+    const X* part = reinterpret_cast<const X*>(bufs.p[6]) + pr.part + e;
+    X s{};
+    for (int q = 0; q < pr.ks; ++q) s += part[q * mn];
+    X* Cm = reinterpret_cast<X*>(bufs.p[pr.bc]);
+    const int64_t c = pr.C + e % pr.M + (e / pr.M) * pr.ldc;
+    const X v = pr.neg ? X{} - s : s;
+    Cm[c] = pr.beta1 ? Cm[c] + v : v;
 }
 
 // dst[(rows, cols) of each job] = src, both column-major: job {src, dst, rows, cols, lds, ldd, bs, bd}
@@ -360,7 +553,8 @@ static int convert_t(Plan& P) {
 // host work or synchronization (and can be captured into a graph)
 // ---------------------------------------------------------------------------
 struct Rec {
-    int kind;   // 0 GEMM list, 1 copy list, 2 forward gather of one level
+    int kind;   // 0 GEMM list, 1 copy list, 2 forward gather of one level, 3 / 4 / 5 skinny products
+                // with op(A) = A / A^T / A^H, 6 reduction of split products
     int level;
     int64_t jobs, prefix, bmap, nblocks;   // byte offsets into the uploaded buffer
 };
@@ -368,14 +562,33 @@ struct Rec {
 struct SolveSched {
     int nrhs = 0;
     char* mem = nullptr;
+    int64_t part_elems = 0;   // partial sums the split products need at once
     std::vector<Rec> recs;
 };
 
 struct BlockState {
     std::vector<SolveSched> scheds;
-    void* y = nullptr;   // inv(A11) operands: the level's XT (or YT), sum of n x 16
-    void* g = nullptr;   // backward: the level's gathered X[lowerStruct], sum of u x 16
+    void* y = nullptr;      // inv(A11) operands: the level's XT (or YT), sum of n x 16
+    void* g = nullptr;      // backward: the level's gathered X[lowerStruct], sum of u x 16
+    void* part = nullptr;   // split products' partial sums
+    int64_t part_elems = 0;
 };
+
+using blk::SProb;
+
+// one skinny product (its K split is chosen per launch list)
+static SProb mk_sprob(int64_t A, int64_t B, int64_t Cc, int M, int N, int K, int lda, int ldb, int ldc, int opA, int ba, int bb,
+                      int bc, bool accumulate, bool negate) {
+    SProb p{};
+    p.A = A; p.B = B; p.C = Cc; p.part = -1;
+    p.M = M; p.N = N; p.K = K; p.lda = lda; p.ldb = ldb; p.ldc = ldc;
+    p.opA = (int8_t)opA; p.ba = (int8_t)ba; p.bb = (int8_t)bb; p.bc = (int8_t)bc;
+    p.beta1 = accumulate ? 1 : 0; p.neg = negate ? 1 : 0;
+    p.rows = opA == 0 ? blk::kSkRows : blk::kSkTRows;
+    p.kc = std::max(1, K);
+    p.ks = 1;
+    return p;
+}
 
 struct Packer {
     std::vector<char> bytes;
@@ -386,6 +599,35 @@ struct Packer {
         bytes.resize(o + (sizeof(V) * v.size() + 15) / 16 * 16);
         if (!v.empty()) std::memcpy(bytes.data() + o, v.data(), sizeof(V) * v.size());
         return o;
+    }
+    int64_t part_max = 0;
+    // a list of skinny products of one kind (opA 0, 1 or 2) and, for the split
+    // ones, the reduction of their partial sums
+    void add_skinny(std::vector<SProb> v) {
+        if (v.empty()) return;
+        List<SProb> L, R;
+        int64_t part = 0;
+        // split K until the list has about 16 CTAs per SM, a split keeping at
+        // least 256 (opA 0) or 512 (opA 1 / 2) columns of K and at most 32 splits
+        int64_t base = 0;
+        for (const SProb& p : v) base += (p.M + p.rows - 1) / p.rows;
+        const int64_t f = std::max<int64_t>(1, (16 * 148 + std::max<int64_t>(base, 1) - 1) / std::max<int64_t>(base, 1));
+        for (SProb& p : v) {
+            if (p.M <= 0 || p.N <= 0 || p.K <= 0) continue;
+            const int kmin = p.opA == 0 ? 256 : 512;
+            const int ks = (int)std::max<int64_t>(1, std::min<int64_t>({f, (int64_t)(p.K / kmin), 32}));
+            p.kc = ((p.K + ks - 1) / ks + 31) / 32 * 32;
+            p.ks = (p.K + p.kc - 1) / p.kc;
+            if (p.ks > 1) {
+                p.part = part;
+                part += (int64_t)p.ks * p.M * p.N;
+                R.add(p, ((int64_t)p.M * p.N + 255) / 256);
+            }
+            L.add(p, (int64_t)((p.M + p.rows - 1) / p.rows) * p.ks);
+        }
+        part_max = std::max(part_max, part);
+        add(v[0].opA == 0 ? 3 : (v[0].opA == 1 ? 4 : 5), L);
+        add(6, R);
     }
     template <class J>
     void add(int kind, const List<J>& L) {
@@ -407,62 +649,76 @@ static int build_sched(Plan& P, int nrhs, SolveSched& S) {
         if (P.solve_levels[d].nfronts == 0) continue;
         pk.recs.push_back(Rec{2, d, 0, 0, 0, 0});
         List<Copy> K;
-        List<Prob> G1, G2;
+        std::vector<SProb> G1, G2;
         int64_t y = 0;
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
             if (f.n <= 0) continue;
             const Copy c = mk_copy(f.off, y, f.n, nrhs, ldx, f.n, 1, 2);
             K.add(c, blk::copy_blocks(c));
-            const Prob p1 = mk_gemm(f.L, y, f.off, f.n, nrhs, f.n, f.m, f.n, ldx, 0, 0, 0, 2, 1, false, false);
-            G1.add(p1, blk::gemm_tiles(p1));
-            if (f.u > 0) {
-                const Prob p2 =
-                    mk_gemm(f.L + f.n, f.off, f.W * nrhs, f.u, nrhs, f.n, f.m, ldx, f.u, 0, 0, 0, 1, 4 + f.pool, true, true);
-                G2.add(p2, blk::gemm_tiles(p2));
-            }
+            G1.push_back(mk_sprob(f.L, y, f.off, f.n, nrhs, f.n, f.m, f.n, ldx, 0, 0, 2, 1, false, false));
+            if (f.u > 0)
+                G2.push_back(mk_sprob(f.L + f.n, f.off, f.W * nrhs, f.u, nrhs, f.n, f.m, ldx, f.u, 0, 0, 1, 4 + f.pool, true, true));
             y += (int64_t)f.n * nrhs;
         }
         pk.add(1, K);
-        pk.add(0, G1);
-        pk.add(0, G2);
+        pk.add_skinny(G1);
+        pk.add_skinny(G2);
     }
     for (int d = 0; d <= P.max_depth; ++d) {   // backward: YT := op(A21)^T XB, XT -= inv(A11) YT
         List<Copy> K;
-        List<Prob> G1, G2;
+        std::vector<SProb> G1, G2;
         int64_t y = 0, g = 0;
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
             if (f.n <= 0 || f.u <= 0) continue;
             const Copy c = mk_copy(0, g, f.u, nrhs, ldx, f.u, 1, 3, f.lower);
             K.add(c, blk::copy_blocks(c));
-            const Prob p1 = mk_gemm(f.L + f.n, g, y, f.n, nrhs, f.u, f.m, f.u, f.n, opT, 0, 0, 3, 2, false, false);
-            G1.add(p1, blk::gemm_tiles(p1));
-            const Prob p2 = mk_gemm(f.L, y, f.off, f.n, nrhs, f.n, f.m, f.n, ldx, 0, 0, 0, 2, 1, true, true);
-            G2.add(p2, blk::gemm_tiles(p2));
+            G1.push_back(mk_sprob(f.L + f.n, g, y, f.n, nrhs, f.u, f.m, f.u, f.n, opT, 0, 3, 2, false, false));
+            G2.push_back(mk_sprob(f.L, y, f.off, f.n, nrhs, f.n, f.m, f.n, ldx, 0, 0, 2, 1, true, true));
             y += (int64_t)f.n * nrhs;
             g += (int64_t)f.u * nrhs;
         }
         pk.add(1, K);
-        pk.add(0, G1);
-        pk.add(0, G2);
+        pk.add_skinny(G1);
+        pk.add_skinny(G2);
     }
     S.nrhs = nrhs;
     S.recs = pk.recs;
+    S.part_elems = pk.part_max;
     if (cudaMalloc((void**)&S.mem, std::max<size_t>(16, pk.bytes.size())) != cudaSuccess) return check_cuda("block solve: schedule");
     if (cudaMemcpy(S.mem, pk.bytes.data(), pk.bytes.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return check_cuda("block solve: schedule");
     return CLIQ_OK;
 }
 
+template <class T, bool C, int NR>
+static void launch_skinny(const Rec& r, const char* mem, const Bufs& b, cudaStream_t st) {
+    const SProb* j = reinterpret_cast<const SProb*>(mem + r.jobs);
+    const int64_t* pf = reinterpret_cast<const int64_t*>(mem + r.prefix);
+    const int32_t* bm = reinterpret_cast<const int32_t*>(mem + r.bmap);
+    const unsigned g = (unsigned)r.nblocks;
+    if (r.kind == 3) blk::skinny_kernel<T, C, NR><<<g, blk::kSkThreads, 0, st>>>(j, pf, bm, b);
+    else if (r.kind == 4) blk::skinny_t_kernel<T, C, NR, false><<<g, blk::kSkThreads, 0, st>>>(j, pf, bm, b);
+    else if constexpr (C) blk::skinny_t_kernel<T, C, NR, true><<<g, blk::kSkThreads, 0, st>>>(j, pf, bm, b);
+}
+
 template <class T, bool C>
 static int64_t run_sched(Plan& P, const SolveSched& S, BlockState& B, T* xn) {
     cudaStream_t st = P.stream;
     Bufs b{};
-    b.p[0] = P.L; b.p[1] = xn; b.p[2] = B.y; b.p[3] = B.g; b.p[4] = P.wpool[0]; b.p[5] = P.wpool[1];
+    b.p[0] = P.L; b.p[1] = xn; b.p[2] = B.y; b.p[3] = B.g; b.p[4] = P.wpool[0]; b.p[5] = P.wpool[1]; b.p[6] = B.part;
     int64_t launches = 0;
     for (const Rec& r : S.recs) {
-        if (r.kind == 2) {
+        if (r.kind >= 3 && r.kind <= 5) {
+            if (S.nrhs <= 4) launch_skinny<T, C, 4>(r, S.mem, b, st);
+            else if (S.nrhs <= 8) launch_skinny<T, C, 8>(r, S.mem, b, st);
+            else launch_skinny<T, C, 16>(r, S.mem, b, st);
+        } else if (r.kind == 6) {
+            blk::skinny_reduce_kernel<T, C><<<(unsigned)r.nblocks, 256, 0, st>>>(
+                reinterpret_cast<const SProb*>(S.mem + r.jobs), reinterpret_cast<const int64_t*>(S.mem + r.prefix),
+                reinterpret_cast<const int32_t*>(S.mem + r.bmap), b);
+        } else if (r.kind == 2) {
             launch_fwd_gather<T, C>(P, P.solve_levels[r.level], xn, reinterpret_cast<T*>(P.wpool[0]),
                                     reinterpret_cast<T*>(P.wpool[1]), S.nrhs);
         } else if (r.kind == 0) {
@@ -508,6 +764,15 @@ static int block_solve_t(Plan& P, T* xn, int nrhs_total) {
             S = &B.scheds.back();
             const int rc = build_sched(P, nrhs, *S);
             if (rc != CLIQ_OK) return rc;
+            if (S->part_elems > B.part_elems) {   // grow the partial-sum buffer (no launch of this plan uses it now)
+                if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("block solve");
+                if (B.part) cudaFree(B.part);
+                B.part = nullptr;
+                if (cudaMalloc(&B.part, (size_t)S->part_elems * sizeof(T) * (C ? 2 : 1)) != cudaSuccess)
+                    return check_cuda("block solve: partial sums");
+                P.device_bytes += (S->part_elems - B.part_elems) * (int64_t)sizeof(T) * (C ? 2 : 1);
+                B.part_elems = S->part_elems;
+            }
         }
         launches += run_sched<T, C>(P, *S, B, xn + (C ? 2 : 1) * (int64_t)j0 * P.n);
     }
@@ -530,6 +795,7 @@ void free_block_state(Plan& P) {
         if (q.mem) cudaFree(q.mem);
     if (B->y) cudaFree(B->y);
     if (B->g) cudaFree(B->g);
+    if (B->part) cudaFree(B->part);
     delete B;
     P.block_state = nullptr;
 }

@@ -591,3 +591,37 @@ def test_block_ldl_matches_oracle(oracle, kind, precision):
         X2 = cliq.Solve(info, L, B.copy(order="F"))
         assert residual(A, X2, B) <= 1e-12
         assert rel(X2, X) <= 1e-10
+
+
+@pytest.mark.parametrize("kind", ["real", "complex"])
+def test_block_ldl_split_products_64cubed(kind):
+    """At 64^3 the block sweeps split the long products over several CTAs
+    (the root's 4096 x 4096 inv(A11) and the 4096-row A21 of its children)
+    and add the partial sums in a second launch: the block solution matches
+    the LDL_2D one on the same matrix."""
+    n = 64
+    if kind == "real":
+        A = ops.laplacian_3d(n, n, n, 6.1)
+        precision = "double"
+    else:
+        A, _, _ = ops.helmholtz_workload_3d(n, seed=2)
+        precision = "single"
+    B = ops.random_rhs(A.n, 5, seed=4, complex_=kind == "complex")
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, 128)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision=precision)
+    cliq.LDL(info, L, cliq.SymmFrontType.LDL_2D)
+    if precision == "double":
+        X0 = cliq.Solve(info, L, B.copy(order="F"))
+    else:
+        X0, _, rr0 = cliq.RefinedSolve(L, B, 1e-10, 40)
+        assert rr0 <= 1e-10
+    L.Initialize(A.values)
+    cliq.LDL(info, L, cliq.SymmFrontType.BLOCK_LDL_2D)
+    if precision == "double":
+        X = cliq.Solve(info, L, B.copy(order="F"))
+        assert residual(A, X, B) <= 1e-11
+        assert rel(X, X0) <= 1e-10
+    else:
+        X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 40)
+        assert rr <= 1e-10, (it, rr)
+        assert rel(X, X0) <= 1e-8
