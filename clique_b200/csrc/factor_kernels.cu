@@ -301,31 +301,49 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
         __syncthreads();
     }
     // ---- off-diagonal blocks of L^{-1}, one block row at a time ----
-    for (int i = 1; i < nb / kSub; ++i) {
-        for (int idx = tid; idx < i * kSub * kSub; idx += kThreads) {
-            const int j = idx / (kSub * kSub), e = idx % (kSub * kSub), r = e % kSub, c = e / kSub;
+    // Linv_ij = -Linv_ii sum_{k=j}^{i-1} L_ik Linv_kj; thread (r, c) forms entry
+    // (r, c) of every block j < i of the row at once (independent sums)
+    {
+        const int r = tid % kSub, c = tid / kSub;
+#pragma unroll
+        for (int i = 1; i < nb / kSub; ++i) {
             const int R = kSub * i + r;
-            // k = j: Linv_jj is unit lower triangular
-            W tsum = sA[(kSub * j + c) * ld + R];
-            for (int t = c + 1; t < kSub; ++t) tsum += sA[(kSub * j + t) * ld + R] * sA[(kSub * j + t) * ld + kSub * j + c];
-            for (int kk = j + 1; kk < i; ++kk)
+            W acc[nb / kSub - 1];
+#pragma unroll
+            for (int j = 0; j < i; ++j) acc[j] = W{};
+#pragma unroll
+            for (int kk = 0; kk < i; ++kk) {
 #pragma unroll 4
-                for (int t = 0; t < kSub; ++t) tsum += sA[(kSub * kk + t) * ld + R] * sA[(kSub * kk + t) * ld + kSub * j + c];
-            sG[(j * kSub + c) * kSub + r] = tsum;
+                for (int t = 0; t < kSub; ++t) {
+                    const W lik = sA[(kSub * kk + t) * ld + R];                   // L[R][16 kk + t]
+#pragma unroll
+                    for (int j = 0; j <= kk; ++j) {
+                        // Linv[16 kk + t][16 j + c]; Linv_jj is unit lower triangular
+                        const W lv = j < kk ? sA[(kSub * kk + t) * ld + kSub * j + c]
+                                            : (t == c ? vone<W>() : (t > c ? sA[(kSub * kk + t) * ld + kSub * j + c] : W{}));
+                        acc[j] += lik * lv;
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < i; ++j) sG[(j * kSub + c) * kSub + r] = acc[j];
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < i; ++j) acc[j] = sG[(j * kSub + c) * kSub + r];
+            for (int t = 0; t < r; ++t) {
+                const W lit = sA[R * ld + kSub * i + t];                            // Linv_ii[r][t]
+#pragma unroll
+                for (int j = 0; j < i; ++j) acc[j] += lit * sG[(j * kSub + c) * kSub + t];
+            }
+#pragma unroll
+            for (int j = 0; j < i; ++j) sA[R * ld + kSub * j + c] = W{} - acc[j];
+            __syncthreads();
         }
-        __syncthreads();
-        for (int idx = tid; idx < i * kSub * kSub; idx += kThreads) {
-            const int j = idx / (kSub * kSub), e = idx % (kSub * kSub), r = e % kSub, c = e / kSub;
-            const int R = kSub * i + r;
-            W v = sG[(j * kSub + c) * kSub + r];
-            for (int t = 0; t < r; ++t) v += sA[R * ld + kSub * i + t] * sG[(j * kSub + c) * kSub + t];
-            sA[R * ld + kSub * j + c] = W{} - v;
-        }
-        __syncthreads();
     }
     // ---- outputs, each written with consecutive threads on consecutive addresses ----
     X* U = reinterpret_cast<X*>(tinv) + (int64_t)slot * nb * nb;
     X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)(k / nb) * nb * nb;
+#pragma unroll 4
     for (int idx = tid; idx < nb * nb; idx += kThreads) {
         const int i = idx % nb, c = idx / nb;
         const bool in = i < kb && c < kb && i >= c;
@@ -336,6 +354,7 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
     }
     if (dinvT) {
         X* DvT = reinterpret_cast<X*>(dinvT) + f.dinv + (int64_t)(k / nb) * nb * nb;
+#pragma unroll 4
         for (int idx = tid; idx < nb * nb; idx += kThreads) {
             const int c = idx % nb, i = idx / nb;
             const bool in = i < kb && c < kb && i >= c;
