@@ -625,3 +625,21 @@ def test_block_ldl_split_products_64cubed(kind):
         X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 40)
         assert rr <= 1e-10, (it, rr)
         assert rel(X, X0) <= 1e-8
+
+
+@pytest.mark.parametrize("form,precision", [("exact", "single"), ("tiles", "double"), ("exact", "double")])
+def test_solve_form_override(oracle, form, precision, monkeypatch):
+    """CLIQGPU_SOLVE_FORM: FP64 plans run either chain form of the sweeps;
+    FP32 plans always run the product form (with its chain tiles), whatever
+    the variable says."""
+    monkeypatch.setenv("CLIQGPU_SOLVE_FORM", form)
+    n = 14
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=6)
+    B = ops.random_rhs(A.n, 3, seed=8, complex_=True)
+    map_, info, L = build(A, (n, n, n), 64, precision=precision)
+    if precision == "double":
+        X = cliq.Solve(info, L, B.copy(order="F"))
+        assert residual(A, X, B) <= 1e-12
+    else:
+        X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 30)
+        assert rr <= 1e-10, (it, rr)
