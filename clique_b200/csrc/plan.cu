@@ -820,9 +820,7 @@ int cliqgpu_plan_create(const cliq_symm_info* info, int64_t n, const int32_t* ma
     if (const char* e = getenv("CLIQGPU_DIAG_FP64")) P.diag_fp64 = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_FP64_DMMA")) P.fp64_dmma = atoi(e) != 0;
     P.solve_exact = P.precision == CLIQ_FP64 ? 1 : 0;
-    // the substitution form exists for FP64 sweeps only; FP32 sweeps always
-    // run the product form and need its chain tiles
-    if (const char* e = getenv("CLIQGPU_SOLVE_FORM")) P.solve_exact = P.precision == CLIQ_FP64 && strcmp(e, "tiles") != 0;
+    if (const char* e = getenv("CLIQGPU_SOLVE_FORM")) P.solve_exact = strcmp(e, "tiles") != 0;
     if (const char* e = getenv("CLIQGPU_SPLIT")) P.split_f16 = strcmp(e, "tf32") != 0;
     if (const char* e = getenv("CLIQGPU_INPANEL_TC")) P.inpanel_tc = atoi(e) != 0;
     if (const char* e = getenv("CLIQGPU_REFINE")) P.refine_gmres = strcmp(e, "ir") != 0;

@@ -326,7 +326,7 @@ __device__ void fwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
     const T* Dinv = reinterpret_cast<const T*>(a.dinv);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
-    const bool exact = std::is_same<T, double>::value && a.exact != 0;   // FP32 sweeps keep the product form
+    const bool exact = a.exact != 0;
     Xv nxt[NR / kQ];
     bool have_next = false;
     Xv dt[kE];   // exact form: L_ss^{-1} of the current step
@@ -574,7 +574,7 @@ __device__ void fwd_worker(const SweepArgs& a, const FrontDev& f, int fi, int nT
     auto finish_pivot = [&](const Xv (&dv)[kE]) {
         Xv out[NR / kQ];
         reduce_slices<NR>(acc, red, out, r, q);
-        if (std::is_same<T, double>::value && a.exact) {
+        if (a.exact) {
             T* Part = reinterpret_cast<T*>(a.partial);
 #pragma unroll
             for (int b = 0; b < NR / kQ; ++b) {
@@ -676,7 +676,7 @@ __device__ void bwd_chain(const SweepArgs& a, const FrontDev& f, int fi, int nT,
     const T* DinvT = reinterpret_cast<const T*>(a.dinvT);
     const T* Part = reinterpret_cast<const T*>(a.partial);
     T* X = reinterpret_cast<T*>(a.X);
-    const bool exact = std::is_same<T, double>::value && a.exact != 0;   // FP32 sweeps keep the product form
+    const bool exact = a.exact != 0;
     Xv nxt[NR / kQ];
     bool have_next = false;
     Xv dt[kE];   // exact form: op(L_cc^{-1})^T of the current step, as a row slice of the row-major inverse
@@ -1023,7 +1023,7 @@ __device__ void bwd_worker(const SweepArgs& a, const FrontDev& f, int fi, int nT
         row_slice<T, C>(pre, reinterpret_cast<const T*>(a.dinvT), f.dinv + (int64_t)c * kTile * kTile, kTile, r, q, kTile, kTile);
 #pragma unroll
     for (int b = 0; b < NR / kQ; ++b) out[b] += hsum[b];
-    if (std::is_same<T, double>::value && a.exact) {   // substitution form: w_c = y_c - sum, the chain applies the inverse
+    if (a.exact) {   // substitution form: w_c = y_c - sum, the chain applies the inverse
         T* Part = reinterpret_cast<T*>(a.partial);
 #pragma unroll
         for (int b = 0; b < NR / kQ; ++b) {

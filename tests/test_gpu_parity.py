@@ -629,9 +629,9 @@ def test_block_ldl_split_products_64cubed(kind):
 
 @pytest.mark.parametrize("form,precision", [("exact", "single"), ("tiles", "double"), ("exact", "double")])
 def test_solve_form_override(oracle, form, precision, monkeypatch):
-    """CLIQGPU_SOLVE_FORM: FP64 plans run either chain form of the sweeps;
-    FP32 plans always run the product form (with its chain tiles), whatever
-    the variable says."""
+    """CLIQGPU_SOLVE_FORM: the plan and its sweeps use the chosen chain form
+    (product form with chain tiles, or substitution form without them) in
+    either precision."""
     monkeypatch.setenv("CLIQGPU_SOLVE_FORM", form)
     n = 14
     A, _, _ = ops.helmholtz_workload_3d(n, seed=6)
