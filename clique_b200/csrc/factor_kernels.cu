@@ -48,53 +48,56 @@ __device__ __forceinline__ float cabsmax(cx<double> v) { return (float)fmax(fabs
 // 1. extend-add (gather form)
 //
 // Work item (front, j0, i0): columns j0 .. j0+15, rows i0 .. i0+kEARows-1 on
-// or below the diagonal; the CTA sweeps one column at a time down a
-// contiguous run of rows (consecutive threads, consecutive rows: few DRAM
-// pages open per CTA), each thread taking kEAUnroll rows per pass with all
-// their loads issued before any store.
+// or below the diagonal.  The children's row maps of the item's rows are
+// staged in shared memory once; the CTA then sweeps one column at a time
+// down a contiguous run of rows (consecutive threads, consecutive rows: few
+// DRAM pages open per CTA), each thread issuing the gathers of all its rows
+// of the column before any store.
 // ---------------------------------------------------------------------------
-constexpr int kEAUnroll = 4;
+constexpr int kEAPer = kEARows / kThreads;   // rows of a column per thread
+static_assert(kEARows % kThreads == 0, "whole rows per thread");
 
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
                                                               T* __restrict__ L, T* __restrict__ pool0, T* __restrict__ pool1,
                                                               const int32_t* __restrict__ cmaps) {
     using X = V<T, C>;
+    __shared__ int32_t s_map[2][kEARows];
     const int4 it = items[blockIdx.x];
     const FrontDev f = F[it.x];
-    const int j0 = it.y;
+    const int j0 = it.y, i0 = it.z;
     T* up = f.pool == 0 ? pool0 : pool1;
     const T* cp = f.pool == 0 ? pool1 : pool0;
     const int32_t* lm = f.cmap >= 0 ? cmaps + f.cmap : nullptr;
     const int32_t* rm = lm ? lm + f.m : nullptr;
-    const int i_end = min(f.m, it.z + kEARows);
-    for (int jj = 0; jj < kEACols; ++jj) {
-        const int j = j0 + jj;
-        if (j >= f.m) break;
+    const int i_end = min(f.m, i0 + kEARows);
+    const int j_end = min(f.m, j0 + kEACols);
+    for (int i = max(j0, i0) + threadIdx.x; i < i_end; i += kThreads) {
+        s_map[0][i - i0] = lm ? lm[i] : -1;
+        s_map[1][i - i0] = rm ? rm[i] : -1;
+    }
+    __syncthreads();
+    for (int j = j0; j < j_end; ++j) {
         const int lj = lm ? lm[j] : -1, rj = rm ? rm[j] : -1;
-        for (int ib = max(j, it.z) + threadIdx.x; ib < i_end; ib += kEAUnroll * blockDim.x) {
-            int li[kEAUnroll], ri[kEAUnroll];
+        const int ib = max(j, i0) + threadIdx.x;
+        X v[kEAPer];
 #pragma unroll
-            for (int u = 0; u < kEAUnroll; ++u) {
-                const int i = ib + u * blockDim.x;
-                li[u] = (lj >= 0 && i < i_end) ? lm[i] : -1;
-                ri[u] = (rj >= 0 && i < i_end) ? rm[i] : -1;
+        for (int u = 0; u < kEAPer; ++u) {
+            const int i = ib + u * kThreads;
+            X t = X{};
+            if (i < i_end) {
+                const int li = lj >= 0 ? s_map[0][i - i0] : -1, ri = rj >= 0 ? s_map[1][i - i0] : -1;
+                if (li >= 0) t += ldv<T, C>(cp, f.CU[0] + li + (int64_t)lj * f.cu[0]);
+                if (ri >= 0) t += ldv<T, C>(cp, f.CU[1] + ri + (int64_t)rj * f.cu[1]);
             }
-            X v[kEAUnroll];
+            v[u] = t;
+        }
 #pragma unroll
-            for (int u = 0; u < kEAUnroll; ++u) {
-                X t = X{};
-                if (li[u] >= 0) t += ldv<T, C>(cp, f.CU[0] + li[u] + (int64_t)lj * f.cu[0]);
-                if (ri[u] >= 0) t += ldv<T, C>(cp, f.CU[1] + ri[u] + (int64_t)rj * f.cu[1]);
-                v[u] = t;
-            }
-#pragma unroll
-            for (int u = 0; u < kEAUnroll; ++u) {
-                const int i = ib + u * blockDim.x;
-                if (i >= i_end) break;
-                if (j < f.n) stv<T, C>(L, f.L + i + (int64_t)j * f.m, v[u]);
-                else stv<T, C>(up, f.U + (i - f.n) + (int64_t)(j - f.n) * f.u, v[u]);
-            }
+        for (int u = 0; u < kEAPer; ++u) {
+            const int i = ib + u * kThreads;
+            if (i >= i_end) break;
+            if (j < f.n) stv<T, C>(L, f.L + i + (int64_t)j * f.m, v[u]);
+            else stv<T, C>(up, f.U + (i - f.n) + (int64_t)(j - f.n) * f.u, v[u]);
         }
     }
 }
