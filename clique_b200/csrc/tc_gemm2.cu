@@ -114,37 +114,30 @@ __global__ void __launch_bounds__(kTcBM) pack_kernel(const PackJob* __restrict__
 // ---------------------------------------------------------------------------
 constexpr int kKS16 = 2 * kKS;
 
-template <bool C, bool CJ>
-__device__ __forceinline__ V<float, C> pack_load(const PackJob& jb, const float* __restrict__ L, const double* __restrict__ D, int r,
-                                                 int k) {
-    using X = V<float, C>;
-    using W = DV<C>;
-    X v{};
-    if (r < jb.R && k < jb.K) {
-        v = ldv<float, C>(L, jb.src + r + (int64_t)k * jb.ld);
-        if (jb.d >= 0) v = conv<X>(reinterpret_cast<const W*>(D)[jb.d + k]) * opc<CJ>(v);
-    }
-    return v;
-}
 __device__ __forceinline__ float absmax(float v) { return fabsf(v); }
 __device__ __forceinline__ float absmax(cx<float> v) { return fmaxf(fabsf(v.r), fabsf(v.i)); }
 
 // scale and split one row's 16 values of block blk into the FP16 planes at
 // float offset dst (inverse row scale at dst_scale + r when ks == 0); the
 // row maxima come from eblk (nkb blocks from emax) or erow
-template <bool C>
-__device__ __forceinline__ void pack_f16_planes(const PackJob& jb, const V<float, C> (&v)[kKS16], int64_t dst, int64_t dst_scale,
-                                                int64_t emax, int R, int64_t blk, int ks, int row, int r,
-                                                const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
-                                                float* __restrict__ out) {
+// largest |component| of row r over the job's K columns (0 beyond R)
+__device__ __forceinline__ float pack_row_max(const PackJob& jb, int64_t emax, int R, int r, const uint32_t* __restrict__ eblk,
+                                              const uint32_t* __restrict__ erow) {
     float mx = 0.f;
     if (r < R) {
         if (jb.nkb > 0) {
+#pragma unroll 4
             for (int b = 0; b < jb.nkb; ++b) mx = fmaxf(mx, __uint_as_float(eblk[emax + (int64_t)r * jb.enT + b]));
         } else {
             mx = __uint_as_float(erow[emax + r]);
         }
     }
+    return mx;
+}
+
+template <bool C>
+__device__ __forceinline__ void pack_f16_planes(const PackJob& jb, const V<float, C> (&v)[kKS16], int64_t dst, int64_t dst_scale,
+                                                float mx, int64_t blk, int ks, int row, int r, float* __restrict__ out) {
     // s = 2^(14 - e) for mx in [2^e, 2^(e+1)): s * mx in [2^14, 2^15)
     int e = mx > 0.f ? ((__float_as_int(mx) >> 23) & 0xff) - 127 : 0;
     e = max(-100, min(100, e));
@@ -186,6 +179,7 @@ __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restri
                                                        float* __restrict__ out) {
     using X = V<float, C>;
     using W = DV<C>;
+    __shared__ X s_da[kKS16], s_ds[kKS16];   // pivots of this k step: A scaling (jb.d) and S = D op(rows) (jb.dS)
     const int64_t bid = blockIdx.x;
     const int lo = bmap[bid];
     const PackJob jb = jobs[lo];
@@ -193,20 +187,38 @@ __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restri
     const int nks = (jb.K + kKS16 - 1) / kKS16;
     const int tile = (int)(blk / nks), ks = (int)(blk % nks);
     const int row = threadIdx.x;
-    if (row >= jb.tile_rows) return;
     const int r = tile * jb.tile_rows + row;
+    const bool sjob = jb.RS > 0 && tile * jb.tile_rows < jb.RS;
+    // every load of the block is issued up front: the L row, the row maxima
+    // of both operands and the k step's pivots (one load per k, shared)
     X v[kKS16];
 #pragma unroll
-    for (int q = 0; q < kKS16; ++q) v[q] = pack_load<C, CJ>(jb, L, D, r, ks * kKS16 + q);
-    pack_f16_planes<C>(jb, v, jb.dst, jb.dst_scale, jb.emax, jb.R, blk, ks, row, r, eblk, erow, out);
+    for (int q = 0; q < kKS16; ++q) {
+        const int k = ks * kKS16 + q;
+        v[q] = (row < jb.tile_rows && r < jb.R && k < jb.K) ? ldv<float, C>(L, jb.src + r + (int64_t)k * jb.ld) : X{};
+    }
+    const float mxa = row < jb.tile_rows ? pack_row_max(jb, jb.emax, jb.R, r, eblk, erow) : 0.f;
+    const float mxs = (sjob && row < jb.tile_rows) ? pack_row_max(jb, jb.emaxS, jb.RS, r, eblk, erow) : 0.f;
+    if (row < kKS16) {
+        const int k = ks * kKS16 + row;
+        s_da[row] = (jb.d >= 0 && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.d + k]) : X{};
+        s_ds[row] = (sjob && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.dS + k]) : X{};
+    }
+    __syncthreads();
+    if (row >= jb.tile_rows) return;
+    if (jb.d >= 0) {
+#pragma unroll
+        for (int q = 0; q < kKS16; ++q) v[q] = s_da[q] * opc<CJ>(v[q]);
+    }
+    pack_f16_planes<C>(jb, v, jb.dst, jb.dst_scale, mxa, blk, ks, row, r, out);
     // the S operand from the same rows (a prefix of this job's rows)
-    if (jb.RS > 0 && tile * jb.tile_rows < jb.RS) {
+    if (sjob) {
 #pragma unroll
         for (int q = 0; q < kKS16; ++q) {
             const int k = ks * kKS16 + q;
-            v[q] = (r < jb.RS && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.dS + k]) * opc<CJ>(v[q]) : X{};
+            v[q] = (r < jb.RS && k < jb.K) ? s_ds[q] * opc<CJ>(v[q]) : X{};
         }
-        pack_f16_planes<C>(jb, v, jb.dstS, jb.dst_scaleS, jb.emaxS, jb.RS, blk, ks, row, r, eblk, erow, out);
+        pack_f16_planes<C>(jb, v, jb.dstS, jb.dst_scaleS, mxs, blk, ks, row, r, out);
     }
 }
 
