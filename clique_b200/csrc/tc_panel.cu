@@ -117,9 +117,19 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
     const int rows = min(kPanelRows, f.m - r0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+    // the in-panel update's packing parameters, fetched now so that the
+    // epilogue does not wait for them
+    __shared__ int64_t s_pk[4];   // packA, packB, scaleA, scaleB (float offsets)
+    __shared__ int32_t s_pkn[2];  // K, N
+    const bool prepack = probs && it.w >= 0;
     if (threadIdx.x == 0) {
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x == kPanelRows && prepack) {
+        const GemmProb& pr = probs[it.w];
+        s_pk[0] = pr.packA; s_pk[1] = pr.packB; s_pk[2] = pr.scaleA; s_pk[3] = pr.scaleB;
+        s_pkn[0] = pr.K; s_pkn[1] = pr.N;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)), "r"(PC::kTmem) : "memory");
@@ -249,11 +259,12 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
             // scaled by the row maximum ml, and for the first N problem rows
             // the S = D op(L21) planes scaled by ms, in the layout and with
             // the scales the operand packing would produce
-            if (probs && it.w >= 0) {
-                const GemmProb pr = probs[it.w];
+            if (prepack) {
+                const int64_t packA = s_pk[0], packB = s_pk[1], scaleA = s_pk[2], scaleB = s_pk[3];
+                const int pK = s_pkn[0], pN = s_pkn[1];
                 const int rp = tile * kPanelRows + i;   // row in the problem
-                const int nks = (pr.K + 15) / 16;
-                const bool srow = tile * kPanelRows < pr.N;
+                const int nks = (pK + 15) / 16;
+                const bool srow = tile * kPanelRows < pN;
                 constexpr int planes = C ? 4 : 2;
                 constexpr int64_t plane_bytes = (int64_t)kPanelRows * 16 * 2;
                 auto scale_of = [](float mx, float* inv) {
@@ -263,9 +274,9 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
                     return __int_as_float((127 + 14 - e) << 23);
                 };
                 float inv_sa, inv_ss;
-                const float sa = scale_of(vr ? ml : 0.f, &inv_sa), ss = scale_of(vr && rp < pr.N ? ms : 0.f, &inv_ss);
-                pack[pr.scaleA + rp] = inv_sa;
-                if (srow) pack[pr.scaleB + rp] = inv_ss;
+                const float sa = scale_of(vr ? ml : 0.f, &inv_sa), ss = scale_of(vr && rp < pN ? ms : 0.f, &inv_ss);
+                pack[scaleA + rp] = inv_sa;
+                if (srow) pack[scaleB + rp] = inv_ss;
 #pragma unroll 1
                 for (int ks = 0; ks < nks; ++ks) {
                     float re[16], im[16];
@@ -280,7 +291,7 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
                         if (c >= kb || !vr) v[q] = X{};
                     }
                     const int64_t blk = (int64_t)tile * nks + ks;
-                    uint8_t* base = reinterpret_cast<uint8_t*>(pack + pr.packA) + blk * plane_bytes * planes;
+                    uint8_t* base = reinterpret_cast<uint8_t*>(pack + packA) + blk * plane_bytes * planes;
                     float y[16];
                     uint4 h, l;
 #pragma unroll
@@ -308,9 +319,9 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
                         for (int q = 0; q < 16; ++q) {
                             X sv = v[q];
                             if constexpr (C) { if (conj) sv.i = -sv.i; }
-                            v[q] = rp < pr.N ? s_d[16 * ks + q] * sv : X{};
+                            v[q] = rp < pN ? s_d[16 * ks + q] * sv : X{};
                         }
-                        uint8_t* bs = reinterpret_cast<uint8_t*>(pack + pr.packB) + blk * plane_bytes * planes;
+                        uint8_t* bs = reinterpret_cast<uint8_t*>(pack + packB) + blk * plane_bytes * planes;
 #pragma unroll
                         for (int q = 0; q < 16; ++q) {
                             if constexpr (C) y[q] = v[q].r * ss; else y[q] = v[q] * ss;
