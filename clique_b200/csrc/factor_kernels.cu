@@ -48,8 +48,8 @@ __device__ __forceinline__ float cabsmax(cx<double> v) { return (float)fmax(fabs
 // 1. extend-add (gather form)
 //
 // Work item (front, j0, i0): columns j0 .. j0+15, rows i0 .. i0+kEARows-1 on
-// or below the diagonal.  The children's row maps of the item's rows are
-// staged in shared memory once; the CTA then sweeps one column at a time
+// or below the diagonal.  The children's maps of the item's rows and
+// columns are staged in shared memory once; the CTA then sweeps one column at a time
 // down a contiguous run of rows (consecutive threads, consecutive rows: few
 // DRAM pages open per CTA), each thread issuing the gathers of all its rows
 // of the column before any store.
@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
                                                               const int32_t* __restrict__ cmaps) {
     using X = V<T, C>;
     __shared__ int32_t s_map[2][kEARows];
+    __shared__ int32_t s_cmap[2][kEACols];
     const int4 it = items[blockIdx.x];
     const FrontDev f = F[it.x];
     const int j0 = it.y, i0 = it.z;
@@ -76,9 +77,14 @@ __global__ void __launch_bounds__(kThreads) extend_add_kernel(const FrontDev* __
         s_map[0][i - i0] = lm ? lm[i] : -1;
         s_map[1][i - i0] = rm ? rm[i] : -1;
     }
+    if (threadIdx.x < kEACols) {
+        const int j = j0 + threadIdx.x;
+        s_cmap[0][threadIdx.x] = (lm && j < j_end) ? lm[j] : -1;
+        s_cmap[1][threadIdx.x] = (rm && j < j_end) ? rm[j] : -1;
+    }
     __syncthreads();
     for (int j = j0; j < j_end; ++j) {
-        const int lj = lm ? lm[j] : -1, rj = rm ? rm[j] : -1;
+        const int lj = s_cmap[0][j - j0], rj = s_cmap[1][j - j0];
         const int ib = max(j, i0) + threadIdx.x;
         X v[kEAPer];
 #pragma unroll
