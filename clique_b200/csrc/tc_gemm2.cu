@@ -239,6 +239,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const Gem
     uint64_t* empty = full + kStages;
     uint64_t* done = empty + kStages;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ float s_sb[kBN];   // 2xFP16: inverse row scales of the tile's S columns
 
     // tile of this CTA: kBM-row tiles ti, kBN-column tiles tj, needed when ti >= kRatio tj
     const int64_t bid = blockIdx.x;
@@ -326,15 +327,22 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const Gem
         }
     } else {
         // ---- epilogue (warps 0-3 own TMEM lanes 32w .. 32w+31) ----
+        // 2xFP16: the row scales of A (this thread's row) and of the tile's S
+        // columns are fetched while the products run
+        const int i = i0 + warp * 32 + lane;
+        const bool vrow = i < pr.M;
+        const float sa = F16 && vrow ? pack[pr.scaleA + i] : 1.f;
+        if constexpr (F16) {
+            static_assert(kBN == 128, "one S column per epilogue thread");
+            const int jt = warp * 32 + lane;
+            s_sb[jt] = j0 + jt < pr.N ? pack[pr.scaleB + j0 + jt] : 0.f;
+            asm volatile("bar.sync 1, 128;" ::: "memory");   // the four epilogue warps
+        }
         const bool ok = mbar_wait(done, 0, status, 3);
         tc_fence_after();
         if (ok) {
             float* Cb = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
-            const int i = i0 + warp * 32 + lane;
             const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-            const bool vrow = i < pr.M;
-            // 2xFP16: undo the row scales of A (this thread's row) and S (columns)
-            const float sa = F16 && vrow ? pack[pr.scaleA + i] : 1.f;
 #pragma unroll 1
             for (int c0 = 0; c0 < kBN; c0 += 16) {
                 if (j0 + c0 >= pr.N || j0 + c0 > i0 + kBM - 1) break;   // warp-uniform: nothing left in this tile row block
@@ -348,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const Gem
                         if (j < pr.N && i >= j) {
                             const int64_t e = pr.C + i + (int64_t)j * pr.ldc;
                             float f = 1.f;
-                            if constexpr (F16) f = sa * __ldg(pack + pr.scaleB + j);
+                            if constexpr (F16) f = sa * s_sb[j - j0];
                             if constexpr (C) red_sub2(Cb + 2 * e, re[q] * f, im[q] * f);
                             else red_sub(Cb + e, re[q] * f);
                         }
