@@ -62,6 +62,9 @@ enum SweepItem : int { kItemChain = 0, kItemPivotRows = 1, kItemLowerRows = 2, k
 // fronts solved by one CTA per sweep (no flags): at most two pivot blocks
 // and kWholeLowerRows rows below the pivots
 constexpr int kWholeLowerRows = 512;
+// fronts of one pivot block and at most kTinyLowerRows rows below it are swept
+// by one warp each, several fronts per CTA
+constexpr int kTinyLowerRows = 64;
 
 // One front as the kernels see it.  Offsets are in elements (a complex
 // element is two scalars).
@@ -167,6 +170,8 @@ struct SolveLevel {
     int32_t nbwd;
     int32_t depth;
     int32_t gather_chunks;   // 1024-row chunks of the level's tallest front (gather grid y)
+    int64_t tiny;            // offset into tiny_fronts: the level's fronts swept one per warp
+    int32_t ntiny;
 };
 
 // ---------------------------------------------------------------------------
@@ -264,6 +269,7 @@ struct Plan {
     std::vector<int64_t> asm_level;
     int32_t* perm = nullptr;      // inverse map: ND -> natural
     int32_t* level_fronts = nullptr;
+    int32_t* tiny_fronts = nullptr;   // per level, fronts swept one per warp (SolveLevel::tiny)
     int32_t* flags = nullptr;     // worker flags (flags_total, one per pivot block), then helper flags
     int32_t* tickets = nullptr;
     int32_t* status = nullptr;    // [0] first zero pivot + 1 (min), [1] timeout flag

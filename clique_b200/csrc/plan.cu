@@ -75,7 +75,7 @@ static int dev_alloc(Plan& P, void** dst, size_t bytes) {
 void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.bmap, P.dest, P.asm_src, P.asm_dst,
-                    P.perm, P.level_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
+                    P.perm, P.level_fronts, P.tiny_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
                     P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov, P.pack3};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -553,7 +553,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     // ---- solve schedule ----
     P.solve_levels.assign(P.max_depth + 1, SolveLevel{});
     P.helpers_total = 0;
-    std::vector<int32_t> level_fronts;
+    std::vector<int32_t> level_fronts, tiny_fronts;
     std::vector<int32_t> chain_items;   // int4 {front, block, 0, 0}: chain tiles to form after the factorization
     int flag = 0;
     for (int d = 0; d <= P.max_depth; ++d) {
@@ -569,6 +569,14 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         // rows below the pivots (they only wait on chains, all issued before)
         // Small fronts (whole()) get one CTA that solves the front alone, last.
         auto whole = [](const FrontDev& f) { return f.n <= 2 * kTile && f.m - f.n <= kWholeLowerRows; };
+        // one pivot block and few rows below: one warp per front (a subset of whole())
+        auto tiny = [](const FrontDev& f) { return f.n <= kTile && f.m - f.n <= kTinyLowerRows; };
+        sl.tiny = (int64_t)tiny_fronts.size();
+        for (int s : P.level_list[d]) {
+            const FrontDev& f = P.hfronts[s];
+            if (f.n > 0 && f.m > 0 && tiny(f)) tiny_fronts.push_back(s);
+        }
+        sl.ntiny = (int32_t)(tiny_fronts.size() - sl.tiny);
         sl.fwd_items = (int64_t)items.size() / 4;
         for (int s : P.level_list[d]) {
             FrontDev& f = P.hfronts[s];
@@ -594,7 +602,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
-            if (f.n > 0 && f.m > 0 && whole(f)) push_item(s, kItemWhole, 0, 0);
+            if (f.n > 0 && f.m > 0 && whole(f) && !tiny(f)) push_item(s, kItemWhole, 0, 0);
         }
         sl.nfwd = (int32_t)(items.size() / 4 - sl.fwd_items);
         // backward: first the helpers (rows below the pivots beyond the first
@@ -622,7 +630,7 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
         }
         for (int s : P.level_list[d]) {
             const FrontDev& f = P.hfronts[s];
-            if (f.n > 0 && f.m > 0 && whole(f)) push_item(s, kItemWhole, 0, 0);
+            if (f.n > 0 && f.m > 0 && whole(f) && !tiny(f)) push_item(s, kItemWhole, 0, 0);
         }
         sl.nbwd = (int32_t)(items.size() / 4 - sl.bwd_items);
     }
@@ -724,6 +732,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.dest, dest));
     TRY(dev_upload(P, &P.perm, inv));
     TRY(dev_upload(P, &P.level_fronts, level_fronts));
+    if (tiny_fronts.empty()) tiny_fronts.push_back(0);
+    TRY(dev_upload(P, &P.tiny_fronts, tiny_fronts));
     std::vector<int32_t> zeros_flags(P.flags_total + P.helpers_total, 0);
     TRY(dev_upload(P, &P.flags, zeros_flags));
     P.nchain_items = (int32_t)(chain_items.size() / 4);

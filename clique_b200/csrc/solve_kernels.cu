@@ -258,19 +258,173 @@ __global__ void __launch_bounds__(kSolveThreads) fwd_gather_kernel(const FrontDe
 }
 
 // ---------------------------------------------------------------------------
+// tiny fronts (one pivot block, at most kTinyLowerRows rows below): one warp
+// per front, kTinyWarps fronts per CTA, no flags.  Lane = pivot row / column
+// (lane and lane + 32); the right-hand-side rows a product needs are staged
+// in the warp's slice of shared memory and read as broadcasts.
+//   forward   x_T = L11^{-1} x_T,   W_B -= L21 x_T
+//   backward  z = x_T - op(L21)^T X[lowerStruct],   x_T = op(L11^{-1})^T z
+// ---------------------------------------------------------------------------
+constexpr int kTinyWarps = 8;
+
+template <class T, bool C, int NR>
+__global__ void __launch_bounds__(32 * kTinyWarps) tiny_fwd_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+                                                                   int nf, T* __restrict__ X, int64_t ldx, T* __restrict__ w0,
+                                                                   T* __restrict__ w1, const T* __restrict__ L,
+                                                                   const T* __restrict__ dinv, int nrhs) {
+    using Xv = V<T, C>;
+    extern __shared__ __align__(16) unsigned char tiny_smem[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int fi = blockIdx.x * kTinyWarps + w;
+    if (fi >= nf) return;   // warp-uniform; only warp barriers below
+    Xv* sb = reinterpret_cast<Xv*>(tiny_smem) + (int64_t)w * kTile * NR;
+    const FrontDev f = F[fl[fi]];
+    const int n = f.n, u = f.m - f.n;
+    for (int e = lane; e < n * NR; e += 32) {
+        const int k = e % n, j = e / n;
+        sb[k * NR + j] = j < nrhs ? ldv<T, C>(X, f.off + k + (int64_t)j * ldx) : Xv{};
+    }
+    __syncwarp();
+    // x_T = L11^{-1} b: rows lane and lane + 32 (column k of the inverse is contiguous)
+    const Xv* Dv = reinterpret_cast<const Xv*>(dinv) + f.dinv;
+    Xv a0[NR], a1[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) a0[j] = a1[j] = Xv{};
+    for (int k = 0; k < n; ++k) {
+        const Xv d0 = lane < n ? Dv[lane + k * kTile] : Xv{};
+        const Xv d1 = lane + 32 < n ? Dv[lane + 32 + k * kTile] : Xv{};
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            const Xv bv = sb[k * NR + j];
+            mac(a0[j], d0, bv);
+            mac(a1[j], d1, bv);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        if (lane < n) {
+            if (j < nrhs) stv<T, C>(X, f.off + lane + (int64_t)j * ldx, a0[j]);
+            sb[lane * NR + j] = a0[j];
+        }
+        if (lane + 32 < n) {
+            if (j < nrhs) stv<T, C>(X, f.off + lane + 32 + (int64_t)j * ldx, a1[j]);
+            sb[(lane + 32) * NR + j] = a1[j];
+        }
+    }
+    __syncwarp();
+    // W_B -= L21 x_T, 32 rows at a time (row i of L21: stride m between columns)
+    T* wb = f.pool == 0 ? w0 : w1;
+    const Xv* Lf = reinterpret_cast<const Xv*>(L) + f.L + f.n;
+    for (int i0 = 0; i0 < u; i0 += 32) {
+        const int i = i0 + lane;
+        Xv acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = Xv{};
+        for (int k = 0; k < n; ++k) {
+            const Xv l = i < u ? Lf[i + (int64_t)k * f.m] : Xv{};
+#pragma unroll
+            for (int j = 0; j < NR; ++j) mac(acc[j], l, sb[k * NR + j]);
+        }
+        if (i < u) {
+#pragma unroll
+            for (int j = 0; j < NR; ++j) {
+                if (j >= nrhs) break;
+                const int64_t e = f.W * nrhs + i + (int64_t)j * f.u;
+                stv<T, C>(wb, e, ldv<T, C>(wb, e) - acc[j]);
+            }
+        }
+    }
+}
+
+template <class T, bool C, bool CJ, int NR>
+__global__ void __launch_bounds__(32 * kTinyWarps) tiny_bwd_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+                                                                   int nf, T* __restrict__ X, int64_t ldx, const T* __restrict__ L,
+                                                                   const T* __restrict__ dinvT, const int32_t* __restrict__ lower,
+                                                                   int nrhs) {
+    using Xv = V<T, C>;
+    extern __shared__ __align__(16) unsigned char tiny_smem[];
+    const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int fi = blockIdx.x * kTinyWarps + w;
+    if (fi >= nf) return;   // warp-uniform; only warp barriers below
+    Xv* sb = reinterpret_cast<Xv*>(tiny_smem) + (int64_t)w * kTile * NR;
+    const FrontDev f = F[fl[fi]];
+    const int n = f.n, u = f.m - f.n;
+    Xv a0[NR], a1[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        a0[j] = (lane < n && j < nrhs) ? ldv<T, C>(X, f.off + lane + (int64_t)j * ldx) : Xv{};
+        a1[j] = (lane + 32 < n && j < nrhs) ? ldv<T, C>(X, f.off + lane + 32 + (int64_t)j * ldx) : Xv{};
+    }
+    // z = y - op(L21)^T x_B, the solved rows below staged 32 at a time
+    const Xv* Lf = reinterpret_cast<const Xv*>(L) + f.L + f.n;
+    for (int i0 = 0; i0 < u; i0 += 32) {
+        const int i = i0 + lane;
+        const int gi = i < u ? lower[f.lower + i] : -1;
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < NR; ++j) sb[lane * NR + j] = (gi >= 0 && j < nrhs) ? ldv<T, C>(X, gi + (int64_t)j * ldx) : Xv{};
+        __syncwarp();
+        const int cn = min(32, u - i0);
+        for (int t = 0; t < cn; ++t) {
+            const Xv l0 = lane < n ? opc<CJ>(Lf[i0 + t + (int64_t)lane * f.m]) : Xv{};
+            const Xv l1 = lane + 32 < n ? opc<CJ>(Lf[i0 + t + (int64_t)(lane + 32) * f.m]) : Xv{};
+#pragma unroll
+            for (int j = 0; j < NR; ++j) {
+                const Xv xv = sb[t * NR + j];
+                a0[j] -= l0 * xv;
+                a1[j] -= l1 * xv;
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        if (lane < n) sb[lane * NR + j] = a0[j];
+        if (lane + 32 < n) sb[(lane + 32) * NR + j] = a1[j];
+    }
+    __syncwarp();
+    // x_T[k] = sum_t op(Linv[t][k]) z[t]; Linv[t][k] is element k + 64 t of the row-major copy
+    const Xv* DvT = reinterpret_cast<const Xv*>(dinvT) + f.dinv;
+    Xv r0[NR], r1[NR];
+#pragma unroll
+    for (int j = 0; j < NR; ++j) r0[j] = r1[j] = Xv{};
+    for (int t = 0; t < n; ++t) {
+        const Xv d0 = lane < n ? opc<CJ>(DvT[lane + t * kTile]) : Xv{};
+        const Xv d1 = lane + 32 < n ? opc<CJ>(DvT[lane + 32 + t * kTile]) : Xv{};
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            const Xv zv = sb[t * NR + j];
+            mac(r0[j], d0, zv);
+            mac(r1[j], d1, zv);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NR; ++j) {
+        if (j >= nrhs) break;
+        if (lane < n) stv<T, C>(X, f.off + lane + (int64_t)j * ldx, r0[j]);
+        if (lane + 32 < n) stv<T, C>(X, f.off + lane + 32 + (int64_t)j * ldx, r1[j]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // diagonal solve X := D^{-1} X (FP64 pivots)
 // ---------------------------------------------------------------------------
+// thread = row p: its pivot is read once for all right-hand sides, the
+// columns' loads issued before the divisions
 template <class T, bool C>
 __global__ void diag_scale_kernel(T* __restrict__ X, int64_t ldx, int64_t n, int nrhs, const double* __restrict__ D) {
     using Xv = V<T, C>;
     using W = DV<C>;
-    const int64_t total = n * nrhs;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t p = idx % n, j = idx / n;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
         const W d = reinterpret_cast<const W*>(D)[p];
-        const int64_t e = p + j * ldx;
-        const W x = conv<W>(ldv<T, C>(X, e));
-        stv<T, C>(X, e, conv<Xv>(x / d));
+        Xv x[kMaxRhsChunk];
+#pragma unroll
+        for (int j = 0; j < kMaxRhsChunk; ++j)
+            if (j < nrhs) x[j] = ldv<T, C>(X, p + j * ldx);
+#pragma unroll
+        for (int j = 0; j < kMaxRhsChunk; ++j)
+            if (j < nrhs) stv<T, C>(X, p + j * ldx, conv<Xv>(conv<W>(x[j]) / d));
     }
 }
 
@@ -1084,10 +1238,13 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     using Xv = V<T, C>;
     const size_t smem_fwd = sizeof(Xv) * (4 + kQ) * kTile * NR;
     const size_t smem_bwd = sizeof(Xv) * ((3 + kQ) * kTile * NR + kTile * (kTile + 1)) + sizeof(int32_t) * kLowerChunkTiles * kTile;
+    const size_t smem_tiny = sizeof(Xv) * kTinyWarps * kTile * NR;
     static bool attr_done = false;
     if (!attr_done) {
         cudaFuncSetAttribute(fwd_sweep_kernel<T, C, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fwd);
         cudaFuncSetAttribute(bwd_sweep_kernel<T, C, CJ, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bwd);
+        cudaFuncSetAttribute(tiny_fwd_kernel<T, C, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tiny);
+        cudaFuncSetAttribute(tiny_bwd_kernel<T, C, CJ, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tiny);
         attr_done = true;
     }
     const int4* items = reinterpret_cast<const int4*>(P.items);
@@ -1122,6 +1279,12 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
         fwd_gather_kernel<T, C><<<dim3(lv.nfronts, lv.gather_chunks), kSolveThreads, 0, P.stream>>>(
             P.fronts, P.level_fronts + lv.fronts, X, P.n, w0, w1, P.cmaps, nrhs);
         ++launches;
+        if (lv.ntiny > 0) {
+            tiny_fwd_kernel<T, C, NR><<<(lv.ntiny + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, smem_tiny, P.stream>>>(
+                P.fronts, P.tiny_fronts + lv.tiny, lv.ntiny, X, P.n, w0, w1, reinterpret_cast<const T*>(P.L),
+                reinterpret_cast<const T*>(P.dinv), nrhs);
+            ++launches;
+        }
         if (lv.nfwd > 0) {
             a.items = items + lv.fwd_items;
             a.ticket = P.tickets + 2 * d;
@@ -1134,6 +1297,12 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
     ++launches;
     for (int d = 0; d <= P.max_depth; ++d) {
         const SolveLevel& lv = P.solve_levels[d];
+        if (lv.ntiny > 0) {
+            tiny_bwd_kernel<T, C, CJ, NR><<<(lv.ntiny + kTinyWarps - 1) / kTinyWarps, 32 * kTinyWarps, smem_tiny, P.stream>>>(
+                P.fronts, P.tiny_fronts + lv.tiny, lv.ntiny, X, P.n, reinterpret_cast<const T*>(P.L),
+                reinterpret_cast<const T*>(P.dinvT), P.lower, nrhs);
+            ++launches;
+        }
         if (lv.nbwd == 0) continue;
         a.items = items + lv.bwd_items;
         a.ticket = P.tickets + 2 * d + 1;
