@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
 #pragma unroll
     for (int p = 0; p < nb / kSub; ++p) {
         const int b0 = kSub * p;
+        if (b0 >= kb) break;   // the rest is the identity padding (kb < 64: small fronts, last blocks)
         // ---- 16 x 16 sub-block: LDL and inverse ----
         W a = sr >= sc ? sA[(b0 + sc) * ld + b0 + sr] : opc<CJ>(sA[(b0 + sr) * ld + b0 + sc]);
         W x = sr == sc ? vone<W>() : W{};
@@ -316,6 +317,7 @@ __global__ void __launch_bounds__(kThreads, 2) diag_ldl_kernel(const FrontDev* _
         const int r = tid % kSub, c = tid / kSub;
 #pragma unroll
         for (int i = 1; i < nb / kSub; ++i) {
+            if (kSub * i >= kb) break;   // block rows of the identity padding are not output
             const int R = kSub * i + r;
             W acc[nb / kSub - 1];
 #pragma unroll

@@ -152,7 +152,8 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
 #pragma unroll
         for (int t = 0; t < nb; ++t) v[t] = v[t] * s;
 #pragma unroll
-        for (int ks = 0; ks < kPanelSteps; ++ks) put_row16<C>(sAop, i, ks, v + 16 * ks, kPanelSteps * PC::kABlock, PC::kABlock);
+        for (int ks = 0; ks < kPanelSteps; ++ks)
+            if (16 * ks < kb) put_row16<C>(sAop, i, ks, v + 16 * ks, kPanelSteps * PC::kABlock, PC::kABlock);
     } else {
         // ---- B: row c of W^T, B[c][t] = U[t][c] / d_c ----
         const int c = threadIdx.x - kPanelRows;
@@ -180,7 +181,8 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
 #pragma unroll
         for (int t = 0; t < nb; ++t) v[t] = v[t] * s;
 #pragma unroll
-        for (int ks = 0; ks < kPanelSteps; ++ks) put_row16<C>(sBop, c, ks, v + 16 * ks, kPanelSteps * PC::kBBlock, PC::kBBlock);
+        for (int ks = 0; ks < kPanelSteps; ++ks)
+            if (16 * ks < kb) put_row16<C>(sBop, c, ks, v + 16 * ks, kPanelSteps * PC::kBBlock, PC::kBBlock);
     }
     // operands written by the generic proxy, read by the tensor cores
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -194,7 +196,8 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
             const uint32_t idp = idesc_f16(kPanelRows, nb, false), idn = idesc_f16(kPanelRows, nb, true);
             const uint32_t dre = tmem, dim = tmem + nb;
             const uint32_t a = su32(sAop), b = su32(sBop);
-            for (int ks = 0; ks < kPanelSteps; ++ks) {
+            // k steps past the block's kb columns hold zeros: skipped (small fronts, last blocks)
+            for (int ks = 0; 16 * ks < kb; ++ks) {
                 auto A = [&](int p) { return sdesc(a + (p * kPanelSteps + ks) * PC::kABlock, 128, 256); };
                 auto B = [&](int p) { return sdesc(b + (p * kPanelSteps + ks) * PC::kBBlock, 128, 256); };
                 const uint32_t acc = ks > 0 ? 1u : 0u;
