@@ -401,11 +401,13 @@ def test_fp32_tensor_core_fronts(oracle, complex_, split, monkeypatch):
         Ls, ds = fronts["0"][s]
         worst_tc = max(worst_tc, rel(Lt, Lo), rel(dt, do))
         worst_cc = max(worst_cc, rel(Ls, Lo), rel(ds, do))
-    # the split products are as accurate as FP32 CUDA-core arithmetic (the
-    # absolute level reflects unpivoted FP32 LDL^T of an indefinite operator)
+    # the split products are about as accurate as FP32 CUDA-core arithmetic
+    # (measured: 1.1-1.6x its error on the Laplacian, 1.0x on the Helmholtz
+    # operator, whose absolute level reflects unpivoted FP32 LDL^T of an
+    # indefinite operator)
     print(f"worst front error: tensor cores {worst_tc:.2e}, CUDA cores {worst_cc:.2e}")
-    assert worst_tc <= 4 * worst_cc + 1e-6, (worst_tc, worst_cc)
-    assert worst_tc <= 1e-3
+    assert worst_tc <= 2.5 * worst_cc, (worst_tc, worst_cc)
+    assert worst_tc <= (2e-3 if complex_ else 1e-6), worst_tc
 
 
 @pytest.mark.parametrize("complex_", [False, True])
