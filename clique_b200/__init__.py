@@ -241,11 +241,19 @@ class DistSymmFrontTree:
                                       C.byref(opt), C.c_void_p(stream), C.byref(h)), "DistSymmFrontTree")
         self._h = h.value
         self._csr = csr
+        # for RefinedSolve(fallback=True): the analysis, options and current
+        # values an FP64 copy of this tree is built from
+        self._twin_args = (map, sepTree, info, conjugate, keep_matrix, stream)
+        self._values_version = 0
+        self._fp64_twin = None
+        self.last_fallback = False
         self.Initialize(csr.values)
 
     def Initialize(self, values):
         """(Re)assemble the fronts from A's values (same pattern)."""
         lib = _capi.load()
+        self._values = values
+        self._values_version = getattr(self, "_values_version", 0) + 1
         if _is_torch_cuda(values):
             values = values.resolve_conj().contiguous()
             check(lib.cliqgpu_assemble(self._h, C.c_void_p(values.data_ptr()), 1), "assemble")
@@ -253,6 +261,19 @@ class DistSymmFrontTree:
             v = np.ascontiguousarray(values, np.complex128 if self.is_complex else np.float64)
             check(lib.cliqgpu_assemble(self._h, v.ctypes.data_as(C.c_void_p), 0), "assemble")
         self.frontType = SymmFrontType.SYMM_2D
+
+    def _fp64_tree(self):
+        """The same matrix, current values, factored with FP64 fronts (built
+        on first use and kept until the values change)."""
+        if self._fp64_twin is not None and self._fp64_twin[0] == self._values_version:
+            return self._fp64_twin[1]
+        self._fp64_twin = None
+        map_, sep, info, conjugate, keep, stream = self._twin_args
+        L64 = DistSymmFrontTree(self._csr, map_, sep, info, conjugate, precision="double", keep_matrix=keep, stream=stream)
+        L64.Initialize(self._values)
+        LDL(info, L64)
+        self._fp64_twin = (self._values_version, L64)
+        return L64
 
     def query(self, key):
         v = C.c_double()
@@ -426,11 +447,16 @@ def Solve(info, L: DistSymmFrontTree, X):
     return _solve_array(L, X, nodal=False)
 
 
-def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20, X=None):
+def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20, X=None, fallback=False):
     """X = A^{-1} B by iterative refinement over the stored factors (FP64
     residuals and updates).  Returns (X, iterations, relative residual).
     For host right-hand sides an output array X (Fortran-ordered, B's shape
-    and dtype, e.g. a view of pinned memory) may be passed and is filled."""
+    and dtype, e.g. a view of pinned memory) may be passed and is filled.
+    fallback=True on an FP32 tree: if the refinement does not reach tol in
+    max_iter steps (unpivoted growth the FP32 factors cannot absorb), the
+    matrix is factored again with FP64 fronts -- once per set of values; the
+    FP64 tree is kept with L -- and refined from there; L.last_fallback says
+    whether that happened, the iterations count both attempts."""
     lib = _capi.load()
     it = C.c_int32()
     rr = C.c_double()
@@ -455,6 +481,13 @@ def RefinedSolve(L: DistSymmFrontTree, B, tol=1e-10, max_iter=20, X=None):
         X = X if X is not None else Xo.reshape(np.asarray(B).shape)
     if st not in (_capi.CLIQ_OK, _capi.CLIQ_ERR_NOCONV):
         check(st, "RefinedSolve")
+    L.last_fallback = False
+    if st == _capi.CLIQ_ERR_NOCONV and fallback and L.precision not in ("double", "fp64", np.float64):
+        # the FP32 factors did not bring the residual to tol (pivot growth
+        # beyond what refinement absorbs): solve with FP64 fronts instead
+        X64, it64, rr64 = RefinedSolve(L._fp64_tree(), B, tol, max_iter, X=X)
+        L.last_fallback = True
+        return X64, it.value + it64, rr64
     return X, it.value, rr.value
 
 

@@ -645,3 +645,28 @@ def test_solve_form_override(oracle, form, precision, monkeypatch):
     else:
         X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 30)
         assert rr <= 1e-10, (it, rr)
+
+
+def test_refined_solve_fp64_fallback():
+    """RefinedSolve(fallback=True): when the FP32 factors cannot bring the
+    residual to tol within max_iter steps, the matrix is factored again with
+    FP64 fronts (kept with the tree for the same values) and the solve
+    reaches tol; without fallback the FP32 attempt reports its residual."""
+    n = 14
+    A, _, _ = ops.helmholtz_workload_3d(n, seed=7)
+    B = ops.random_rhs(A.n, 2, seed=9, complex_=True)
+    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, 64)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="single")
+    cliq.LDL(info, L)
+    _, it0, rr0 = cliq.RefinedSolve(L, B, 1e-13, 1)
+    assert rr0 > 1e-13 and not L.last_fallback
+    X, it, rr = cliq.RefinedSolve(L, B, 1e-13, 1, fallback=True)
+    assert L.last_fallback and rr <= 1e-13, (it, rr)
+    assert residual(A, X, B) <= 1e-12
+    twin = L._fp64_tree()
+    X2, _, rr2 = cliq.RefinedSolve(L, B, 1e-13, 1, fallback=True)
+    assert L._fp64_tree() is twin and rr2 <= 1e-13
+    L.Initialize(A.values)
+    cliq.LDL(info, L)
+    _, _, rr3 = cliq.RefinedSolve(L, B, 1e-10, 30, fallback=True)
+    assert rr3 <= 1e-10 and not L.last_fallback
