@@ -37,6 +37,17 @@ template <class T> __host__ __device__ __forceinline__ cx<T>& operator-=(cx<T>& 
 template <class T, bool C>
 using V = typename std::conditional<C, cx<T>, T>::type;
 
+// Whether an earlier bounded wait gave up (status[1] set): read once per
+// CTA by thread 0 and shared, so that every thread of the CTA takes the same
+// branch (a flag set by another CTA between two threads' reads would
+// otherwise split the CTA at its barriers).
+__device__ __forceinline__ bool cta_timed_out(const int32_t* status) {
+    __shared__ int s_timed_out;
+    if (threadIdx.x == 0) s_timed_out = *reinterpret_cast<const volatile int32_t*>(&status[1]) != 0;
+    __syncthreads();
+    return s_timed_out != 0;
+}
+
 template <class T> __device__ __forceinline__ T conjv(T a) { return a; }
 template <class T> __device__ __forceinline__ cx<T> conjv(cx<T> a) { return {a.r, -a.i}; }
 template <bool CJ, class X> __device__ __forceinline__ X opc(X a) { if constexpr (CJ) return conjv(a); else return a; }

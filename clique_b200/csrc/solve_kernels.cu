@@ -801,10 +801,13 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) f
     Xv* sx = reinterpret_cast<Xv*>(smem_raw);     // 2 x [64][NR]
     Xv* red = sx + 2 * kTile * NR;                // [kQ][NR][64]
     Xv* sq = red + kQ * NR * kTile;               // 2 x [64][NR]: solved blocks of a small front
-    __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
+    __shared__ int s_item, s_timed_out;
+    if (threadIdx.x == 0) {
+        s_item = atomicAdd(a.ticket, 1);
+        s_timed_out = *reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0;
+    }
     __syncthreads();
-    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
+    if (s_timed_out) return;   // an earlier wait gave up (one read for the whole CTA)
     const int4 it = a.items[s_item];
     const FrontDev f = a.F[it.x];
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;
@@ -1217,10 +1220,13 @@ __global__ void __launch_bounds__(kSolveThreads, sweep_min_blocks<T, C, NR>()) b
     Xv* red = sx + 3 * kTile * NR;                // [kQ][NR][64]
     Xv* sL = red + kQ * NR * kTile;               // [64 columns][65]
     int32_t* sidx = reinterpret_cast<int32_t*>(sL + kTile * ldl);   // gather indices, kLowerChunkTiles x 64
-    __shared__ int s_item;
-    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1);
+    __shared__ int s_item, s_timed_out;
+    if (threadIdx.x == 0) {
+        s_item = atomicAdd(a.ticket, 1);
+        s_timed_out = *reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0;
+    }
     __syncthreads();
-    if (*reinterpret_cast<volatile int32_t*>(&a.status[1]) != 0) return;   // an earlier wait gave up
+    if (s_timed_out) return;   // an earlier wait gave up (one read for the whole CTA)
     const int4 it = a.items[s_item];
     const FrontDev f = a.F[it.x];
     const int r = threadIdx.x % kTile, q = threadIdx.x / kTile;

@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) tc_gemm_kernel(const Gem
                                                               float* __restrict__ pool0, float* __restrict__ pool1,
                                                               int32_t* __restrict__ status) {
     using CF = Cfg<C>;
-    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
+    if (cta_timed_out(status)) return;   // an earlier wait timed out
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * CF::kStage);

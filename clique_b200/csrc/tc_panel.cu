@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kPanelThreads, 2) panel_tc_kernel(const FrontD
     using W = DV<C>;
     using PC = PanelCfg<C>;
     constexpr int nb = kTile;
-    if (*reinterpret_cast<volatile int32_t*>(&status[1]) != 0) return;   // an earlier wait timed out
+    if (cta_timed_out(status)) return;   // an earlier wait timed out
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sAop = smem;                                   // A planes: [plane][k step][128 rows x 32 B]
