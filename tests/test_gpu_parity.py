@@ -670,3 +670,36 @@ def test_refined_solve_fp64_fallback():
     cliq.LDL(info, L)
     _, _, rr3 = cliq.RefinedSolve(L, B, 1e-10, 30, fallback=True)
     assert rr3 <= 1e-10 and not L.last_fallback
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+@pytest.mark.parametrize("nrhs", [3, 9, 20])
+def test_tiny_front_sweeps_match_oracle(oracle, kind, nrhs):
+    """A 2D grid whose leaves have one pivot block and at most 64 rows below
+    (the one-warp-per-front sweeps) solved in FP64 for 3, 9 and 20
+    right-hand sides (the 4-, 16- and 16 + 4-column sweep instantiations),
+    against the oracle's solve on the same ordering."""
+    n1, n2, cutoff = 41, 37, 32
+    conj = kind == "hermitian"
+    if kind == "real":
+        A = ops.laplacian_2d(n1, n2, 4.1)
+    elif kind == "complex":
+        A = ops.helmholtz_pml_2d(n1, n2, omega=18.0, b=4)
+    else:
+        L0 = ops.laplacian_2d(n1, n2, 4.5)
+        vals = L0.values.astype(np.complex128)
+        rows = np.repeat(np.arange(L0.n), np.diff(L0.rowptr))
+        off = L0.colind != rows
+        vals[off] = vals[off] * np.exp(1j * 0.3 * np.sign(L0.colind - rows))[off]
+        A = ops.CSR(L0.n, L0.rowptr, L0.colind, vals)
+    cplx = kind != "real"
+    map_, info, L = build(A, (n1, n2, 1), cutoff, conjugate=conj)
+    sizes = [(nd.size, len(nd.lowerStruct)) for nd in info.localNodes]
+    assert any(0 < s <= 64 and u <= 64 for s, u in sizes)
+    B = ops.random_rhs(A.n, nrhs, seed=nrhs, complex_=cplx)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    S = oracle.Symbolic(n1, n2, 1, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=cplx, conjugate=conj)
+    assert F.ldl(96) == 0
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+    assert residual(A, X, B) <= 1e-11
