@@ -24,6 +24,10 @@
  *   front assembly .............. include/clique/numeric/dist_symm_front_tree/impl.hpp:244-297
  *   multifrontal factor ......... include/clique/numeric/ldl/local.hpp:25-122 (LocalLDL)
  *   dense partial front LDL^T ... include/clique/numeric/ldl/local_front.hpp:30-71 (FrontLDL)
+ *   pivoted front LDL^T ......... include/clique/numeric/ldl/local_front.hpp:74-94 (FrontLDLIntraPiv;
+ *                                 Bunch-Kaufman partial pivoting restated from its publication)
+ *   pivoted front solves ........ include/clique/numeric/lower_solve/local_front.hpp:53-93,
+ *                                 include/clique/numeric/diagonal_solve.hpp:53-59 (QuasiDiagonalSolve)
  *   forward / backward sweeps ... include/clique/numeric/lower_solve/local.hpp:42-119,203-277
  *   front triangular solves ..... include/clique/numeric/lower_solve/local_front.hpp:36-82
  *   root backward solve (P=1) ... include/clique/numeric/lower_solve/dist.hpp:374-387
@@ -498,10 +502,23 @@ void orc_fronts_free(orc_fronts* f) {
 }
 /* LocalLDL with blocksize nb; returns 0, or 1 + (ND index) of the first zero pivot. */
 i64 orc_ldl(orc_fronts* f, int nb) { return f->is_complex ? local_ldl_z(f->impl, nb) : local_ldl_d(f->impl, nb); }
-/* LocalLDL with the front type chosen: block = 1 for BLOCK_LDL_2D (FrontBlockLDL, block solves) */
-i64 orc_ldl_ex(orc_fronts* f, int nb, int block) {
-    if (f->is_complex) set_block_z(f->impl, block); else set_block_d(f->impl, block);
+/* LocalLDL with the front type chosen: kind = 1 for BLOCK_LDL_2D (FrontBlockLDL,
+ * block solves), 2 for LDL_INTRAPIV_2D (FrontLDLIntraPiv, pivoted solves) */
+i64 orc_ldl_ex(orc_fronts* f, int nb, int kind) {
+    if (f->is_complex) { set_block_z(f->impl, kind == 1); set_pivot_z(f->impl, kind == 2); }
+    else { set_block_d(f->impl, kind == 1); set_pivot_d(f->impl, kind == 2); }
     return orc_ldl(f, nb);
+}
+/* pivoted fronts: D[k + 1, k] of the 2 x 2 blocks (n) and the pivot rows (n) of node s */
+void orc_front_pivots(const orc_fronts* f, int s, double* sub_out, int* piv_out) {
+    if (f->is_complex) front_pivots_z(f->impl, s, (zd*)sub_out, piv_out); else front_pivots_d(f->impl, s, sub_out, piv_out);
+}
+/* FrontLDLIntraPiv on one dense front: AL (m x n, ld lda), ABR ((m-n)^2, ld
+ * ldb); diag, sub, piv get n entries (AL's diagonal keeps D) */
+i64 orc_front_ldl_intrapiv(int is_complex, int m, int n, double* AL, i64 lda, double* ABR, i64 ldb, double* diag, double* sub,
+                           int* piv, int conjugate) {
+    return is_complex ? front_ldl_intrapiv_z(m, n, (zd*)AL, lda, (zd*)ABR, ldb, (zd*)diag, (zd*)sub, piv, conjugate)
+                      : front_ldl_intrapiv_d(m, n, AL, lda, ABR, ldb, diag, sub, piv, conjugate);
 }
 /* copy frontL (m x n, column-major) or diag (n) of node s */
 void orc_front_get(const orc_fronts* f, int s, double* L_out, double* d_out) {

@@ -49,6 +49,10 @@ def lib():
     L.orc_ldl.argtypes = [C.c_void_p, C.c_int]
     L.orc_ldl_ex.restype = C.c_int64
     L.orc_ldl_ex.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.orc_front_pivots.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.orc_front_ldl_intrapiv.restype = C.c_int64
+    L.orc_front_ldl_intrapiv.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     L.orc_front_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     L.orc_front_dims.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.orc_front_set.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -141,9 +145,20 @@ class Fronts:
         self.h = lib().orc_fronts_create(symb.h, symb._rowptr, symb._colind, _ptr(self._vals),
                                          int(self.is_complex), int(conjugate))
 
-    def ldl(self, nb=96, block=False):
-        """LocalLDL; block=True for the BLOCK_LDL_2D front type (FrontBlockLDL)."""
-        return int(lib().orc_ldl_ex(self.h, nb, int(bool(block))))
+    def ldl(self, nb=96, block=False, pivot=False):
+        """LocalLDL; block=True for the BLOCK_LDL_2D front type (FrontBlockLDL),
+        pivot=True for LDL_INTRAPIV_2D (FrontLDLIntraPiv, Bunch-Kaufman)."""
+        kind = 1 if block else (2 if pivot else 0)
+        return int(lib().orc_ldl_ex(self.h, nb, kind))
+
+    def pivots(self, s):
+        """Pivoted fronts: (sub, piv) of node s -- D[k+1, k] of each 2x2 block
+        starting at k (0 elsewhere) and the assembled row of each pivoted row."""
+        _, n = self.dims(s)
+        sub = np.zeros(n, np.complex128 if self.is_complex else np.float64)
+        piv = np.zeros(n, np.int32)
+        lib().orc_front_pivots(self.h, s, _ptr(sub), piv.ctypes.data_as(C.c_void_p))
+        return sub, piv
 
     def dims(self, s):
         m, n = C.c_int(), C.c_int()
@@ -198,6 +213,20 @@ def front_ldl(AL, ABR, conjugate=False, nb=96):
     m, n = AL.shape
     assert AL.flags.f_contiguous and ABR.flags.f_contiguous
     return int(lib().orc_front_ldl(int(is_complex), m, n, _ptr(AL), m, _ptr(ABR), max(m - n, 1), int(conjugate), nb))
+
+
+def front_ldl_intrapiv(AL, ABR, conjugate=False):
+    """FrontLDLIntraPiv on one dense front, in place (AL m x n, ABR (m-n)^2,
+    Fortran order).  Returns (status, diag, sub, piv); AL's diagonal keeps D."""
+    is_complex = np.iscomplexobj(AL)
+    m, n = AL.shape
+    assert AL.flags.f_contiguous and ABR.flags.f_contiguous
+    dt = np.complex128 if is_complex else np.float64
+    diag, sub = np.zeros(n, dt), np.zeros(n, dt)
+    piv = np.zeros(n, np.int32)
+    st = int(lib().orc_front_ldl_intrapiv(int(is_complex), m, n, _ptr(AL), m, _ptr(ABR), max(m - n, 1), _ptr(diag),
+                                          _ptr(sub), piv.ctypes.data_as(C.c_void_p), int(conjugate)))
+    return st, diag, sub, piv
 
 
 def multiply(rowptr, colind, vals, alpha, X, beta, Y):
