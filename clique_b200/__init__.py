@@ -50,7 +50,9 @@ class SymmFrontType:
     # 86-98 inverts distributed nodes 1 ..), so they factor and solve as LDL;
     # the unpivoted block-LDL forms keep inv(A11) and A21 in every front
     # (ldl/local.hpp:30-33, ldl/local_front_block.hpp:27-71)
-    SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D)
+    # and the intra-front Bunch-Kaufman forms (ldl/local.hpp:31-33,106-111)
+    PIVOTED = (LDL_INTRAPIV_1D, LDL_INTRAPIV_2D)
+    SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D) + PIVOTED
     BLOCK = (BLOCK_LDL_1D, BLOCK_LDL_2D)
 
 
@@ -271,7 +273,7 @@ class DistSymmFrontTree:
         map_, sep, info, conjugate, keep, stream = self._twin_args
         L64 = DistSymmFrontTree(self._csr, map_, sep, info, conjugate, precision="double", keep_matrix=keep, stream=stream)
         L64.Initialize(self._values)
-        LDL(info, L64)
+        LDL(info, L64, self.frontType if self.frontType in SymmFrontType.PIVOTED else SymmFrontType.LDL_2D)
         self._fp64_twin = (self._values_version, L64)
         return L64
 
@@ -315,6 +317,19 @@ class DistSymmFrontTree:
         check(lib.cliqgpu_get_front(self._h, s, L.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p), dims))
         return L, d
 
+    def front_pivots(self, s):
+        """(subdiag, piv) of node s after an LDL_INTRAPIV factorization:
+        subdiag[k] = D[k+1, k] of the 2x2 block starting at k (0 elsewhere),
+        piv[i] = the front's assembled pivot row at pivoted position i."""
+        lib = _capi.load()
+        dims = (C.c_int32 * 2)()
+        check(lib.cliqgpu_get_front(self._h, s, None, None, dims))
+        n = dims[1]
+        sub = np.zeros(n, np.complex128 if self.is_complex else np.float64)
+        piv = np.zeros(n, np.int32)
+        check(lib.cliqgpu_get_front_pivots(self._h, s, sub.ctypes.data_as(C.c_void_p), piv.ctypes.data_as(C.c_void_p)))
+        return sub, piv
+
     def synchronize(self):
         check(_capi.load().cliqgpu_synchronize(self._h))
 
@@ -331,12 +346,16 @@ class DistSymmFrontTree:
 def LDL(info, L: DistSymmFrontTree, frontType=SymmFrontType.LDL_2D):
     """Multifrontal LDL^T in place (ldl.hpp:57-75).  Returns None; raises on a zero pivot."""
     if frontType not in SymmFrontType.SUPPORTED:
-        raise LogicError(_capi.CLIQ_ERR_ARG, "only the unpivoted LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D and "
-                                             "BLOCK_LDL_1D / BLOCK_LDL_2D front types are provided")
+        raise LogicError(_capi.CLIQ_ERR_ARG, "only the LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D, "
+                                             "LDL_INTRAPIV_1D / LDL_INTRAPIV_2D and BLOCK_LDL_1D / BLOCK_LDL_2D "
+                                             "front types are provided")
     if L.frontType not in (SymmFrontType.SYMM_1D, SymmFrontType.SYMM_2D):
         raise LogicError(_capi.CLIQ_ERR_STATE, "Matrix is already factored")
     zp = C.c_int64(-1)
-    st = _capi.load().cliqgpu_factor(L._h, C.byref(zp))
+    if frontType in SymmFrontType.PIVOTED:
+        st = _capi.load().cliqgpu_factor_intrapiv(L._h, C.byref(zp))
+    else:
+        st = _capi.load().cliqgpu_factor(L._h, C.byref(zp))
     L.zero_pivot = zp.value
     L.frontType = frontType
     check(st, "LDL")
@@ -508,12 +527,14 @@ def Multiply(alpha, L: DistSymmFrontTree, X, beta, Y):
     return Y
 
 
-def SymmetricSolve(A, X, nx, ny, nz, conjugate=False, cutoff=128, precision="double", tol=1e-10, max_iter=20):
+def SymmetricSolve(A, X, nx, ny, nz, conjugate=False, cutoff=128, precision="double", tol=1e-10, max_iter=20,
+                   frontType=SymmFrontType.LDL_INTRAPIV_1D):
     """Black-box solve (solve.hpp:95-116) with natural nested dissection on an
-    nx*ny*nz grid; unpivoted fronts.  Returns the solution (natural order)."""
+    nx*ny*nz grid; intra-front pivoted fronts as in the reference (LDL_2D
+    etc. on request).  Returns the solution (natural order)."""
     map_, sepTree, info = NaturalNestedDissection(nx, ny, nz, A, cutoff)
     L = DistSymmFrontTree(A, map_, sepTree, info, conjugate, precision=precision, keep_matrix=True)
-    LDL(info, L, SymmFrontType.LDL_2D)
+    LDL(info, L, frontType)
     if precision == "double":
         Y = np.array(X, copy=True, order="F")
         return Solve(info, L, Y)

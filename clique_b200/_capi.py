@@ -48,6 +48,8 @@ _SIGS = {
     "cliqgpu_assemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "cliqgpu_factor": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "cliqgpu_block_ldl": (C.c_int, [C.c_void_p]),
+    "cliqgpu_factor_intrapiv": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "cliqgpu_get_front_pivots": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "cliqgpu_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32]),
     "cliqgpu_multiply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
     "cliqgpu_sparse_multiply": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

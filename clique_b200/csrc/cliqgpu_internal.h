@@ -291,6 +291,21 @@ struct Plan {
     bool assembled = false, factored = false;
     bool block = false;           // fronts hold the block-LDL form (inv(A11), A21)
     void* block_state = nullptr;  // block sweeps: schedules per right-hand-side count and scratch
+    // intra-front pivoting (cliqgpu_factor_intrapiv; LDL_INTRAPIV_*): Bunch-
+    // Kaufman pivots within each front's pivot rows
+    bool pivoted = false;         // the current factorization is the pivoted one
+    double* E = nullptr;          // like D: D(k + 1, k) of each 2 x 2 pivot block starting at k, 0 elsewhere
+    int32_t* pivg = nullptr;      // ND index of the assembled row at pivoted position q
+    int32_t* qpos = nullptr;      // inverse of pivg
+    int32_t* perm_piv = nullptr;  // natural index of pivoted position q: perm[pivg[q]]
+    int32_t* cmaps_orig = nullptr;   // child maps and lowerStruct in assembled order (the extend-add's);
+    int32_t* lower_orig = nullptr;   // cmaps / lower hold the solves' pivoted order after a pivoted factorization
+    int64_t cmaps_len = 0, lower_len = 0;
+    bool maps_pivoted = false;
+    int32_t* pstate = nullptr;    // per front: first and one-past-last column of its latest panel
+    void* pvec = nullptr;         // 2 n entries: a panel step's candidate columns
+    int32_t* pivot_items = nullptr;   // int4 {front, 64-block, 0, 0} of every front's pivot blocks
+    int32_t pivot_dinv_items = 0;
     int64_t last_launches = 0;
     int64_t total_launches = 0;   // every kernel this plan has launched
     // FP32 updates on the tensor cores (tcgen05 3xTF32); CLIQGPU_TENSOR_CORES=0 selects the CUDA-core kernel
@@ -373,6 +388,13 @@ int launch_wait_selftest(Plan& P, uint64_t limit_ns);
 // runs the GEMM, all on stream st
 int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, void* pack);
 size_t tc2_smem(bool cplx);
+// intra-front pivoting (pivot_ldl.cu)
+int pivot_begin(Plan& P, cudaStream_t st);
+int pivot_level(Plan& P, int depth, cudaStream_t st);
+int pivot_finish(Plan& P, cudaStream_t st);
+int pivot_restore_maps(Plan& P, cudaStream_t st);
+int launch_quasi_diag(Plan& P, void* X, int64_t ldx, int nrhs);
+const int32_t* solve_perm(const Plan& P, bool nodal);
 // FP64 update C -= A D op(B)^T on the FP64 tensor cores (dmma_update.cu); same tiles as gemm_update_kernel
 int launch_dmma_update(Plan& P, const Launch& ln, cudaStream_t st);
 int launch_panel_tc(Plan& P, const Launch& ln, cudaStream_t st, void* pack);

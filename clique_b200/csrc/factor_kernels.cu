@@ -804,6 +804,56 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
     return launches;
 }
 
+#ifndef TRY
+#define TRY(x)                          \
+    do {                                \
+        int _st = (x);                  \
+        if (_st != CLIQ_OK) return _st; \
+    } while (0)
+#endif
+
+// Intra-front pivoting (LDL_INTRAPIV_*): per tree level its extend-add and
+// assembly, then the level's Bunch-Kaufman panels and updates (pivot_ldl.cu),
+// all on the plan's stream; the extend-add reads the child maps in assembled
+// order.  Afterwards the sweeps' diagonal-block inverses, the solves' maps in
+// the pivoted order and, for the product form, the chain tiles.
+template <class T, bool C, bool CJ>
+static int issue_factor_pivoted(Plan& P, int64_t* nlaunch) {
+    T* L = reinterpret_cast<T*>(P.L);
+    T* p0 = reinterpret_cast<T*>(P.pool[0]);
+    T* p1 = reinterpret_cast<T*>(P.pool[1]);
+    const int4* items = reinterpret_cast<const int4*>(P.items);
+    cudaStream_t st = P.stream;
+    const int64_t before = P.total_launches;
+    int64_t launches = 0;
+    TRY(pivot_begin(P, st));
+    for (const Launch& ln : P.launches) {
+        if (ln.kind != Launch::EXTEND_ADD || ln.nblocks <= 0) continue;
+        extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps_orig);
+        ++launches;
+        TRY(launch_assemble_level(P, ln.depth, st));
+        TRY(pivot_level(P, ln.depth, st));
+    }
+    TRY(pivot_finish(P, st));
+    if (P.nchain_items > 0 && !P.solve_exact) {
+        static bool ct_attr = false;
+        if (!ct_attr) {
+            cudaFuncSetAttribute(chain_tiles_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)chain_tiles_smem_bytes<T, C>());
+            ct_attr = true;
+        }
+        chain_tiles_kernel<T, C, CJ><<<(unsigned)P.nchain_items, kThreads, chain_tiles_smem_bytes<T, C>(), st>>>(
+            P.fronts, reinterpret_cast<const int4*>(P.chain_items), L, reinterpret_cast<const T*>(P.dinv),
+            reinterpret_cast<T*>(P.m1), reinterpret_cast<T*>(P.n1));
+        ++launches;
+    }
+    // the pivoted launchers counted theirs in total_launches
+    launches += P.total_launches - before;
+    P.total_launches = before;
+    *nlaunch = launches;
+    return check_cuda("pivoted factor launch");
+}
+
 // Direct launches for the first factorization of a plan and for profiled
 // ones; otherwise the launch sequence (static for a plan: same grids, items
 // and buffers every time) is captured once from the plan's stream, across
@@ -811,6 +861,16 @@ static int64_t issue_factor(Plan& P, bool captured = false) {
 template <class T, bool C, bool CJ>
 static int run_factor_impl(Plan& P) {
     int64_t launches = 0;
+    if (P.pivoted) {
+        const int st = issue_factor_pivoted<T, C, CJ>(P, &launches);
+        if (st != CLIQ_OK) return st;
+        P.prof_pending = false;
+        ++P.factor_runs;
+        P.last_launches = launches;
+        P.total_launches += launches;
+        return CLIQ_OK;
+    }
+    TRY(pivot_restore_maps(P, P.stream));
     const bool graphs = P.use_graph && P.stream1 && P.stream2 && P.sync_events.size() >= 2;
     if (graphs && !P.profile && P.factor_runs > 0 && !P.factor_exec) {
         if (cudaStreamBeginCapture(P.stream1, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {

@@ -1,0 +1,732 @@
+// Intra-front pivoting: the LDL_INTRAPIV_1D / LDL_INTRAPIV_2D front types
+// (ldl/local.hpp:31-33,106-111; FrontLDLIntraPiv, ldl/local_front.hpp:74-94).
+//
+// Each front's pivot block A11 is factored with Bunch-Kaufman partial
+// pivoting restricted to the front's own pivot rows: P A11 P^T = L D op(L)^T
+// with D block diagonal (1 x 1 and 2 x 2 blocks, alpha = (1 + sqrt 17) / 8,
+// magnitudes |re| + |im|), the columns of A21 permuted with P, and the Schur
+// complement ABR -= L21 D op(L21)^T passed up as in the unpivoted form.  The
+// reference gets this from Elemental's El::LDL( A11, dSub, p, conjugate,
+// BUNCH_KAUFMAN_A ), PermuteCols, Trsm, QuasiDiagonalSolve and Trrk.
+//
+// GPU form, per tree level after its extend-add and assembly, right-looking
+// in panels of 64 (65 when a 2 x 2 block closes the panel) columns:
+//   bk_panel_kernel   one CTA per front: the panel's pivots one column at a
+//                     time.  The candidate columns are formed with the
+//                     panel's pending update (A(:,k) - L(:,panel) B(k,panel)^T,
+//                     B = D op(L)^T built from L and D on the fly), the pivot
+//                     search runs over the front's remaining pivot rows, a
+//                     chosen interchange swaps rows and columns of the whole
+//                     front (the factored columns of L and the columns of A21
+//                     included), and the pivot columns of L are written for
+//                     the pivot rows;
+//   bk_lower_kernel   rows below the pivots (A21): L21(:,panel) = A21(:,panel)
+//                     op(L11)^{-T} D^{-1} for the panel's diagonal block, one
+//                     thread per row;
+//   bk_update_kernel  the panel's rank-kb update of the front's remaining
+//                     columns (pivot rows and A21 rows, lower part), and once
+//                     per front at the end of the level the Schur complement
+//                     into the update pool with K = n.
+// Then the 64 x 64 diagonal-block inverses the sweeps use, and the index
+// maps the solves read are rewritten for the pivoted row order (the
+// reference's PermuteRows / InversePermuteRows around each front solve,
+// lower_solve/local_front.hpp:53-93, become a relabelling of the front's
+// pivot rows).
+#include "cliqgpu_internal.h"
+#include "device_common.cuh"
+
+#include <climits>
+#include <cmath>
+
+#ifndef TRY
+#define TRY(x)                          \
+    do {                                \
+        int _st = (x);                  \
+        if (_st != CLIQ_OK) return _st; \
+    } while (0)
+#endif
+
+namespace cliqgpu {
+namespace piv {
+
+constexpr int kNb = 64;                 // panel width (one more when a 2 x 2 block closes it)
+constexpr int kMaxPanel = kNb + 1;
+constexpr int kPanelThreads = 512;
+constexpr int kLowerRows = 128;         // rows of A21 per bk_lower_kernel CTA
+constexpr int kUpdThreads = 256;
+constexpr int kUpdTile = 64;
+constexpr double kAlpha = 0.64038820320220756872767623199676;   // (1 + sqrt(17)) / 8
+
+static inline unsigned grid1d(int64_t work, int threads) {
+    const int64_t g = (work + threads - 1) / threads;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+}
+
+template <class T> __device__ __forceinline__ T mag1(T a) { return fabs(a); }
+template <class T> __device__ __forceinline__ T mag1(cx<T> a) { return fabs(a.r) + fabs(a.i); }
+template <class T> __device__ __forceinline__ T realpart(T a) { return a; }
+template <class T> __device__ __forceinline__ cx<T> realpart(cx<T> a) { return {a.r, T(0)}; }
+template <class X> __device__ __forceinline__ X neg(X a) { return X{} - a; }
+
+// B(j, p) = sum_l D(p, l) op(L(j, l)) over the block of D that holds p:
+// D(p, p) = d[p]; D(p, p + 1) = op(e[p]) when a 2 x 2 block starts at p;
+// D(p, p - 1) = e[p - 1] when one starts at p - 1.  Lrow(q) reads L(j, q).
+template <bool CJ, class X, class Get>
+__device__ __forceinline__ X bval(int p, X d, X e, X em1, bool first, Get Lrow) {
+    X b = d * opc<CJ>(Lrow(p));
+    if (!is_zero(e)) b += opc<CJ>(e) * opc<CJ>(Lrow(p + 1));
+    if (first && !is_zero(em1)) b += em1 * opc<CJ>(Lrow(p - 1));
+    return b;
+}
+
+// block-wide max with the smallest index on ties
+template <class T>
+__device__ __forceinline__ void block_argmax(T& v, int& idx, T* sv, int* si) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_down_sync(0xffffffffu, v, o);
+        const int oi = __shfl_down_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+    }
+    if (lane == 0) { sv[w] = v; si[w] = idx; }
+    __syncthreads();
+    if (w == 0) {
+        v = lane < nw ? sv[lane] : T(-1);
+        idx = lane < nw ? si[lane] : INT_MAX;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T ov = __shfl_down_sync(0xffffffffu, v, o);
+            const int oi = __shfl_down_sync(0xffffffffu, idx, o);
+            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+        }
+        if (lane == 0) { sv[0] = v; si[0] = idx; }
+    }
+    __syncthreads();
+    v = sv[0];
+    idx = si[0];
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// one panel of Bunch-Kaufman pivots per front
+// ---------------------------------------------------------------------------
+template <class T, bool C, bool CJ>
+__global__ void __launch_bounds__(kPanelThreads) bk_panel_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+                                                                 T* __restrict__ L, double* __restrict__ D, double* __restrict__ E,
+                                                                 int32_t* __restrict__ pivg, T* __restrict__ cvec, T* __restrict__ vvec,
+                                                                 int32_t* __restrict__ state, int32_t* __restrict__ status) {
+    using X = V<T, C>;
+    using W = DV<C>;
+    __shared__ X s_d[kMaxPanel], s_e[kMaxPanel];   // the panel's D (diagonal, and D(p+1,p) of 2 x 2 blocks)
+    __shared__ X s_w[kMaxPanel];                   // B(k, p)
+    __shared__ X s_lr[kMaxPanel], s_wi[kMaxPanel]; // L(imax, p), B(imax, p)
+    __shared__ T s_rv[32];
+    __shared__ int s_ri[32];
+    __shared__ X s_akk, s_ar;
+    const int s = fl[blockIdx.x];
+    const FrontDev f = F[s];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = f.n, m = f.m;
+    const int j0 = state[2 * s + 1];
+    if (j0 >= n) {
+        if (tid == 0) state[2 * s] = j0;
+        return;
+    }
+    const int64_t base = f.L;
+    auto at = [&](int i, int j) -> int64_t { return base + i + (int64_t)j * m; };
+    if (j0 == 0)
+        for (int i = tid; i < n; i += nt) pivg[f.off + i] = f.off + i;
+    const int jend = min(n, j0 + kNb);
+    int k = j0;
+    while (k < jend) {
+        const int np = k - j0;
+        // B(k, p) for the panel's factored columns
+        if (tid < np) {
+            const int p = j0 + tid;
+            s_w[tid] = bval<CJ>(p, s_d[tid], s_e[tid], tid > 0 ? s_e[tid - 1] : X{}, tid > 0,
+                                [&](int q) { return ldv<T, C>(L, at(k, q)); });
+        }
+        __syncthreads();
+        // candidate column k with the panel's pending update; column maximum below the diagonal
+        T best = T(-1);
+        int bi = INT_MAX;
+        for (int i = k + tid; i < n; i += nt) {
+            X a = ldv<T, C>(L, at(i, k));
+            for (int p = 0; p < np; ++p) a -= ldv<T, C>(L, at(i, j0 + p)) * s_w[p];
+            if (i == k) {
+                if constexpr (CJ) a = realpart(a);
+                s_akk = a;
+            } else {
+                const T g = mag1(a);
+                if (g > best) { best = g; bi = i; }
+            }
+            stv<T, C>(cvec, f.off + i, a);
+        }
+        block_argmax(best, bi, s_rv, s_ri);   // (its barriers publish s_akk and cvec)
+        const T colmax = best > T(0) ? best : T(0);
+        const int imax = bi == INT_MAX ? k : bi;
+        const T absakk = mag1(s_akk);
+        int kp = k, kstep = 1;
+        bool use_v = false, zero = false;
+        if (fmax((double)absakk, (double)colmax) == 0.0) {
+            zero = true;
+        } else if (absakk >= (T)kAlpha * colmax) {
+            kp = k;
+        } else {
+            // candidate column imax (the full matrix's column, rows k .. n-1)
+            if (tid < np) {
+                const int p = j0 + tid;
+                s_lr[tid] = ldv<T, C>(L, at(imax, p));
+                s_wi[tid] = bval<CJ>(p, s_d[tid], s_e[tid], tid > 0 ? s_e[tid - 1] : X{}, tid > 0,
+                                     [&](int q) { return ldv<T, C>(L, at(imax, q)); });
+            }
+            __syncthreads();
+            T rbest = T(-1);
+            int rbi = INT_MAX;
+            for (int j = k + tid; j < n; j += nt) {
+                X a;
+                if (j < imax) {
+                    a = ldv<T, C>(L, at(imax, j));
+                    for (int p = 0; p < np; ++p) {
+                        const X b = bval<CJ>(j0 + p, s_d[p], s_e[p], p > 0 ? s_e[p - 1] : X{}, p > 0,
+                                             [&](int q) { return ldv<T, C>(L, at(j, q)); });
+                        a -= s_lr[p] * b;
+                    }
+                    a = opc<CJ>(a);
+                } else if (j == imax) {
+                    a = ldv<T, C>(L, at(imax, imax));
+                    for (int p = 0; p < np; ++p) a -= s_lr[p] * s_wi[p];
+                    if constexpr (CJ) a = realpart(a);
+                    s_ar = a;
+                } else {
+                    a = ldv<T, C>(L, at(j, imax));
+                    for (int p = 0; p < np; ++p) a -= ldv<T, C>(L, at(j, j0 + p)) * s_wi[p];
+                }
+                stv<T, C>(vvec, f.off + j, a);
+                if (j != imax) {
+                    const T g = mag1(a);
+                    if (g > rbest) { rbest = g; rbi = j; }
+                }
+            }
+            block_argmax(rbest, rbi, s_rv, s_ri);
+            const T rowmax = rbest > T(0) ? rbest : T(0);
+            if (absakk >= (T)kAlpha * colmax * (colmax / rowmax)) {
+                kp = k;
+            } else if (mag1(s_ar) >= (T)kAlpha * rowmax) {
+                kp = imax;
+                use_v = true;
+            } else {
+                kp = imax;
+                kstep = 2;
+            }
+        }
+        if (zero && tid == 0) atomicMin(&status[0], f.off + k + 1);
+        // symmetric interchange of a = kk and b = kp over the whole front
+        const int kk = k + kstep - 1;
+        if (kp != kk) {
+            const int a = kk, b = kp;
+            for (int j = tid; j < a; j += nt) {   // factored columns: rows a and b
+                const X t = ldv<T, C>(L, at(a, j));
+                stv<T, C>(L, at(a, j), ldv<T, C>(L, at(b, j)));
+                stv<T, C>(L, at(b, j), t);
+            }
+            for (int i = a + 1 + tid; i < b; i += nt) {   // column a between the two, row b between the two
+                const X t = ldv<T, C>(L, at(i, a));
+                stv<T, C>(L, at(i, a), opc<CJ>(ldv<T, C>(L, at(b, i))));
+                stv<T, C>(L, at(b, i), opc<CJ>(t));
+            }
+            for (int i = b + 1 + tid; i < m; i += nt) {   // rows below b (A21 included): columns a and b
+                const X t = ldv<T, C>(L, at(i, a));
+                stv<T, C>(L, at(i, a), ldv<T, C>(L, at(i, b)));
+                stv<T, C>(L, at(i, b), t);
+            }
+            if (tid == 0) {
+                const X t = ldv<T, C>(L, at(a, a));
+                stv<T, C>(L, at(a, a), ldv<T, C>(L, at(b, b)));
+                stv<T, C>(L, at(b, b), t);
+                stv<T, C>(L, at(b, a), opc<CJ>(ldv<T, C>(L, at(b, a))));
+                const int32_t g = pivg[f.off + a];
+                pivg[f.off + a] = pivg[f.off + b];
+                pivg[f.off + b] = g;
+                const X c0 = ldv<T, C>(cvec, f.off + a);
+                stv<T, C>(cvec, f.off + a, ldv<T, C>(cvec, f.off + b));
+                stv<T, C>(cvec, f.off + b, c0);
+                const X v0 = ldv<T, C>(vvec, f.off + a);
+                stv<T, C>(vvec, f.off + a, ldv<T, C>(vvec, f.off + b));
+                stv<T, C>(vvec, f.off + b, v0);
+            }
+        }
+        __syncthreads();
+        // pivot columns of L (pivot rows), D and E
+        if (kstep == 1) {
+            const T* col = use_v ? vvec : cvec;
+            X d = ldv<T, C>(col, f.off + k);
+            if constexpr (CJ) d = realpart(d);
+            for (int i = k + 1 + tid; i < n; i += nt) {
+                const X c = ldv<T, C>(col, f.off + i);
+                stv<T, C>(L, at(i, k), is_zero(d) ? X{} : c / d);
+            }
+            if (tid == 0) {
+                stv<T, C>(L, at(k, k), vone<X>());
+                reinterpret_cast<W*>(D)[f.off + k] = conv<W>(d);
+                reinterpret_cast<W*>(E)[f.off + k] = W{};
+                s_d[np] = d;
+                s_e[np] = X{};
+            }
+        } else {
+            X d11 = ldv<T, C>(cvec, f.off + k), d21 = ldv<T, C>(cvec, f.off + k + 1), d22 = ldv<T, C>(vvec, f.off + k + 1);
+            if constexpr (CJ) { d11 = realpart(d11); d22 = realpart(d22); }
+            const X det = d11 * d22 - d21 * opc<CJ>(d21);
+            for (int i = k + 2 + tid; i < n; i += nt) {
+                const X c = ldv<T, C>(cvec, f.off + i), v = ldv<T, C>(vvec, f.off + i);
+                stv<T, C>(L, at(i, k), (c * d22 - v * d21) / det);
+                stv<T, C>(L, at(i, k + 1), (v * d11 - c * opc<CJ>(d21)) / det);
+            }
+            if (tid == 0) {
+                stv<T, C>(L, at(k, k), vone<X>());
+                stv<T, C>(L, at(k + 1, k + 1), vone<X>());
+                stv<T, C>(L, at(k + 1, k), X{});
+                reinterpret_cast<W*>(D)[f.off + k] = conv<W>(d11);
+                reinterpret_cast<W*>(D)[f.off + k + 1] = conv<W>(d22);
+                reinterpret_cast<W*>(E)[f.off + k] = conv<W>(d21);
+                reinterpret_cast<W*>(E)[f.off + k + 1] = W{};
+                s_d[np] = d11;
+                s_e[np] = d21;
+                s_d[np + 1] = d22;
+                s_e[np + 1] = X{};
+            }
+        }
+        __syncthreads();
+        k += kstep;
+    }
+    if (tid == 0) {
+        state[2 * s] = j0;
+        state[2 * s + 1] = k;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// rows below the pivots: L21(:, panel) = A21(:, panel) op(L11)^{-T} D^{-1}
+// ---------------------------------------------------------------------------
+template <class T, bool C, bool CJ>
+__global__ void __launch_bounds__(kLowerRows) bk_lower_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl, int chunks,
+                                                              T* __restrict__ L, const double* __restrict__ D,
+                                                              const double* __restrict__ E, const int32_t* __restrict__ state) {
+    using X = V<T, C>;
+    using W = DV<C>;
+    extern __shared__ __align__(16) unsigned char bk_smem[];
+    X* s_l = reinterpret_cast<X*>(bk_smem);   // L11 of the panel, kMaxPanel x kMaxPanel, column-major
+    __shared__ X s_d[kMaxPanel], s_e[kMaxPanel];
+    const int fi = blockIdx.x / chunks, ch = blockIdx.x % chunks;
+    const int s = fl[fi];
+    const FrontDev f = F[s];
+    const int j0 = state[2 * s], j1 = state[2 * s + 1], kb = j1 - j0;
+    const int u = f.m - f.n;
+    if (kb <= 0 || ch * kLowerRows >= u) return;
+    const int64_t base = f.L;
+    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
+        const int r = idx % kb, c = idx / kb;
+        s_l[r + c * kMaxPanel] = r > c ? ldv<T, C>(L, base + (j0 + r) + (int64_t)(j0 + c) * f.m) : X{};
+    }
+    for (int q = threadIdx.x; q < kb; q += blockDim.x) {
+        s_d[q] = conv<X>(reinterpret_cast<const W*>(D)[f.off + j0 + q]);
+        s_e[q] = conv<X>(reinterpret_cast<const W*>(E)[f.off + j0 + q]);
+    }
+    __syncthreads();
+    const int i = f.n + ch * kLowerRows + threadIdx.x;
+    if (i >= f.m) return;
+    const int64_t row = base + i;
+    // y(q) = a(q) - sum_{p<q} y(p) op(L11(q, p)), kept in place
+    for (int q = 0; q < kb; ++q) {
+        X a = ldv<T, C>(L, row + (int64_t)(j0 + q) * f.m);
+        for (int p = 0; p < q; ++p) a -= ldv<T, C>(L, row + (int64_t)(j0 + p) * f.m) * opc<CJ>(s_l[q + p * kMaxPanel]);
+        stv<T, C>(L, row + (int64_t)(j0 + q) * f.m, a);
+    }
+    // l = y D^{-1}
+    for (int q = 0; q < kb; ++q) {
+        const int64_t e0 = row + (int64_t)(j0 + q) * f.m;
+        if (!is_zero(s_e[q])) {
+            const X d11 = s_d[q], d22 = s_d[q + 1], d21 = s_e[q];
+            const X det = d11 * d22 - d21 * opc<CJ>(d21);
+            const X y0 = ldv<T, C>(L, e0), y1 = ldv<T, C>(L, e0 + f.m);
+            stv<T, C>(L, e0, (y0 * d22 - y1 * d21) / det);
+            stv<T, C>(L, e0 + f.m, (y1 * d11 - y0 * opc<CJ>(d21)) / det);
+            ++q;
+        } else {
+            const X d = s_d[q];
+            stv<T, C>(L, e0, is_zero(d) ? X{} : ldv<T, C>(L, e0) / d);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// C -= A B^T on the lower part, B(j, p) = sum_l D(p, l) op(L(j, l)):
+//   kind 0: the front's remaining columns after its latest panel
+//           (rows and columns from j1, K = the panel);
+//   kind 1: the Schur complement ABR -= L21 D op(L21)^T (K = n) into the pool.
+// One 64 x 64 tile per CTA; tiles beyond the front's actual extent return.
+// ---------------------------------------------------------------------------
+template <class T, bool C, bool CJ>
+__global__ void __launch_bounds__(kUpdThreads) bk_update_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+                                                                int64_t tiles_per_front, int kind, T* __restrict__ L,
+                                                                T* __restrict__ pool0, T* __restrict__ pool1,
+                                                                const double* __restrict__ D, const double* __restrict__ E,
+                                                                const int32_t* __restrict__ state) {
+    using X = V<T, C>;
+    using W = DV<C>;
+    constexpr int BM = kUpdTile, BK = C ? 8 : 16, PAD = 1;
+    __shared__ X sA[BK][BM + PAD];
+    __shared__ X sB[BK][BM + PAD];
+    __shared__ X s_d[BK], s_e[BK], s_em1[BK];
+    const int64_t fi = blockIdx.x / tiles_per_front;
+    int64_t t = blockIdx.x % tiles_per_front;
+    const int s = fl[fi];
+    const FrontDev f = F[s];
+    int r0, c0, k0, K, M, N;
+    if (kind == 0) {
+        const int j0 = state[2 * s], j1 = state[2 * s + 1];
+        r0 = j1; c0 = j1; k0 = j0; K = j1 - j0; M = f.m - j1; N = f.n - j1;
+    } else {
+        r0 = f.n; c0 = f.n; k0 = 0; K = f.n; M = N = f.m - f.n;
+    }
+    if (K <= 0 || M <= 0 || N <= 0) return;
+    const int Mt = (M + BM - 1) / BM, Nt = (N + BM - 1) / BM;
+    int tj = 0;
+    while (tj < Nt && t >= Mt - tj) { t -= Mt - tj; ++tj; }
+    if (tj >= Nt) return;
+    const int ti = tj + (int)t;
+    const int i0 = ti * BM, jb0 = tj * BM;
+    const int64_t base = f.L;
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    X acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = X{};
+    for (int kq = 0; kq < K; kq += BK) {
+        if (threadIdx.x < BK) {
+            const int p = k0 + kq + threadIdx.x;
+            const bool in = kq + (int)threadIdx.x < K;
+            s_d[threadIdx.x] = in ? conv<X>(reinterpret_cast<const W*>(D)[f.off + p]) : X{};
+            s_e[threadIdx.x] = in ? conv<X>(reinterpret_cast<const W*>(E)[f.off + p]) : X{};
+            s_em1[threadIdx.x] = (in && p > 0) ? conv<X>(reinterpret_cast<const W*>(E)[f.off + p - 1]) : X{};
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / kUpdThreads; ++q) {
+            const int idx = threadIdx.x + kUpdThreads * q;
+            const int r = idx % BM, kk = idx / BM;
+            const int kg = kq + kk;
+            X av{}, bv{};
+            if (kg < K) {
+                const int p = k0 + kg;
+                if (i0 + r < M) av = ldv<T, C>(L, base + (r0 + i0 + r) + (int64_t)p * f.m);
+                if (jb0 + r < N) {
+                    const int64_t rowj = base + (c0 + jb0 + r);
+                    bv = bval<CJ>(p, s_d[kk], s_e[kk], s_em1[kk], p > 0,
+                                  [&](int qq) { return ldv<T, C>(L, rowj + (int64_t)qq * f.m); });
+                }
+            }
+            sA[kk][r] = av;
+            sB[kk][r] = bv;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            X av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) av[a] = sA[kk][ty + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bv[b] = sB[kk][tx + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) mac(acc[a][b], av[a], bv[b]);
+        }
+        __syncthreads();
+    }
+    T* Cb;
+    int64_t cbase, ldc;
+    if (kind == 0) {
+        Cb = L; cbase = base + r0 + (int64_t)c0 * f.m; ldc = f.m;
+    } else {
+        Cb = f.pool == 0 ? pool0 : pool1; cbase = f.U; ldc = f.m - f.n;
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int j = jb0 + tx + 16 * b;
+        if (j >= N) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = i0 + ty + 16 * a;
+            if (i < M && i >= j) {   // one tile writes each entry per launch
+                const int64_t e = cbase + i + (int64_t)j * ldc;
+                stv<T, C>(Cb, e, ldv<T, C>(Cb, e) - acc[a][b]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// inverses of the 64 x 64 diagonal blocks of the unit lower L11 (the sweeps'
+// dinv / dinvT blocks), one CTA of 64 threads per block
+// ---------------------------------------------------------------------------
+template <class T, bool C>
+__global__ void __launch_bounds__(kTile) bk_dinv_kernel(const FrontDev* __restrict__ F, const int4* __restrict__ items,
+                                                        const T* __restrict__ L, T* __restrict__ dinv, T* __restrict__ dinvT) {
+    using X = V<T, C>;
+    extern __shared__ __align__(16) unsigned char bk_dinv_smem[];
+    X* s_a = reinterpret_cast<X*>(bk_dinv_smem);   // the block's strictly lower part, kTile x (kTile + 1)
+    const int4 it = items[blockIdx.x];
+    const FrontDev f = F[it.x];
+    const int b = it.y, k = b * kTile, kb = min(kTile, f.n - k);
+    const int c = threadIdx.x;
+    for (int r = 0; r < kTile; ++r)
+        s_a[r + c * (kTile + 1)] = (r > c && r < kb && c < kb) ? ldv<T, C>(L, f.L + (k + r) + (int64_t)(k + c) * f.m) : X{};
+    __syncthreads();
+    // column c of the inverse, written in place: x(c) = 1, x(r) = -sum_{c <= t < r} L(r, t) x(t)
+    X* Dv = reinterpret_cast<X*>(dinv) + f.dinv + (int64_t)b * kTile * kTile;
+    for (int r = 0; r < kTile; ++r) {
+        X x{};
+        if (c < kb && r == c) x = vone<X>();
+        else if (c < kb && r > c && r < kb) {
+            for (int t = c; t < r; ++t) mac(x, s_a[r + t * (kTile + 1)], Dv[t + c * kTile]);
+            x = neg(x);
+        }
+        Dv[r + c * kTile] = x;
+    }
+    if (dinvT) {
+        __syncthreads();
+        X* DvT = reinterpret_cast<X*>(dinvT) + f.dinv + (int64_t)b * kTile * kTile;
+        for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+            const int cc = idx % kTile, i = idx / kTile;
+            DvT[cc + i * kTile] = Dv[i + cc * kTile];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// index maps for the solves in the pivoted order
+// ---------------------------------------------------------------------------
+__global__ void remap_positions_kernel(int64_t n, const int32_t* __restrict__ pivg, const int32_t* __restrict__ perm,
+                                       int32_t* __restrict__ qpos, int32_t* __restrict__ perm_piv) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t g = pivg[q];
+        qpos[g] = (int32_t)q;
+        perm_piv[q] = perm[g];
+    }
+}
+
+__global__ void remap_lower_kernel(int64_t cnt, const int32_t* __restrict__ qpos, const int32_t* __restrict__ lower_orig,
+                                   int32_t* __restrict__ lower) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < cnt; r += (int64_t)gridDim.x * blockDim.x)
+        lower[r] = qpos[lower_orig[r]];
+}
+
+// parent row i < n gathers / scatters what the assembled row pivg[off + i] did
+__global__ void remap_cmaps_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ pivg,
+                                   const int32_t* __restrict__ cmaps_orig, int32_t* __restrict__ cmaps) {
+    const FrontDev f = F[blockIdx.x];
+    if (f.cmap < 0) return;
+    for (int i = threadIdx.x; i < f.n; i += blockDim.x) {
+        const int src = pivg[f.off + i] - f.off;
+        cmaps[f.cmap + i] = cmaps_orig[f.cmap + src];
+        cmaps[f.cmap + f.m + i] = cmaps_orig[f.cmap + f.m + src];
+    }
+}
+
+// quasi-diagonal solve X := D^{-1} X (diagonal_solve.hpp:53-59): a 2 x 2
+// block [[d11, op(e)], [e, d22]] starting at p is solved by p's thread
+template <class T, bool C, bool CJ>
+__global__ void quasi_diag_kernel(T* __restrict__ X, int64_t ldx, int64_t n, int nrhs, const double* __restrict__ D,
+                                  const double* __restrict__ E) {
+    using Xv = V<T, C>;
+    using W = DV<C>;
+    const W* d = reinterpret_cast<const W*>(D);
+    const W* e = reinterpret_cast<const W*>(E);
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        if (p > 0 && !is_zero(e[p - 1])) continue;   // second row of a 2 x 2 block
+        if (!is_zero(e[p])) {
+            const W d11 = d[p], d22 = d[p + 1], d21 = e[p];
+            const W det = d11 * d22 - d21 * opc<CJ>(d21);
+            for (int j = 0; j < nrhs; ++j) {
+                const W b0 = conv<W>(ldv<T, C>(X, p + j * ldx)), b1 = conv<W>(ldv<T, C>(X, p + 1 + j * ldx));
+                stv<T, C>(X, p + j * ldx, conv<Xv>((d22 * b0 - opc<CJ>(d21) * b1) / det));
+                stv<T, C>(X, p + 1 + j * ldx, conv<Xv>((d11 * b1 - d21 * b0) / det));
+            }
+        } else {
+            const W dp = d[p];
+            for (int j = 0; j < nrhs; ++j) stv<T, C>(X, p + j * ldx, conv<Xv>(conv<W>(ldv<T, C>(X, p + j * ldx)) / dp));
+        }
+    }
+}
+
+template <class T, bool C, bool CJ>
+static int level_t(Plan& P, int depth, cudaStream_t st) {
+    const SolveLevel& lv = P.solve_levels[depth];
+    if (lv.nfronts <= 0) return CLIQ_OK;
+    const int32_t* fl = P.level_fronts + lv.fronts;
+    int max_n = 0, max_u = 0;
+    for (int s : P.level_list[depth]) {
+        max_n = std::max(max_n, P.hfronts[s].n);
+        max_u = std::max(max_u, P.hfronts[s].m - P.hfronts[s].n);
+    }
+    T* L = reinterpret_cast<T*>(P.L);
+    T* p0 = reinterpret_cast<T*>(P.pool[0]);
+    T* p1 = reinterpret_cast<T*>(P.pool[1]);
+    T* cvec = reinterpret_cast<T*>(P.pvec);
+    T* vvec = cvec + (C ? 2 : 1) * P.n;
+    const size_t smem_lower = sizeof(V<T, C>) * kMaxPanel * kMaxPanel;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(bk_lower_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lower);
+        attr = true;
+    }
+    const int chunks = std::max(1, (max_u + kLowerRows - 1) / kLowerRows);
+    auto tiles = [](int64_t M, int64_t N) -> int64_t {
+        if (M <= 0 || N <= 0) return 0;
+        const int64_t Mt = (M + kUpdTile - 1) / kUpdTile, Nt = (N + kUpdTile - 1) / kUpdTile;
+        return Nt * Mt - Nt * (Nt - 1) / 2;
+    };
+    const int steps = (max_n + kNb - 1) / kNb;
+    for (int step = 0; step < steps; ++step) {
+        bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, kPanelThreads, 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec, vvec,
+                                                                                   P.pstate, P.status);
+        if (max_u > 0)
+            bk_lower_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * chunks), kLowerRows, smem_lower, st>>>(
+                P.fronts, fl, chunks, L, P.D, P.E, P.pstate);
+        // every panel is at least kNb wide until the front is done
+        int64_t tpf = 0;
+        for (int s : P.level_list[depth]) {
+            const FrontDev& f = P.hfronts[s];
+            const int64_t jb = std::min<int64_t>(f.n, (int64_t)(step + 1) * kNb);
+            tpf = std::max(tpf, tiles(f.m - jb, f.n - jb));
+        }
+        if (tpf > 0)
+            bk_update_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * tpf), kUpdThreads, 0, st>>>(
+                P.fronts, fl, tpf, 0, L, p0, p1, P.D, P.E, P.pstate);
+        P.total_launches += 3;
+    }
+    // the Schur complement of every front of the level, K = n
+    int64_t tpf = 0;
+    for (int s : P.level_list[depth]) tpf = std::max(tpf, tiles(P.hfronts[s].m - P.hfronts[s].n, P.hfronts[s].m - P.hfronts[s].n));
+    if (tpf > 0)
+        bk_update_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * tpf), kUpdThreads, 0, st>>>(P.fronts, fl, tpf, 1, L, p0, p1,
+                                                                                                   P.D, P.E, P.pstate);
+    P.total_launches += 1;
+    return check_cuda("pivoted level");
+}
+
+template <class T, bool C, bool CJ>
+static int finish_t(Plan& P, cudaStream_t st) {
+    const size_t smem = sizeof(V<T, C>) * kTile * (kTile + 1);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(bk_dinv_kernel<T, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    if (P.pivot_dinv_items > 0)
+        bk_dinv_kernel<T, C><<<(unsigned)P.pivot_dinv_items, kTile, smem, st>>>(P.fronts, reinterpret_cast<const int4*>(P.pivot_items),
+                                                                            reinterpret_cast<const T*>(P.L), reinterpret_cast<T*>(P.dinv),
+                                                                            reinterpret_cast<T*>(P.dinvT));
+    const unsigned g = grid1d(P.n, 256);
+    remap_positions_kernel<<<g, 256, 0, st>>>(P.n, P.pivg, P.perm, P.qpos, P.perm_piv);
+    if (P.lower_len > 0) remap_lower_kernel<<<grid1d(P.lower_len, 256), 256, 0, st>>>(P.lower_len, P.qpos, P.lower_orig, P.lower);
+    if (P.num_fronts > 0) remap_cmaps_kernel<<<(unsigned)P.num_fronts, 256, 0, st>>>(P.fronts, P.pivg, P.cmaps_orig, P.cmaps);
+    P.total_launches += 4;
+    return check_cuda("pivoted maps");
+}
+
+}  // namespace piv
+
+// allocations on first use; the extend-add's maps in assembled order
+int pivot_begin(Plan& P, cudaStream_t st) {
+    const int w = P.cplx() ? 2 : 1;
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        if (*p) return CLIQ_OK;
+        if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+            cudaGetLastError();
+            set_last_error("cudaMalloc failed for the pivoted factorization's buffers");
+            return CLIQ_ERR_OOM;
+        }
+        P.device_bytes += (int64_t)std::max<size_t>(bytes, 16);
+        return CLIQ_OK;
+    };
+    const bool first = P.E == nullptr;
+    TRY(alloc((void**)&P.E, sizeof(double) * w * (size_t)P.n));
+    TRY(alloc((void**)&P.pivg, sizeof(int32_t) * (size_t)P.n));
+    TRY(alloc((void**)&P.qpos, sizeof(int32_t) * (size_t)P.n));
+    TRY(alloc((void**)&P.perm_piv, sizeof(int32_t) * (size_t)P.n));
+    TRY(alloc((void**)&P.cmaps_orig, sizeof(int32_t) * (size_t)P.cmaps_len));
+    TRY(alloc((void**)&P.lower_orig, sizeof(int32_t) * (size_t)P.lower_len));
+    TRY(alloc((void**)&P.pstate, sizeof(int32_t) * 2 * (size_t)P.num_fronts));
+    TRY(alloc(&P.pvec, (size_t)P.elem_bytes() * 2 * (size_t)P.n));
+    if (first) {
+        if (P.cmaps_len > 0) cudaMemcpyAsync(P.cmaps_orig, P.cmaps, sizeof(int32_t) * P.cmaps_len, cudaMemcpyDeviceToDevice, st);
+        if (P.lower_len > 0) cudaMemcpyAsync(P.lower_orig, P.lower, sizeof(int32_t) * P.lower_len, cudaMemcpyDeviceToDevice, st);
+        // the 64-blocks of every front, for the diagonal-block inverses
+        std::vector<int32_t> items;
+        for (int s = 0; s < P.num_fronts; ++s)
+            for (int b = 0; b * kTile < P.hfronts[s].n; ++b) { items.push_back(s); items.push_back(b); items.push_back(0); items.push_back(0); }
+        P.pivot_dinv_items = (int32_t)(items.size() / 4);
+        if (items.empty()) items.assign(4, 0);
+        TRY(alloc((void**)&P.pivot_items, sizeof(int32_t) * items.size()));
+        if (cudaMemcpyAsync(P.pivot_items, items.data(), sizeof(int32_t) * items.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return check_cuda("pivot items");
+        if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("pivot items");   // items is host memory
+    }
+    cudaMemsetAsync(P.pstate, 0, sizeof(int32_t) * 2 * (size_t)P.num_fronts, st);
+    return check_cuda("pivoted factorization setup");
+}
+
+// the solves' maps back in assembled order (an unpivoted factorization after a pivoted one)
+int pivot_restore_maps(Plan& P, cudaStream_t st) {
+    if (!P.maps_pivoted) return CLIQ_OK;
+    if (P.cmaps_len > 0) cudaMemcpyAsync(P.cmaps, P.cmaps_orig, sizeof(int32_t) * P.cmaps_len, cudaMemcpyDeviceToDevice, st);
+    if (P.lower_len > 0) cudaMemcpyAsync(P.lower, P.lower_orig, sizeof(int32_t) * P.lower_len, cudaMemcpyDeviceToDevice, st);
+    P.maps_pivoted = false;
+    return check_cuda("restore maps");
+}
+
+int pivot_level(Plan& P, int depth, cudaStream_t st) {
+    if (depth < 0 || depth > P.max_depth) return CLIQ_OK;
+    const bool cj = P.conjugate && P.cplx();
+    if (P.precision == CLIQ_FP64) {
+        if (!P.cplx()) return piv::level_t<double, false, false>(P, depth, st);
+        return cj ? piv::level_t<double, true, true>(P, depth, st) : piv::level_t<double, true, false>(P, depth, st);
+    }
+    if (!P.cplx()) return piv::level_t<float, false, false>(P, depth, st);
+    return cj ? piv::level_t<float, true, true>(P, depth, st) : piv::level_t<float, true, false>(P, depth, st);
+}
+
+int pivot_finish(Plan& P, cudaStream_t st) {
+    const bool cj = P.conjugate && P.cplx();
+    int r;
+    if (P.precision == CLIQ_FP64) {
+        if (!P.cplx()) r = piv::finish_t<double, false, false>(P, st);
+        else r = cj ? piv::finish_t<double, true, true>(P, st) : piv::finish_t<double, true, false>(P, st);
+    } else {
+        if (!P.cplx()) r = piv::finish_t<float, false, false>(P, st);
+        else r = cj ? piv::finish_t<float, true, true>(P, st) : piv::finish_t<float, true, false>(P, st);
+    }
+    if (r == CLIQ_OK) P.maps_pivoted = true;
+    return r;
+}
+
+int launch_quasi_diag(Plan& P, void* X, int64_t ldx, int nrhs) {
+    const unsigned g = 1184;
+    const bool cj = P.conjugate && P.cplx();
+    if (P.precision == CLIQ_FP64) {
+        if (!P.cplx()) piv::quasi_diag_kernel<double, false, false><<<g, 256, 0, P.stream>>>((double*)X, ldx, P.n, nrhs, P.D, P.E);
+        else if (cj) piv::quasi_diag_kernel<double, true, true><<<g, 256, 0, P.stream>>>((double*)X, ldx, P.n, nrhs, P.D, P.E);
+        else piv::quasi_diag_kernel<double, true, false><<<g, 256, 0, P.stream>>>((double*)X, ldx, P.n, nrhs, P.D, P.E);
+    } else {
+        if (!P.cplx()) piv::quasi_diag_kernel<float, false, false><<<g, 256, 0, P.stream>>>((float*)X, ldx, P.n, nrhs, P.D, P.E);
+        else if (cj) piv::quasi_diag_kernel<float, true, true><<<g, 256, 0, P.stream>>>((float*)X, ldx, P.n, nrhs, P.D, P.E);
+        else piv::quasi_diag_kernel<float, true, false><<<g, 256, 0, P.stream>>>((float*)X, ldx, P.n, nrhs, P.D, P.E);
+    }
+    return check_cuda("quasi-diagonal solve");
+}
+
+}  // namespace cliqgpu

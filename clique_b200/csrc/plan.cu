@@ -76,7 +76,8 @@ void free_plan(Plan& P) {
     void* ptrs[] = {P.L, P.D, P.pool[0], P.pool[1], P.tinv, P.dinv, P.dinvT, P.m1, P.n1, P.chain_items, P.xprog, P.hpart, P.partial, P.eblk, P.erow, P.fronts, P.cmaps, P.lower, P.items, P.probs, P.packjobs, P.pack,
                     P.prefix, P.bmap, P.dest, P.asm_src, P.asm_dst,
                     P.perm, P.level_fronts, P.tiny_fronts, P.flags, P.tickets, P.status, P.rowptr, P.colind, P.aval, P.wpool[0], P.pack2,
-                    P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov, P.pack3};
+                    P.wpool[1], P.xnodal, P.xwork, P.norms, P.krylov, P.pack3, P.E, P.pivg, P.qpos, P.perm_piv,
+                    P.cmaps_orig, P.lower_orig, P.pstate, P.pvec, P.pivot_items};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : P.events) cudaEventDestroy(e);
@@ -710,6 +711,8 @@ int build_plan(Plan& P, const cliq_symm_info* info, int64_t n, const int32_t* ma
     TRY(dev_upload(P, &P.cmaps, cmaps));
     std::vector<int32_t> lowv(low, low + info->lower_ptr[nn]);
     TRY(dev_upload(P, &P.lower, lowv));
+    P.cmaps_len = (int64_t)cmaps.size();
+    P.lower_len = (int64_t)lowv.size();
     TRY(dev_upload(P, &P.items, items));
     TRY(dev_upload(P, &P.probs, probs));
     TRY(dev_upload(P, &P.packjobs, packjobs));
@@ -779,6 +782,14 @@ int solve_nodal_dispatch(Plan& P, void* xn, int nrhs) {
     if (P.precision == CLIQ_FP64)
         return P.cplx() ? run_solve_nodal<double, true>(P, xn, nrhs) : run_solve_nodal<double, false>(P, xn, nrhs);
     return P.cplx() ? run_solve_nodal<float, true>(P, xn, nrhs) : run_solve_nodal<float, false>(P, xn, nrhs);
+}
+
+// Row order of the solves' nodal vectors: ND order, or after a pivoted
+// factorization each front's pivot rows in pivoted order.  The map takes a
+// natural-order (nodal = false) or ND-order (nodal = true) vector there.
+const int32_t* solve_perm(const Plan& P, bool nodal) {
+    if (P.pivoted) return nodal ? P.pivg : P.perm_piv;
+    return nodal ? nullptr : P.perm;
 }
 
 int read_status(Plan& P, int64_t* zero_pivot) {
@@ -881,7 +892,7 @@ int run_factor_dispatch(Plan& P) {
 
 extern "C" {
 
-int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
+static int factor_common(cliqgpu_plan h, int64_t* zero_pivot, bool pivoted) {
     if (!h) return CLIQ_ERR_ARG;
     Plan& P = h->p;
     if (!P.assembled) { set_last_error("factor: fronts were not assembled"); return CLIQ_ERR_STATE; }
@@ -889,16 +900,45 @@ int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) {
     int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
     P.block = false;
+    P.pivoted = pivoted;
     const int st = run_factor_dispatch(P);
     if (st != CLIQ_OK) return st;
     P.factored = true;
     return read_status(P, zero_pivot);
 }
 
+int cliqgpu_factor(cliqgpu_plan h, int64_t* zero_pivot) { return factor_common(h, zero_pivot, false); }
+
+int cliqgpu_factor_intrapiv(cliqgpu_plan h, int64_t* zero_pivot) { return factor_common(h, zero_pivot, true); }
+
+int cliqgpu_get_front_pivots(cliqgpu_plan h, int32_t s, double* sub, int32_t* piv) {
+    if (!h) return CLIQ_ERR_ARG;
+    Plan& P = h->p;
+    if (s < 0 || s >= P.num_fronts) return CLIQ_ERR_ARG;
+    const FrontDev& f = P.hfronts[s];
+    const int w = P.cplx() ? 2 : 1;
+    if (cudaStreamSynchronize(P.stream) != cudaSuccess) return check_cuda("sync");
+    if (!P.pivoted || !P.factored) {   // unpivoted fronts: no 2 x 2 blocks, identity order
+        if (sub) for (int64_t i = 0; i < (int64_t)w * f.n; ++i) sub[i] = 0.0;
+        if (piv) for (int i = 0; i < f.n; ++i) piv[i] = i;
+        return CLIQ_OK;
+    }
+    if (sub && f.n > 0 &&
+        cudaMemcpy(sub, P.E + (size_t)w * f.off, sizeof(double) * w * f.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return check_cuda("get pivots");
+    if (piv && f.n > 0) {
+        if (cudaMemcpy(piv, P.pivg + f.off, sizeof(int32_t) * f.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return check_cuda("get pivots");
+        for (int i = 0; i < f.n; ++i) piv[i] -= f.off;
+    }
+    return CLIQ_OK;
+}
+
 int cliqgpu_block_ldl(cliqgpu_plan h) {
     if (!h) return CLIQ_ERR_ARG;
     Plan& P = h->p;
     if (!P.factored) { set_last_error("block LDL: the front tree is not factored"); return CLIQ_ERR_STATE; }
+    if (P.pivoted) { set_last_error("block LDL: the block form of pivoted fronts (BLOCK_LDL_INTRAPIV_*) is not provided"); return CLIQ_ERR_ARG; }
     if (P.block) return CLIQ_OK;
     const int st = convert_to_block(P);
     if (st != CLIQ_OK) return st;
@@ -928,7 +968,7 @@ int cliqgpu_solve(cliqgpu_plan h, void* X, int64_t ldx, int32_t nrhs, int32_t x_
     }
     int32_t st0[4] = {INT_MAX, 0, 0, 0};
     cudaMemcpyAsync(P.status, st0, sizeof(st0), cudaMemcpyHostToDevice, P.stream);
-    const int32_t* perm = nodal ? nullptr : P.perm;   // nodal: X is already in ND order
+    const int32_t* perm = solve_perm(P, nodal != 0);
     TRY(launch_pull(P, perm, xd, ldx, nrhs, P.xnodal, 1.0));
     TRY(solve_nodal_dispatch(P, P.xnodal, nrhs));
     TRY(launch_push(P, perm, P.xnodal, xd, ldx, nrhs, 1.0, 0));
@@ -1042,9 +1082,9 @@ static int refine_fgmres(Plan& P, const double* b, double* x, double* r, int nrh
         double est = rel;
         for (; k < kKrylovMax && it < max_iter; ++k) {
             // z_k = M^{-1} v_k (natural order FP64 -> nodal storage precision -> solve -> back)
-            TRY(launch_pull(P, P.perm, V + k * vec, n, nrhs, P.xnodal, 1.0));
+            TRY(launch_pull(P, solve_perm(P, false), V + k * vec, n, nrhs, P.xnodal, 1.0));
             TRY(solve_nodal_dispatch(P, P.xnodal, nrhs));
-            TRY(launch_push(P, P.perm, P.xnodal, Z + k * vec, n, nrhs, 1.0, 0));
+            TRY(launch_push(P, solve_perm(P, false), P.xnodal, Z + k * vec, n, nrhs, 1.0, 0));
             ++it;
             // w = A z_k, orthogonalised twice against v_0 .. v_k
             TRY(launch_spmv(P, 1.0, 0.0, Z + k * vec, 0.0, 0.0, wv, n, nrhs));
@@ -1157,9 +1197,9 @@ int cliqgpu_refine(cliqgpu_plan h, const void* B, void* X, int64_t ld, int32_t n
         }
         if (rel <= tol || it >= max_iter || !(rel == rel)) break;
         const double scale = rmax > 0 ? 1.0 / rmax : 1.0;
-        TRY(launch_pull(P, P.perm, r, n, nrhs, P.xnodal, scale));
+        TRY(launch_pull(P, solve_perm(P, false), r, n, nrhs, P.xnodal, scale));
         TRY(solve_nodal_dispatch(P, P.xnodal, nrhs));
-        TRY(launch_push(P, P.perm, P.xnodal, x, n, nrhs, 1.0 / scale, 1));
+        TRY(launch_push(P, solve_perm(P, false), P.xnodal, x, n, nrhs, 1.0 / scale, 1));
         cudaMemcpyAsync(r, b, colbytes * nrhs, cudaMemcpyDeviceToDevice, P.stream);
         TRY(launch_spmv(P, -1.0, 0.0, x, 1.0, 0.0, r, n, nrhs));
         ++it;

@@ -1299,7 +1299,8 @@ static int64_t run_sweeps(Plan& P, T* X, int nrhs) {
             ++launches;
         }
     }
-    diag_scale_kernel<T, C><<<1184, 256, 0, P.stream>>>(X, P.n, P.n, nrhs, P.D);
+    if (P.pivoted) launch_quasi_diag(P, X, P.n, nrhs);   // 1 x 1 and 2 x 2 blocks of D
+    else diag_scale_kernel<T, C><<<1184, 256, 0, P.stream>>>(X, P.n, P.n, nrhs, P.D);
     ++launches;
     for (int d = 0; d <= P.max_depth; ++d) {
         const SolveLevel& lv = P.solve_levels[d];

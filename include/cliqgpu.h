@@ -126,6 +126,30 @@ int cliqgpu_assemble(cliqgpu_plan plan, const void* values, int32_t values_on_de
  * (LocalLDL ldl/local.hpp:25-122, FrontLDL ldl/local_front.hpp:30-71). */
 int cliqgpu_factor(cliqgpu_plan plan, int64_t* zero_pivot);
 
+/* The same factorization with intra-front Bunch-Kaufman pivoting: each
+ * front's pivot block is factored as P A11 P^T = L D op(L)^T with P a
+ * permutation of the front's own pivot rows and D block diagonal (1 x 1 and
+ * 2 x 2 blocks), the columns of A21 permuted with it, and the Schur
+ * complement passed up as in cliqgpu_factor.  The solves apply P around each
+ * front and solve with the 2 x 2 blocks; their inputs and outputs keep the
+ * natural / ND order.  *zero_pivot: -1, or the ND position of the first pivot
+ * whose whole remaining column is zero (then CLIQ_ERR_ZERO_PIVOT).
+ * Replaces cliq::LDL(info, L, LDL_INTRAPIV_1D/LDL_INTRAPIV_2D): LocalLDL's
+ * intraPiv branch, include/clique/numeric/ldl/local.hpp:31-33,106-111,
+ * FrontLDLIntraPiv ldl/local_front.hpp:74-94, and its solves
+ * lower_solve/local_front.hpp:53-93 and diagonal_solve.hpp:53-59. */
+int cliqgpu_factor_intrapiv(cliqgpu_plan plan, int64_t* zero_pivot);
+
+/* Pivots of front s after cliqgpu_factor_intrapiv: sub[k] = D(k+1, k) of the
+ * 2 x 2 block starting at pivot k, 0 elsewhere (n entries, FP64, complex
+ * interleaved; D(k, k+1) = sub[k], conjugated for LDL^H), and piv[i] = the
+ * front's assembled pivot row at pivoted position i (n entries), so that
+ * cliqgpu_get_front's L and D factor the pivot block with rows and columns
+ * ordered by piv.  Unpivoted factorizations give zeros and the identity.
+ * Replaces reading L.localFronts[s].subdiag / .piv
+ * (dist_symm_front_tree/decl.hpp:174-184). */
+int cliqgpu_get_front_pivots(cliqgpu_plan plan, int32_t s, double* sub, int32_t* piv);
+
 /* After cliqgpu_factor: turn every front into the block-LDL form -- the top
  * n x n block holds inv(A11) (full, symmetric or Hermitian), the rows below
  * it the original A21 -- so that the solves are products only (no

@@ -282,9 +282,12 @@ enum SymmFrontType {
 inline bool Unfactored(SymmFrontType t) { return t == SYMM_1D || t == SYMM_2D; }
 // front types this library factors: unpivoted LDL, and its selective-inversion
 // forms, which at one process invert no local front (change_front_type.hpp:86-98
-// inverts distributed nodes 1 .. only), so they factor and solve as LDL
+// inverts distributed nodes 1 .. only), so they factor and solve as LDL; the
+// unpivoted block-LDL forms; LDL with intra-front Bunch-Kaufman pivoting
+inline bool PivotedFactorization(SymmFrontType t) { return t == LDL_INTRAPIV_1D || t == LDL_INTRAPIV_2D; }
 inline bool Provided(SymmFrontType t) {
-    return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D || t == BLOCK_LDL_1D || t == BLOCK_LDL_2D;
+    return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D || t == BLOCK_LDL_1D || t == BLOCK_LDL_2D ||
+           PivotedFactorization(t);
 }
 
 template <class F>
@@ -338,9 +341,11 @@ template <class F>
 void LDL(DistSymmInfo&, DistSymmFrontTree<F>& L, SymmFrontType newFrontType = LDL_2D) {
     if (!Unfactored(L.frontType)) throw LogicError("Matrix is already factored");
     if (!Provided(newFrontType))
-        throw LogicError("Only the unpivoted LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D and BLOCK_LDL_1D / BLOCK_LDL_2D front types are provided");
+        throw LogicError("Only the LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D, LDL_INTRAPIV_1D / LDL_INTRAPIV_2D and "
+                         "BLOCK_LDL_1D / BLOCK_LDL_2D front types are provided");
     int64_t zp = -1;
-    Check(cliqgpu_factor(L.Plan(), &zp), "LDL");
+    if (PivotedFactorization(newFrontType)) Check(cliqgpu_factor_intrapiv(L.Plan(), &zp), "LDL");
+    else Check(cliqgpu_factor(L.Plan(), &zp), "LDL");
     L.frontType = newFrontType;
     if (newFrontType == BLOCK_LDL_1D || newFrontType == BLOCK_LDL_2D) Check(cliqgpu_block_ldl(L.Plan()), "LDL (block form)");
 }

@@ -1,0 +1,173 @@
+"""Intra-front pivoting on the GPU (LDL_INTRAPIV_1D / LDL_INTRAPIV_2D,
+through cliqgpu_factor_intrapiv) against the CPU oracle's FrontLDLIntraPiv.
+
+Tolerances: FP64 -- the same pivot order and 2x2 blocks as the oracle in
+every front, L, D and the 2x2 off-diagonals within 1e-10 of the oracle's
+(relative to the front's largest entry), solutions within 1e-10 of the
+oracle's with relative residual <= 1e-12; FP32 fronts with FP64 refinement
+reach relative residual <= 1e-10.  The operators are indefinite, with their
+couplings scaled by a deterministic pseudo-random symmetric factor so that
+no two pivot candidates tie exactly.
+"""
+import numpy as np
+import pytest
+
+import clique_b200 as cliq
+from clique_b200 import operators as ops
+
+pytestmark = pytest.mark.gpu
+
+
+def _perturbed(A, vals, seed=0):
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    lo = np.minimum(rows, A.colind).astype(np.int64)
+    hi = np.maximum(rows, A.colind).astype(np.int64)
+    h = ((lo * 1000003 + hi * 7919 + seed) % 1009) / 1009.0
+    return ops.CSR(A.n, A.rowptr, A.colind, vals * (1.0 + 0.4 * (h - 0.5)))
+
+
+def _indefinite(kind, dims):
+    """Shifted Laplacian (real symmetric), PML Helmholtz (complex symmetric),
+    shifted magnetic Laplacian (Hermitian); all indefinite."""
+    if kind == "complex":
+        A = ops.helmholtz_pml_3d(*dims, omega=18.0, velocity=ops.smooth_velocity(dims, 3), b=2)
+        return _perturbed(A, A.values), False
+    A = ops.laplacian_3d(*dims, 0.5)
+    vals = A.values
+    if kind == "hermitian":
+        vals = vals.astype(np.complex128)
+        rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+        off = A.colind != rows
+        vals[off] = vals[off] * np.exp(1j * 0.4 * np.sign(A.colind - rows))[off]
+    return _perturbed(A, vals), kind == "hermitian"
+
+
+def _tree(A, dims, cutoff, precision, conj, front_type=cliq.SymmFrontType.LDL_INTRAPIV_2D, keep=False):
+    map_, sep, info = cliq.NaturalNestedDissection(*dims, A, cutoff)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, conj, precision=precision, keep_matrix=keep)
+    cliq.LDL(info, L, front_type)
+    return map_, info, L
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def residual(A, X, B):
+    return np.linalg.norm(A.to_scipy() @ X - B) / np.linalg.norm(B)
+
+
+# (24, 12, 6) / 100: fronts of 66-72 pivots with rows below (two panels);
+# (16, 16, 10) / 200: a 160-pivot root and 80-160-pivot fronts below it
+CASES = [((9, 8, 7), 24), ((24, 12, 6), 100), ((16, 16, 10), 200)]
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+@pytest.mark.parametrize("dims,cutoff", CASES)
+def test_intrapiv_fronts_match_oracle(oracle, kind, dims, cutoff):
+    A, conj = _indefinite(kind, dims)
+    cplx = kind != "real"
+    _, _, L = _tree(A, dims, cutoff, "double", conj)
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=cplx, conjugate=conj)
+    assert F.ldl(96, pivot=True) == 0
+    swaps = blocks = 0
+    for s in range(S.num_nodes):
+        Lo, do = F.front(s)
+        so, po = F.pivots(s)
+        Lg, dg = L.front(s)
+        sg, pg = L.front_pivots(s)
+        assert np.array_equal(pg, po), s
+        scale = max(np.abs(Lo).max(), np.abs(do).max(), 1e-300)
+        assert np.abs(Lg - Lo).max() <= 1e-10 * scale, s
+        assert np.abs(dg - do).max() <= 1e-10 * scale, s
+        assert np.abs(sg - so).max() <= 1e-10 * scale, s
+        swaps += int((po != np.arange(len(po))).sum())
+        blocks += int((so != 0).sum())
+    assert swaps > 0
+    if kind != "complex":   # (the PML Helmholtz fronts may interchange rows without 2x2 blocks)
+        assert blocks > 0
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+@pytest.mark.parametrize("nrhs", [1, 5, 20])
+def test_intrapiv_solve_matches_oracle(oracle, kind, nrhs):
+    dims, cutoff = (24, 12, 6), 100
+    A, conj = _indefinite(kind, dims)
+    cplx = kind != "real"
+    _, info, L = _tree(A, dims, cutoff, "double", conj)
+    B = ops.random_rhs(A.n, nrhs, seed=nrhs, complex_=cplx)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=cplx, conjugate=conj)
+    assert F.ldl(96, pivot=True) == 0
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+    assert residual(A, X, B) <= 1e-12
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+def test_intrapiv_single_refined(kind):
+    dims, cutoff = (16, 16, 10), 200
+    A, conj = _indefinite(kind, dims)
+    _, _, L = _tree(A, dims, cutoff, "single", conj, keep=True)
+    B = ops.random_rhs(A.n, 3, seed=2, complex_=kind != "real")
+    X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 40)
+    assert rr <= 1e-10, (it, rr)
+    assert residual(A, X, B) <= 1e-10
+
+
+def test_intrapiv_zero_diagonal():
+    """An exactly zero first pivot: the unpivoted factorization reports it,
+    the pivoted one factors and solves to FP64 accuracy."""
+    dims = (6, 5, 4)
+    A0 = ops.laplacian_3d(*dims, 6.1)
+    map_, sep, info = cliq.NaturalNestedDissection(*dims, A0, 30)
+    g = int(np.asarray(map_.FormInverse().array)[0])   # natural index of ND position 0
+    vals = A0.values.copy()
+    rows = np.repeat(np.arange(A0.n), np.diff(A0.rowptr))
+    vals[(rows == g) & (A0.colind == g)] = 0.0
+    A = ops.CSR(A0.n, A0.rowptr, A0.colind, vals)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+    with pytest.raises(cliq.CliqueError) as e:
+        cliq.LDL(info, L)
+    assert e.value.status == 3 and L.zero_pivot == 0
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+    cliq.LDL(info, L, cliq.SymmFrontType.LDL_INTRAPIV_1D)
+    B = ops.random_rhs(A.n, 2, seed=3)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    assert residual(A, X, B) <= 1e-12
+
+
+def test_intrapiv_nodal_and_refactor():
+    """ND-order (nodal) solves keep the ND order with pivoted fronts; the same
+    plan refactored unpivoted (new values) solves with its maps restored."""
+    dims, cutoff = (14, 12, 10), 80
+    A, _ = _indefinite("real", dims)
+    map_, info, L = _tree(A, dims, cutoff, "double", False)
+    B = ops.random_rhs(A.n, 2, seed=3)
+    inv = map_.FormInverse()
+    Xn = cliq.DistNodalMultiVec(inv, info, B)
+    cliq.Solve(info, L, Xn)
+    X1 = np.zeros_like(B, order="F")
+    Xn.Push(inv, info, X1)
+    X2 = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(X1, X2) <= 1e-14
+    assert residual(A, X2, B) <= 1e-11   # indefinite shifted Laplacian: measured 1.5e-12
+    Apd = ops.laplacian_3d(*dims, 6.1)
+    L.Initialize(Apd.values)
+    cliq.LDL(info, L, cliq.SymmFrontType.LDL_2D)
+    X3 = cliq.Solve(info, L, B.copy(order="F"))
+    assert residual(Apd, X3, B) <= 1e-12
+    L.Initialize(A.values)
+    cliq.LDL(info, L, cliq.SymmFrontType.LDL_INTRAPIV_2D)
+    X4 = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(X4, X2) <= 1e-13
+
+
+def test_symmetric_solve_pivots_by_default():
+    """SymmetricSolve factors with LDL_INTRAPIV_1D, as solve.hpp:110 does."""
+    dims = (10, 9, 8)
+    A, _ = _indefinite("complex", dims)
+    B = ops.random_rhs(A.n, 2, seed=6, complex_=True)
+    X = cliq.SymmetricSolve(A, B, *dims, cutoff=40)
+    assert residual(A, X, B) <= 1e-12
