@@ -45,15 +45,16 @@ class SymmFrontType:
     LDL_SELINV_1D, LDL_SELINV_2D, LDL_INTRAPIV_1D, LDL_INTRAPIV_2D = 4, 5, 6, 7
     LDL_INTRAPIV_SELINV_1D, LDL_INTRAPIV_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D = 8, 9, 10, 11
     BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D = 12, 13
-    # unpivoted LDL and its selective-inversion forms: at one process the
-    # reference inverts no local front for the latter (change_front_type.hpp:
-    # 86-98 inverts distributed nodes 1 ..), so they factor and solve as LDL;
-    # the unpivoted block-LDL forms keep inv(A11) and A21 in every front
-    # (ldl/local.hpp:30-33, ldl/local_front_block.hpp:27-71)
-    # and the intra-front Bunch-Kaufman forms (ldl/local.hpp:31-33,106-111)
-    PIVOTED = (LDL_INTRAPIV_1D, LDL_INTRAPIV_2D)
+    # Every factored type is provided.  The selective-inversion forms invert
+    # no local front at one process (change_front_type.hpp:86-98 inverts
+    # distributed nodes 1 ..), so they factor and solve as their LDL /
+    # pivoted LDL base types; the block-LDL forms keep inv(A11) and A21 in
+    # every front (ldl/local.hpp:30-33, ldl/local_front_block.hpp:27-71); the
+    # INTRAPIV forms pivot within each front (ldl/local.hpp:31-33,104-111)
+    PIVOTED = (LDL_INTRAPIV_1D, LDL_INTRAPIV_2D, LDL_INTRAPIV_SELINV_1D, LDL_INTRAPIV_SELINV_2D,
+               BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D)
     SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D) + PIVOTED
-    BLOCK = (BLOCK_LDL_1D, BLOCK_LDL_2D)
+    BLOCK = (BLOCK_LDL_1D, BLOCK_LDL_2D, BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D)
 
 
 # ---------------------------------------------------------------------------
@@ -273,7 +274,8 @@ class DistSymmFrontTree:
         map_, sep, info, conjugate, keep, stream = self._twin_args
         L64 = DistSymmFrontTree(self._csr, map_, sep, info, conjugate, precision="double", keep_matrix=keep, stream=stream)
         L64.Initialize(self._values)
-        LDL(info, L64, self.frontType if self.frontType in SymmFrontType.PIVOTED else SymmFrontType.LDL_2D)
+        pivoted = self.frontType in SymmFrontType.PIVOTED
+        LDL(info, L64, SymmFrontType.LDL_INTRAPIV_2D if pivoted else SymmFrontType.LDL_2D)
         self._fp64_twin = (self._values_version, L64)
         return L64
 
@@ -346,9 +348,7 @@ class DistSymmFrontTree:
 def LDL(info, L: DistSymmFrontTree, frontType=SymmFrontType.LDL_2D):
     """Multifrontal LDL^T in place (ldl.hpp:57-75).  Returns None; raises on a zero pivot."""
     if frontType not in SymmFrontType.SUPPORTED:
-        raise LogicError(_capi.CLIQ_ERR_ARG, "only the LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D, "
-                                             "LDL_INTRAPIV_1D / LDL_INTRAPIV_2D and BLOCK_LDL_1D / BLOCK_LDL_2D "
-                                             "front types are provided")
+        raise LogicError(_capi.CLIQ_ERR_ARG, "the symmetric (unfactored) front types are no factorization")
     if L.frontType not in (SymmFrontType.SYMM_1D, SymmFrontType.SYMM_2D):
         raise LogicError(_capi.CLIQ_ERR_STATE, "Matrix is already factored")
     zp = C.c_int64(-1)

@@ -19,6 +19,11 @@
 //   3. inv(A11) = op(W)^T D^{-1} W into the front's top n x n block.
 // The block sweeps gather the children's / ancestors' entries as the
 // standard ones do and run two GEMM launches per tree level.
+//
+// After a pivoted factorization (BLOCK_LDL_INTRAPIV_*, the intraPiv branch
+// of FrontBlockLDL) the same three steps run with D's 2 x 2 blocks; the
+// front then holds inv(P A11 P^T) and A21 P^T -- the reference's inv(A11)
+// and A21 in the front's pivoted order, which the solves' maps already use.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -49,9 +54,21 @@ struct Bufs {
     void* p[kBufs];
 };
 
+// op(B)(k, j) of a problem, the unit-lower mask applied
+template <class X>
+__device__ __forceinline__ X bload(const Prob& pr, const X* B, int k, int j) {
+    if (pr.maskB && j <= k) return j == k ? vone<X>() : X{};
+    X v = pr.opB == 0 ? B[pr.B + k + (int64_t)j * pr.ldb] : B[pr.B + j + (int64_t)k * pr.ldb];
+    return pr.opB == 2 ? conjv(v) : v;
+}
+
+// E (pivoted fronts, else null): D(k + 1, k) of each 2 x 2 block of D starting
+// at k; D(k, k + 1) is E[k], conjugated when cj.  The diagonal scaling then
+// mixes rows k and k +- 1 of op(B) within a block (dmode 1: D op(B), 2: D^{-1} op(B)).
 template <class T, bool C>
 __global__ void __launch_bounds__(kThreads) bgemm_kernel(const Prob* __restrict__ probs, const int64_t* __restrict__ prefix,
-                                                         const int32_t* __restrict__ bmap, Bufs bufs, const double* __restrict__ D) {
+                                                         const int32_t* __restrict__ bmap, Bufs bufs, const double* __restrict__ D,
+                                                         const double* __restrict__ E, int cj) {
     using X = V<T, C>;
     using W = DV<C>;
     constexpr int BK = C ? 8 : 16;
@@ -86,14 +103,30 @@ __global__ void __launch_bounds__(kThreads) bgemm_kernel(const Prob* __restrict_
                     if (pr.opA == 2) av = conjv(av);
                 }
                 if (j < pr.N) {
-                    if (pr.maskB && j <= kg) bv = j == kg ? vone<X>() : X{};
-                    else {
-                        bv = pr.opB == 0 ? B[pr.B + kg + (int64_t)j * pr.ldb] : B[pr.B + j + (int64_t)kg * pr.ldb];
-                        if (pr.opB == 2) bv = conjv(bv);
-                    }
+                    bv = bload(pr, B, kg, j);
                     if (pr.dmode) {
-                        const W d = reinterpret_cast<const W*>(D)[pr.dk + kg];
-                        bv = pr.dmode == 1 ? conv<X>(d * conv<W>(bv)) : conv<X>(conv<W>(bv) / d);
+                        const W* Dw = reinterpret_cast<const W*>(D) + pr.dk;
+                        const W* Ew = E ? reinterpret_cast<const W*>(E) + pr.dk : nullptr;
+                        const W d = Dw[kg];
+                        const bool first = Ew && !is_zero(Ew[kg]);
+                        const bool second = Ew && kg > 0 && !is_zero(Ew[kg - 1]);
+                        auto oc = [&](W v) { return cj ? conjv(v) : v; };
+                        if (!first && !second) {
+                            bv = pr.dmode == 1 ? conv<X>(d * conv<W>(bv)) : conv<X>(conv<W>(bv) / d);
+                        } else {
+                            // the 2 x 2 block [[d11, op(e)], [e, d22]] holding k
+                            const int k0 = first ? kg : kg - 1;
+                            const W d11 = Dw[k0], d22 = Dw[k0 + 1], e = Ew[k0];
+                            const W b0 = conv<W>(first ? bv : bload(pr, B, k0, j));
+                            const W b1 = conv<W>(first ? bload(pr, B, k0 + 1, j) : bv);
+                            W y;
+                            if (pr.dmode == 1) y = first ? d11 * b0 + oc(e) * b1 : e * b0 + d22 * b1;
+                            else {
+                                const W det = d11 * d22 - e * oc(e);
+                                y = first ? (d22 * b0 - oc(e) * b1) / det : (d11 * b1 - e * b0) / det;
+                            }
+                            bv = conv<X>(y);
+                        }
                     }
                 }
             }
@@ -400,7 +433,8 @@ static int run_gemms(Plan& P, const List<Prob>& L, const Bufs& b, std::vector<vo
     const Prob* j; const int64_t* pf; const int32_t* bm;
     int rc = blk::upload(L, owned, &j, &pf, &bm);
     if (rc != CLIQ_OK) return rc;
-    blk::bgemm_kernel<T, C><<<(unsigned)L.nblocks, blk::kThreads, 0, st>>>(j, pf, bm, b, P.D);
+    blk::bgemm_kernel<T, C><<<(unsigned)L.nblocks, blk::kThreads, 0, st>>>(j, pf, bm, b, P.D, P.pivoted ? P.E : nullptr,
+                                                                         P.conjugate ? 1 : 0);
     P.total_launches += 1;
     P.last_launches += 1;
     return check_cuda("block LDL: gemm");
@@ -724,7 +758,7 @@ static int64_t run_sched(Plan& P, const SolveSched& S, BlockState& B, T* xn) {
         } else if (r.kind == 0) {
             blk::bgemm_kernel<T, C><<<(unsigned)r.nblocks, blk::kThreads, 0, st>>>(
                 reinterpret_cast<const Prob*>(S.mem + r.jobs), reinterpret_cast<const int64_t*>(S.mem + r.prefix),
-                reinterpret_cast<const int32_t*>(S.mem + r.bmap), b, P.D);
+                reinterpret_cast<const int32_t*>(S.mem + r.bmap), b, P.D, nullptr, 0);
         } else {
             blk::copy_kernel<T, C><<<(unsigned)r.nblocks, 256, 0, st>>>(
                 reinterpret_cast<const Copy*>(S.mem + r.jobs), reinterpret_cast<const int64_t*>(S.mem + r.prefix),

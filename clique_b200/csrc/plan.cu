@@ -938,7 +938,6 @@ int cliqgpu_block_ldl(cliqgpu_plan h) {
     if (!h) return CLIQ_ERR_ARG;
     Plan& P = h->p;
     if (!P.factored) { set_last_error("block LDL: the front tree is not factored"); return CLIQ_ERR_STATE; }
-    if (P.pivoted) { set_last_error("block LDL: the block form of pivoted fronts (BLOCK_LDL_INTRAPIV_*) is not provided"); return CLIQ_ERR_ARG; }
     if (P.block) return CLIQ_OK;
     const int st = convert_to_block(P);
     if (st != CLIQ_OK) return st;

@@ -156,10 +156,14 @@ int cliqgpu_get_front_pivots(cliqgpu_plan plan, int32_t s, double* sub, int32_t*
  * triangular or diagonal solves).  cliqgpu_solve, cliqgpu_refined_solve and
  * cliqgpu_get_front then use / return that form until the next
  * cliqgpu_factor.  Runs on the plan's stream and returns when done.
+ * After cliqgpu_factor_intrapiv the same form is built from the pivoted
+ * factors, in each front's pivoted order: inv(P A11 P^T) and A21 P^T, with
+ * P from cliqgpu_get_front_pivots.
  * Replaces the blockLDL branch of LocalLDL, include/clique/numeric/ldl/
- * local.hpp:30-33 with FrontBlockLDL (ldl/local_front_block.hpp:27-71,
- * unpivoted), i.e. cliq::LDL(info, L, BLOCK_LDL_1D/BLOCK_LDL_2D), and its
- * solves lower_solve/local_front_block.hpp:29-70, solve.hpp:48-53. */
+ * local.hpp:30-33 with FrontBlockLDL (ldl/local_front_block.hpp:27-71, both
+ * branches), i.e. cliq::LDL(info, L, BLOCK_LDL_1D/BLOCK_LDL_2D) and
+ * (after cliqgpu_factor_intrapiv) BLOCK_LDL_INTRAPIV_1D/2D, and its solves
+ * lower_solve/local_front_block.hpp:29-70, solve.hpp:48-53. */
 int cliqgpu_block_ldl(cliqgpu_plan plan);
 
 /* Solve A X = B in place using the stored factors: forward sweep, diagonal

@@ -280,11 +280,17 @@ enum SymmFrontType {
     LDL_INTRAPIV_SELINV_1D, LDL_INTRAPIV_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D, BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D
 };
 inline bool Unfactored(SymmFrontType t) { return t == SYMM_1D || t == SYMM_2D; }
-// front types this library factors: unpivoted LDL, and its selective-inversion
-// forms, which at one process invert no local front (change_front_type.hpp:86-98
-// inverts distributed nodes 1 .. only), so they factor and solve as LDL; the
-// unpivoted block-LDL forms; LDL with intra-front Bunch-Kaufman pivoting
-inline bool PivotedFactorization(SymmFrontType t) { return t == LDL_INTRAPIV_1D || t == LDL_INTRAPIV_2D; }
+// front types this library factors: every factored type.  The
+// selective-inversion forms invert no local front at one process
+// (change_front_type.hpp:86-98 inverts distributed nodes 1 .. only), so they
+// factor and solve as their LDL / pivoted LDL base types.
+inline bool PivotedFactorization(SymmFrontType t) {
+    return t == LDL_INTRAPIV_1D || t == LDL_INTRAPIV_2D || t == LDL_INTRAPIV_SELINV_1D || t == LDL_INTRAPIV_SELINV_2D ||
+           t == BLOCK_LDL_INTRAPIV_1D || t == BLOCK_LDL_INTRAPIV_2D;
+}
+inline bool BlockFactorization(SymmFrontType t) {
+    return t == BLOCK_LDL_1D || t == BLOCK_LDL_2D || t == BLOCK_LDL_INTRAPIV_1D || t == BLOCK_LDL_INTRAPIV_2D;
+}
 inline bool Provided(SymmFrontType t) {
     return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D || t == BLOCK_LDL_1D || t == BLOCK_LDL_2D ||
            PivotedFactorization(t);
@@ -341,13 +347,12 @@ template <class F>
 void LDL(DistSymmInfo&, DistSymmFrontTree<F>& L, SymmFrontType newFrontType = LDL_2D) {
     if (!Unfactored(L.frontType)) throw LogicError("Matrix is already factored");
     if (!Provided(newFrontType))
-        throw LogicError("Only the LDL_1D / LDL_2D, LDL_SELINV_1D / LDL_SELINV_2D, LDL_INTRAPIV_1D / LDL_INTRAPIV_2D and "
-                         "BLOCK_LDL_1D / BLOCK_LDL_2D front types are provided");
+        throw LogicError("The symmetric (unfactored) front types are no factorization");
     int64_t zp = -1;
     if (PivotedFactorization(newFrontType)) Check(cliqgpu_factor_intrapiv(L.Plan(), &zp), "LDL");
     else Check(cliqgpu_factor(L.Plan(), &zp), "LDL");
     L.frontType = newFrontType;
-    if (newFrontType == BLOCK_LDL_1D || newFrontType == BLOCK_LDL_2D) Check(cliqgpu_block_ldl(L.Plan()), "LDL (block form)");
+    if (BlockFactorization(newFrontType)) Check(cliqgpu_block_ldl(L.Plan()), "LDL (block form)");
 }
 
 template <class F>

@@ -26,6 +26,7 @@
  *   dense partial front LDL^T ... include/clique/numeric/ldl/local_front.hpp:30-71 (FrontLDL)
  *   pivoted front LDL^T ......... include/clique/numeric/ldl/local_front.hpp:74-94 (FrontLDLIntraPiv;
  *                                 Bunch-Kaufman partial pivoting restated from its publication)
+ *   pivoted block front ......... include/clique/numeric/ldl/local_front_block.hpp:36-58
  *   pivoted front solves ........ include/clique/numeric/lower_solve/local_front.hpp:53-93,
  *                                 include/clique/numeric/diagonal_solve.hpp:53-59 (QuasiDiagonalSolve)
  *   forward / backward sweeps ... include/clique/numeric/lower_solve/local.hpp:42-119,203-277
@@ -503,10 +504,12 @@ void orc_fronts_free(orc_fronts* f) {
 /* LocalLDL with blocksize nb; returns 0, or 1 + (ND index) of the first zero pivot. */
 i64 orc_ldl(orc_fronts* f, int nb) { return f->is_complex ? local_ldl_z(f->impl, nb) : local_ldl_d(f->impl, nb); }
 /* LocalLDL with the front type chosen: kind = 1 for BLOCK_LDL_2D (FrontBlockLDL,
- * block solves), 2 for LDL_INTRAPIV_2D (FrontLDLIntraPiv, pivoted solves) */
+ * block solves), 2 for LDL_INTRAPIV_2D (FrontLDLIntraPiv, pivoted solves),
+ * 3 for BLOCK_LDL_INTRAPIV_2D (FrontBlockLDL's intraPiv branch) */
 i64 orc_ldl_ex(orc_fronts* f, int nb, int kind) {
-    if (f->is_complex) { set_block_z(f->impl, kind == 1); set_pivot_z(f->impl, kind == 2); }
-    else { set_block_d(f->impl, kind == 1); set_pivot_d(f->impl, kind == 2); }
+    const int block = kind == 1 || kind == 3, pivot = kind == 2 || kind == 3;
+    if (f->is_complex) { set_block_z(f->impl, block); set_pivot_z(f->impl, pivot); }
+    else { set_block_d(f->impl, block); set_pivot_d(f->impl, pivot); }
     return orc_ldl(f, nb);
 }
 /* pivoted fronts: D[k + 1, k] of the 2 x 2 blocks (n) and the pivot rows (n) of node s */

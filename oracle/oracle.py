@@ -147,8 +147,9 @@ class Fronts:
 
     def ldl(self, nb=96, block=False, pivot=False):
         """LocalLDL; block=True for the BLOCK_LDL_2D front type (FrontBlockLDL),
-        pivot=True for LDL_INTRAPIV_2D (FrontLDLIntraPiv, Bunch-Kaufman)."""
-        kind = 1 if block else (2 if pivot else 0)
+        pivot=True for LDL_INTRAPIV_2D (FrontLDLIntraPiv, Bunch-Kaufman), both
+        for BLOCK_LDL_INTRAPIV_2D."""
+        kind = (3 if pivot else 1) if block else (2 if pivot else 0)
         return int(lib().orc_ldl_ex(self.h, nb, kind))
 
     def pivots(self, s):

@@ -171,3 +171,38 @@ def test_symmetric_solve_pivots_by_default():
     B = ops.random_rhs(A.n, 2, seed=6, complex_=True)
     X = cliq.SymmetricSolve(A, B, *dims, cutoff=40)
     assert residual(A, X, B) <= 1e-12
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+def test_block_intrapiv_matches_oracle(oracle, kind):
+    """BLOCK_LDL_INTRAPIV_2D: the GPU fronts hold inv(P A11 P^T) over A21 P^T
+    (the pivoted order its solves use); the oracle's hold inv(A11) over A21 in
+    the assembled order (FrontBlockLDL's intraPiv branch).  Same pivots, the
+    same blocks once permuted, the same solutions; FP32 fronts refine."""
+    dims, cutoff = (24, 12, 6), 100
+    A, conj = _indefinite(kind, dims)
+    cplx = kind != "real"
+    bt = cliq.SymmFrontType.BLOCK_LDL_INTRAPIV_2D
+    _, info, L = _tree(A, dims, cutoff, "double", conj, front_type=bt)
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=cplx, conjugate=conj)
+    assert F.ldl(96, block=True, pivot=True) == 0
+    for s in range(S.num_nodes):
+        Lo, _ = F.front(s)
+        _, po = F.pivots(s)
+        Lg, _ = L.front(s)
+        _, pg = L.front_pivots(s)
+        assert np.array_equal(pg, po), s
+        n = Lg.shape[1]
+        top = Lo[:n][np.ix_(po, po)]
+        assert np.abs(Lg[:n] - top).max() <= 1e-9 * np.abs(top).max(), s
+        if Lg.shape[0] > n:
+            low = Lo[n:][:, po]
+            assert np.abs(Lg[n:] - low).max() <= 1e-10 * max(np.abs(low).max(), 1.0), s
+    B = ops.random_rhs(A.n, 4, seed=8, complex_=cplx)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-9
+    assert residual(A, X, B) <= 1e-10   # explicit inverses of the pivot blocks: measured up to 1.5e-11
+    _, _, L32 = _tree(A, dims, cutoff, "single", conj, front_type=bt, keep=True)
+    X32, it, rr = cliq.RefinedSolve(L32, B, 1e-10, 40)
+    assert rr <= 1e-10, (it, rr)
