@@ -29,16 +29,19 @@ def main():
     p.add_argument("--cutoff", type=int, default=128)
     p.add_argument("--precision", default="single")
     p.add_argument("--nrhs", type=int, default=4)
+    p.add_argument("--types", default="LDL_2D,LDL_INTRAPIV_2D", help="front types to time, comma-separated")
+    p.add_argument("--reps", type=int, default=2, help="factorizations per type (the last one is reported)")
     a = p.parse_args()
     n = a.n
     A, _, _ = ops.helmholtz_workload_3d(n, seed=0)
     map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, a.cutoff)
     B = ops.random_rhs(A.n, a.nrhs, seed=1, complex_=True)
     out = {"n": n, "precision": a.precision, "nrhs": a.nrhs}
-    for name, ft in (("LDL_2D", cliq.SymmFrontType.LDL_2D), ("LDL_INTRAPIV_2D", cliq.SymmFrontType.LDL_INTRAPIV_2D)):
+    for name in a.types.split(","):
+        ft = getattr(cliq.SymmFrontType, name)
         L = cliq.DistSymmFrontTree(A, map_, sep, info, precision=a.precision, keep_matrix=True)
         r = {}
-        for rep in range(2):   # the second run reuses the plan (new values, same pattern)
+        for rep in range(a.reps):   # later runs reuse the plan (new values, same pattern)
             if rep:
                 L.Initialize(A.values)
             torch.cuda.synchronize()
@@ -54,7 +57,7 @@ def main():
         X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 40)
         r["refined"] = {"s": round(time.perf_counter() - t0, 4), "iterations": it, "relres": rr}
         r["residual"] = float(np.linalg.norm(A.to_scipy() @ X - B) / np.linalg.norm(B))
-        if ft == cliq.SymmFrontType.LDL_INTRAPIV_2D:
+        if ft in cliq.SymmFrontType.PIVOTED:
             swaps = blocks = 0
             for s in range(info.num_nodes):
                 sub, piv = L.front_pivots(s)
