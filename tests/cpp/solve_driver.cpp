@@ -1,8 +1,10 @@
 // The flow of the reference's tests/Solve.cpp written against the drop-in
 // header: 3D 7-point Laplacian (diagonal 6 + shift), manufactured solution
 // X, Y := A X, natural nested dissection, front tree, LDL, Pull / Solve /
-// Push, and the error || X - X_hat || / || X || per right-hand side.
-// Exit status 0 when every error is below the tolerance.
+// Push, and the error || X - X_hat || / || X || per right-hand side.  The
+// last case shifts the diagonal to 0.5 (indefinite) and factors with
+// intra-front pivoting (LDL_INTRAPIV_1D, the front type of the reference's
+// SymmetricSolve).  Exit status 0 when every error is below the tolerance.
 #include <cstdio>
 #include <cstdlib>
 
@@ -11,7 +13,7 @@
 using namespace cliq;
 
 template <class F>
-int run(int n1, int n2, int n3, int numRhs, int cutoff, double shift, double tol) {
+int run(int n1, int n2, int n3, int numRhs, int cutoff, double shift, double tol, SymmFrontType ft = LDL_2D) {
     const int N = n1 * n2 * n3;
     DistSparseMatrix<F> A(N, mpi::COMM_WORLD);
     A.StartAssembly();
@@ -39,7 +41,7 @@ int run(int n1, int n2, int n3, int numRhs, int cutoff, double shift, double tol
     map.FormInverse(inverseMap);
     DistSymmFrontTree<F> frontTree(A, map, sepTree, info, false);
     const double t0 = mpi::Time();
-    LDL(info, frontTree, LDL_2D);
+    LDL(info, frontTree, ft);
     const double t1 = mpi::Time();
     DistNodalMultiVec<F> YNodal;
     YNodal.Pull(inverseMap, info, Y);
@@ -79,6 +81,7 @@ int main(int argc, char* argv[]) {
         rc |= run<double>(n, n, n, 5, 128, 0.1, 1e-10);
         rc |= run<Complex<double>>(n / 2 + 3, n / 2, n / 2 + 1, 3, 64, 0.1, 1e-10);
         rc |= run<float>(n / 2, n / 2, n / 2, 2, 64, 0.1, 1e-4);
+        rc |= run<double>(n / 2 + 2, n / 2 + 1, n / 2, 3, 64, -5.5, 1e-9, LDL_INTRAPIV_1D);
     } catch (const std::exception& e) {
         std::printf("exception: %s\n", e.what());
         rc = 1;

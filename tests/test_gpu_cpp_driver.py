@@ -1,6 +1,7 @@
 """The C++ drop-in header (include/clique_b200/clique.hpp): the flow of the
 reference's tests/Solve.cpp, compiled with g++ against libcliqgpu.so and run
-on the GPU (FP64 real and complex, FP32 real)."""
+on the GPU (FP64 real and complex, FP32 real, and an indefinite FP64 case
+with intra-front pivoting)."""
 import os
 import shutil
 import subprocess

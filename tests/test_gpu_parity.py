@@ -531,7 +531,8 @@ def test_fp64_dmma_updates_match_cuda_cores(oracle, complex_, conjugate, monkeyp
 def test_selinv_front_types_factor_and_solve_as_ldl():
     """LDL_SELINV_1D / LDL_SELINV_2D at one process: the reference inverts only
     distributed fronts (change_front_type.hpp:86-98), so the factorization and
-    the solve are the LDL_2D ones; the pivoted types are refused."""
+    the solve are the LDL_2D ones; likewise LDL_INTRAPIV_SELINV_* and
+    LDL_INTRAPIV_*; the unfactored types are refused."""
     n = 12
     A, _, _ = ops.helmholtz_workload_3d(n, seed=4)
     B = ops.random_rhs(A.n, 2, seed=5, complex_=True)
@@ -544,7 +545,15 @@ def test_selinv_front_types_factor_and_solve_as_ldl():
         X[ft] = cliq.Solve(info, L, B.copy(order="F"))
     assert rel(X[cliq.SymmFrontType.LDL_SELINV_2D], X[cliq.SymmFrontType.LDL_2D]) <= 1e-14
     assert residual(A, X[cliq.SymmFrontType.LDL_SELINV_1D], B) <= 1e-12
-    for ft in (cliq.SymmFrontType.LDL_INTRAPIV_2D, cliq.SymmFrontType.BLOCK_LDL_INTRAPIV_2D):
+    Xp = {}
+    for ft in (cliq.SymmFrontType.LDL_INTRAPIV_2D, cliq.SymmFrontType.LDL_INTRAPIV_SELINV_2D,
+               cliq.SymmFrontType.LDL_INTRAPIV_SELINV_1D):
+        L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+        cliq.LDL(info, L, ft)
+        Xp[ft] = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(Xp[cliq.SymmFrontType.LDL_INTRAPIV_SELINV_2D], Xp[cliq.SymmFrontType.LDL_INTRAPIV_2D]) <= 1e-14
+    assert residual(A, Xp[cliq.SymmFrontType.LDL_INTRAPIV_SELINV_1D], B) <= 1e-12
+    for ft in (cliq.SymmFrontType.SYMM_1D, cliq.SymmFrontType.SYMM_2D):
         L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
         with pytest.raises(cliq.LogicError):
             cliq.LDL(info, L, ft)
