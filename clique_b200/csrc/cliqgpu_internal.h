@@ -390,7 +390,8 @@ int launch_tc2(Plan& P, const Launch& ln, cudaEvent_t between, cudaStream_t st, 
 size_t tc2_smem(bool cplx);
 // intra-front pivoting (pivot_ldl.cu)
 int pivot_begin(Plan& P, cudaStream_t st);
-int pivot_level(Plan& P, int depth, cudaStream_t st);
+int pivot_level(Plan& P, int depth, cudaStream_t st, bool schur);
+int pivot_rowmax(Plan& P, int depth, cudaStream_t st);
 int pivot_finish(Plan& P, cudaStream_t st);
 int pivot_restore_maps(Plan& P, cudaStream_t st);
 int launch_quasi_diag(Plan& P, void* X, int64_t ldx, int nrhs);

@@ -827,12 +827,33 @@ static int issue_factor_pivoted(Plan& P, int64_t* nlaunch) {
     const int64_t before = P.total_launches;
     int64_t launches = 0;
     TRY(pivot_begin(P, st));
+    // FP32 plans with the 2xFP16 tensor-core path: each level's Schur
+    // complements (fixed shapes, K = n) run as the plan's tcgen05 Schur
+    // launches, packed with D's 2 x 2 blocks; otherwise (and for launches the
+    // autotuner moved to the CUDA cores) on the CUDA cores with the panels
+    const bool tc = std::is_same<T, float>::value && P.f16_scales() && P.schur_chunk == 0;
+    std::vector<std::vector<size_t>> schur(P.max_depth + 1);
+    std::vector<char> tc_ok(P.max_depth + 1, tc ? 1 : 0);
+    for (size_t li = 0; li < P.launches.size(); ++li) {
+        const Launch& ln = P.launches[li];
+        if (ln.kind != Launch::GEMM || !ln.schur || ln.nblocks <= 0) continue;
+        schur[ln.depth].push_back(li);
+        if (ln.simt || ln.bulk || ln.prepacked) tc_ok[ln.depth] = 0;
+    }
     for (const Launch& ln : P.launches) {
         if (ln.kind != Launch::EXTEND_ADD || ln.nblocks <= 0) continue;
         extend_add_kernel<T, C><<<(unsigned)ln.nblocks, kThreads, 0, st>>>(P.fronts, items + ln.items, L, p0, p1, P.cmaps_orig);
         ++launches;
         TRY(launch_assemble_level(P, ln.depth, st));
-        TRY(pivot_level(P, ln.depth, st));
+        const bool on_tc = tc_ok[ln.depth] != 0;
+        TRY(pivot_level(P, ln.depth, st, !on_tc));
+        if (on_tc && !schur[ln.depth].empty()) {
+            TRY(pivot_rowmax(P, ln.depth, st));
+            for (size_t li : schur[ln.depth]) {
+                launch_tc2(P, P.launches[li], nullptr, st, P.pack);
+                ++launches;
+            }
+        }
     }
     TRY(pivot_finish(P, st));
     if (P.nchain_items > 0 && !P.solve_exact) {

@@ -507,6 +507,48 @@ __global__ void __launch_bounds__(kTile) bk_dinv_kernel(const FrontDev* __restri
 }
 
 // ---------------------------------------------------------------------------
+// 2xFP16 split of a level's Schur complements on the tensor cores: largest
+// |component| of each row of L21 and of S21 = B = L21 D (D with its 2 x 2
+// blocks), over the front's n columns, into the two halves of erow (float
+// bits), one thread per row below the pivots
+// ---------------------------------------------------------------------------
+template <bool C, bool CJ>
+__global__ void __launch_bounds__(256) bk_rowmax_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl, int chunks,
+                                                        const float* __restrict__ L, const double* __restrict__ D,
+                                                        const double* __restrict__ E, uint32_t* __restrict__ erow, int64_t erow_total) {
+    using X = V<float, C>;
+    using W = DV<C>;
+    const int fi = blockIdx.x / chunks, ch = blockIdx.x % chunks;
+    const FrontDev f = F[fl[fi]];
+    const int i = f.n + ch * 256 + threadIdx.x;
+    if (i >= f.m) return;
+    const int64_t row = f.L + i;
+    float ml = 0.f, ms = 0.f;
+    X prev{}, cur = f.n > 0 ? ldv<float, C>(L, row) : X{};
+    X em1{};
+    for (int k = 0; k < f.n; ++k) {
+        const X next = k + 1 < f.n ? ldv<float, C>(L, row + (int64_t)(k + 1) * f.m) : X{};
+        const X d = conv<X>(reinterpret_cast<const W*>(D)[f.off + k]);
+        const X e = conv<X>(reinterpret_cast<const W*>(E)[f.off + k]);
+        X b = d * opc<CJ>(cur);
+        if (!is_zero(e)) b += opc<CJ>(e) * opc<CJ>(next);
+        if (!is_zero(em1)) b += em1 * opc<CJ>(prev);
+        if constexpr (C) {
+            ml = fmaxf(ml, fmaxf(fabsf(cur.r), fabsf(cur.i)));
+            ms = fmaxf(ms, fmaxf(fabsf(b.r), fabsf(b.i)));
+        } else {
+            ml = fmaxf(ml, fabsf(cur));
+            ms = fmaxf(ms, fabsf(b));
+        }
+        prev = cur;
+        cur = next;
+        em1 = e;
+    }
+    erow[f.erow + i] = __float_as_uint(ml);
+    erow[erow_total + f.erow + i] = __float_as_uint(ms);
+}
+
+// ---------------------------------------------------------------------------
 // index maps for the solves in the pivoted order
 // ---------------------------------------------------------------------------
 __global__ void remap_positions_kernel(int64_t n, const int32_t* __restrict__ pivg, const int32_t* __restrict__ perm,
@@ -563,7 +605,7 @@ __global__ void quasi_diag_kernel(T* __restrict__ X, int64_t ldx, int64_t n, int
 }
 
 template <class T, bool C, bool CJ>
-static int level_t(Plan& P, int depth, cudaStream_t st) {
+static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
     const SolveLevel& lv = P.solve_levels[depth];
     if (lv.nfronts <= 0) return CLIQ_OK;
     const int32_t* fl = P.level_fronts + lv.fronts;
@@ -608,6 +650,7 @@ static int level_t(Plan& P, int depth, cudaStream_t st) {
                 P.fronts, fl, tpf, 0, L, p0, p1, P.D, P.E, P.pstate);
         P.total_launches += 3;
     }
+    if (!schur) return check_cuda("pivoted level");   // the Schur complements go to the tensor cores
     // the Schur complement of every front of the level, K = n
     int64_t tpf = 0;
     for (int s : P.level_list[depth]) tpf = std::max(tpf, tiles(P.hfronts[s].m - P.hfronts[s].n, P.hfronts[s].m - P.hfronts[s].n));
@@ -689,15 +732,33 @@ int pivot_restore_maps(Plan& P, cudaStream_t st) {
     return check_cuda("restore maps");
 }
 
-int pivot_level(Plan& P, int depth, cudaStream_t st) {
+int pivot_level(Plan& P, int depth, cudaStream_t st, bool schur) {
     if (depth < 0 || depth > P.max_depth) return CLIQ_OK;
     const bool cj = P.conjugate && P.cplx();
     if (P.precision == CLIQ_FP64) {
-        if (!P.cplx()) return piv::level_t<double, false, false>(P, depth, st);
-        return cj ? piv::level_t<double, true, true>(P, depth, st) : piv::level_t<double, true, false>(P, depth, st);
+        if (!P.cplx()) return piv::level_t<double, false, false>(P, depth, st, schur);
+        return cj ? piv::level_t<double, true, true>(P, depth, st, schur) : piv::level_t<double, true, false>(P, depth, st, schur);
     }
-    if (!P.cplx()) return piv::level_t<float, false, false>(P, depth, st);
-    return cj ? piv::level_t<float, true, true>(P, depth, st) : piv::level_t<float, true, false>(P, depth, st);
+    if (!P.cplx()) return piv::level_t<float, false, false>(P, depth, st, schur);
+    return cj ? piv::level_t<float, true, true>(P, depth, st, schur) : piv::level_t<float, true, false>(P, depth, st, schur);
+}
+
+// row maxima of the level's Schur operands for the 2xFP16 split (FP32 plans)
+int pivot_rowmax(Plan& P, int depth, cudaStream_t st) {
+    const SolveLevel& lv = P.solve_levels[depth];
+    if (lv.nfronts <= 0 || !P.erow || P.precision != CLIQ_FP32) return CLIQ_OK;
+    int max_u = 0;
+    for (int s : P.level_list[depth]) max_u = std::max(max_u, P.hfronts[s].m - P.hfronts[s].n);
+    if (max_u <= 0) return CLIQ_OK;
+    const int chunks = (max_u + 255) / 256;
+    const unsigned g = (unsigned)((int64_t)lv.nfronts * chunks);
+    const int32_t* fl = P.level_fronts + lv.fronts;
+    const float* L = reinterpret_cast<const float*>(P.L);
+    if (!P.cplx()) piv::bk_rowmax_kernel<false, false><<<g, 256, 0, st>>>(P.fronts, fl, chunks, L, P.D, P.E, P.erow, P.erow_total);
+    else if (P.conjugate) piv::bk_rowmax_kernel<true, true><<<g, 256, 0, st>>>(P.fronts, fl, chunks, L, P.D, P.E, P.erow, P.erow_total);
+    else piv::bk_rowmax_kernel<true, false><<<g, 256, 0, st>>>(P.fronts, fl, chunks, L, P.D, P.E, P.erow, P.erow_total);
+    P.total_launches += 1;
+    return check_cuda("pivoted row maxima");
 }
 
 int pivot_finish(Plan& P, cudaStream_t st) {

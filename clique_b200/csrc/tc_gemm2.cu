@@ -171,15 +171,37 @@ __device__ __forceinline__ void pack_f16_planes(const PackJob& jb, const V<float
     }
 }
 
-template <bool C, bool CJ>
+// S = D op(L) of one row over the k step when D has 2 x 2 blocks (pivoted
+// fronts): e[q + 1] = D(k + 1, k) of a block starting at k = k0 + q (index 0
+// is k0 - 1), D(k, k + 1) = op(e); vm / vp are L at k0 - 1 and k0 + 16
+template <bool CJ, class X>
+__device__ __forceinline__ void quasi_scale(X (&v)[kKS16], const X* d, const X* e, X vm, X vp) {
+    X w[kKS16];
+#pragma unroll
+    for (int q = 0; q < kKS16; ++q) {
+        const X lo = q > 0 ? v[q - 1] : vm, hi = q + 1 < kKS16 ? v[q + 1] : vp;
+        X y = d[q] * opc<CJ>(v[q]);
+        if (!is_zero(e[q + 1])) y += opc<CJ>(e[q + 1]) * opc<CJ>(hi);
+        if (!is_zero(e[q])) y += e[q] * opc<CJ>(lo);
+        w[q] = y;
+    }
+#pragma unroll
+    for (int q = 0; q < kKS16; ++q) v[q] = w[q];
+}
+
+// PV: the fronts were factored with intra-front pivoting; E (like D) holds
+// D(k + 1, k) of each 2 x 2 block of D, and the D-scaled operands mix the
+// two rows of a block (the Schur complements of such fronts)
+template <bool C, bool CJ, bool PV = false>
 __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restrict__ jobs, const int64_t* __restrict__ prefix,
                                                        const int32_t* __restrict__ bmap,
                                                        const float* __restrict__ L, const double* __restrict__ D,
                                                        const uint32_t* __restrict__ eblk, const uint32_t* __restrict__ erow,
-                                                       float* __restrict__ out) {
+                                                       float* __restrict__ out, const double* __restrict__ E = nullptr) {
     using X = V<float, C>;
     using W = DV<C>;
     __shared__ X s_da[kKS16], s_ds[kKS16];   // pivots of this k step: A scaling (jb.d) and S = D op(rows) (jb.dS)
+    __shared__ X s_ea[kKS16 + 2], s_es[kKS16 + 2];   // PV: 2 x 2 block entries from k0 - 1 to k0 + 16
     const int64_t bid = blockIdx.x;
     const int lo = bmap[bid];
     const PackJob jb = jobs[lo];
@@ -204,19 +226,46 @@ __global__ void __launch_bounds__(kTcBM) pack_f16_kernel(const PackJob* __restri
         s_da[row] = (jb.d >= 0 && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.d + k]) : X{};
         s_ds[row] = (sjob && k < jb.K) ? conv<X>(reinterpret_cast<const W*>(D)[jb.dS + k]) : X{};
     }
+    X vm{}, vp{};
+    if constexpr (PV) {
+        if (row < kKS16 + 2) {
+            const int k = ks * kKS16 + row - 1;
+            const bool in = k >= 0 && k < jb.K;
+            s_ea[row] = (jb.d >= 0 && in) ? conv<X>(reinterpret_cast<const W*>(E)[jb.d + k]) : X{};
+            s_es[row] = (sjob && in) ? conv<X>(reinterpret_cast<const W*>(E)[jb.dS + k]) : X{};
+        }
+        const int k0 = ks * kKS16;
+        if (row < jb.tile_rows && r < jb.R) {
+            if (k0 > 0) vm = ldv<float, C>(L, jb.src + r + (int64_t)(k0 - 1) * jb.ld);
+            if (k0 + kKS16 < jb.K) vp = ldv<float, C>(L, jb.src + r + (int64_t)(k0 + kKS16) * jb.ld);
+        }
+    }
     __syncthreads();
     if (row >= jb.tile_rows) return;
     if (jb.d >= 0) {
+        if constexpr (PV) {
+            quasi_scale<CJ>(v, s_da, s_ea, vm, vp);
+        } else {
 #pragma unroll
-        for (int q = 0; q < kKS16; ++q) v[q] = s_da[q] * opc<CJ>(v[q]);
+            for (int q = 0; q < kKS16; ++q) v[q] = s_da[q] * opc<CJ>(v[q]);
+        }
     }
     pack_f16_planes<C>(jb, v, jb.dst, jb.dst_scale, mxa, blk, ks, row, r, out);
     // the S operand from the same rows (a prefix of this job's rows)
     if (sjob) {
+        if constexpr (PV) {
+            if (r < jb.RS) quasi_scale<CJ>(v, s_ds, s_es, vm, vp);
 #pragma unroll
-        for (int q = 0; q < kKS16; ++q) {
-            const int k = ks * kKS16 + q;
-            v[q] = (r < jb.RS && k < jb.K) ? s_ds[q] * opc<CJ>(v[q]) : X{};
+            for (int q = 0; q < kKS16; ++q) {
+                const int k = ks * kKS16 + q;
+                if (!(r < jb.RS && k < jb.K)) v[q] = X{};
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kKS16; ++q) {
+                const int k = ks * kKS16 + q;
+                v[q] = (r < jb.RS && k < jb.K) ? s_ds[q] * opc<CJ>(v[q]) : X{};
+            }
         }
         pack_f16_planes<C>(jb, v, jb.dstS, jb.dst_scaleS, mxs, blk, ks, row, r, out);
     }
@@ -391,10 +440,14 @@ static void launch_pair(Plan& P, const Launch& ln, cudaEvent_t between, cudaStre
     if (ln.pack_blocks <= 0 && !ln.prepacked) return;   // nothing to update
     if (ln.pack_blocks <= 0) {
         // operands written by the panel kernel
-    } else if constexpr (F16)
-        tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, P.eblk, P.erow,
-                                                                                   pk);
-    else
+    } else if constexpr (F16) {
+        if (P.pivoted)   // Schur complements of pivoted fronts: D with 2 x 2 blocks
+            tc2::pack_f16_kernel<C, CJ, true><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(
+                jobs, jpre, P.bmap + ln.pack_map, L, P.D, P.eblk, P.erow, pk, P.E);
+        else
+            tc2::pack_f16_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, P.eblk,
+                                                                                       P.erow, pk);
+    } else
         tc2::pack_kernel<C, CJ><<<(unsigned)ln.pack_blocks, kTcBM, 0, st>>>(jobs, jpre, P.bmap + ln.pack_map, L, P.D, pk);
     if (between) cudaEventRecord(between, st);
     const size_t smem = tc2_smem(C);

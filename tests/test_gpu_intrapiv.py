@@ -206,3 +206,35 @@ def test_block_intrapiv_matches_oracle(oracle, kind):
     _, _, L32 = _tree(A, dims, cutoff, "single", conj, front_type=bt, keep=True)
     X32, it, rr = cliq.RefinedSolve(L32, B, 1e-10, 40)
     assert rr <= 1e-10, (it, rr)
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+def test_intrapiv_fp32_tensor_core_schur(kind, monkeypatch):
+    """FP32 pivoted fronts with the Schur complements on the tensor cores
+    (2xFP16 split, D's 2x2 blocks packed into the S operand) are about as
+    accurate as with the CUDA-core Schur update, measured against the FP64
+    pivoted fronts on the fronts whose pivot order all three share."""
+    dims, cutoff = (16, 16, 10), 200
+    A, conj = _indefinite(kind, dims)
+    runs = {}
+    for name, prec, tc in (("fp64", "double", "1"), ("tc", "single", "1"), ("cc", "single", "0")):
+        monkeypatch.setenv("CLIQGPU_TENSOR_CORES", tc)
+        _, info, L = _tree(A, dims, cutoff, prec, conj)
+        runs[name] = [(L.front(s), L.front_pivots(s)) for s in range(info.num_nodes)]
+    err = {"tc": 0.0, "cc": 0.0}
+    same = 0
+    for s in range(len(runs["fp64"])):
+        (L64, d64), (_, p64) = runs["fp64"][s]
+        if not all(np.array_equal(runs[k][s][1][1], p64) for k in ("tc", "cc")):
+            continue
+        same += 1
+        scale = max(np.abs(L64).max(), np.abs(d64).max(), 1e-300)
+        for k in ("tc", "cc"):
+            (Lk, dk), _ = runs[k][s]
+            err[k] = max(err[k], np.abs(Lk - L64).max() / scale, np.abs(dk - d64).max() / scale)
+    print(f"{same} of {len(runs['fp64'])} fronts with the FP64 pivot order; worst error vs FP64: "
+          f"tensor-core Schur {err['tc']:.2e}, CUDA-core Schur {err['cc']:.2e}")
+    assert same >= len(runs["fp64"]) // 2
+    # measured: 5.6e-3 / 1.5e-3 (real), 1.8e-6 / 1.8e-6 (complex), 2.8e-3 / 3.2e-3
+    # (Hermitian); a wrong 2x2 term in the packed operand gives O(1)
+    assert err["tc"] <= 6.0 * err["cc"] + 1e-6, err
