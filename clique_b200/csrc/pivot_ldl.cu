@@ -11,7 +11,7 @@
 //
 // GPU form, per tree level after its extend-add and assembly, right-looking
 // in panels of 64 (65 when a 2 x 2 block closes the panel) columns:
-//   bk_panel_kernel   one CTA per front: the panel's pivots one column at a
+//   bk_panel_kernel   one CTA per front (1024 threads, 512 for FP64): the panel's pivots one column at a
 //                     time.  The candidate columns are formed with the
 //                     panel's pending update (A(:,k) - L(:,panel) B(k,panel)^T,
 //                     B = D op(L)^T built from L and D on the fly), the pivot
@@ -51,7 +51,9 @@ namespace piv {
 
 constexpr int kNb = 64;                 // panel width (one more when a 2 x 2 block closes it)
 constexpr int kMaxPanel = kNb + 1;
-constexpr int kPanelThreads = 512;
+// threads of a panel CTA: as many loads in flight as the registers allow
+// (FP32: 51-62 registers a thread, 1024 threads; FP64: up to 126, 512)
+template <class T> constexpr int panel_threads() { return sizeof(T) == 4 ? 1024 : 512; }
 constexpr int kLowerRows = 128;         // rows of A21 per bk_lower_kernel CTA
 constexpr int kUpdThreads = 256;
 constexpr int kUpdTile = 64;
@@ -77,6 +79,28 @@ __device__ __forceinline__ X bval(int p, X d, X e, X em1, bool first, Get Lrow) 
     if (!is_zero(e)) b += opc<CJ>(e) * opc<CJ>(Lrow(p + 1));
     if (first && !is_zero(em1)) b += em1 * opc<CJ>(Lrow(p - 1));
     return b;
+}
+
+// sum_p L(i, j0 + p) w[p] over the panel's factored columns (row element
+// offset e0 of column j0, column stride m): eight loads in flight, two
+// partial sums
+template <class T, class X>
+__device__ __forceinline__ X panel_dot(const T* L, int64_t e0, int m, int np, const X* w) {
+    constexpr bool C = !std::is_same<X, T>::value;
+    X s0{}, s1{};
+    int p = 0;
+    for (; p + 8 <= np; p += 8) {
+        X l[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) l[q] = ldv<T, C>(L, e0 + (int64_t)(p + q) * m);
+#pragma unroll
+        for (int q = 0; q < 8; q += 2) {
+            mac(s0, l[q], w[p + q]);
+            mac(s1, l[q + 1], w[p + q + 1]);
+        }
+    }
+    for (; p < np; ++p) mac(s0, ldv<T, C>(L, e0 + (int64_t)p * m), w[p]);
+    return s0 + s1;
 }
 
 // block-wide max with the smallest index on ties
@@ -112,7 +136,7 @@ __device__ __forceinline__ void block_argmax(T& v, int& idx, T* sv, int* si) {
 // one panel of Bunch-Kaufman pivots per front
 // ---------------------------------------------------------------------------
 template <class T, bool C, bool CJ>
-__global__ void __launch_bounds__(kPanelThreads) bk_panel_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+__global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
                                                                  T* __restrict__ L, double* __restrict__ D, double* __restrict__ E,
                                                                  int32_t* __restrict__ pivg, T* __restrict__ cvec, T* __restrict__ vvec,
                                                                  int32_t* __restrict__ state, int32_t* __restrict__ status) {
@@ -152,8 +176,7 @@ __global__ void __launch_bounds__(kPanelThreads) bk_panel_kernel(const FrontDev*
         T best = T(-1);
         int bi = INT_MAX;
         for (int i = k + tid; i < n; i += nt) {
-            X a = ldv<T, C>(L, at(i, k));
-            for (int p = 0; p < np; ++p) a -= ldv<T, C>(L, at(i, j0 + p)) * s_w[p];
+            X a = ldv<T, C>(L, at(i, k)) - panel_dot(L, at(i, j0), m, np, s_w);
             if (i == k) {
                 if constexpr (CJ) a = realpart(a);
                 s_akk = a;
@@ -200,8 +223,7 @@ __global__ void __launch_bounds__(kPanelThreads) bk_panel_kernel(const FrontDev*
                     if constexpr (CJ) a = realpart(a);
                     s_ar = a;
                 } else {
-                    a = ldv<T, C>(L, at(j, imax));
-                    for (int p = 0; p < np; ++p) a -= ldv<T, C>(L, at(j, j0 + p)) * s_wi[p];
+                    a = ldv<T, C>(L, at(j, imax)) - panel_dot(L, at(j, j0), m, np, s_wi);
                 }
                 stv<T, C>(vvec, f.off + j, a);
                 if (j != imax) {
@@ -633,7 +655,7 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
     };
     const int steps = (max_n + kNb - 1) / kNb;
     for (int step = 0; step < steps; ++step) {
-        bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, kPanelThreads, 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec, vvec,
+        bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, panel_threads<T>(), 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec, vvec,
                                                                                    P.pstate, P.status);
         if (max_u > 0)
             bk_lower_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * chunks), kLowerRows, smem_lower, st>>>(
