@@ -238,3 +238,19 @@ def test_intrapiv_fp32_tensor_core_schur(kind, monkeypatch):
     # measured: 5.6e-3 / 1.5e-3 (real), 1.8e-6 / 1.8e-6 (complex), 2.8e-3 / 3.2e-3
     # (Hermitian); a wrong 2x2 term in the packed operand gives O(1)
     assert err["tc"] <= 6.0 * err["cc"] + 1e-6, err
+
+
+@pytest.mark.parametrize("dims,cutoff", [((1, 1, 1), 1), ((5, 1, 1), 1), ((2, 2, 2), 100), ((17, 3, 1), 4),
+                                         ((7, 5, 3), 6), ((65, 2, 1), 16), ((3, 70, 1), 100)])
+def test_intrapiv_edge_grids(oracle, dims, cutoff):
+    """Degenerate trees (one node, empty leaves, thin grids, one front of
+    210 pivots) with pivoting: the oracle's pivoted solution."""
+    A0 = ops.laplacian_3d(*dims, 0.5)
+    A = _perturbed(A0, A0.values)
+    B = ops.random_rhs(A.n, 2, seed=4)
+    _, info, L = _tree(A, dims, cutoff, "double", False)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values)
+    assert F.ldl(96, pivot=True) == 0
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
