@@ -103,33 +103,28 @@ __device__ __forceinline__ X panel_dot(const T* L, int64_t e0, int m, int np, co
     return s0 + s1;
 }
 
-// block-wide max with the smallest index on ties
+// block-wide max with the smallest index on ties, one barrier: every warp
+// reduces the per-warp partials itself (the partials are rewritten only
+// after a later barrier of the caller)
 template <class T>
 __device__ __forceinline__ void block_argmax(T& v, int& idx, T* sv, int* si) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        const T ov = __shfl_down_sync(0xffffffffu, v, o);
-        const int oi = __shfl_down_sync(0xffffffffu, idx, o);
+        const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
         if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
     }
     if (lane == 0) { sv[w] = v; si[w] = idx; }
     __syncthreads();
-    if (w == 0) {
-        v = lane < nw ? sv[lane] : T(-1);
-        idx = lane < nw ? si[lane] : INT_MAX;
+    v = lane < nw ? sv[lane] : T(-1);
+    idx = lane < nw ? si[lane] : INT_MAX;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const T ov = __shfl_down_sync(0xffffffffu, v, o);
-            const int oi = __shfl_down_sync(0xffffffffu, idx, o);
-            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
-        }
-        if (lane == 0) { sv[0] = v; si[0] = idx; }
+    for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
     }
-    __syncthreads();
-    v = sv[0];
-    idx = si[0];
-    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -145,8 +140,8 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
     __shared__ X s_d[kMaxPanel], s_e[kMaxPanel];   // the panel's D (diagonal, and D(p+1,p) of 2 x 2 blocks)
     __shared__ X s_w[kMaxPanel];                   // B(k, p)
     __shared__ X s_lr[kMaxPanel], s_wi[kMaxPanel]; // L(imax, p), B(imax, p)
-    __shared__ T s_rv[32];
-    __shared__ int s_ri[32];
+    __shared__ T s_rv[32], s_rv2[32];   // per-warp partials of the two reductions of a column step
+    __shared__ int s_ri[32], s_ri2[32];
     __shared__ X s_akk, s_ar;
     const int s = fl[blockIdx.x];
     const FrontDev f = F[s];
@@ -186,7 +181,7 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
             }
             stv<T, C>(cvec, f.off + i, a);
         }
-        block_argmax(best, bi, s_rv, s_ri);   // (its barriers publish s_akk and cvec)
+        block_argmax(best, bi, s_rv, s_ri);   // (its barrier publishes s_akk)
         const T colmax = best > T(0) ? best : T(0);
         const int imax = bi == INT_MAX ? k : bi;
         const T absakk = mag1(s_akk);
@@ -207,6 +202,7 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
             __syncthreads();
             T rbest = T(-1);
             int rbi = INT_MAX;
+            // (the rows of vvec follow the same thread mapping as those of cvec)
             for (int j = k + tid; j < n; j += nt) {
                 X a;
                 if (j < imax) {
@@ -231,7 +227,7 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
                     if (g > rbest) { rbest = g; rbi = j; }
                 }
             }
-            block_argmax(rbest, rbi, s_rv, s_ri);
+            block_argmax(rbest, rbi, s_rv2, s_ri2);   // (publishes s_ar)
             const T rowmax = rbest > T(0) ? rbest : T(0);
             if (absakk >= (T)kAlpha * colmax * (colmax / rowmax)) {
                 kp = k;
@@ -279,13 +275,19 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
                 stv<T, C>(vvec, f.off + b, v0);
             }
         }
-        __syncthreads();
+        // the common step (1 x 1 pivot at k, no interchange) needs no barrier
+        // here: each thread divides the column entries it formed itself (the
+        // rows k + tid + q nt of both candidate columns), and the pivot is in
+        // shared memory
+        const bool plain = kstep == 1 && kp == k;
+        if (!plain) __syncthreads();
         // pivot columns of L (pivot rows), D and E
         if (kstep == 1) {
             const T* col = use_v ? vvec : cvec;
-            X d = ldv<T, C>(col, f.off + k);
+            X d = plain ? s_akk : ldv<T, C>(col, f.off + k);
             if constexpr (CJ) d = realpart(d);
-            for (int i = k + 1 + tid; i < n; i += nt) {
+            for (int i = k + tid; i < n; i += nt) {
+                if (i == k) continue;
                 const X c = ldv<T, C>(col, f.off + i);
                 stv<T, C>(L, at(i, k), is_zero(d) ? X{} : c / d);
             }
