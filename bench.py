@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end pass (a second FP32 plan)")
     p.add_argument("--operator", default="helmholtz", choices=["helmholtz", "laplacian"])
+    p.add_argument("--ordering", default="natural", choices=["natural", "graph"],
+                   help="natural nested dissection (the reference's default) or the general-graph one")
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the baseline sample")
     p.add_argument("--ref-steps", type=int, default=1, help="full-size steps of the reference arm")
     p.add_argument("--autotune", type=int, default=0,
@@ -341,7 +343,10 @@ def run_ours(args):
     cplx = np.iscomplexobj(A.values)
     n = args.n
     stream = torch.cuda.current_stream()
-    map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, args.cutoff)
+    if args.ordering == "graph":
+        map_, sep, info = cliq.NestedDissection(A, args.cutoff)
+    else:
+        map_, sep, info = cliq.NaturalNestedDissection(n, n, n, A, args.cutoff)
     vals_d = torch.from_numpy(A.values).cuda()
     B_d = torch.from_numpy(B).cuda().t().contiguous().t()
 
@@ -492,7 +497,7 @@ def run_ours(args):
     line = {"metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64+c128-IR" if cplx else "f32+f64-IR", "data": "synthetic",
-            "config": {"workload": f"{wdesc}, {args.nrhs} RHS, natural ND cutoff {args.cutoff}",
+            "config": {"workload": f"{wdesc}, {args.nrhs} RHS, {args.ordering} ND cutoff {args.cutoff}",
                        "precision": ("CFP32" if cplx else "FP32") + " fronts, FP64 pivots, FP64 refinement",
                        "tol": args.tol,
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (factor arena >> 126 MB)"},

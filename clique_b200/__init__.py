@@ -200,6 +200,22 @@ def NaturalNestedDissection(nx, ny, nz, A, cutoff=128):
     return DistMap(m), DistSeparatorTree(info), info
 
 
+def NestedDissection(A, cutoff=128, numSeqSeps=1):
+    """Nested dissection of A's graph (any structurally symmetric pattern),
+    nested_dissection.hpp:35-44,115-230 at one process; returns (map,
+    sepTree, info).  The separators come from the library's own bisection
+    (breadth-first level structures), not METIS."""
+    csr = _as_csr(A)
+    lib = _capi.load()
+    h = C.c_void_p()
+    check(lib.cliq_nested_dissection(csr.n, csr.rowptr.ctypes.data_as(C.c_void_p), csr.colind.ctypes.data_as(C.c_void_p),
+                                     cutoff, numSeqSeps, C.byref(h)), "NestedDissection")
+    info = DistSymmInfo(h.value, csr.n)
+    m = np.zeros(csr.n, np.int32)
+    check(lib.cliq_symbolic_map(h.value, m.ctypes.data_as(C.c_void_p), None))
+    return DistMap(m), DistSeparatorTree(info), info
+
+
 # ---------------------------------------------------------------------------
 # device front tree
 # ---------------------------------------------------------------------------

@@ -61,6 +61,7 @@ _SIGS = {
                                      C.c_int32, C.c_void_p]),
     "cliqgpu_grad_A_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
                                          C.c_void_p]),
+    "cliq_nested_dissection": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
     "cliq_batch_nested_dissection": (C.c_int, [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int32,
                                                C.POINTER(C.c_void_p)]),
     "cliqgpu_batch_run": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,

@@ -31,6 +31,26 @@ int cliq_natural_nested_dissection(int32_t nx, int32_t ny, int32_t nz, int64_t n
     return CLIQ_OK;
 }
 
+int cliq_nested_dissection(int64_t n, const int64_t* rowptr, const int32_t* colind, int32_t cutoff, int32_t num_seps,
+                           cliq_symbolic* out) {
+    if (!out) return CLIQ_ERR_ARG;
+    *out = nullptr;
+    cliq_symbolic h = new (std::nothrow) cliq_symbolic_s;
+    if (!h) return CLIQ_ERR_OOM;
+    int st;
+    try {
+        st = cliqgpu::graph_nested_dissection(n, rowptr, colind, cutoff, num_seps, h->s);
+    } catch (const std::bad_alloc&) {
+        st = CLIQ_ERR_OOM;
+    }
+    if (st != CLIQ_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CLIQ_OK;
+}
+
 int cliq_batch_nested_dissection(int32_t count, const int32_t* dims, int64_t n, const int64_t* rowptr,
                                  const int32_t* colind, int32_t cutoff, cliq_symbolic* out) {
     if (!out) return CLIQ_ERR_ARG;

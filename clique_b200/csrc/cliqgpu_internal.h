@@ -36,6 +36,7 @@ struct Symbolic {
 int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* rowptr, const int32_t* colind,
                               int cutoff, Symbolic& S);
 
+int graph_nested_dissection(int64_t n, const int64_t* rowptr, const int32_t* colind, int cutoff, int num_seps, Symbolic& S);
 int batch_nested_dissection(int count, const int32_t* dims, int64_t n, const int64_t* rowptr, const int32_t* colind,
                             int cutoff, Symbolic& S);
 

@@ -9,6 +9,10 @@
 //   ReverseOrder              include/clique/symbolic/nested_dissection.hpp:817-886
 //   BuildMap (P=1)            include/clique/symbolic/nested_dissection.hpp:1206-1363
 //   LocalSymmetricAnalysis    src/symbolic/LocalSymmetricAnalysis.cpp:15-114
+//   NestedDissection (general graphs, P=1)
+//                             include/clique/symbolic/nested_dissection.hpp:115-230
+//                             (the tree and numbering; the bisection is this
+//                             file's own, see graph_nested_dissection)
 //
 // Design: instead of materialising a child graph at every bisection (the
 // reference copies the graph into left/right children), the recursion here
@@ -120,13 +124,11 @@ static void relative_indices(const std::vector<int>& sub, const std::vector<int>
 
 }  // namespace
 
-int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* rowptr, const int32_t* colind,
-                              int cutoff, Symbolic& S) {
-    if (nx < 0 || ny < 0 || nz < 0 || (int64_t)nx * ny * nz != n || n <= 0 || !rowptr || !colind) return CLIQ_ERR_ARG;
-    if (n > INT32_MAX / 2) return CLIQ_ERR_ARG;
-    NDBuilder B{nx, ny, nz, cutoff, {}};
-    B.recurse(Box{0, 0, 0, nx, ny, nz}, -1, 0);
-
+// ReverseOrder, BuildMap, the original lower structures and
+// LocalSymmetricAnalysis for a separator tree in pre-order (each separator
+// before its right then left subtree, as the recursions above build it)
+static int finish_symbolic(std::vector<PreNode>& pre, int64_t n, const int64_t* rowptr, const int32_t* colind, Symbolic& S) {
+    struct Holder { std::vector<PreNode>& nodes; } B{pre};
     // ReverseOrder: new index = last - old; the root keeps parent -1 unless it is the only node.
     const int nn = (int)B.nodes.size(), last = nn - 1;
     S.num_nodes = nn;
@@ -196,6 +198,239 @@ int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* 
     }
     S.finalize_views();
     return CLIQ_OK;
+}
+
+int natural_nested_dissection(int nx, int ny, int nz, int64_t n, const int64_t* rowptr, const int32_t* colind,
+                              int cutoff, Symbolic& S) {
+    if (nx < 0 || ny < 0 || nz < 0 || (int64_t)nx * ny * nz != n || n <= 0 || !rowptr || !colind) return CLIQ_ERR_ARG;
+    if (n > INT32_MAX / 2) return CLIQ_ERR_ARG;
+    NDBuilder B{nx, ny, nz, cutoff, {}};
+    B.recurse(Box{0, 0, 0, nx, ny, nz}, -1, 0);
+    return finish_symbolic(B.nodes, n, rowptr, colind, S);
+}
+
+// ---------------------------------------------------------------------------
+// NestedDissection for a general (structurally symmetric) graph at P=1.
+// The recursion, node numbering and the rest of the analysis follow the
+// reference (nested_dissection.hpp:115-230: a sub-graph of at most cutoff
+// vertices is a leaf; otherwise a vertex separator splits it, the separator
+// becomes the node, the right part is recursed on, then the left).  The
+// reference bisects with METIS; this bisection is its own:
+//   * a pseudo-peripheral start vertex (repeated breadth-first searches,
+//     George & Liu) and its level structure; the level at which the count
+//     of vertices reaches half is a vertex separator (edges join only equal
+//     or adjacent levels);
+//   * separator vertices with no neighbour on one side move to the other
+//     (to the smaller side when they touch neither), which keeps the split
+//     a separation and shrinks the separator;
+//   * num_seps start vertices are tried (the reference's numSeqSeps) and the
+//     smallest separator whose smaller side holds at least a fifth of the
+//     vertices is kept;
+//   * a disconnected sub-graph is split between its components (each whole
+//     component to the side with fewer vertices so far) with an empty
+//     separator;
+//     a sub-graph with no useful separator (fewer than three levels, as in
+//     a dense block) becomes a leaf.
+// Vertices keep the order of the input within leaves, and breadth-first
+// order within separators.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct GraphND {
+    int64_t n;
+    const int64_t* rp;
+    const int32_t* ci;
+    int cutoff, num_seps;
+    std::vector<int> stamp_of, level, part, seen;
+    int stamp = 0, visit = 0;
+    std::vector<PreNode> nodes;
+
+    // breadth-first level structure of the current sub-graph (stamp) from s:
+    // order of visit; level[] set for the visited vertices
+    int bfs(int s, std::vector<int>& order) {
+        order.clear();
+        order.push_back(s);
+        level[s] = 0;
+        seen[s] = ++visit;
+        int depth = 0;
+        for (size_t h = 0; h < order.size(); ++h) {
+            const int v = order[h];
+            depth = level[v];
+            for (int64_t e = rp[v]; e < rp[v + 1]; ++e) {
+                const int t = ci[e];
+                if (t < 0 || t >= n || stamp_of[t] != stamp || seen[t] == visit) continue;
+                seen[t] = visit;
+                level[t] = level[v] + 1;
+                order.push_back(t);
+            }
+        }
+        return depth;
+    }
+
+    // a disconnected sub-graph: its components (in the order of their first
+    // vertex) assigned whole, each to the side holding fewer vertices so far;
+    // no separator.  Returns false for a connected one.
+    bool split_components(const std::vector<int>& verts, std::vector<int>& L, std::vector<int>& R) {
+        std::vector<int> order;
+        bfs(verts[0], order);
+        if (order.size() == verts.size()) return false;
+        const int first = visit;   // searches from here on label components
+        for (int v : verts) {
+            if (seen[v] >= first && seen[v] <= visit) continue;
+            bfs(v, order);
+        }
+        // component sizes by their search number, then the assignment
+        std::vector<int> size(visit - first + 1, 0);
+        for (int v : verts) ++size[seen[v] - first];
+        std::vector<char> left(size.size(), 0);
+        int64_t nl = 0, nr = 0;
+        for (size_t c = 0; c < size.size(); ++c) {   // each component to the smaller side so far
+            if (nl <= nr) { left[c] = 1; nl += size[c]; }
+            else nr += size[c];
+        }
+        for (int v : verts) (left[seen[v] - first] ? L : R).push_back(v);
+        return !L.empty() && !R.empty();
+    }
+
+    int degree_in(int v) const {
+        int d = 0;
+        for (int64_t e = rp[v]; e < rp[v + 1]; ++e) {
+            const int t = ci[e];
+            if (t >= 0 && t < n && stamp_of[t] == stamp && t != v) ++d;
+        }
+        return d;
+    }
+
+    // one separator attempt from start vertex s0; returns false when no
+    // useful split exists.  part[] = 0 left, 1 right, 2 separator
+    bool attempt(const std::vector<int>& verts, int s0, std::vector<int>& order, int& sep_size, int& small) {
+        int s = s0, ecc = bfs(s, order);
+        for (int it = 0; it < 8; ++it) {   // pseudo-peripheral vertex
+            int best = -1, bd = INT32_MAX;
+            for (size_t h = order.size(); h-- > 0;) {
+                const int v = order[h];
+                if (level[v] != ecc) break;
+                const int d = degree_in(v);
+                if (d < bd) { bd = d; best = v; }
+            }
+            std::vector<int> o2;
+            const int e2 = bfs(best, o2);
+            if (e2 <= ecc) { bfs(s, order); break; }
+            s = best; ecc = e2; order.swap(o2);
+        }
+        const int cnt = (int)verts.size();
+        std::vector<int> per(ecc + 1, 0);
+        for (int v : order) ++per[level[v]];
+        int lsep = 0, acc = 0;
+        while (lsep <= ecc && acc + per[lsep] < cnt / 2) acc += per[lsep++];
+        if (lsep == 0 && ecc > 0) lsep = 1;
+        if (lsep >= ecc) lsep = ecc - 1;
+        if (lsep <= 0) return false;   // no level strictly inside the structure
+        int nl = 0, nr = 0;
+        std::vector<int> sep;
+        for (int v : order) {
+            if (level[v] < lsep) { part[v] = 0; ++nl; }
+            else if (level[v] > lsep) { part[v] = 1; ++nr; }
+            else { part[v] = 2; sep.push_back(v); }
+        }
+        if (nl == 0 || nr == 0) return false;
+        for (int v : sep) {   // shrink: a vertex touching one side only joins it
+            bool hl = false, hr = false;
+            for (int64_t e = rp[v]; e < rp[v + 1]; ++e) {
+                const int t = ci[e];
+                if (t < 0 || t >= n || stamp_of[t] != stamp || t == v) continue;
+                if (part[t] == 0) hl = true;
+                else if (part[t] == 1) hr = true;
+            }
+            if (!hr && (!hl || nl <= nr)) { part[v] = 0; ++nl; }
+            else if (!hl) { part[v] = 1; ++nr; }
+        }
+        sep_size = cnt - nl - nr;
+        small = std::min(nl, nr);
+        return true;
+    }
+
+    void leaf(std::vector<int>& verts, int parent, int off, int id) {
+        PreNode& nd = nodes[id];
+        nd.size = (int)verts.size(); nd.off = off; nd.parent = parent; nd.sep_parent = parent;
+        nd.inds = std::move(verts);
+        nd.subtree_end = off + nd.size;
+    }
+
+    void recurse(std::vector<int>& verts, int parent, int off) {
+        const int cnt = (int)verts.size();
+        const int id = (int)nodes.size();
+        nodes.emplace_back();
+        if (cnt <= cutoff) { leaf(verts, parent, off, id); return; }
+        ++stamp;
+        for (int v : verts) stamp_of[v] = stamp;
+        {
+            std::vector<int> L, R;
+            if (split_components(verts, L, R)) {   // empty separator
+                verts.clear();
+                verts.shrink_to_fit();
+                const int nl = (int)L.size(), nr = (int)R.size();
+                PreNode& nd = nodes[id];
+                nd.size = 0; nd.off = off + nl + nr; nd.parent = parent; nd.sep_parent = parent;
+                nd.nchild = 2; nd.subtree_end = off + cnt;
+                nodes[id].child[1] = (int)nodes.size();
+                recurse(R, id, off + nl);
+                nodes[id].child[0] = (int)nodes.size();
+                recurse(L, id, off);
+                return;
+            }
+        }
+        // tries: the first vertex, then vertices spread over the input order
+        std::vector<int> order, best_part;
+        int best_sep = INT32_MAX, best_small = -1;
+        for (int t = 0; t < std::max(1, num_seps); ++t) {
+            const int s0 = verts[(size_t)((int64_t)t * cnt / std::max(1, num_seps))];
+            int sep_size = 0, small = 0;
+            if (!attempt(verts, s0, order, sep_size, small)) continue;
+            const bool balanced = 5 * small >= cnt, best_balanced = 5 * best_small >= cnt;
+            if (best_small < 0 || (balanced && !best_balanced) ||
+                (balanced == best_balanced && (sep_size < best_sep || (sep_size == best_sep && small > best_small)))) {
+                best_sep = sep_size; best_small = small;
+                best_part.resize(cnt);
+                for (int i = 0; i < cnt; ++i) best_part[i] = part[verts[i]];
+            }
+        }
+        if (best_small <= 0) { leaf(verts, parent, off, id); return; }   // no useful split
+        std::vector<int> L, R, sep;
+        for (int i = 0; i < cnt; ++i) (best_part[i] == 0 ? L : best_part[i] == 1 ? R : sep).push_back(verts[i]);
+        if (L.empty() || R.empty()) { leaf(verts, parent, off, id); return; }
+        verts.clear();
+        verts.shrink_to_fit();
+        const int nl = (int)L.size(), nr = (int)R.size();
+        {
+            PreNode& nd = nodes[id];
+            nd.size = (int)sep.size();
+            nd.off = off + nl + nr;
+            nd.parent = parent; nd.sep_parent = parent;
+            nd.nchild = 2;
+            nd.inds = std::move(sep);
+            nd.subtree_end = off + cnt;
+        }
+        nodes[id].child[1] = (int)nodes.size();
+        recurse(R, id, off + nl);
+        nodes[id].child[0] = (int)nodes.size();
+        recurse(L, id, off);
+    }
+};
+
+}  // namespace
+
+int graph_nested_dissection(int64_t n, const int64_t* rowptr, const int32_t* colind, int cutoff, int num_seps, Symbolic& S) {
+    if (n <= 0 || !rowptr || !colind || n > INT32_MAX / 2) return CLIQ_ERR_ARG;
+    GraphND G{n, rowptr, colind, std::max(1, cutoff), std::max(1, num_seps), {}, {}, {}, {}, 0, 0, {}};
+    G.stamp_of.assign(n, 0);
+    G.level.assign(n, 0);
+    G.part.assign(n, 0);
+    G.seen.assign(n, 0);
+    std::vector<int> all(n);
+    for (int64_t i = 0; i < n; ++i) all[i] = (int)i;
+    G.recurse(all, -1, 0);
+    return finish_symbolic(G.nodes, n, rowptr, colind, S);
 }
 
 // Forest of independent grid problems: the block-diagonal matrix whose

@@ -66,6 +66,19 @@ int cliq_natural_nested_dissection(int32_t nx, int32_t ny, int32_t nz, int64_t n
                                    const int64_t* rowptr, const int32_t* colind,
                                    int32_t cutoff, cliq_symbolic* out);
 
+/* Nested dissection of a general graph (the CSR pattern of A, both
+ * triangles; structurally symmetric) followed by the symbolic analysis.
+ * The tree and numbering follow the reference's sequential recursion; the
+ * vertex separators come from this library's own bisection (breadth-first
+ * level structures from pseudo-peripheral vertices, the balanced middle
+ * level, shrunk greedily; num_seps start vertices tried) instead of METIS.
+ * Disconnected graphs split between components with empty separators.
+ * Replaces cliq::NestedDissection(graph, map, sepTree, info, sequential,
+ * numDistSeps, numSeqSeps, cutoff), include/clique/symbolic/
+ * nested_dissection.hpp:35-44,115-230 at P=1 (num_seps = numSeqSeps). */
+int cliq_nested_dissection(int64_t n, const int64_t* rowptr, const int32_t* colind, int32_t cutoff,
+                           int32_t num_seps, cliq_symbolic* out);
+
 /* Views into the analysis (pointers stay valid until cliq_symbolic_destroy).
  * Replaces reading cliq::DistSymmInfo::localNodes,
  * include/clique/symbolic/dist_symm_info.hpp:108-113. */

@@ -242,11 +242,8 @@ public:
     std::vector<std::vector<int>> inds;   // natural indices of each separator / leaf (post-order)
 };
 
-inline void NaturalNestedDissection(int nx, int ny, int nz, const DistGraph& graph, DistMap& map, DistSeparatorTree& sepTree,
-                                    DistSymmInfo& info, int cutoff = 128, bool /*storeFactRecvInds*/ = false) {
-    cliq_symbolic h = nullptr;
-    Check(cliq_natural_nested_dissection(nx, ny, nz, graph.n_, graph.rowptr_.data(), graph.colind_.data(), cutoff, &h),
-          "NaturalNestedDissection");
+// the symbolic handle's tree, analysis and map into the reference's containers
+inline void FillSymbolic(cliq_symbolic h, int64_t n, DistMap& map, DistSeparatorTree& sepTree, DistSymmInfo& info) {
     info.handle.reset(h, cliq_symbolic_destroy);
     Check(cliq_symbolic_info(h, &info.view), "NaturalNestedDissection");
     const int nn = info.view.num_nodes;
@@ -269,8 +266,27 @@ inline void NaturalNestedDissection(int nx, int ny, int nz, const DistGraph& gra
         arr(s, 0, nd.lowerStruct); arr(s, 1, nd.origLowerStruct); arr(s, 2, nd.origLowerRelInds);
         arr(s, 3, nd.leftRelInds); arr(s, 4, nd.rightRelInds); arr(s, 5, sepTree.inds[s]);
     }
-    map.map.assign(graph.n_, 0);
+    map.map.assign(n, 0);
     Check(cliq_symbolic_map(h, map.map.data(), nullptr), "NaturalNestedDissection");
+}
+
+inline void NaturalNestedDissection(int nx, int ny, int nz, const DistGraph& graph, DistMap& map, DistSeparatorTree& sepTree,
+                                    DistSymmInfo& info, int cutoff = 128, bool /*storeFactRecvInds*/ = false) {
+    cliq_symbolic h = nullptr;
+    Check(cliq_natural_nested_dissection(nx, ny, nz, graph.n_, graph.rowptr_.data(), graph.colind_.data(), cutoff, &h),
+          "NaturalNestedDissection");
+    FillSymbolic(h, graph.n_, map, sepTree, info);
+}
+
+// nested_dissection.hpp:35-44 at one process: general graphs, this library's
+// own bisection in place of METIS (numSeqSeps start vertices tried)
+inline void NestedDissection(const DistGraph& graph, DistMap& map, DistSeparatorTree& sepTree, DistSymmInfo& info,
+                             bool /*sequential*/ = true, int /*numDistSeps*/ = 1, int numSeqSeps = 1, int cutoff = 128,
+                             bool /*storeFactRecvInds*/ = false) {
+    cliq_symbolic h = nullptr;
+    Check(cliq_nested_dissection(graph.n_, graph.rowptr_.data(), graph.colind_.data(), cutoff, numSeqSeps, &h),
+          "NestedDissection");
+    FillSymbolic(h, graph.n_, map, sepTree, info);
 }
 
 // ---- numeric ---------------------------------------------------------------
