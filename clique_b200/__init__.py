@@ -543,12 +543,16 @@ def Multiply(alpha, L: DistSymmFrontTree, X, beta, Y):
     return Y
 
 
-def SymmetricSolve(A, X, nx, ny, nz, conjugate=False, cutoff=128, precision="double", tol=1e-10, max_iter=20,
-                   frontType=SymmFrontType.LDL_INTRAPIV_1D):
-    """Black-box solve (solve.hpp:95-116) with natural nested dissection on an
-    nx*ny*nz grid; intra-front pivoted fronts as in the reference (LDL_2D
-    etc. on request).  Returns the solution (natural order)."""
-    map_, sepTree, info = NaturalNestedDissection(nx, ny, nz, A, cutoff)
+def SymmetricSolve(A, X, nx=None, ny=None, nz=None, conjugate=False, cutoff=128, precision="double", tol=1e-10,
+                   max_iter=20, frontType=SymmFrontType.LDL_INTRAPIV_1D, numSeqSeps=1):
+    """Black-box solve (solve.hpp:95-116): nested dissection of A's graph, as
+    the reference orders it (or natural nested dissection when the grid
+    dimensions nx, ny, nz are given), intra-front pivoted fronts as in the
+    reference (LDL_2D etc. on request).  Returns the solution (natural order)."""
+    if nx is None or ny is None or nz is None:
+        map_, sepTree, info = NestedDissection(A, cutoff, numSeqSeps)
+    else:
+        map_, sepTree, info = NaturalNestedDissection(nx, ny, nz, A, cutoff)
     L = DistSymmFrontTree(A, map_, sepTree, info, conjugate, precision=precision, keep_matrix=True)
     LDL(info, L, frontType)
     if precision == "double":

@@ -68,3 +68,12 @@ def test_graph_nd_helmholtz_grid_matches_natural():
     Xn = cliq.Solve(info, L, B.copy(order="F"))
     assert rel(X, Xn) <= 1e-10
     assert residual(A, X, B) <= 1e-12
+
+
+def test_symmetric_solve_orders_the_graph():
+    """SymmetricSolve without grid dimensions orders A's graph, as the
+    reference's does (solve.hpp:95-116)."""
+    A = knn_graph(2000, 8, seed=21, dim=2, shift=-0.9)
+    B = ops.random_rhs(A.n, 2, seed=3)
+    X = cliq.SymmetricSolve(A, B, cutoff=64)
+    assert residual(A, X, B) <= 1e-11
