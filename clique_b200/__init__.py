@@ -560,3 +560,9 @@ def SymmetricSolve(A, X, nx=None, ny=None, nz=None, conjugate=False, cutoff=128,
         return Solve(info, L, Y)
     Y, _, _ = RefinedSolve(L, X, tol, max_iter)
     return Y
+
+
+def HermitianSolve(A, X, nx=None, ny=None, nz=None, cutoff=128, precision="double", tol=1e-10, max_iter=20,
+                   frontType=SymmFrontType.LDL_INTRAPIV_1D, numSeqSeps=1):
+    """SymmetricSolve with conjugate=True (LDL^H of a Hermitian A), solve.hpp:132-140."""
+    return SymmetricSolve(A, X, nx, ny, nz, True, cutoff, precision, tol, max_iter, frontType, numSeqSeps)

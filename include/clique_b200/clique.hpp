@@ -409,4 +409,29 @@ void Solve(const DistSymmInfo&, const DistSymmFrontTree<F>& L, DistNodalMultiVec
     }
 }
 
+// Black-box solves (solve.hpp:95-140 at one process): nested dissection of
+// A's graph, the front tree, LDL with intra-front pivoting (LDL_INTRAPIV_1D),
+// Pull / Solve / Push; X is overwritten with the solution
+template <class F>
+void SymmetricSolve(const DistSparseMatrix<F>& A, DistMultiVec<F>& X, bool conjugate = false, bool sequential = true,
+                    int numDistSeps = 1, int numSeqSeps = 1, int cutoff = 128) {
+    DistSymmInfo info;
+    DistSeparatorTree sepTree;
+    DistMap map, inverseMap;
+    NestedDissection(A.LockedDistGraph(), map, sepTree, info, sequential, numDistSeps, numSeqSeps, cutoff);
+    map.FormInverse(inverseMap);
+    DistSymmFrontTree<F> frontTree(A, map, sepTree, info, conjugate);
+    LDL(info, frontTree, LDL_INTRAPIV_1D);
+    DistNodalMultiVec<F> XNodal;
+    XNodal.Pull(inverseMap, info, X);
+    Solve(info, frontTree, XNodal);
+    XNodal.Push(inverseMap, info, X);
+}
+
+template <class F>
+void HermitianSolve(const DistSparseMatrix<F>& A, DistMultiVec<F>& X, bool sequential = true, int numDistSeps = 1,
+                    int numSeqSeps = 1, int cutoff = 128) {
+    SymmetricSolve(A, X, true, sequential, numDistSeps, numSeqSeps, cutoff);
+}
+
 }  // namespace cliq

@@ -73,6 +73,49 @@ int run(int n1, int n2, int n3, int numRhs, int cutoff, double shift, double tol
     return bad;
 }
 
+// the black-box solve (solve.hpp:95-116): nested dissection of A's graph and
+// pivoted fronts; HermitianSolve on a Hermitian indefinite operator
+template <class F>
+int run_blackbox(int n1, int n2, int n3, double shift, double tol, bool hermitian) {
+    const int N = n1 * n2 * n3;
+    DistSparseMatrix<F> A(N, mpi::COMM_WORLD);
+    A.StartAssembly();
+    A.Reserve(7 * N);
+    F up = F(-1), down = F(-1);   // x couplings: conjugate pair for the Hermitian operator
+    if constexpr (Traits<F>::complex) {
+        if (hermitian) { up = F(-0.8, -0.6); down = F(-0.8, 0.6); }
+    }
+    for (int i = 0; i < N; ++i) {
+        const int x = i % n1, y = (i / n1) % n2, z = i / (n1 * n2);
+        A.Update(i, i, F(6. + shift));
+        if (x != 0) A.Update(i, i - 1, down);
+        if (x != n1 - 1) A.Update(i, i + 1, up);
+        if (y != 0) A.Update(i, i - n1, F(-1));
+        if (y != n2 - 1) A.Update(i, i + n1, F(-1));
+        if (z != 0) A.Update(i, i - n1 * n2, F(-1));
+        if (z != n3 - 1) A.Update(i, i + n1 * n2, F(-1));
+    }
+    A.StopAssembly();
+    DistMultiVec<F> X(N, 2), Y(N, 2);
+    MakeUniform(X, 11);
+    Zero(Y);
+    Multiply(F(1), A, X, F(0), Y);
+    if (hermitian) HermitianSolve(A, Y);
+    else SymmetricSolve(A, Y);
+    int bad = 0;
+    for (int j = 0; j < 2; ++j) {
+        double e = 0, x = 0;
+        for (int i = 0; i < N; ++i) {
+            e += std::norm(Y.GetLocal(i, j) - X.GetLocal(i, j));
+            x += std::norm(X.GetLocal(i, j));
+        }
+        const double rel = std::sqrt(e / x);
+        std::printf("%s ||X - X_hat|| / ||X|| (rhs %d) = %.3e\n", hermitian ? "HermitianSolve" : "SymmetricSolve", j, rel);
+        if (!(rel <= tol)) bad = 1;
+    }
+    return bad;
+}
+
 int main(int argc, char* argv[]) {
     Initialize(argc, argv);
     const int n = argc > 1 ? std::atoi(argv[1]) : 30;
@@ -82,6 +125,8 @@ int main(int argc, char* argv[]) {
         rc |= run<Complex<double>>(n / 2 + 3, n / 2, n / 2 + 1, 3, 64, 0.1, 1e-10);
         rc |= run<float>(n / 2, n / 2, n / 2, 2, 64, 0.1, 1e-4);
         rc |= run<double>(n / 2 + 2, n / 2 + 1, n / 2, 3, 64, -5.5, 1e-9, LDL_INTRAPIV_1D);
+        rc |= run_blackbox<double>(n / 2, n / 2 + 1, n / 2 + 2, -5.5, 1e-9, false);
+        rc |= run_blackbox<Complex<double>>(n / 2, n / 2, n / 2 + 1, -5.5, 1e-9, true);
     } catch (const std::exception& e) {
         std::printf("exception: %s\n", e.what());
         rc = 1;

@@ -77,3 +77,18 @@ def test_symmetric_solve_orders_the_graph():
     B = ops.random_rhs(A.n, 2, seed=3)
     X = cliq.SymmetricSolve(A, B, cutoff=64)
     assert residual(A, X, B) <= 1e-11
+
+
+def test_hermitian_solve_black_box():
+    """HermitianSolve (solve.hpp:132-140): SymmetricSolve with LDL^H, on an
+    indefinite magnetic Laplacian ordered as a general graph."""
+    dims = (9, 8, 7)
+    A0 = ops.laplacian_3d(*dims, 0.5)
+    vals = A0.values.astype(np.complex128)
+    rows = np.repeat(np.arange(A0.n), np.diff(A0.rowptr))
+    off = A0.colind != rows
+    vals[off] = vals[off] * np.exp(1j * 0.4 * np.sign(A0.colind - rows))[off]
+    A = ops.CSR(A0.n, A0.rowptr, A0.colind, vals)
+    B = ops.random_rhs(A.n, 2, seed=4, complex_=True)
+    X = cliq.HermitianSolve(A, B, cutoff=40)
+    assert residual(A, X, B) <= 1e-11
