@@ -451,6 +451,12 @@ class DistNodalMultiVec:
         return 1 if self.X.ndim == 1 else self.X.shape[1]
 
 
+# DistNodalMatrix (dist_nodal_matrix/decl.hpp:19-50): at one process the
+# reference's [MC,MR] nodal matrix holds the same per-node blocks as the
+# nodal multivector, and Solve takes either (solve.hpp:17-24)
+DistNodalMatrix = DistNodalMultiVec
+
+
 def _solve_array(L, X, nodal):
     lib = _capi.load()
     if _is_torch_cuda(X):

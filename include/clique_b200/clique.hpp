@@ -409,6 +409,28 @@ void Solve(const DistSymmInfo&, const DistSymmFrontTree<F>& L, DistNodalMultiVec
     }
 }
 
+// DistNodalMatrix (dist_nodal_matrix/decl.hpp:19-50): the [MC,MR] nodal
+// matrix of the reference; at one process its nodes hold the same blocks as
+// a DistNodalMultiVec, so it is one, with the reference's constructors
+template <class F>
+class DistNodalMatrix : public DistNodalMultiVec<F> {
+public:
+    DistNodalMatrix() = default;
+    DistNodalMatrix(const DistMap& inverseMap, const DistSymmInfo& info, const DistMultiVec<F>& X)
+        : DistNodalMultiVec<F>(inverseMap, info, X) {}
+    explicit DistNodalMatrix(const DistNodalMultiVec<F>& X) : DistNodalMultiVec<F>(X) {}
+    const DistNodalMatrix<F>& operator=(const DistNodalMultiVec<F>& X) {
+        DistNodalMultiVec<F>::operator=(X);
+        return *this;
+    }
+};
+
+// the DistNodalMatrix overload of Solve (solve.hpp:21-24)
+template <class F>
+void Solve(const DistSymmInfo& info, const DistSymmFrontTree<F>& L, DistNodalMatrix<F>& X) {
+    Solve(info, L, static_cast<DistNodalMultiVec<F>&>(X));
+}
+
 // Black-box solves (solve.hpp:95-140 at one process): nested dissection of
 // A's graph, the front tree, LDL with intra-front pivoting (LDL_INTRAPIV_1D),
 // Pull / Solve / Push; X is overwritten with the solution

@@ -45,8 +45,14 @@ int run(int n1, int n2, int n3, int numRhs, int cutoff, double shift, double tol
     const double t1 = mpi::Time();
     DistNodalMultiVec<F> YNodal;
     YNodal.Pull(inverseMap, info, Y);
-    Solve(info, frontTree, YNodal);
-    YNodal.Push(inverseMap, info, Y);
+    if (numRhs > 3) {   // the DistNodalMatrix overload (solve.hpp:21-24)
+        DistNodalMatrix<F> YMat(YNodal);
+        Solve(info, frontTree, YMat);
+        YMat.Push(inverseMap, info, Y);
+    } else {
+        Solve(info, frontTree, YNodal);
+        YNodal.Push(inverseMap, info, Y);
+    }
     const double t2 = mpi::Time();
     double local, mn, mx, flops;
     frontTree.FactorizationWork(local, mn, mx, flops);
