@@ -34,8 +34,11 @@ from .operators import CSR, from_triplets
 
 __all__ = [
     "CSR", "DistSparseMatrix", "DistMap", "DistSeparatorTree", "DistSymmInfo", "SymmNodeInfo",
-    "NaturalNestedDissection", "DistSymmFrontTree", "LDL", "Solve", "DistNodalMultiVec", "Multiply",
-    "RefinedSolve", "SymmetricSolve", "SymmFrontType", "LogicError", "CliqueError",
+    "NaturalNestedDissection", "NestedDissection", "DistSymmFrontTree", "LDL", "ChangeFrontType", "Solve",
+    "DistNodalMultiVec", "DistNodalMatrix", "Multiply", "RefinedSolve", "SymmetricSolve", "HermitianSolve",
+    "SymmFrontType", "Unfactored", "FrontsAre1d", "BlockFactorization", "SelInvFactorization",
+    "PivotedFactorization", "ConvertTo2d", "ConvertTo1d", "AppendSelInv", "RemoveSelInv", "LogicError",
+    "CliqueError",
 ]
 
 
@@ -55,6 +58,59 @@ class SymmFrontType:
                BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D)
     SUPPORTED = (LDL_1D, LDL_2D, LDL_SELINV_1D, LDL_SELINV_2D, BLOCK_LDL_1D, BLOCK_LDL_2D) + PIVOTED
     BLOCK = (BLOCK_LDL_1D, BLOCK_LDL_2D, BLOCK_LDL_INTRAPIV_1D, BLOCK_LDL_INTRAPIV_2D)
+
+
+# front-type helpers (dist_symm_front_tree/decl.hpp:27-165): the 1D / 2D
+# members of each family are adjacent (1D even, 2D odd)
+def Unfactored(t):
+    return t in (SymmFrontType.SYMM_1D, SymmFrontType.SYMM_2D)
+
+
+def FrontsAre1d(t):
+    return t % 2 == 0
+
+
+def BlockFactorization(t):
+    return t in SymmFrontType.BLOCK
+
+
+def SelInvFactorization(t):
+    T = SymmFrontType
+    return t in (T.LDL_SELINV_1D, T.LDL_SELINV_2D, T.LDL_INTRAPIV_SELINV_1D, T.LDL_INTRAPIV_SELINV_2D)
+
+
+def PivotedFactorization(t):
+    return t in SymmFrontType.PIVOTED
+
+
+def ConvertTo2d(t):
+    if not 0 <= t <= 13:
+        raise LogicError(_capi.CLIQ_ERR_ARG, "Invalid front type")
+    return t | 1
+
+
+def ConvertTo1d(t):
+    if not 0 <= t <= 13:
+        raise LogicError(_capi.CLIQ_ERR_ARG, "Invalid front type")
+    return t & ~1
+
+
+def AppendSelInv(t):
+    T = SymmFrontType
+    m = {T.LDL_1D: T.LDL_SELINV_1D, T.LDL_2D: T.LDL_SELINV_2D,
+         T.LDL_INTRAPIV_1D: T.LDL_INTRAPIV_SELINV_1D, T.LDL_INTRAPIV_2D: T.LDL_INTRAPIV_SELINV_2D}
+    if t not in m:
+        raise LogicError(_capi.CLIQ_ERR_ARG, "Sel-inv does not make sense for this type")
+    return m[t]
+
+
+def RemoveSelInv(t):
+    T = SymmFrontType
+    m = {T.LDL_SELINV_1D: T.LDL_1D, T.LDL_SELINV_2D: T.LDL_2D,
+         T.LDL_INTRAPIV_SELINV_1D: T.LDL_INTRAPIV_1D, T.LDL_INTRAPIV_SELINV_2D: T.LDL_INTRAPIV_2D}
+    if t not in m:
+        raise LogicError(_capi.CLIQ_ERR_ARG, "This type did not involve selective inversion")
+    return m[t]
 
 
 # ---------------------------------------------------------------------------
@@ -377,6 +433,28 @@ def LDL(info, L: DistSymmFrontTree, frontType=SymmFrontType.LDL_2D):
     check(st, "LDL")
     if frontType in SymmFrontType.BLOCK:
         check(_capi.load().cliqgpu_block_ldl(L._h), "LDL (block form)")
+
+
+def ChangeFrontType(L, frontType):
+    """change_front_type.hpp:27-107 at one process: 1D <-> 2D and appending
+    selective inversion (which the reference applies to distributed fronts
+    1 .. only) leave the device fronts as they are and relabel the tree;
+    other changes are a LogicError, as in the reference."""
+    if frontType == L.frontType:
+        return
+    old = L.frontType
+    if frontType == ConvertTo2d(old) or frontType == ConvertTo1d(old):
+        L.frontType = frontType
+        return
+    if SelInvFactorization(frontType):
+        try:
+            ok = ConvertTo2d(frontType) == ConvertTo2d(AppendSelInv(old))
+        except LogicError:
+            ok = False
+        if ok:
+            L.frontType = frontType
+            return
+    raise LogicError(_capi.CLIQ_ERR_ARG, "Unavailable front type change")
 
 
 class DistNodalMultiVec:

@@ -307,6 +307,31 @@ inline bool PivotedFactorization(SymmFrontType t) {
 inline bool BlockFactorization(SymmFrontType t) {
     return t == BLOCK_LDL_1D || t == BLOCK_LDL_2D || t == BLOCK_LDL_INTRAPIV_1D || t == BLOCK_LDL_INTRAPIV_2D;
 }
+inline bool FrontsAre1d(SymmFrontType t) { return ((int)t & 1) == 0; }
+inline bool SelInvFactorization(SymmFrontType t) {
+    return t == LDL_SELINV_1D || t == LDL_SELINV_2D || t == LDL_INTRAPIV_SELINV_1D || t == LDL_INTRAPIV_SELINV_2D;
+}
+// the 1D / 2D members of a family are adjacent in the enum (1D even, 2D odd)
+inline SymmFrontType ConvertTo2d(SymmFrontType t) { return (SymmFrontType)((int)t | 1); }
+inline SymmFrontType ConvertTo1d(SymmFrontType t) { return (SymmFrontType)((int)t & ~1); }
+inline SymmFrontType AppendSelInv(SymmFrontType t) {
+    switch (t) {
+        case LDL_1D: return LDL_SELINV_1D;
+        case LDL_2D: return LDL_SELINV_2D;
+        case LDL_INTRAPIV_1D: return LDL_INTRAPIV_SELINV_1D;
+        case LDL_INTRAPIV_2D: return LDL_INTRAPIV_SELINV_2D;
+        default: throw LogicError("Sel-inv does not make sense for this type");
+    }
+}
+inline SymmFrontType RemoveSelInv(SymmFrontType t) {
+    switch (t) {
+        case LDL_SELINV_1D: return LDL_1D;
+        case LDL_SELINV_2D: return LDL_2D;
+        case LDL_INTRAPIV_SELINV_1D: return LDL_INTRAPIV_1D;
+        case LDL_INTRAPIV_SELINV_2D: return LDL_INTRAPIV_2D;
+        default: throw LogicError("This type did not involve selective inversion");
+    }
+}
 inline bool Provided(SymmFrontType t) {
     return t == LDL_1D || t == LDL_2D || t == LDL_SELINV_1D || t == LDL_SELINV_2D || t == BLOCK_LDL_1D || t == BLOCK_LDL_2D ||
            PivotedFactorization(t);
@@ -407,6 +432,26 @@ void Solve(const DistSymmInfo&, const DistSymmFrontTree<F>& L, DistNodalMultiVec
         Check(cliqgpu_solve(L.Plan(), tmp.data(), n, w, 0, 1), "Solve");
         for (size_t i = 0; i < tmp.size(); ++i) X.data[i] = F(tmp[i]);
     }
+}
+
+// ChangeFrontType (change_front_type.hpp:27-107) at one process: 1D <-> 2D
+// and appending selective inversion (applied by the reference to distributed
+// fronts 1 .. only) leave the device fronts as they are and relabel the tree
+template <class F>
+void ChangeFrontType(DistSymmFrontTree<F>& L, SymmFrontType frontType) {
+    if (frontType == L.frontType) return;
+    const SymmFrontType old = L.frontType;
+    if (frontType == ConvertTo2d(old) || frontType == ConvertTo1d(old)) {
+        L.frontType = frontType;
+        return;
+    }
+    if (SelInvFactorization(frontType) &&
+        (old == LDL_1D || old == LDL_2D || old == LDL_INTRAPIV_1D || old == LDL_INTRAPIV_2D) &&
+        ConvertTo2d(frontType) == ConvertTo2d(AppendSelInv(old))) {
+        L.frontType = frontType;
+        return;
+    }
+    throw LogicError("Unavailable front type change");
 }
 
 // DistNodalMatrix (dist_nodal_matrix/decl.hpp:19-50): the [MC,MR] nodal
