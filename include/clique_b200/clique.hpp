@@ -192,6 +192,21 @@ void Norms(const DistMultiVec<F>& X, std::vector<double>& norms) {
     }
 }
 
+// the one-column norm and Y := alpha X + Y (dist_multi_vec/decl.hpp:75-84)
+template <class F>
+double Norm(const DistMultiVec<F>& x) {
+    std::vector<double> n;
+    Norms(x, n);
+    return n.empty() ? 0.0 : n[0];
+}
+
+template <class F>
+void Axpy(F alpha, const DistMultiVec<F>& X, DistMultiVec<F>& Y) {
+    if (X.Height() != Y.Height() || X.Width() != Y.Width()) throw LogicError("X and Y must be the same size");
+    for (int j = 0; j < X.Width(); ++j)
+        for (int i = 0; i < X.Height(); ++i) Y.SetLocal(i, j, Y.GetLocal(i, j) + alpha * X.GetLocal(i, j));
+}
+
 // Y := alpha A X + beta Y (multiply.hpp:28-166 at P=1), computed on the
 // device by cliqgpu_sparse_multiply (host buffers staged through device
 // memory; FP64 arithmetic for every scalar type)
