@@ -118,3 +118,33 @@ def test_graph_nd_dense_block_is_a_leaf():
     map_, _, info = cliq.NestedDissection(A, 16)
     check_tree(A, info, map_, 16)
     assert info.num_nodes == 1 and info.localNodes[0].size == n
+
+
+def _pattern(n, edges):
+    e = np.asarray(edges, np.int64).reshape(-1, 2)
+    r = np.concatenate([e[:, 0], e[:, 1], np.arange(n)])
+    c = np.concatenate([e[:, 1], e[:, 0], np.arange(n)])
+    v = np.concatenate([-np.ones(2 * len(e)), np.full(n, 10.0)])
+    return ops.from_triplets(n, r, c, v)
+
+
+def _shapes(rng):
+    n = 700
+    yield "star", _pattern(n, [(0, i) for i in range(1, n)])
+    yield "path", _pattern(n, [(i, i + 1) for i in range(n - 1)])
+    yield "tree", _pattern(n, [(i, int(rng.integers(0, i))) for i in range(1, n)])
+    a, b = 40, 30
+    yield "bipartite", _pattern(a + b, [(i, a + j) for i in range(a) for j in range(b)])
+    yield "random", _pattern(n, rng.integers(0, n, size=(3 * n, 2)))
+    g1 = [(i, i + 1) for i in range(299)]
+    g2 = [(300 + i, 300 + int(rng.integers(0, i + 1))) for i in range(1, 300)]
+    yield "union", _pattern(700, g1 + g2)   # a path, a tree and 100 isolated vertices
+
+
+@pytest.mark.parametrize("seps", [1, 3])
+def test_graph_nd_shapes(seps):
+    rng = np.random.default_rng(7)
+    for name, A in _shapes(rng):
+        for cutoff in (1, 8, 64):
+            map_, _, info = cliq.NestedDissection(A, cutoff, numSeqSeps=seps)
+            check_tree(A, info, map_, cutoff)
