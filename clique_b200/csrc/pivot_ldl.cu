@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(kLowerRows) bk_lower_kernel(const FrontDev* __
     using X = V<T, C>;
     using W = DV<C>;
     extern __shared__ __align__(16) unsigned char bk_smem[];
-    X* s_l = reinterpret_cast<X*>(bk_smem);   // L11 of the panel, kMaxPanel x kMaxPanel, column-major
+    X* s_l = reinterpret_cast<X*>(bk_smem);   // L11 of the panel, kMaxPanel x kMaxPanel, column-major, then the rows' y
     __shared__ X s_d[kMaxPanel], s_e[kMaxPanel];
     const int fi = blockIdx.x / chunks, ch = blockIdx.x % chunks;
     const int s = fl[fi];
@@ -361,11 +361,14 @@ __global__ void __launch_bounds__(kLowerRows) bk_lower_kernel(const FrontDev* __
     const int i = f.n + ch * kLowerRows + threadIdx.x;
     if (i >= f.m) return;
     const int64_t row = base + i;
-    // y(q) = a(q) - sum_{p<q} y(p) op(L11(q, p)), kept in place
-    for (int q = 0; q < kb; ++q) {
-        X a = ldv<T, C>(L, row + (int64_t)(j0 + q) * f.m);
-        for (int p = 0; p < q; ++p) a -= ldv<T, C>(L, row + (int64_t)(j0 + p) * f.m) * opc<CJ>(s_l[q + p * kMaxPanel]);
-        stv<T, C>(L, row + (int64_t)(j0 + q) * f.m, a);
+    // this thread's row of the panel in shared memory (column q at q * kLowerRows + tid): all loads first
+    X* y = s_l + kMaxPanel * kMaxPanel + threadIdx.x;
+    for (int q = 0; q < kb; ++q) y[q * kLowerRows] = ldv<T, C>(L, row + (int64_t)(j0 + q) * f.m);
+    // y(q) = a(q) - sum_{p<q} y(p) op(L11(q, p))
+    for (int q = 1; q < kb; ++q) {
+        X a = y[q * kLowerRows];
+        for (int p = 0; p < q; ++p) a -= y[p * kLowerRows] * opc<CJ>(s_l[q + p * kMaxPanel]);
+        y[q * kLowerRows] = a;
     }
     // l = y D^{-1}
     for (int q = 0; q < kb; ++q) {
@@ -373,13 +376,13 @@ __global__ void __launch_bounds__(kLowerRows) bk_lower_kernel(const FrontDev* __
         if (!is_zero(s_e[q])) {
             const X d11 = s_d[q], d22 = s_d[q + 1], d21 = s_e[q];
             const X det = d11 * d22 - d21 * opc<CJ>(d21);
-            const X y0 = ldv<T, C>(L, e0), y1 = ldv<T, C>(L, e0 + f.m);
+            const X y0 = y[q * kLowerRows], y1 = y[(q + 1) * kLowerRows];
             stv<T, C>(L, e0, (y0 * d22 - y1 * d21) / det);
             stv<T, C>(L, e0 + f.m, (y1 * d11 - y0 * opc<CJ>(d21)) / det);
             ++q;
         } else {
             const X d = s_d[q];
-            stv<T, C>(L, e0, is_zero(d) ? X{} : ldv<T, C>(L, e0) / d);
+            stv<T, C>(L, e0, is_zero(d) ? X{} : y[q * kLowerRows] / d);
         }
     }
 }
@@ -643,7 +646,7 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
     T* p1 = reinterpret_cast<T*>(P.pool[1]);
     T* cvec = reinterpret_cast<T*>(P.pvec);
     T* vvec = cvec + (C ? 2 : 1) * P.n;
-    const size_t smem_lower = sizeof(V<T, C>) * kMaxPanel * kMaxPanel;
+    const size_t smem_lower = sizeof(V<T, C>) * kMaxPanel * (kMaxPanel + kLowerRows);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(bk_lower_kernel<T, C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_lower);
