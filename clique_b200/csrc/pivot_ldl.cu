@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
                 kstep = 2;
             }
         }
-        if (zero && tid == 0) atomicMin(&status[0], f.off + k + 1);
+        if (zero && tid == 0) atomicMin(&status[0], pivg[f.off + k] + 1);   // the row's ND index (no interchange here)
         // symmetric interchange of a = kk and b = kp over the whole front
         const int kk = k + kstep - 1;
         if (kp != kk) {

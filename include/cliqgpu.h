@@ -145,8 +145,9 @@ int cliqgpu_factor(cliqgpu_plan plan, int64_t* zero_pivot);
  * 2 x 2 blocks), the columns of A21 permuted with it, and the Schur
  * complement passed up as in cliqgpu_factor.  The solves apply P around each
  * front and solve with the 2 x 2 blocks; their inputs and outputs keep the
- * natural / ND order.  *zero_pivot: -1, or the ND position of the first pivot
- * whose whole remaining column is zero (then CLIQ_ERR_ZERO_PIVOT).
+ * natural / ND order.  *zero_pivot: -1, or the smallest ND index of a pivot
+ * row whose whole remaining column within its front's pivot rows is zero
+ * (then CLIQ_ERR_ZERO_PIVOT).
  * Replaces cliq::LDL(info, L, LDL_INTRAPIV_1D/LDL_INTRAPIV_2D): LocalLDL's
  * intraPiv branch, include/clique/numeric/ldl/local.hpp:31-33,106-111,
  * FrontLDLIntraPiv ldl/local_front.hpp:74-94, and its solves

@@ -92,3 +92,20 @@ def test_hermitian_solve_black_box():
     B = ops.random_rhs(A.n, 2, seed=4, complex_=True)
     X = cliq.HermitianSolve(A, B, cutoff=40)
     assert residual(A, X, B) <= 1e-11
+
+
+def test_intrapiv_reports_a_singular_row():
+    """A vertex with no couplings and a zero diagonal: its pivot column is
+    zero in any order, and the pivoted factorization reports its ND index."""
+    A0 = knn_graph(500, 6, seed=9, isolated=1)
+    vals = A0.values.copy()
+    v = A0.n - 1
+    rows = np.repeat(np.arange(A0.n), np.diff(A0.rowptr))
+    vals[(rows == v) & (A0.colind == v)] = 0.0
+    A = ops.CSR(A0.n, A0.rowptr, A0.colind, vals)
+    map_, sep, info = cliq.NestedDissection(A, 32)
+    L = cliq.DistSymmFrontTree(A, map_, sep, info, precision="double")
+    with pytest.raises(cliq.CliqueError) as e:
+        cliq.LDL(info, L, cliq.SymmFrontType.LDL_INTRAPIV_2D)
+    assert e.value.status == 3
+    assert L.zero_pivot == int(np.asarray(map_.array)[v])
