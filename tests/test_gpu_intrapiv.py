@@ -254,3 +254,20 @@ def test_intrapiv_edge_grids(oracle, dims, cutoff):
     F = oracle.Fronts(S, A.values)
     assert F.ldl(96, pivot=True) == 0
     assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+
+
+@pytest.mark.parametrize("front", ["LDL_2D", "LDL_INTRAPIV_2D"])
+def test_many_right_hand_sides(oracle, front):
+    """A SolveRange-sized solve (tests/SolveRange.cpp solves 100-1000
+    right-hand sides): 130 columns, several 16-column chunks and a ragged
+    tail, against the oracle's solve."""
+    dims, cutoff = (14, 12, 10), 80
+    A, conj = _indefinite("complex", dims)
+    _, info, L = _tree(A, dims, cutoff, "double", conj, front_type=getattr(cliq.SymmFrontType, front))
+    B = ops.random_rhs(A.n, 130, seed=13, complex_=True)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=True, conjugate=conj)
+    assert F.ldl(96, pivot=front != "LDL_2D") == 0
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+    assert residual(A, X, B) <= 1e-12
