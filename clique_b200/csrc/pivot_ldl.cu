@@ -38,6 +38,9 @@
 #include <climits>
 #include <cmath>
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 #ifndef TRY
 #define TRY(x)                          \
     do {                                \
@@ -54,6 +57,7 @@ constexpr int kMaxPanel = kNb + 1;
 // threads of a panel CTA: as many loads in flight as the registers allow
 // (FP32: 51-62 registers a thread, 1024 threads; FP64: up to 126, 512)
 template <class T> constexpr int panel_threads() { return sizeof(T) == 4 ? 1024 : 512; }
+constexpr int kClusterCTAs = 8;         // CTAs sharing a front's panel on the top levels
 constexpr int kLowerRows = 128;         // rows of A21 per bk_lower_kernel CTA
 constexpr int kUpdThreads = 256;
 constexpr int kUpdTile = 64;
@@ -84,23 +88,52 @@ __device__ __forceinline__ X bval(int p, X d, X e, X em1, bool first, Get Lrow) 
 // sum_p L(i, j0 + p) w[p] over the panel's factored columns (row element
 // offset e0 of column j0, column stride m): eight loads in flight, two
 // partial sums
-template <class T, class X>
+// (L1: false reads from L2, for entries other CTAs of the cluster wrote)
+template <bool L1, class T, class X>
 __device__ __forceinline__ X panel_dot(const T* L, int64_t e0, int m, int np, const X* w) {
     constexpr bool C = !std::is_same<X, T>::value;
+    auto ld = [&](int64_t e) -> X {
+        if constexpr (L1) return ldv<T, C>(L, e);
+        else return ldv_cg<T, C>(L, e);
+    };
     X s0{}, s1{};
     int p = 0;
     for (; p + 8 <= np; p += 8) {
         X l[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) l[q] = ldv<T, C>(L, e0 + (int64_t)(p + q) * m);
+        for (int q = 0; q < 8; ++q) l[q] = ld(e0 + (int64_t)(p + q) * m);
 #pragma unroll
         for (int q = 0; q < 8; q += 2) {
             mac(s0, l[q], w[p + q]);
             mac(s1, l[q + 1], w[p + q + 1]);
         }
     }
-    for (; p < np; ++p) mac(s0, ldv<T, C>(L, e0 + (int64_t)p * m), w[p]);
+    for (; p < np; ++p) mac(s0, ld(e0 + (int64_t)p * m), w[p]);
     return s0 + s1;
+}
+
+// the CTAs' block-argmax results combined across a cluster (G > 1): each
+// CTA's thread 0 writes its partial into the first CTA's slots, and after the
+// cluster barrier every thread reduces the G slots in the same order
+template <int G, class T>
+__device__ __forceinline__ void cluster_argmax(T& v, int& idx, T* slot_v, int* slot_i) {
+    if constexpr (G > 1) {
+        cg::cluster_group cl = cg::this_cluster();
+        if (threadIdx.x == 0) {
+            cl.map_shared_rank(slot_v, 0)[cl.block_rank()] = v;
+            cl.map_shared_rank(slot_i, 0)[cl.block_rank()] = idx;
+        }
+        cl.sync();
+        const T* rv = cl.map_shared_rank(slot_v, 0);
+        const int* ri = cl.map_shared_rank(slot_i, 0);
+        v = rv[0];
+        idx = ri[0];
+        for (int q = 1; q < G; ++q) {
+            const T ov = rv[q];
+            const int oi = ri[q];
+            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+        }
+    }
 }
 
 // block-wide max with the smallest index on ties, one barrier: every warp
@@ -128,9 +161,16 @@ __device__ __forceinline__ void block_argmax(T& v, int& idx, T* sv, int* si) {
 }
 
 // ---------------------------------------------------------------------------
-// one panel of Bunch-Kaufman pivots per front
+// one panel of Bunch-Kaufman pivots per front: one CTA (G = 1), or a
+// cluster of G CTAs sharing the front's rows (the top levels, whose few
+// large fronts would leave most SMs idle).  With G > 1 every CTA takes the
+// rows k + rank nt + tid + q G nt, the argmax partials meet in the first
+// CTA's shared memory, every CTA reaches the same pivot decisions from the
+// same combined values (so all pass the same cluster barriers), the entries
+// other CTAs wrote are read from L2 (ld.global.cg), and the first CTA's
+// thread 0 does the single-entry work
 // ---------------------------------------------------------------------------
-template <class T, bool C, bool CJ>
+template <class T, bool C, bool CJ, int G = 1>
 __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
                                                                  T* __restrict__ L, double* __restrict__ D, double* __restrict__ E,
                                                                  int32_t* __restrict__ pivg, T* __restrict__ cvec, T* __restrict__ vvec,
@@ -143,19 +183,40 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
     __shared__ T s_rv[32], s_rv2[32];   // per-warp partials of the two reductions of a column step
     __shared__ int s_ri[32], s_ri2[32];
     __shared__ X s_akk, s_ar;
-    const int s = fl[blockIdx.x];
+    __shared__ T s_slot_v[G], s_slot2_v[G];   // G > 1: the CTAs' argmax partials (in the first CTA)
+    __shared__ int s_slot_i[G], s_slot2_i[G];
+    int rank = 0;
+    if constexpr (G > 1) rank = (int)cg::this_cluster().block_rank();
+    const int s = fl[blockIdx.x / G];
     const FrontDev f = F[s];
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int t0 = rank * nt + tid, ntot = G * nt;
+    const bool lead = tid == 0 && rank == 0;
     const int n = f.n, m = f.m;
     const int j0 = state[2 * s + 1];
-    if (j0 >= n) {
-        if (tid == 0) state[2 * s] = j0;
+    if (j0 >= n) {   // (the same for every CTA of a cluster)
+        if (lead) state[2 * s] = j0;
         return;
     }
     const int64_t base = f.L;
     auto at = [&](int i, int j) -> int64_t { return base + i + (int64_t)j * m; };
+    auto ld = [&](const T* p, int64_t e) -> X {
+        if constexpr (G > 1) return ldv_cg<T, C>(p, e);
+        else return ldv<T, C>(p, e);
+    };
+    auto sync = [&]() {
+        if constexpr (G > 1) cg::this_cluster().sync();
+        else __syncthreads();
+    };
+    auto bcast = [&](X* p, X v) {   // a value every CTA needs, into every CTA's copy
+        if constexpr (G > 1) {
+            for (int q = 0; q < G; ++q) *cg::this_cluster().map_shared_rank(p, q) = v;
+        } else {
+            *p = v;
+        }
+    };
     if (j0 == 0)
-        for (int i = tid; i < n; i += nt) pivg[f.off + i] = f.off + i;
+        for (int i = t0; i < n; i += ntot) pivg[f.off + i] = f.off + i;
     const int jend = min(n, j0 + kNb);
     int k = j0;
     while (k < jend) {
@@ -164,17 +225,17 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
         if (tid < np) {
             const int p = j0 + tid;
             s_w[tid] = bval<CJ>(p, s_d[tid], s_e[tid], tid > 0 ? s_e[tid - 1] : X{}, tid > 0,
-                                [&](int q) { return ldv<T, C>(L, at(k, q)); });
+                                [&](int q) { return ld(L, at(k, q)); });
         }
         __syncthreads();
         // candidate column k with the panel's pending update; column maximum below the diagonal
         T best = T(-1);
         int bi = INT_MAX;
-        for (int i = k + tid; i < n; i += nt) {
-            X a = ldv<T, C>(L, at(i, k)) - panel_dot(L, at(i, j0), m, np, s_w);
+        for (int i = k + t0; i < n; i += ntot) {
+            X a = ld(L, at(i, k)) - panel_dot<G == 1>(L, at(i, j0), m, np, s_w);
             if (i == k) {
                 if constexpr (CJ) a = realpart(a);
-                s_akk = a;
+                bcast(&s_akk, a);
             } else {
                 const T g = mag1(a);
                 if (g > best) { best = g; bi = i; }
@@ -182,6 +243,7 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
             stv<T, C>(cvec, f.off + i, a);
         }
         block_argmax(best, bi, s_rv, s_ri);   // (its barrier publishes s_akk)
+        cluster_argmax<G>(best, bi, s_slot_v, s_slot_i);
         const T colmax = best > T(0) ? best : T(0);
         const int imax = bi == INT_MAX ? k : bi;
         const T absakk = mag1(s_akk);
@@ -195,31 +257,31 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
             // candidate column imax (the full matrix's column, rows k .. n-1)
             if (tid < np) {
                 const int p = j0 + tid;
-                s_lr[tid] = ldv<T, C>(L, at(imax, p));
+                s_lr[tid] = ld(L, at(imax, p));
                 s_wi[tid] = bval<CJ>(p, s_d[tid], s_e[tid], tid > 0 ? s_e[tid - 1] : X{}, tid > 0,
-                                     [&](int q) { return ldv<T, C>(L, at(imax, q)); });
+                                     [&](int q) { return ld(L, at(imax, q)); });
             }
             __syncthreads();
             T rbest = T(-1);
             int rbi = INT_MAX;
             // (the rows of vvec follow the same thread mapping as those of cvec)
-            for (int j = k + tid; j < n; j += nt) {
+            for (int j = k + t0; j < n; j += ntot) {
                 X a;
                 if (j < imax) {
-                    a = ldv<T, C>(L, at(imax, j));
+                    a = ld(L, at(imax, j));
                     for (int p = 0; p < np; ++p) {
                         const X b = bval<CJ>(j0 + p, s_d[p], s_e[p], p > 0 ? s_e[p - 1] : X{}, p > 0,
-                                             [&](int q) { return ldv<T, C>(L, at(j, q)); });
+                                             [&](int q) { return ld(L, at(j, q)); });
                         a -= s_lr[p] * b;
                     }
                     a = opc<CJ>(a);
                 } else if (j == imax) {
-                    a = ldv<T, C>(L, at(imax, imax));
+                    a = ld(L, at(imax, imax));
                     for (int p = 0; p < np; ++p) a -= s_lr[p] * s_wi[p];
                     if constexpr (CJ) a = realpart(a);
-                    s_ar = a;
+                    bcast(&s_ar, a);
                 } else {
-                    a = ldv<T, C>(L, at(j, imax)) - panel_dot(L, at(j, j0), m, np, s_wi);
+                    a = ld(L, at(j, imax)) - panel_dot<G == 1>(L, at(j, j0), m, np, s_wi);
                 }
                 stv<T, C>(vvec, f.off + j, a);
                 if (j != imax) {
@@ -228,6 +290,7 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
                 }
             }
             block_argmax(rbest, rbi, s_rv2, s_ri2);   // (publishes s_ar)
+            cluster_argmax<G>(rbest, rbi, s_slot2_v, s_slot2_i);
             const T rowmax = rbest > T(0) ? rbest : T(0);
             if (absakk >= (T)kAlpha * colmax * (colmax / rowmax)) {
                 kp = k;
@@ -239,39 +302,39 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
                 kstep = 2;
             }
         }
-        if (zero && tid == 0) atomicMin(&status[0], pivg[f.off + k] + 1);   // the row's ND index (no interchange here)
+        if (zero && lead) atomicMin(&status[0], __ldcg(pivg + f.off + k) + 1);   // the row's ND index (no interchange here)
         // symmetric interchange of a = kk and b = kp over the whole front
         const int kk = k + kstep - 1;
         if (kp != kk) {
             const int a = kk, b = kp;
-            for (int j = tid; j < a; j += nt) {   // factored columns: rows a and b
-                const X t = ldv<T, C>(L, at(a, j));
-                stv<T, C>(L, at(a, j), ldv<T, C>(L, at(b, j)));
+            for (int j = t0; j < a; j += ntot) {   // factored columns: rows a and b
+                const X t = ld(L, at(a, j));
+                stv<T, C>(L, at(a, j), ld(L, at(b, j)));
                 stv<T, C>(L, at(b, j), t);
             }
-            for (int i = a + 1 + tid; i < b; i += nt) {   // column a between the two, row b between the two
-                const X t = ldv<T, C>(L, at(i, a));
-                stv<T, C>(L, at(i, a), opc<CJ>(ldv<T, C>(L, at(b, i))));
+            for (int i = a + 1 + t0; i < b; i += ntot) {   // column a between the two, row b between the two
+                const X t = ld(L, at(i, a));
+                stv<T, C>(L, at(i, a), opc<CJ>(ld(L, at(b, i))));
                 stv<T, C>(L, at(b, i), opc<CJ>(t));
             }
-            for (int i = b + 1 + tid; i < m; i += nt) {   // rows below b (A21 included): columns a and b
-                const X t = ldv<T, C>(L, at(i, a));
-                stv<T, C>(L, at(i, a), ldv<T, C>(L, at(i, b)));
+            for (int i = b + 1 + t0; i < m; i += ntot) {   // rows below b (A21 included): columns a and b
+                const X t = ld(L, at(i, a));
+                stv<T, C>(L, at(i, a), ld(L, at(i, b)));
                 stv<T, C>(L, at(i, b), t);
             }
-            if (tid == 0) {
-                const X t = ldv<T, C>(L, at(a, a));
-                stv<T, C>(L, at(a, a), ldv<T, C>(L, at(b, b)));
+            if (lead) {
+                const X t = ld(L, at(a, a));
+                stv<T, C>(L, at(a, a), ld(L, at(b, b)));
                 stv<T, C>(L, at(b, b), t);
-                stv<T, C>(L, at(b, a), opc<CJ>(ldv<T, C>(L, at(b, a))));
-                const int32_t g = pivg[f.off + a];
-                pivg[f.off + a] = pivg[f.off + b];
+                stv<T, C>(L, at(b, a), opc<CJ>(ld(L, at(b, a))));
+                const int32_t g = __ldcg(pivg + f.off + a);
+                pivg[f.off + a] = __ldcg(pivg + f.off + b);
                 pivg[f.off + b] = g;
-                const X c0 = ldv<T, C>(cvec, f.off + a);
-                stv<T, C>(cvec, f.off + a, ldv<T, C>(cvec, f.off + b));
+                const X c0 = ld(cvec, f.off + a);
+                stv<T, C>(cvec, f.off + a, ld(cvec, f.off + b));
                 stv<T, C>(cvec, f.off + b, c0);
-                const X v0 = ldv<T, C>(vvec, f.off + a);
-                stv<T, C>(vvec, f.off + a, ldv<T, C>(vvec, f.off + b));
+                const X v0 = ld(vvec, f.off + a);
+                stv<T, C>(vvec, f.off + a, ld(vvec, f.off + b));
                 stv<T, C>(vvec, f.off + b, v0);
             }
         }
@@ -280,34 +343,36 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
         // rows k + tid + q nt of both candidate columns), and the pivot is in
         // shared memory
         const bool plain = kstep == 1 && kp == k;
-        if (!plain) __syncthreads();
+        if (!plain) sync();
         // pivot columns of L (pivot rows), D and E
         if (kstep == 1) {
             const T* col = use_v ? vvec : cvec;
-            X d = plain ? s_akk : ldv<T, C>(col, f.off + k);
+            X d = plain ? s_akk : ld(col, f.off + k);
             if constexpr (CJ) d = realpart(d);
-            for (int i = k + tid; i < n; i += nt) {
+            for (int i = k + t0; i < n; i += ntot) {
                 if (i == k) continue;
-                const X c = ldv<T, C>(col, f.off + i);
+                const X c = ld(col, f.off + i);
                 stv<T, C>(L, at(i, k), is_zero(d) ? X{} : c / d);
             }
-            if (tid == 0) {
+            if (lead) {
                 stv<T, C>(L, at(k, k), vone<X>());
                 reinterpret_cast<W*>(D)[f.off + k] = conv<W>(d);
                 reinterpret_cast<W*>(E)[f.off + k] = W{};
+            }
+            if (tid == 0) {
                 s_d[np] = d;
                 s_e[np] = X{};
             }
         } else {
-            X d11 = ldv<T, C>(cvec, f.off + k), d21 = ldv<T, C>(cvec, f.off + k + 1), d22 = ldv<T, C>(vvec, f.off + k + 1);
+            X d11 = ld(cvec, f.off + k), d21 = ld(cvec, f.off + k + 1), d22 = ld(vvec, f.off + k + 1);
             if constexpr (CJ) { d11 = realpart(d11); d22 = realpart(d22); }
             const X det = d11 * d22 - d21 * opc<CJ>(d21);
-            for (int i = k + 2 + tid; i < n; i += nt) {
-                const X c = ldv<T, C>(cvec, f.off + i), v = ldv<T, C>(vvec, f.off + i);
+            for (int i = k + 2 + t0; i < n; i += ntot) {
+                const X c = ld(cvec, f.off + i), v = ld(vvec, f.off + i);
                 stv<T, C>(L, at(i, k), (c * d22 - v * d21) / det);
                 stv<T, C>(L, at(i, k + 1), (v * d11 - c * opc<CJ>(d21)) / det);
             }
-            if (tid == 0) {
+            if (lead) {
                 stv<T, C>(L, at(k, k), vone<X>());
                 stv<T, C>(L, at(k + 1, k + 1), vone<X>());
                 stv<T, C>(L, at(k + 1, k), X{});
@@ -315,16 +380,18 @@ __global__ void __launch_bounds__(panel_threads<T>()) bk_panel_kernel(const Fron
                 reinterpret_cast<W*>(D)[f.off + k + 1] = conv<W>(d22);
                 reinterpret_cast<W*>(E)[f.off + k] = conv<W>(d21);
                 reinterpret_cast<W*>(E)[f.off + k + 1] = W{};
+            }
+            if (tid == 0) {
                 s_d[np] = d11;
                 s_e[np] = d21;
                 s_d[np + 1] = d22;
                 s_e[np + 1] = X{};
             }
         }
-        __syncthreads();
+        sync();
         k += kstep;
     }
-    if (tid == 0) {
+    if (lead) {
         state[2 * s] = j0;
         state[2 * s + 1] = k;
     }
@@ -659,9 +726,31 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
         return Nt * Mt - Nt * (Nt - 1) / 2;
     };
     const int steps = (max_n + kNb - 1) / kNb;
+    // the top levels (a few large fronts): each front's panels on a cluster
+    // of kClusterCTAs CTAs; a refused cluster launch falls back to one CTA a front
+    const bool clustered = (int64_t)lv.nfronts * kClusterCTAs <= 148 && max_n >= 512;
     for (int step = 0; step < steps; ++step) {
-        bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, panel_threads<T>(), 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec, vvec,
-                                                                                   P.pstate, P.status);
+        bool done = false;
+        if (clustered) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)(lv.nfronts * kClusterCTAs));
+            cfg.blockDim = dim3(panel_threads<T>());
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = st;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = kClusterCTAs;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            done = cudaLaunchKernelEx(&cfg, bk_panel_kernel<T, C, CJ, kClusterCTAs>, (const FrontDev*)P.fronts, fl, L, P.D, P.E,
+                                      P.pivg, cvec, vvec, P.pstate, P.status) == cudaSuccess;
+            if (!done) cudaGetLastError();
+        }
+        if (!done)
+            bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, panel_threads<T>(), 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec,
+                                                                                       vvec, P.pstate, P.status);
         if (max_u > 0)
             bk_lower_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * chunks), kLowerRows, smem_lower, st>>>(
                 P.fronts, fl, chunks, L, P.D, P.E, P.pstate);

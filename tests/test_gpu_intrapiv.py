@@ -271,3 +271,31 @@ def test_many_right_hand_sides(oracle, front):
     assert F.ldl(96, pivot=front != "LDL_2D") == 0
     assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
     assert residual(A, X, B) <= 1e-12
+
+
+@pytest.mark.parametrize("kind", ["real", "complex"])
+def test_intrapiv_clustered_panels(oracle, kind):
+    """A root front of 528 pivots (26 x 24 x 22 grid, cutoff 256): the top
+    levels' panels run on clusters of CTAs; pivots and fronts as the
+    oracle's, and the oracle's solution."""
+    dims, cutoff = (26, 24, 22), 256
+    A, conj = _indefinite(kind, dims)
+    cplx = kind != "real"
+    _, info, L = _tree(A, dims, cutoff, "double", conj)
+    S = oracle.Symbolic(*dims, A.rowptr, A.colind, cutoff=cutoff)
+    F = oracle.Fronts(S, A.values, is_complex=cplx, conjugate=conj)
+    assert F.ldl(96, pivot=True) == 0
+    assert max(L.front(s)[0].shape[1] for s in range(S.num_nodes)) >= 512
+    for s in range(S.num_nodes):
+        Lo, do = F.front(s)
+        so, po = F.pivots(s)
+        Lg, dg = L.front(s)
+        sg, pg = L.front_pivots(s)
+        assert np.array_equal(pg, po), s
+        scale = max(np.abs(Lo).max(), np.abs(do).max(), 1e-300)
+        assert np.abs(Lg - Lo).max() <= 1e-10 * scale, s
+        assert np.abs(dg - do).max() <= 1e-10 * scale, s
+        assert np.abs(sg - so).max() <= 1e-10 * scale, s
+    B = ops.random_rhs(A.n, 3, seed=5, complex_=cplx)
+    X = cliq.Solve(info, L, B.copy(order="F"))
+    assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
