@@ -11,7 +11,8 @@
 //
 // GPU form, per tree level after its extend-add and assembly, right-looking
 // in panels of 64 (65 when a 2 x 2 block closes the panel) columns:
-//   bk_panel_kernel   one CTA per front (1024 threads, 512 for FP64): the panel's pivots one column at a
+//   bk_panel_kernel   one CTA per front (1024 threads, 512 for FP64; on the
+//                     top levels a cluster of 8 CTAs per front): the panel's pivots one column at a
 //                     time.  The candidate columns are formed with the
 //                     panel's pending update (A(:,k) - L(:,panel) B(k,panel)^T,
 //                     B = D op(L)^T built from L and D on the fly), the pivot
