@@ -289,7 +289,10 @@ int cliqgpu_autotune(cliqgpu_plan plan, int32_t reps, double* report);
 
 /* Copy front s back to the host: L (m x n, column-major, in the plan's
  * storage precision widened to FP64) and D (n entries, FP64).
- * Either pointer may be NULL.  dims[0..1] receives m, n.
+ * Either pointer may be NULL.  dims[0..1] receives m, n.  After
+ * cliqgpu_factor_intrapiv the pivot rows of L are in the front's pivoted
+ * order and D is the diagonal of the block-diagonal D; the order and the
+ * 2 x 2 blocks' off-diagonals come from cliqgpu_get_front_pivots.
  * Replaces reading L.localFronts[s].frontL / .diag
  * (dist_symm_front_tree/decl.hpp:174-184). */
 int cliqgpu_get_front(cliqgpu_plan plan, int32_t s, double* L, double* D, int32_t dims[2]);
