@@ -40,6 +40,9 @@ struct Cfg {
     static constexpr int EB = C ? 16 : 8;         // bytes per element
     static constexpr int SLICE = BK * LD;         // elements per operand per stage
     static constexpr size_t smem() { return (size_t)kStages * (2 * SLICE + BK) * EB; }
+    // pivoted fronts: also the B rows on either side of the slice and the
+    // 2 x 2 blocks' D(k + 1, k) from k0 - 1 to k0 + BK
+    static constexpr size_t smem_pv() { return (size_t)kStages * (2 * SLICE + BK + 2 * kBM + BK + 2) * EB; }
 };
 
 __device__ __forceinline__ uint32_t sptr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -64,17 +67,24 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-template <bool C, bool CJ>
+// PV: the fronts were factored with intra-front pivoting; D has 2 x 2 blocks
+// (E holds D(k + 1, k) of a block starting at k, D(k, k + 1) = op of it), so
+// D op(B) mixes the two rows of a block -- the neighbour across a slice edge
+// comes from the staged halo rows
+template <bool C, bool CJ, bool PV = false>
 __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
                                                                const int32_t* __restrict__ bmap, double* __restrict__ L,
                                                                double* __restrict__ pool0, double* __restrict__ pool1,
-                                                               const double* __restrict__ D) {
+                                                               const double* __restrict__ D, const double* __restrict__ E = nullptr) {
     using X = V<double, C>;
     using G = Cfg<C>;
     constexpr int BK = G::BK, LD = G::LD;
+    static_assert(kThreads == 2 * kBM, "one halo element per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     X* sOp = reinterpret_cast<X*>(smem_raw);                       // [stage][A slice | B slice]
     X* sDv = sOp + (size_t)kStages * 2 * G::SLICE;                 // [stage][BK] pivots
+    X* sBh = sDv + (size_t)kStages * BK;                           // PV: [stage][2][kBM] B rows k0 - 1, k0 + BK
+    X* sEv = sBh + (size_t)kStages * 2 * kBM;                      // PV: [stage][BK + 2] D(k + 1, k), k0 - 1 .. k0 + BK
 
     const int64_t bid = blockIdx.x;
     const int lo = bmap[bid];
@@ -89,6 +99,7 @@ __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* _
     double* Cbase = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
     const X* Lx = reinterpret_cast<const X*>(L);
     const X* Dx = reinterpret_cast<const X*>(D);
+    const X* Ex = reinterpret_cast<const X*>(E);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tg = lane & 3;
@@ -113,6 +124,18 @@ __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* _
         if (tid < BK) {
             const bool v = k0 + tid < pr.K;
             cp_elem<G::EB>(sDv + slot * BK + tid, v ? Dx + pr.d + k0 + tid : Dx, v);
+        }
+        if constexpr (PV) {
+            X* sh = sBh + (size_t)slot * 2 * kBM;
+            const int h = tid / kBM, r = tid % kBM;
+            const int kh = h == 0 ? k0 - 1 : k0 + BK;
+            const bool vh = kh >= 0 && kh < pr.K && j0 + r < pr.N;
+            cp_elem<G::EB>(sh + h * kBM + r, vh ? Lx + pr.B + (j0 + r) + (int64_t)kh * pr.lda : Lx, vh);
+            if (tid < BK + 2) {
+                const int ke = k0 - 1 + tid;
+                const bool ve = ke >= 0 && ke < pr.K;
+                cp_elem<G::EB>(sEv + (size_t)slot * (BK + 2) + tid, ve ? Ex + pr.d + ke : Ex, ve);
+            }
         }
     };
 
@@ -148,8 +171,22 @@ __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* _
             X af[4], bf[4];
 #pragma unroll
             for (int a = 0; a < 4; ++a) af[a] = sA[k * LD + wr + 8 * a + g];
+            if constexpr (PV) {
+                const X* se = sEv + (size_t)slot * (BK + 2);
+                const X* sh = sBh + (size_t)slot * 2 * kBM;
+                const X ek = se[k + 1], ekm1 = se[k];   // D(k+1, k) of a block at k; D(k, k-1) of one at k - 1
 #pragma unroll
-            for (int b = 0; b < 4; ++b) bf[b] = dk * opc<CJ>(sB[k * LD + wc + 8 * b + g]);
+                for (int b = 0; b < 4; ++b) {
+                    const int col = wc + 8 * b + g;
+                    X v = dk * opc<CJ>(sB[k * LD + col]);
+                    if (!is_zero(ek)) v += opc<CJ>(ek) * opc<CJ>(k + 1 < BK ? sB[(k + 1) * LD + col] : sh[kBM + col]);
+                    if (!is_zero(ekm1)) v += ekm1 * opc<CJ>(k > 0 ? sB[(k - 1) * LD + col] : sh[col]);
+                    bf[b] = v;
+                }
+            } else {
+#pragma unroll
+                for (int b = 0; b < 4; ++b) bf[b] = dk * opc<CJ>(sB[k * LD + wc + 8 * b + g]);
+            }
             if constexpr (C) {
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
@@ -196,26 +233,28 @@ __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* _
     }
 }
 
-template <bool C, bool CJ>
+template <bool C, bool CJ, bool PV>
 static void launch_t(const Plan& P, const Launch& ln, cudaStream_t st) {
+    const size_t smem = PV ? Cfg<C>::smem_pv() : Cfg<C>::smem();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(dmma_update_kernel<C, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg<C>::smem());
+        cudaFuncSetAttribute(dmma_update_kernel<C, CJ, PV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    dmma_update_kernel<C, CJ><<<(unsigned)ln.nblocks, kThreads, Cfg<C>::smem(), st>>>(
+    dmma_update_kernel<C, CJ, PV><<<(unsigned)ln.nblocks, kThreads, smem, st>>>(
         P.probs + ln.items, P.prefix + ln.prefix, P.bmap + ln.gemm_map, reinterpret_cast<double*>(P.L),
-        reinterpret_cast<double*>(P.pool[0]), reinterpret_cast<double*>(P.pool[1]), P.D);
+        reinterpret_cast<double*>(P.pool[0]), reinterpret_cast<double*>(P.pool[1]), P.D, PV ? P.E : nullptr);
 }
 
 }  // namespace dmma
 
 int launch_dmma_update(Plan& P, const Launch& ln, cudaStream_t st) {
+    const bool pv = P.pivoted;   // (the Schur complements of pivoted fronts)
     if (P.cplx()) {
-        if (P.conjugate) dmma::launch_t<true, true>(P, ln, st);
-        else dmma::launch_t<true, false>(P, ln, st);
+        if (P.conjugate) pv ? dmma::launch_t<true, true, true>(P, ln, st) : dmma::launch_t<true, true, false>(P, ln, st);
+        else pv ? dmma::launch_t<true, false, true>(P, ln, st) : dmma::launch_t<true, false, false>(P, ln, st);
     } else {
-        dmma::launch_t<false, false>(P, ln, st);
+        pv ? dmma::launch_t<false, false, true>(P, ln, st) : dmma::launch_t<false, false, false>(P, ln, st);
     }
     return CLIQ_OK;
 }

@@ -827,11 +827,13 @@ static int issue_factor_pivoted(Plan& P, int64_t* nlaunch) {
     const int64_t before = P.total_launches;
     int64_t launches = 0;
     TRY(pivot_begin(P, st));
-    // FP32 plans with the 2xFP16 tensor-core path: each level's Schur
-    // complements (fixed shapes, K = n) run as the plan's tcgen05 Schur
-    // launches, packed with D's 2 x 2 blocks; otherwise (and for launches the
-    // autotuner moved to the CUDA cores) on the CUDA cores with the panels
-    const bool tc = std::is_same<T, float>::value && P.f16_scales() && P.schur_chunk == 0;
+    // Each level's Schur complements (fixed shapes, K = n) run as the plan's
+    // own Schur launches: tcgen05 for FP32 plans with the 2xFP16 split (the
+    // S operand packed with D's 2 x 2 blocks), DMMA for FP64 plans (the
+    // 2 x 2 terms formed from staged halo rows); otherwise (and for launches
+    // the autotuner moved to the CUDA cores) on the CUDA cores with the panels
+    const bool tc = ((std::is_same<T, float>::value && P.f16_scales()) || (std::is_same<T, double>::value && P.fp64_dmma)) &&
+                    P.schur_chunk == 0;
     std::vector<std::vector<size_t>> schur(P.max_depth + 1);
     std::vector<char> tc_ok(P.max_depth + 1, tc ? 1 : 0);
     for (size_t li = 0; li < P.launches.size(); ++li) {
@@ -848,9 +850,10 @@ static int issue_factor_pivoted(Plan& P, int64_t* nlaunch) {
         const bool on_tc = tc_ok[ln.depth] != 0;
         TRY(pivot_level(P, ln.depth, st, !on_tc));
         if (on_tc && !schur[ln.depth].empty()) {
-            TRY(pivot_rowmax(P, ln.depth, st));
+            if (std::is_same<T, float>::value) TRY(pivot_rowmax(P, ln.depth, st));
             for (size_t li : schur[ln.depth]) {
-                launch_tc2(P, P.launches[li], nullptr, st, P.pack);
+                if (std::is_same<T, float>::value) launch_tc2(P, P.launches[li], nullptr, st, P.pack);
+                else launch_dmma_update(P, P.launches[li], st);
                 ++launches;
             }
         }
