@@ -25,9 +25,13 @@
 //                     op(L11)^{-T} D^{-1} for the panel's diagonal block, one
 //                     thread per row;
 //   bk_update_kernel  the panel's rank-kb update of the front's remaining
-//                     columns (pivot rows and A21 rows, lower part), and once
-//                     per front at the end of the level the Schur complement
-//                     into the update pool with K = n.
+//                     columns (pivot rows and A21 rows, lower part, CUDA
+//                     cores).
+// At the end of the level the Schur complements (K = n) go into the update
+// pool through the plan's own Schur launches -- tcgen05 for FP32 plans
+// (bk_rowmax_kernel gives the 2xFP16 split's row maxima; the packing's
+// pivoted variant forms S = D op(L) with the 2 x 2 terms), DMMA for FP64
+// plans (halo rows for the 2 x 2 terms) -- or through bk_update_kernel.
 // Then the 64 x 64 diagonal-block inverses the sweeps use, and the index
 // maps the solves read are rewritten for the pivoted row order (the
 // reference's PermuteRows / InversePermuteRows around each front solve,
