@@ -42,6 +42,8 @@
 
 #include <climits>
 #include <cmath>
+#include <cstdlib>
+#include <string>
 
 #include <cooperative_groups.h>
 namespace cg = cooperative_groups;
@@ -568,6 +570,166 @@ __global__ void __launch_bounds__(kUpdThreads) bk_update_kernel(const FrontDev* 
 }
 
 // ---------------------------------------------------------------------------
+// FP32 plans' in-front update (kind 0 above): 128 x 64 tiles, 8 x 4 entries
+// a thread, lanes along the rows (coalesced read-modify-write of L), the
+// next k slice's operands loaded into registers while the current slice is
+// multiplied out of shared memory (two buffers, one barrier a slice).
+// Column block tj (64 columns) holds the row tiles tj / 2 .. Mt - 1, so the
+// two column blocks of pair u hold Mt - u row tiles each, and the tiles
+// before pair u number S(u) = u (2 Mt + 1) - u^2.
+// ---------------------------------------------------------------------------
+constexpr int kU2M = 128, kU2N = 64;
+
+__host__ __device__ __forceinline__ int64_t upd2_tiles_dev(int64_t M, int64_t N) {
+    if (M <= 0 || N <= 0) return 0;
+    const int64_t Mt = (M + kU2M - 1) / kU2M, Nt = (N + kU2N - 1) / kU2N;
+    const int64_t pairs = Nt / 2;
+    return pairs * (2 * Mt + 1) - pairs * pairs + ((Nt & 1) ? Mt - pairs : 0);
+}
+
+template <bool C, bool CJ>
+__global__ void __launch_bounds__(kUpdThreads, 2) bk_update2_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+                                                                    int64_t tiles_per_front, float* __restrict__ L,
+                                                                    const double* __restrict__ D, const double* __restrict__ E,
+                                                                    const int32_t* __restrict__ state) {
+    using X = V<float, C>;
+    using W = DV<C>;
+    constexpr int BK = C ? 8 : 16;
+    constexpr int LA = kU2M * BK / kUpdThreads, LB = kU2N * BK / kUpdThreads;
+    static_assert(LA * kUpdThreads == kU2M * BK && LB * kUpdThreads == kU2N * BK, "slice split");
+    __shared__ __align__(16) X sA[2][BK][kU2M];
+    __shared__ __align__(16) X sB[2][BK][kU2N];
+    const int64_t fi = blockIdx.x / tiles_per_front;
+    const int64_t t = blockIdx.x % tiles_per_front;
+    const int s = fl[fi];
+    const FrontDev f = F[s];
+    const int j0 = state[2 * s], j1 = state[2 * s + 1];
+    const int K = j1 - j0, M = f.m - j1, N = f.n - j1;
+    if (K <= 0 || M <= 0 || N <= 0) return;
+    if (t >= upd2_tiles_dev(M, N)) return;
+    // pair u: the largest with S(u) <= t (the smaller root of u^2 - (2 Mt + 1) u + t, then corrected)
+    const int64_t Mt = (M + kU2M - 1) / kU2M, Nt = (N + kU2N - 1) / kU2N;
+    const double b2 = 2.0 * (double)Mt + 1.0;
+    int64_t u = (int64_t)floor((b2 - sqrt(fmax(b2 * b2 - 4.0 * (double)t, 0.0))) * 0.5);
+    auto S = [&](int64_t v) { return v * (2 * Mt + 1) - v * v; };
+    if (u < 0) u = 0;
+    for (int it = 0; it < 3 && u > 0 && S(u) > t; ++it) --u;
+    for (int it = 0; it < 3 && S(u + 1) <= t; ++it) ++u;
+    const int64_t rem = t - S(u);
+    int64_t tj, ti;
+    if (rem < Mt - u) { tj = 2 * u; ti = u + rem; }
+    else { tj = 2 * u + 1; ti = u + rem - (Mt - u); }
+    if (rem < 0 || tj >= Nt || ti >= Mt || ti < tj / 2) return;
+    const int i0 = (int)ti * kU2M, jb0 = (int)tj * kU2N;
+    const int64_t base = f.L;
+    const int64_t arow = base + j1 + i0;          // row i0 of the trailing block
+    const int64_t brow = base + j1 + jb0;         // row (= column of C) jb0
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const W* Dw = reinterpret_cast<const W*>(D) + f.off;
+    const W* Ew = reinterpret_cast<const W*>(E) + f.off;
+
+    X ra[LA], rl[LB], rd[LB], re[LB], rem1[LB];
+    auto fetch = [&](int kq) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            const int idx = threadIdx.x + kUpdThreads * q;
+            const int r = idx % kU2M, kg = kq + idx / kU2M;
+            ra[q] = (kg < K && i0 + r < M) ? ldv<float, C>(L, arow + r + (int64_t)(j0 + kg) * f.m) : X{};
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int idx = threadIdx.x + kUpdThreads * q;
+            const int r = idx % kU2N, kg = kq + idx / kU2N;
+            const int p = j0 + kg;
+            const bool in = kg < K && jb0 + r < N;
+            rl[q] = in ? ldv<float, C>(L, brow + r + (int64_t)p * f.m) : X{};
+            rd[q] = in ? conv<X>(Dw[p]) : X{};
+            re[q] = in ? conv<X>(Ew[p]) : X{};
+            rem1[q] = (in && p > 0) ? conv<X>(Ew[p - 1]) : X{};
+        }
+    };
+    auto stage = [&](int buf, int kq) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            const int idx = threadIdx.x + kUpdThreads * q;
+            sA[buf][idx / kU2M][idx % kU2M] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int idx = threadIdx.x + kUpdThreads * q;
+            const int r = idx % kU2N, kg = kq + idx / kU2N;
+            X bv = rd[q] * opc<CJ>(rl[q]);   // B(j, p) as bval forms it; the 2 x 2 terms are rare
+            if (kg + 1 < K && !is_zero(re[q]))
+                bv += opc<CJ>(re[q]) * opc<CJ>(ldv<float, C>(L, brow + r + (int64_t)(j0 + kg + 1) * f.m));
+            if (kg >= 1 && !is_zero(rem1[q])) bv += rem1[q] * opc<CJ>(ldv<float, C>(L, brow + r + (int64_t)(j0 + kg - 1) * f.m));
+            sB[buf][idx / kU2N][r] = bv;
+        }
+    };
+
+    X acc[8][4];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = X{};
+    const int ns = (K + BK - 1) / BK;
+    fetch(0);
+    stage(0, 0);
+    __syncthreads();
+    for (int sl = 0; sl < ns; ++sl) {
+        const int buf = sl & 1;
+        if (sl + 1 < ns) fetch((sl + 1) * BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            X av[8], bv[4];
+            // rows 32 h + 2 tx + {0, 1} (h < 4), columns 4 ty .. 4 ty + 3
+            if constexpr (C) {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const float4 v = *reinterpret_cast<const float4*>(&sA[buf][kk][32 * h + 2 * tx]);
+                    av[2 * h] = X{v.x, v.y};
+                    av[2 * h + 1] = X{v.z, v.w};
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float4 v = *reinterpret_cast<const float4*>(&sB[buf][kk][4 * ty + 2 * h]);
+                    bv[2 * h] = X{v.x, v.y};
+                    bv[2 * h + 1] = X{v.z, v.w};
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const float2 v = *reinterpret_cast<const float2*>(&sA[buf][kk][32 * h + 2 * tx]);
+                    av[2 * h] = v.x;
+                    av[2 * h + 1] = v.y;
+                }
+                const float4 v = *reinterpret_cast<const float4*>(&sB[buf][kk][4 * ty]);
+                bv[0] = v.x; bv[1] = v.y; bv[2] = v.z; bv[3] = v.w;
+            }
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) mac(acc[a][b], av[a], bv[b]);
+        }
+        if (sl + 1 < ns) stage(buf ^ 1, (sl + 1) * BK);
+        __syncthreads();
+    }
+    const int64_t cbase = base + j1 + (int64_t)j1 * f.m;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int j = jb0 + 4 * ty + b;
+        if (j >= N) continue;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int i = i0 + 32 * (a >> 1) + 2 * tx + (a & 1);
+            if (i < M && i >= j) {   // one tile writes each entry per launch
+                const int64_t e = cbase + i + (int64_t)j * f.m;
+                stv<float, C>(L, e, ldv<float, C>(L, e) - acc[a][b]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // inverses of the 64 x 64 diagonal blocks of the unit lower L11 (the sweeps'
 // dinv / dinvT blocks), one CTA of 64 threads per block
 // ---------------------------------------------------------------------------
@@ -731,6 +893,9 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
         return Nt * Mt - Nt * (Nt - 1) / 2;
     };
     const int steps = (max_n + kNb - 1) / kNb;
+    // FP32: the in-front updates on bk_update2_kernel (CLIQGPU_PIV_UPDATE=tile64 keeps bk_update_kernel)
+    const char* upd_env = std::getenv("CLIQGPU_PIV_UPDATE");
+    const bool wide = std::is_same<T, float>::value && !(upd_env && std::string(upd_env) == "tile64");
     // the top levels (a few large fronts): each front's panels on a cluster
     // of kClusterCTAs CTAs; a refused cluster launch falls back to one CTA a front
     const bool clustered = (int64_t)lv.nfronts * kClusterCTAs <= 148 && max_n >= 512;
@@ -759,16 +924,26 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
         if (max_u > 0)
             bk_lower_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * chunks), kLowerRows, smem_lower, st>>>(
                 P.fronts, fl, chunks, L, P.D, P.E, P.pstate);
-        // every panel is at least kNb wide until the front is done
+        // every panel is at least kNb wide until the front is done, so the
+        // trailing extents below bound the ones the kernels read from pstate
         int64_t tpf = 0;
         for (int s : P.level_list[depth]) {
             const FrontDev& f = P.hfronts[s];
             const int64_t jb = std::min<int64_t>(f.n, (int64_t)(step + 1) * kNb);
-            tpf = std::max(tpf, tiles(f.m - jb, f.n - jb));
+            tpf = std::max(tpf, wide ? upd2_tiles_dev(f.m - jb, f.n - jb) : tiles(f.m - jb, f.n - jb));
         }
-        if (tpf > 0)
+        if (tpf > 0) {
+            if constexpr (std::is_same<T, float>::value) {
+                if (wide) {
+                    bk_update2_kernel<C, CJ><<<(unsigned)((int64_t)lv.nfronts * tpf), kUpdThreads, 0, st>>>(
+                        P.fronts, fl, tpf, L, P.D, P.E, P.pstate);
+                    P.total_launches += 3;
+                    continue;
+                }
+            }
             bk_update_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * tpf), kUpdThreads, 0, st>>>(
                 P.fronts, fl, tpf, 0, L, p0, p1, P.D, P.E, P.pstate);
+        }
         P.total_launches += 3;
     }
     if (!schur) return check_cuda("pivoted level");   // the Schur complements go to the tensor cores

@@ -299,3 +299,42 @@ def test_intrapiv_clustered_panels(oracle, kind):
     B = ops.random_rhs(A.n, 3, seed=5, complex_=cplx)
     X = cliq.Solve(info, L, B.copy(order="F"))
     assert rel(X, F.solve(B.copy(order="F"))) <= 1e-10
+
+
+@pytest.mark.parametrize("kind", ["real", "complex", "hermitian"])
+@pytest.mark.parametrize("dims,cutoff", [((16, 16, 10), 200), ((26, 24, 22), 256)])
+def test_intrapiv_fp32_in_front_update_kernels(kind, dims, cutoff, monkeypatch):
+    """The FP32 in-front updates on the 128 x 64 tile kernel are as accurate
+    as on the 64 x 64 one (CLIQGPU_PIV_UPDATE=tile64), measured against the
+    FP64 pivoted fronts on the fronts whose pivot order all three share, and
+    the refined solve reaches 1e-10.  The 26 x 24 x 22 grid's top fronts
+    (528 and 264 pivots, trailing blocks of several 128-row tiles and odd
+    numbers of 64-column blocks) exercise the tile map."""
+    A, conj = _indefinite(kind, dims)
+    runs = {}
+    for name, prec, upd in (("fp64", "double", ""), ("wide", "single", ""), ("tile64", "single", "tile64")):
+        monkeypatch.setenv("CLIQGPU_PIV_UPDATE", upd)
+        _, info, L = _tree(A, dims, cutoff, prec, conj, keep=name == "wide")
+        runs[name] = [(L.front(s), L.front_pivots(s)) for s in range(info.num_nodes)]
+        if name == "wide":
+            B = ops.random_rhs(A.n, 2, seed=9, complex_=kind != "real")
+            X, it, rr = cliq.RefinedSolve(L, B, 1e-10, 40)
+            assert rr <= 1e-10, (it, rr)
+            assert residual(A, X, B) <= 1e-9
+    err = {"wide": 0.0, "tile64": 0.0}
+    same = 0
+    for s in range(len(runs["fp64"])):
+        (L64, d64), (_, p64) = runs["fp64"][s]
+        if not all(np.array_equal(runs[k][s][1][1], p64) for k in err):
+            continue
+        same += 1
+        scale = max(np.abs(L64).max(), np.abs(d64).max(), 1e-300)
+        for k in err:
+            (Lk, dk), _ = runs[k][s]
+            err[k] = max(err[k], np.abs(Lk - L64).max() / scale, np.abs(dk - d64).max() / scale)
+    print(f"{same} of {len(runs['fp64'])} fronts with the FP64 pivot order; worst error vs FP64: "
+          f"128 x 64 tiles {err['wide']:.2e}, 64 x 64 tiles {err['tile64']:.2e}")
+    assert same >= len(runs["fp64"]) // 2
+    # both sum the same products in different orders; a wrong tile or a lost
+    # 2x2 term gives O(1)
+    assert err["wide"] <= 4.0 * err["tile64"] + 1e-6, err
