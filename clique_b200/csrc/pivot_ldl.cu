@@ -899,6 +899,12 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
     // the top levels (a few large fronts): each front's panels on a cluster
     // of kClusterCTAs CTAs; a refused cluster launch falls back to one CTA a front
     const bool clustered = (int64_t)lv.nfronts * kClusterCTAs <= 148 && max_n >= 512;
+    // one CTA a front otherwise; a column step works over the front's pivot
+    // rows only, so fronts of at most 128 / 256 pivots take CTAs of that many
+    // threads (several CTAs a SM on the deep levels' many small fronts; at
+    // least kMaxPanel threads, which the panel's per-column loads need)
+    const int narrow = max_n <= 128 ? 128 : max_n <= 256 ? 256 : panel_threads<T>();
+    static_assert(kMaxPanel <= 128, "panel CTAs of 128 threads");
     for (int step = 0; step < steps; ++step) {
         bool done = false;
         if (clustered) {
@@ -919,8 +925,8 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
             if (!done) cudaGetLastError();
         }
         if (!done)
-            bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, panel_threads<T>(), 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec,
-                                                                                       vvec, P.pstate, P.status);
+            bk_panel_kernel<T, C, CJ><<<(unsigned)lv.nfronts, narrow, 0, st>>>(P.fronts, fl, L, P.D, P.E, P.pivg, cvec, vvec,
+                                                                           P.pstate, P.status);
         if (max_u > 0)
             bk_lower_kernel<T, C, CJ><<<(unsigned)((int64_t)lv.nfronts * chunks), kLowerRows, smem_lower, st>>>(
                 P.fronts, fl, chunks, L, P.D, P.E, P.pstate);
