@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kLowerRows) bk_lower_kernel(const FrontDev* __
 // One 64 x 64 tile per CTA; tiles beyond the front's actual extent return.
 // ---------------------------------------------------------------------------
 template <class T, bool C, bool CJ>
-__global__ void __launch_bounds__(kUpdThreads) bk_update_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
+__global__ void __launch_bounds__(kUpdThreads, (sizeof(T) == 8 && C) ? 2 : 3) bk_update_kernel(const FrontDev* __restrict__ F, const int32_t* __restrict__ fl,
                                                                 int64_t tiles_per_front, int kind, T* __restrict__ L,
                                                                 T* __restrict__ pool0, T* __restrict__ pool1,
                                                                 const double* __restrict__ D, const double* __restrict__ E,
