@@ -392,6 +392,7 @@ size_t tc2_smem(bool cplx);
 // intra-front pivoting (pivot_ldl.cu)
 int pivot_begin(Plan& P, cudaStream_t st);
 int pivot_level(Plan& P, int depth, cudaStream_t st, bool schur);
+int launch_dmma_front_update(Plan& P, const int32_t* fl, int64_t nfronts, int64_t tpf, cudaStream_t st);
 int pivot_rowmax(Plan& P, int depth, cudaStream_t st);
 int pivot_finish(Plan& P, cudaStream_t st);
 int pivot_restore_maps(Plan& P, cudaStream_t st);

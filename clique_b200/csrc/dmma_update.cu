@@ -70,12 +70,19 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 // PV: the fronts were factored with intra-front pivoting; D has 2 x 2 blocks
 // (E holds D(k + 1, k) of a block starting at k, D(k, k + 1) = op of it), so
 // D op(B) mixes the two rows of a block -- the neighbour across a slice edge
-// comes from the staged halo rows
-template <bool C, bool CJ, bool PV = false>
+// comes from the staged halo rows.
+// FRONT: the in-front update of a pivoted panel step, whose extents the
+// panels wrote on the device: CTA b updates front fl[b / tpf] (tile
+// b % tpf) with C -= A D op(A)^T over the columns j0 .. j1 - 1 of the
+// panel (state[2 s], state[2 s + 1]), rows and columns from j1, in place
+template <bool C, bool CJ, bool PV = false, bool FRONT = false>
 __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* __restrict__ probs, const int64_t* __restrict__ prefix,
                                                                const int32_t* __restrict__ bmap, double* __restrict__ L,
                                                                double* __restrict__ pool0, double* __restrict__ pool1,
-                                                               const double* __restrict__ D, const double* __restrict__ E = nullptr) {
+                                                               const double* __restrict__ D, const double* __restrict__ E = nullptr,
+                                                               const FrontDev* __restrict__ F = nullptr,
+                                                               const int32_t* __restrict__ fl = nullptr, int64_t tpf = 0,
+                                                               const int32_t* __restrict__ state = nullptr) {
     using X = V<double, C>;
     using G = Cfg<C>;
     constexpr int BK = G::BK, LD = G::LD;
@@ -87,13 +94,32 @@ __global__ void __launch_bounds__(kThreads) dmma_update_kernel(const GemmProb* _
     X* sEv = sBh + (size_t)kStages * 2 * kBM;                      // PV: [stage][BK + 2] D(k + 1, k), k0 - 1 .. k0 + BK
 
     const int64_t bid = blockIdx.x;
-    const int lo = bmap[bid];
-    const GemmProb pr = probs[lo];
-    int64_t t = bid - prefix[lo];
+    GemmProb pr{};
+    int64_t t;
+    if constexpr (FRONT) {
+        const int s = fl[bid / tpf];
+        const FrontDev f = F[s];
+        const int pj0 = state[2 * s], pj1 = state[2 * s + 1];
+        t = bid % tpf;
+        pr.A = f.L + pj1 + (int64_t)pj0 * f.m;
+        pr.B = pr.A;
+        pr.C = f.L + pj1 + (int64_t)pj1 * f.m;
+        pr.d = f.off + pj0;
+        pr.lda = pr.ldc = f.m;
+        pr.M = f.m - pj1;
+        pr.N = f.n - pj1;
+        pr.K = pj1 - pj0;
+        pr.cpool = -1;
+        if (pr.K <= 0 || pr.M <= 0 || pr.N <= 0) return;
+    } else {
+        const int lo = bmap[bid];
+        pr = probs[lo];
+        t = bid - prefix[lo];
+    }
     const int Mt = (pr.M + kBM - 1) / kBM, Nt = (pr.N + kBM - 1) / kBM;
     int tj = 0;
     while (tj < Nt && t >= Mt - tj) { t -= Mt - tj; ++tj; }
-    if (tj >= Nt) return;   // cannot happen with a consistent schedule
+    if (tj >= Nt) return;   // FRONT: tiles beyond the actual extents; otherwise cannot happen
     const int ti = tj + (int)t;
     const int i0 = ti * kBM, j0 = tj * kBM;
     double* Cbase = pr.cpool < 0 ? L : (pr.cpool == 0 ? pool0 : pool1);
@@ -247,6 +273,34 @@ static void launch_t(const Plan& P, const Launch& ln, cudaStream_t st) {
 }
 
 }  // namespace dmma
+
+namespace dmma {
+template <bool C, bool CJ>
+static void launch_front_t(const Plan& P, const int32_t* fl, int64_t nfronts, int64_t tpf, cudaStream_t st) {
+    const size_t smem = Cfg<C>::smem_pv();
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(dmma_update_kernel<C, CJ, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    dmma_update_kernel<C, CJ, true, true><<<(unsigned)(nfronts * tpf), kThreads, smem, st>>>(
+        nullptr, nullptr, nullptr, reinterpret_cast<double*>(P.L), nullptr, nullptr, P.D, P.E, P.fronts, fl, tpf, P.pstate);
+}
+}  // namespace dmma
+
+// the in-front update of one pivoted panel step of a level (FP64 plans):
+// nfronts x tpf CTAs, tpf the 64 x 64 lower-trapezoid tiles of the largest
+// trailing block the planned panel widths allow
+int launch_dmma_front_update(Plan& P, const int32_t* fl, int64_t nfronts, int64_t tpf, cudaStream_t st) {
+    if (nfronts <= 0 || tpf <= 0) return CLIQ_OK;
+    if (P.cplx()) {
+        if (P.conjugate) dmma::launch_front_t<true, true>(P, fl, nfronts, tpf, st);
+        else dmma::launch_front_t<true, false>(P, fl, nfronts, tpf, st);
+    } else {
+        dmma::launch_front_t<false, false>(P, fl, nfronts, tpf, st);
+    }
+    return CLIQ_OK;
+}
 
 int launch_dmma_update(Plan& P, const Launch& ln, cudaStream_t st) {
     const bool pv = P.pivoted;   // (the Schur complements of pivoted fronts)

@@ -24,9 +24,11 @@
 //   bk_lower_kernel   rows below the pivots (A21): L21(:,panel) = A21(:,panel)
 //                     op(L11)^{-T} D^{-1} for the panel's diagonal block, one
 //                     thread per row;
-//   bk_update_kernel  the panel's rank-kb update of the front's remaining
-//                     columns (pivot rows and A21 rows, lower part, CUDA
-//                     cores).
+//   bk_update2_kernel the panel's rank-kb update of the front's remaining
+//                     columns (pivot rows and A21 rows, lower part) for FP32
+//                     plans, CUDA cores; FP64 plans run it on DMMA (the
+//                     DMMA update kernel's FRONT mode, extents read from the
+//                     panel state), bk_update_kernel without DMMA.
 // At the end of the level the Schur complements (K = n) go into the update
 // pool through the plan's own Schur launches -- tcgen05 for FP32 plans
 // (bk_rowmax_kernel gives the 2xFP16 split's row maxima; the packing's
@@ -895,7 +897,10 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
     const int steps = (max_n + kNb - 1) / kNb;
     // FP32: the in-front updates on bk_update2_kernel (CLIQGPU_PIV_UPDATE=tile64 keeps bk_update_kernel)
     const char* upd_env = std::getenv("CLIQGPU_PIV_UPDATE");
-    const bool wide = std::is_same<T, float>::value && !(upd_env && std::string(upd_env) == "tile64");
+    const bool tile64 = upd_env && std::string(upd_env) == "tile64";
+    const bool wide = std::is_same<T, float>::value && !tile64;
+    // FP64: the in-front updates on DMMA where the plan's FP64 updates are
+    const bool dmma_front = std::is_same<T, double>::value && P.fp64_dmma && !tile64;
     // the top levels (a few large fronts): each front's panels on a cluster
     // of kClusterCTAs CTAs; a refused cluster launch falls back to one CTA a front
     const bool clustered = (int64_t)lv.nfronts * kClusterCTAs <= 148 && max_n >= 512;
@@ -939,6 +944,13 @@ static int level_t(Plan& P, int depth, cudaStream_t st, bool schur) {
             tpf = std::max(tpf, wide ? upd2_tiles_dev(f.m - jb, f.n - jb) : tiles(f.m - jb, f.n - jb));
         }
         if (tpf > 0) {
+            if constexpr (std::is_same<T, double>::value) {
+                if (dmma_front) {   // 64 x 64 tiles, the same tile count as bk_update_kernel's
+                    TRY(launch_dmma_front_update(P, fl, lv.nfronts, tpf, st));
+                    P.total_launches += 3;
+                    continue;
+                }
+            }
             if constexpr (std::is_same<T, float>::value) {
                 if (wide) {
                     bk_update2_kernel<C, CJ><<<(unsigned)((int64_t)lv.nfronts * tpf), kUpdThreads, 0, st>>>(
